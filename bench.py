@@ -1,0 +1,444 @@
+#!/usr/bin/env python
+"""Benchmark of the CELERIS B200 hot path.
+
+Headline (one JSON line on rank 0): RS terms/s of the far-field sum in the
+chosen (FP32-compensated) form on the 785,456-pillar metalens with a 1024 x 1024
+focal grid (+/-20 um at z = 1 mm, lambda 532 nm), with its error against the
+FP64 form stated. A step is one evaluation of the whole focal grid. Secondary
+objects on the same line: the plain FP64 form on the same workload, both forms
+on the 70,688-pillar x 161^2 metalens, the roofline of the dominant kernel
+against in-run measured pipe peaks, the reference's own CPU far-field timed on
+this host (cpu_baseline), the end-to-end C-ABI call with host buffers (e2e),
+RCWA cells/s when the RCWA kernels are present, and the SM clocks seen.
+
+Multi-GPU (torchrun, one rank per GPU): the focal plane is sharded by row
+blocks - each rank evaluates its own 1024 x 1024 tile of a taller focal window
+(pillars replicated, no data-path collective): weak scaling. Timing is CUDA
+events, barrier + synchronize around the timed region, max over ranks.
+
+--impl reference times the reference's own CPU propagate_pillars (compiled from
+its sources into oracle/_ref) on this host's cores, on bounded samples of the
+same workload, and prints the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RS terms/s"
+UNIT = "terms/s"
+WORKLOAD = "metalens_785k_1024sq_f32c"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="celeris", choices=["celeris", "reference"])
+    ap.add_argument("--quick", action="store_true", help="skip secondary measurements")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--case", default=None,
+                    help="run one small named case and exit (ncu captures): ff785k_f32c_256, "
+                         "ff785k_f64_128, ff70k_f32c, ff70k_f64, ff70k_adj")
+    ap.add_argument("--reps", type=int, default=2)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- distributed
+def dist_init(n):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(world, x):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- workloads
+def workload(rank):
+    from celeris_b200.workloads import metalens_785k
+
+    ap, g = metalens_785k()
+    # rank r evaluates the r-th 1024-row tile of a taller focal window
+    step = 2.0 * g.half_window_um / (g.n - 1)
+    cy = rank * g.n * step
+    return ap, g, cy
+
+
+def choose_cpu_sample(npil, seconds, rate_guess, threads):
+    """Grid side n for a CPU sample of ~`seconds` (n >= threads so every host
+    thread gets a row, as parallel_rows hands out rows)."""
+    terms = seconds * rate_guess
+    n = int(max(threads, min(1024, np.sqrt(terms / npil))))
+    return max(n, 2)
+
+
+def cpu_reference_sample(ap, g, seconds=12.0):
+    """Time the reference's own CPU propagate_pillars on a bounded sample: all
+    pillars, an n x n grid over the same window."""
+    from oracle import farfield as F
+
+    threads = F.ref_threads() or os.cpu_count()
+    # calibrate on a tiny grid
+    n0 = 2
+    t0 = time.perf_counter()
+    F.ref_propagate_pillars(ap.px, ap.py, ap.t, 0.0, 0.0, g.z_um, ap.wavelength_um, n0, g.half_window_um)
+    dt0 = time.perf_counter() - t0
+    rate0 = ap.npil * n0 * n0 / max(dt0, 1e-6) * max(1, threads // (n0))  # rough, rows cap threads
+    n = choose_cpu_sample(ap.npil, seconds, rate0, threads)
+    t0 = time.perf_counter()
+    F.ref_propagate_pillars(ap.px, ap.py, ap.t, 0.0, 0.0, g.z_um, ap.wavelength_um, n, g.half_window_um)
+    dt = time.perf_counter() - t0
+    terms = ap.npil * n * n
+    return {"value": terms / dt, "unit": UNIT, "cores": int(threads), "kind": "reference",
+            "sample": f"{ap.npil} pillars x {n}x{n} pixels over the same +/-{g.half_window_um} um window "
+                      f"({terms:.3e} terms, {dt:.2f} s), reference celeris::propagate_pillars FP64 CPU path "
+                      f"compiled from its sources (-O3 -mavx2 -mfma), {threads} host threads"}
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    from oracle import farfield as F
+
+    if F.ref_lib() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_farfield.so not built"}))
+        return
+    ap, g, _ = workload(0)
+    threads = F.ref_threads() or os.cpu_count()
+    # size each step to ~5 s of host work
+    n0 = max(2, threads)
+    t0 = time.perf_counter()
+    F.ref_propagate_pillars(ap.px, ap.py, ap.t, 0.0, 0.0, g.z_um, ap.wavelength_um, n0, g.half_window_um)
+    rate = ap.npil * n0 * n0 / (time.perf_counter() - t0)
+    n = choose_cpu_sample(ap.npil, 5.0, rate, threads)
+    for _ in range(args.warmup):
+        F.ref_propagate_pillars(ap.px, ap.py, ap.t, 0.0, 0.0, g.z_um, ap.wavelength_um, max(2, n // 4),
+                                g.half_window_um)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        F.ref_propagate_pillars(ap.px, ap.py, ap.t, 0.0, 0.0, g.z_um, ap.wavelength_um, n, g.half_window_um)
+        times.append(time.perf_counter() - t0)
+    terms = ap.npil * n * n
+    value = terms * len(times) / sum(times)
+    sample = (f"each step: {ap.npil} pillars x {n}x{n} pixels ({terms:.3e} terms) of the "
+              f"{g.n}x{g.n} workload, reference propagate_pillars FP64 CPU, {threads} host threads")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "pillars": ap.npil, "grid": f"{g.n}x{g.n}", "sampled_grid": f"{n}x{n}"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": int(threads), "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+# ---------------------------------------------------------------- GPU arm
+def profiles_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}.md")
+    if not os.path.exists(path):
+        return None
+    for ln in open(path):
+        if ln.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(ln.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def timed_steps(fn, steps, stream, flush):
+    import torch
+
+    ms = []
+    kms = []
+    from celeris_b200 import capi
+
+    for _ in range(steps):
+        flush()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+        kms.append(capi.last_kernel_ms())
+    return ms, kms
+
+
+def run_gpu(args):
+    import torch
+
+    from celeris_b200 import capi
+    from celeris_b200 import torch_ops as T
+
+    world, rank, local = dist_init(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    ap, g, cy = workload(rank)
+    grid = T.FarFieldGrid(g.n, g.half_window_um, g.z_um, ap.wavelength_um, 0.0, cy)
+    px = torch.tensor(ap.px, device=dev)
+    py = torch.tensor(ap.py, device=dev)
+    t = torch.tensor(ap.t, device=dev)
+    flush_buf = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def flush():
+        flush_buf.zero_()
+
+    capi.set_kernel_timing(True)
+    f32 = lambda: T.rs_field_dev(px, py, t, grid, capi.FORM_F32C)  # noqa: E731
+    for _ in range(args.warmup):
+        f32()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = capi.launch_count()
+    ms, kms = timed_steps(f32, args.steps, stream, flush)
+    launches = capi.launch_count() - l0
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    total_ms = max_over_ranks(world, float(sum(ms)))
+    terms = float(ap.npil) * g.npix
+    value = terms * args.steps * world / (total_ms * 1e-3)
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 terms, f64 k*z phase + chunk sums, TwoSum-compensated f32 tile sums",
+        "data": "synthetic (seeded metalens aperture, default_rng(0))",
+        "config": {"workload": WORKLOAD, "pillars": ap.npil, "grid": f"{g.n}x{g.n}",
+                   "half_window_um": g.half_window_um, "z_um": g.z_um, "wavelength_um": ap.wavelength_um,
+                   "form": "f32c", "sharding": "focal row blocks per rank, pillars replicated",
+                   "l2": "flushed between timed steps (256 MiB write, outside the events)"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if rank != 0:
+        return
+    # ---- error of the chosen form against the FP64 form (full grid) ----------
+    E32 = f32()
+    E64 = T.rs_field_dev(px, py, t, grid, capi.FORM_PLAIN_F64)
+    torch.cuda.synchronize()
+    err = float((E32 - E64).abs().max() / E64.abs().max())
+    out["error_vs_fp64"] = err
+    # ---- roofline: dominant kernel = rs_f32c_kernel ---------------------------
+    peaks = capi.probe_peaks()
+    k_ms = float(np.mean(kms))
+    achieved = terms / (k_ms * 1e-3)
+    peak_mufu = peaks["mufu_per_s"] / 3.0      # rsqrt + sin + cos per term
+    peak_fp32 = peaks["ffma_per_s"] * 2.0 / 28.0  # 28 FP32 flops per term as FMA pairs
+    peak = min(peak_mufu, peak_fp32)
+    out["roofline"] = {
+        "kernel": "rs_f32c_kernel", "bound": "sfu" if peak_mufu <= peak_fp32 else "fp32",
+        "achieved": achieved, "peak": peak, "unit": "terms/s", "frac": achieved / peak,
+        "traffic": profiles_traffic("rs_f32c_kernel_metalens_785k"),
+        "peak_source": "in-run probe kernels (MUFU sin.approx and FP32 FMA throughput on this GPU)",
+        "measured_peaks": peaks, "kernel_ms_per_launch": k_ms,
+        "algorithmic_bytes_per_launch": ap.npil * 16 + g.npix * 16,
+    }
+    # ---- plain FP64 form, same workload ----------------------------------------
+    f64 = lambda: T.rs_field_dev(px, py, t, grid, capi.FORM_PLAIN_F64)  # noqa: E731
+    f64()
+    ms64, kms64 = timed_steps(f64, 1 if args.quick else 2, stream, flush)
+    v64 = terms / (np.mean(ms64) * 1e-3)
+    out["plain_f64"] = {"value": v64, "unit": UNIT, "ms_per_step": float(np.mean(ms64)),
+                        "roofline_frac_dfma": (terms / (np.mean(kms64) * 1e-3)) / (peaks["dfma_per_s"] * 2 / 21),
+                        "chosen_over_plain": value / v64}
+    # ---- the 70,688-pillar x 161^2 metalens, both forms ------------------------
+    if not args.quick:
+        from celeris_b200.workloads import metalens_70k
+
+        a0, g0 = metalens_70k()
+        grid0 = T.FarFieldGrid(g0.n, g0.half_window_um, g0.z_um, a0.wavelength_um)
+        px0, py0, t0_ = (torch.tensor(v, device=dev) for v in (a0.px, a0.py, a0.t))
+        res = {}
+        for name, form in (("f32c", capi.FORM_F32C), ("plain_f64", capi.FORM_PLAIN_F64)):
+            fn = lambda form=form: T.rs_field_dev(px0, py0, t0_, grid0, form)  # noqa: E731
+            for _ in range(3):
+                fn()
+            m, km = timed_steps(fn, 10, stream, flush)
+            res[name] = {"value": a0.npil * g0.npix / (np.mean(m) * 1e-3), "ms_per_step": float(np.mean(m)),
+                         "kernel_ms": float(np.mean(km))}
+        Ea = T.rs_field_dev(px0, py0, t0_, grid0, capi.FORM_F32C)
+        Eb = T.rs_field_dev(px0, py0, t0_, grid0, capi.FORM_PLAIN_F64)
+        res["f32c"]["error_vs_fp64"] = float((Ea - Eb).abs().max() / Eb.abs().max())
+        out["metalens_70k_161sq"] = res
+    # ---- e2e: the C-ABI host-buffer call ----------------------------------------
+    E_host = None
+    for _ in range(2):
+        E_host, _, _ = capi.rs_field(ap.px, ap.py, ap.t, 0.0, cy, g.z_um, ap.k, g.n, g.half_window_um,
+                                     form=capi.FORM_F32C, want_intensity=False, want_err=True)
+    e2e_t = []
+    stated = None
+    for _ in range(args.steps):
+        flush()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        E_host, _, stated = capi.rs_field(ap.px, ap.py, ap.t, 0.0, cy, g.z_um, ap.k, g.n, g.half_window_um,
+                                          form=capi.FORM_F32C, want_intensity=False, want_err=True)
+        e2e_t.append(time.perf_counter() - t0)
+    out["e2e"] = {"value": terms / float(np.mean(e2e_t)), "unit": UNIT,
+                  "h2d_bytes_per_step": int(ap.npil * 32), "d2h_bytes_per_step": int(g.npix * 16),
+                  "api": "celeris_rs_field (C ABI, host buffers, F32C form, stated error on)",
+                  "stated_error": stated, "ms_per_step": 1e3 * float(np.mean(e2e_t))}
+    # ---- RCWA cells/s ------------------------------------------------------------
+    try:
+        from celeris_b200 import rcwa_bench
+
+        out["rcwa"] = rcwa_bench.measure(quick=args.quick)
+    except Exception as exc:  # RCWA kernels not built into this library yet
+        out["rcwa"] = {"unavailable": str(exc)[:200]}
+    # ---- CPU baseline: the reference's own far-field on this host --------------
+    if not args.no_cpu:
+        try:
+            out["cpu_baseline"] = cpu_reference_sample(ap, g)
+        except Exception as exc:
+            out["cpu_baseline"] = {"unavailable": str(exc)[:200]}
+    print(json.dumps(out), flush=True)
+
+
+def run_case(name, reps):
+    """Run one named small case `reps` times (for ncu captures)."""
+    import torch
+
+    from celeris_b200 import capi
+    from celeris_b200 import torch_ops as T
+    from celeris_b200.workloads import metalens_70k, metalens_785k
+
+    dev = torch.device("cuda")
+    if name.startswith("ff785k"):
+        ap, g = metalens_785k()
+        n = int(name.split("_")[2]) if name.count("_") >= 2 else 256
+        grid = T.FarFieldGrid(n, g.half_window_um, g.z_um, ap.wavelength_um)
+    else:
+        ap, g = metalens_70k()
+        grid = T.FarFieldGrid(g.n, g.half_window_um, g.z_um, ap.wavelength_um)
+    form = capi.FORM_PLAIN_F64 if "_f64" in name else capi.FORM_F32C
+    px, py, t = (torch.tensor(v, device=dev) for v in (ap.px, ap.py, ap.t))
+    for _ in range(reps):
+        if "_adj" in name:
+            v = torch.ones((grid.n, grid.n), dtype=torch.complex128, device=dev)
+            T.rs_adjoint_dev(px, py, v, grid)
+        else:
+            T.rs_field_dev(px, py, t, grid, form)
+    torch.cuda.synchronize()
+    print(json.dumps({"case": name, "reps": reps, "pillars": ap.npil, "grid": grid.n}))
+
+
+def main():
+    args = parse()
+    if args.case:
+        run_case(args.case, args.reps)
+        return
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    run_gpu(args)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,899 @@
+// Rayleigh-Sommerfeld far-field sum on sm_100a.
+//
+//   E(p) = sum_j t_j exp(i k R_pj) / R_pj
+//
+// Reference: src/celeris/cuda/propagate.cu:36-130 (FP32 psf/zx kernels, one
+// thread per pixel, 256-pillar shared tiles), src/celeris/analysis/focal.cpp:
+// 205-238 (CPU FP64 loop that the plain form reproduces) and
+// throughfocus.cpp:105-118 (CPU caustic loop).
+//
+// Layout in HBM
+//   pillar records  f64 form: double4 {x, y, Re t, Im t}            32 B/pillar
+//                   f32 form: float4  {x - ox, y - oy, |t|, arg t/2pi} 16 B/pillar
+//   partial sums    double2 [nchunk][npix] (pillar-chunk split of the sum)
+//   outputs         double2 field [npix] and/or double |E|^2 [npix]
+//
+// Kernels
+//   ff_pack_*        FP64 inputs -> pillar records (one pass over the pillars)
+//   rs_f64_kernel    plain form: FP64 terms exactly as focal.cpp:229-233
+//   rs_f32c_kernel   precision form: FP32 terms; R - z refined by one Newton
+//                    step on (R - z)(R + z) = dx^2 + dy^2 so the large k*z part
+//                    of the phase never enters FP32; phase reduced in turns;
+//                    MUFU rsqrt/sin/cos; per-tile FP32 partial sums folded into
+//                    TwoSum-compensated (hi, lo) pairs.
+//   rs_reduce_kernel ordered FP64 sum over chunks; f32 form multiplies by the
+//                    FP64 global phase exp(i k z).
+//   rs_adj_f64_kernel conjugate-transpose (pixel -> pillar) sum for the adjoint.
+// Every main kernel stages its tiles in shared memory with cp.async.bulk
+// (TMA bulk copies) completing on an mbarrier, 3-4 stages deep, so each record
+// is read from HBM once per CTA.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "runtime.cuh"
+
+namespace {
+
+using celeris_rt::count_launch;
+using celeris_rt::set_error;
+using celeris_rt::Workspace;
+using namespace celeris_dev;
+
+__device__ int g_ff_status;  // CELERIS_ERR_DEVICE_TIMEOUT after a wait ran out
+
+constexpr int kThreads = 256;
+constexpr int kTile64 = 256;  // pillars (or pixels) per stage, 32 B records -> 8 KB
+constexpr int kTile32 = 512;  // pillars per stage, 16 B records -> 8 KB
+constexpr int kStages = 4;
+constexpr int kPPT64 = 2;     // pixels per thread, plain form
+constexpr int kPPT32 = 4;     // pixels per thread, precision form
+constexpr int kAdjPPT = 2;    // pillars per thread, adjoint
+
+enum { GEOM_PSF = 0, GEOM_ZX = 1 };
+
+// Pixel grid. GEOM_PSF: fx = (cx - W) + i*step, fy = (cy - W) + j*step, z const
+// (focal.cpp:223-227). GEOM_ZX: fx = xmin + (xmax - xmin)*i/(nx-1), fy = 0,
+// z = zmin + (zmax - zmin)*j/(nz-1) (throughfocus.cpp:108-110).
+struct Geom {
+    int mode;
+    int nx, ny;
+    double a0, a1;  // PSF: cx - W, step      ZX: xmin, xmax
+    double b0, b1;  // PSF: cy - W, step      ZX: zmin, zmax
+    double z;       // PSF: z
+    double ox, oy;  // origin subtracted from pillars and pixels in the f32 form
+};
+
+__device__ __forceinline__ void pixel_pos(const Geom& g, int i, int j, double& fx,
+                                          double& fy, double& fz) {
+    if (g.mode == GEOM_PSF) {
+        fx = g.a0 + i * g.a1;
+        fy = g.b0 + j * g.b1;
+        fz = g.z;
+    } else {
+        fx = g.a0 + (g.a1 - g.a0) * i / (g.nx - 1);
+        fy = 0.0;
+        fz = g.b0 + (g.b1 - g.b0) * j / (g.ny - 1);
+    }
+}
+
+__device__ __forceinline__ void record_timeout() {
+    atomicExch(&g_ff_status, CELERIS_ERR_DEVICE_TIMEOUT);
+}
+
+// ---- packing ----------------------------------------------------------------
+__global__ void ff_pack_f64(const double* __restrict__ px, const double* __restrict__ py,
+                            const double2* __restrict__ pt, int npil,
+                            double4* __restrict__ rec) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= npil) return;
+    double2 t = pt[j];
+    rec[j] = make_double4(px[j], py[j], t.x, t.y);
+}
+
+__global__ void ff_pack_f32(const double* __restrict__ px, const double* __restrict__ py,
+                            const double2* __restrict__ pt, int npil, double ox, double oy,
+                            float4* __restrict__ rec) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= npil) return;
+    double2 t = pt[j];
+    double A = hypot(t.x, t.y);
+    double psi = atan2(t.y, t.x) * 0.15915494309189533577;  // turns
+    rec[j] = make_float4((float)(px[j] - ox), (float)(py[j] - oy), (float)A, (float)psi);
+}
+
+// pixel records for the adjoint: {fx, fy, Re v, Im v}
+__global__ void ff_pack_pix(Geom g, const double2* __restrict__ v, double4* __restrict__ rec) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    int npix = g.nx * g.ny;
+    if (p >= npix) return;
+    int j = p / g.nx, i = p - j * g.nx;
+    double fx, fy, fz;
+    pixel_pos(g, i, j, fx, fy, fz);
+    double2 vv = v[p];
+    rec[p] = make_double4(fx, fy, vv.x, vv.y);
+}
+
+// ---- tile pipeline (shared by all main kernels) ----------------------------
+// Thread 0 owns the producer role: it arms stage s's mbarrier with the byte
+// count and issues one bulk copy. All threads consume. A stage is refilled only
+// after a __syncthreads that follows its last read.
+template <typename Rec, int TILE>
+struct TilePipe {
+    Rec (*buf)[TILE];
+    uint64_t* full;
+    const Rec* src;
+    int c0, c1, ntiles;
+
+    __device__ void init(Rec (*b)[TILE], uint64_t* f, const Rec* s, int lo, int hi) {
+        buf = b;
+        full = f;
+        src = s;
+        c0 = lo;
+        c1 = hi;
+        ntiles = hi > lo ? (hi - lo + TILE - 1) / TILE : 0;
+        if (threadIdx.x == 0) {
+            for (int st = 0; st < kStages; ++st) mbar_init(&full[st], 1);
+            fence_barrier_init();
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int t = 0; t < kStages && t < ntiles; ++t) issue(t);
+    }
+    __device__ int count(int t) const { return min(TILE, c1 - (c0 + t * TILE)); }
+    __device__ void issue(int t) {
+        const int st = t % kStages;
+        const int base = c0 + t * TILE;
+        const uint32_t bytes = (uint32_t)(count(t) * sizeof(Rec));
+        mbar_arrive_expect_tx(&full[st], bytes);
+        bulk_g2s(&buf[st][0], src + base, bytes, &full[st]);
+    }
+    __device__ bool wait(int t) { return mbar_wait(&full[t % kStages], (t / kStages) & 1); }
+    // call after every thread finished reading tile t; returns false on timeout
+    __device__ bool release(int t, bool got) {
+        if (!__syncthreads_and(got)) {
+            if (threadIdx.x == 0) record_timeout();
+            return false;
+        }
+        if (threadIdx.x == 0 && t + kStages < ntiles) {
+            fence_proxy_async_smem();
+            issue(t + kStages);
+        }
+        return true;
+    }
+};
+
+// ---- plain FP64 form ----------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) rs_f64_kernel(const double4* __restrict__ rec,
+                                                          int npil, int chunk_len, Geom g,
+                                                          double k, double2* __restrict__ partial) {
+    __shared__ __align__(128) double4 buf[kStages][kTile64];
+    __shared__ __align__(8) uint64_t full[kStages];
+
+    const int npix = g.nx * g.ny;
+    const int spr = (g.nx + kPPT64 - 1) / kPPT64;
+    const int strip = blockIdx.x * kThreads + threadIdx.x;
+    const int j = strip / spr;
+    const int i0 = (strip - j * spr) * kPPT64;
+    const int jj = min(j, g.ny - 1);
+
+    double fx[kPPT64], fy = 0.0, fz = 0.0;
+#pragma unroll
+    for (int q = 0; q < kPPT64; ++q) pixel_pos(g, min(i0 + q, g.nx - 1), jj, fx[q], fy, fz);
+    const double z2 = fz * fz;
+
+    TilePipe<double4, kTile64> pipe;
+    const int lo = blockIdx.y * chunk_len;
+    pipe.init(buf, full, rec, lo, min(npil, lo + chunk_len));
+
+    double er[kPPT64], ei[kPPT64];
+#pragma unroll
+    for (int q = 0; q < kPPT64; ++q) er[q] = ei[q] = 0.0;
+
+    for (int t = 0; t < pipe.ntiles; ++t) {
+        const bool got = pipe.wait(t);
+        if (got) {
+            const double4* tile = buf[t % kStages];
+            const int cnt = pipe.count(t);
+            for (int p = 0; p < cnt; ++p) {
+                const double4 r = tile[p];
+                const double dy = fy - r.y;
+                const double dy2 = dy * dy;
+#pragma unroll
+                for (int q = 0; q < kPPT64; ++q) {
+                    const double dx = fx[q] - r.x;
+                    const double R = sqrt(dx * dx + dy2 + z2);
+                    double s, c;
+                    sincos(k * R, &s, &c);
+                    const double inv = 1.0 / R;
+                    const double pr = inv * c, pim = inv * s;  // std::polar(1/R, kR)
+                    er[q] += r.z * pr - r.w * pim;             // t * polar
+                    ei[q] += r.z * pim + r.w * pr;
+                }
+            }
+        }
+        if (!pipe.release(t, got)) return;
+    }
+    if (j < g.ny) {
+#pragma unroll
+        for (int q = 0; q < kPPT64; ++q)
+            if (i0 + q < g.nx)
+                partial[(size_t)blockIdx.y * npix + (size_t)j * g.nx + i0 + q] =
+                    make_double2(er[q], ei[q]);
+    }
+}
+
+// ---- precision form: FP32 terms, compensated accumulation -------------------
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float sin_approx(float x) {
+    float y;
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float cos_approx(float x) {
+    float y;
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+// Knuth TwoSum: s + c += x with the rounding error of s + x kept in c.
+__device__ __forceinline__ void two_sum_acc(float& s, float& c, float x) {
+    const float t = s + x;
+    const float bp = t - s;
+    const float ap = t - bp;
+    c += (s - ap) + (x - bp);
+    s = t;
+}
+
+__global__ void __launch_bounds__(kThreads) rs_f32c_kernel(const float4* __restrict__ rec,
+                                                           int npil, int chunk_len, Geom g,
+                                                           float il_hi, float il_lo,
+                                                           double2* __restrict__ partial) {
+    __shared__ __align__(128) float4 buf[kStages][kTile32];
+    __shared__ __align__(8) uint64_t full[kStages];
+
+    const int npix = g.nx * g.ny;
+    const int spr = (g.nx + kPPT32 - 1) / kPPT32;
+    const int strip = blockIdx.x * kThreads + threadIdx.x;
+    const int j = strip / spr;
+    const int i0 = (strip - j * spr) * kPPT32;
+    const int jj = min(j, g.ny - 1);
+
+    float fxr[kPPT32], fyr = 0.f, z = 0.f;
+#pragma unroll
+    for (int q = 0; q < kPPT32; ++q) {
+        double fx, fy, fz;
+        pixel_pos(g, min(i0 + q, g.nx - 1), jj, fx, fy, fz);
+        fxr[q] = (float)(fx - g.ox);
+        fyr = (float)(fy - g.oy);
+        z = (float)fz;
+    }
+    const float z2 = z * z;
+    const float z2x = 2.0f * z;
+    const float kMagic = 12582912.0f;  // 1.5 * 2^23: x + M - M rounds x to an integer
+    const float kTwoPi = 6.28318530717958647692f;
+
+    TilePipe<float4, kTile32> pipe;
+    const int lo = blockIdx.y * chunk_len;
+    pipe.init(buf, full, rec, lo, min(npil, lo + chunk_len));
+
+    float sr[kPPT32], cr[kPPT32], si[kPPT32], ci[kPPT32];
+#pragma unroll
+    for (int q = 0; q < kPPT32; ++q) sr[q] = cr[q] = si[q] = ci[q] = 0.f;
+
+    for (int t = 0; t < pipe.ntiles; ++t) {
+        const bool got = pipe.wait(t);
+        if (got) {
+            const float4* tile = buf[t % kStages];
+            const int cnt = pipe.count(t);
+            float er[kPPT32], ei[kPPT32];
+#pragma unroll
+            for (int q = 0; q < kPPT32; ++q) er[q] = ei[q] = 0.f;
+#pragma unroll 2
+            for (int p = 0; p < cnt; ++p) {
+                const float4 r = tile[p];  // {x, y, |t|, arg t / 2pi}
+                const float dy = fyr - r.y;
+                const float dy2 = dy * dy;
+#pragma unroll
+                for (int q = 0; q < kPPT32; ++q) {
+                    const float dx = fxr[q] - r.x;
+                    const float s = fmaf(dx, dx, dy2);     // rho^2
+                    const float u = s + z2;                // R^2 (rounded; seed only)
+                    const float ri = rsqrt_approx(u);      // ~1/R
+                    const float d0 = u * ri - z;           // ~R - z
+                    // Newton on f(d) = d^2 + 2 z d - rho^2 (exact root R - z)
+                    const float gg = fmaf(d0, d0, fmaf(z2x, d0, -s));
+                    const float d = fmaf(gg * ri, -0.5f, d0);
+                    // phase in turns: (R - z)/lambda + arg(t)/2pi; k z is added in FP64
+                    const float th = fmaf(d, il_hi, fmaf(d, il_lo, r.w));
+                    const float rn = (th + kMagic) - kMagic;
+                    const float ang = (th - rn) * kTwoPi;  // in [-pi, pi]
+                    const float a = r.z * ri;              // |t| / R
+                    er[q] = fmaf(a, cos_approx(ang), er[q]);
+                    ei[q] = fmaf(a, sin_approx(ang), ei[q]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kPPT32; ++q) {
+                two_sum_acc(sr[q], cr[q], er[q]);
+                two_sum_acc(si[q], ci[q], ei[q]);
+            }
+        }
+        if (!pipe.release(t, got)) return;
+    }
+    if (j < g.ny) {
+#pragma unroll
+        for (int q = 0; q < kPPT32; ++q)
+            if (i0 + q < g.nx)
+                partial[(size_t)blockIdx.y * npix + (size_t)j * g.nx + i0 + q] =
+                    make_double2((double)sr[q] + (double)cr[q], (double)si[q] + (double)ci[q]);
+    }
+}
+
+// ---- chunk reduction + epilogue ---------------------------------------------
+__global__ void rs_reduce_kernel(const double2* __restrict__ partial, int nchunk, Geom g,
+                                 double k, int apply_phase, double2* __restrict__ field,
+                                 double* __restrict__ intensity) {
+    const int npix = g.nx * g.ny;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npix) return;
+    double er = 0.0, ei = 0.0;
+    for (int c = 0; c < nchunk; ++c) {
+        const double2 v = partial[(size_t)c * npix + p];
+        er += v.x;
+        ei += v.y;
+    }
+    if (apply_phase) {
+        const int j = p / g.nx;
+        double fx, fy, fz;
+        pixel_pos(g, 0, j, fx, fy, fz);
+        const double zf = (double)(float)fz;  // the z the FP32 terms used
+        double s, c;
+        sincos(k * zf, &s, &c);
+        const double r = er * c - ei * s;
+        ei = er * s + ei * c;
+        er = r;
+    }
+    if (field) field[p] = make_double2(er, ei);
+    if (intensity) intensity[p] = er * er + ei * ei;  // std::norm(E)
+}
+
+// ---- adjoint: out_j = sum_p conj(g_pj) v_p ----------------------------------
+__global__ void __launch_bounds__(kThreads) rs_adj_f64_kernel(const double4* __restrict__ pix,
+                                                              int npix, int chunk_len,
+                                                              const double* __restrict__ px,
+                                                              const double* __restrict__ py,
+                                                              int npil, double z, double k,
+                                                              double2* __restrict__ partial) {
+    __shared__ __align__(128) double4 buf[kStages][kTile64];
+    __shared__ __align__(8) uint64_t full[kStages];
+
+    const int j0 = (blockIdx.x * kThreads + threadIdx.x) * kAdjPPT;
+    double x[kAdjPPT], y[kAdjPPT];
+#pragma unroll
+    for (int q = 0; q < kAdjPPT; ++q) {
+        const int jq = min(j0 + q, npil - 1);
+        x[q] = px[jq];
+        y[q] = py[jq];
+    }
+    const double z2 = z * z;
+
+    TilePipe<double4, kTile64> pipe;
+    const int lo = blockIdx.y * chunk_len;
+    pipe.init(buf, full, pix, lo, min(npix, lo + chunk_len));
+
+    double gr[kAdjPPT], gi[kAdjPPT];
+#pragma unroll
+    for (int q = 0; q < kAdjPPT; ++q) gr[q] = gi[q] = 0.0;
+
+    for (int t = 0; t < pipe.ntiles; ++t) {
+        const bool got = pipe.wait(t);
+        if (got) {
+            const double4* tile = buf[t % kStages];
+            const int cnt = pipe.count(t);
+            for (int p = 0; p < cnt; ++p) {
+                const double4 r = tile[p];  // {fx, fy, Re v, Im v}
+#pragma unroll
+                for (int q = 0; q < kAdjPPT; ++q) {
+                    const double dx = r.x - x[q];
+                    const double dy = r.y - y[q];
+                    const double R = sqrt(dx * dx + dy * dy + z2);
+                    double s, c;
+                    sincos(k * R, &s, &c);
+                    const double inv = 1.0 / R;
+                    const double pr = inv * c, pim = inv * s;
+                    gr[q] += pr * r.z + pim * r.w;  // conj(g) * v
+                    gi[q] += pr * r.w - pim * r.z;
+                }
+            }
+        }
+        if (!pipe.release(t, got)) return;
+    }
+#pragma unroll
+    for (int q = 0; q < kAdjPPT; ++q)
+        if (j0 + q < npil)
+            partial[(size_t)blockIdx.y * npil + j0 + q] = make_double2(gr[q], gi[q]);
+}
+
+__global__ void chunk_sum_kernel(const double2* __restrict__ partial, int nchunk, int n,
+                                 double2* __restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double r = 0.0, i = 0.0;
+    for (int c = 0; c < nchunk; ++c) {
+        const double2 v = partial[(size_t)c * n + j];
+        r += v.x;
+        i += v.y;
+    }
+    out[j] = make_double2(r, i);
+}
+
+// ---- sampled FP64 check -------------------------------------------------------
+__global__ void rs_check_kernel(const double4* __restrict__ rec, int npil, Geom g, double k,
+                                const double2* __restrict__ field, const int* __restrict__ idx,
+                                int ns, unsigned long long* __restrict__ maxerr_bits) {
+    __shared__ double red[2][32];
+    const int b = blockIdx.x;
+    if (b >= ns) return;
+    const int p = idx[b];
+    const int npix = g.nx * g.ny;
+    if (p < 0 || p >= npix) return;
+    const int j = p / g.nx, i = p - j * g.nx;
+    double fx, fy, fz;
+    pixel_pos(g, i, j, fx, fy, fz);
+    const double z2 = fz * fz;
+    double er = 0.0, ei = 0.0;
+    for (int q = threadIdx.x; q < npil; q += blockDim.x) {
+        const double4 r = rec[q];
+        const double dx = fx - r.x, dy = fy - r.y;
+        const double R = sqrt(dx * dx + dy * dy + z2);
+        double s, c;
+        sincos(k * R, &s, &c);
+        const double inv = 1.0 / R;
+        er += r.z * inv * c - r.w * inv * s;
+        ei += r.z * inv * s + r.w * inv * c;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        er += __shfl_down_sync(0xffffffffu, er, o);
+        ei += __shfl_down_sync(0xffffffffu, ei, o);
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0) {
+        red[0][w] = er;
+        red[1][w] = ei;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sr = 0.0, si = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+            sr += red[0][q];
+            si += red[1][q];
+        }
+        const double2 f = field[p];
+        const double err = hypot(f.x - sr, f.y - si);
+        atomicMax(maxerr_bits, (unsigned long long)__double_as_longlong(err));
+    }
+}
+
+__global__ void abs_max_kernel(const double2* __restrict__ field, int npix,
+                               unsigned long long* __restrict__ out_bits) {
+    double m = 0.0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        const double2 v = field[p];
+        m = fmax(m, hypot(v.x, v.y));
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out_bits, (unsigned long long)__double_as_longlong(m));
+}
+
+// ---- host-side planning -----------------------------------------------------
+int g_sm_count = 0;
+
+int sm_count() {
+    if (g_sm_count == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+        if (g_sm_count <= 0) g_sm_count = 148;
+    }
+    return g_sm_count;
+}
+
+// Split the pillar (or pixel) axis into chunks so the grid holds about eight
+// CTAs per SM-slot while every chunk keeps whole tiles.
+void plan_chunks(int ctas_other, int nrec, int tile, int resident_per_sm, int* nchunk,
+                 int* chunk_len) {
+    const int ntiles = std::max(1, (nrec + tile - 1) / tile);
+    const long target = (long)sm_count() * resident_per_sm * 8;
+    long want = (target + ctas_other - 1) / std::max(1, ctas_other);
+    want = std::max(1L, std::min<long>(want, ntiles));
+    const int tiles_per = (int)((ntiles + want - 1) / want);
+    *chunk_len = tiles_per * tile;
+    *nchunk = (nrec + *chunk_len - 1) / *chunk_len;
+    if (*nchunk < 1) *nchunk = 1;
+}
+
+int check_status_and_reset() {
+    int st = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&st, g_ff_status, sizeof(int));
+    if (e != cudaSuccess) return celeris_rt::cuda_error(e, "read far-field status");
+    if (st != 0) {
+        int zero = 0;
+        cudaMemcpyToSymbol(g_ff_status, &zero, sizeof(int));
+        return set_error(st, "far-field kernel: a bounded device wait ran out");
+    }
+    return CELERIS_OK;
+}
+
+Geom psf_geom(double cx, double cy, double z, int n, double W) {
+    Geom g;
+    g.mode = GEOM_PSF;
+    g.nx = g.ny = n;
+    const double step = 2.0 * W / (n - 1);  // focal.cpp:223 (n == 1 gives inf, as the reference)
+    g.a0 = cx - W;
+    g.a1 = step;
+    g.b0 = cy - W;
+    g.b1 = step;
+    g.z = z;
+    g.ox = cx;
+    g.oy = cy;
+    return g;
+}
+
+Geom zx_geom(double xmin, double xmax, int nx, double zmin, double zmax, int nz) {
+    Geom g;
+    g.mode = GEOM_ZX;
+    g.nx = nx;
+    g.ny = nz;
+    g.a0 = xmin;
+    g.a1 = xmax;
+    g.b0 = zmin;
+    g.b1 = zmax;
+    g.z = 0.0;
+    g.ox = 0.0;
+    g.oy = 0.0;
+    return g;
+}
+
+// Optional CUDA-event timing of the main kernel (bench instrumentation).
+std::atomic<int> g_time_kernels{0};
+struct KernelTimer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    bool pending = false;
+};
+thread_local KernelTimer t_timer;
+
+void timer_begin(cudaStream_t st) {
+    if (!g_time_kernels.load()) return;
+    if (!t_timer.a) {
+        cudaEventCreate(&t_timer.a);
+        cudaEventCreate(&t_timer.b);
+    }
+    cudaEventRecord(t_timer.a, st);
+}
+void timer_end(cudaStream_t st) {
+    if (!g_time_kernels.load()) return;
+    cudaEventRecord(t_timer.b, st);
+    t_timer.pending = true;
+}
+
+// Full far-field on device buffers (inputs SoA px, py + interleaved complex pt).
+int ff_run(int form, const double* d_px, const double* d_py, const double* d_pt, int npil,
+           const Geom& g, double k, double* d_field, double* d_int, cudaStream_t st) {
+    const long npix = (long)g.nx * g.ny;
+    if (npix <= 0) return CELERIS_OK;
+    if (npix > (1L << 30)) return set_error(CELERIS_ERR_TOO_LARGE, "grid too large (%ld pixels)", npix);
+    if (npil == 0) {
+        if (d_field) CEL_CUDA(cudaMemsetAsync(d_field, 0, npix * 2 * sizeof(double), st));
+        if (d_int) CEL_CUDA(cudaMemsetAsync(d_int, 0, npix * sizeof(double), st));
+        return CELERIS_OK;
+    }
+    const bool f32 = (form == CELERIS_FORM_F32C);
+    const int ppt = f32 ? kPPT32 : kPPT64;
+    const int tile = f32 ? kTile32 : kTile64;
+    const long spr = (g.nx + ppt - 1) / ppt;
+    const long strips = spr * g.ny;
+    const int ctas_pix = (int)((strips + kThreads - 1) / kThreads);
+    int nchunk = 1, chunk_len = npil;
+    plan_chunks(ctas_pix, npil, tile, f32 ? 3 : 2, &nchunk, &chunk_len);
+
+    Workspace& ws = Workspace::for_stream(st);
+    const size_t rec_bytes = (size_t)npil * (f32 ? sizeof(float4) : sizeof(double4));
+    const size_t part_bytes = (size_t)nchunk * npix * sizeof(double2);
+    CEL_TRY(ws.reserve(st, celeris_rt::align256(rec_bytes) + celeris_rt::align256(part_bytes)));
+    void* rec = ws.take(rec_bytes);
+    double2* partial = static_cast<double2*>(ws.take(part_bytes));
+
+    const int pb = (npil + 255) / 256;
+    if (f32) {
+        ff_pack_f32<<<pb, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil,
+                                        g.ox, g.oy, static_cast<float4*>(rec));
+    } else {
+        ff_pack_f64<<<pb, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil,
+                                        static_cast<double4*>(rec));
+    }
+    dim3 grid(ctas_pix, nchunk);
+    timer_begin(st);
+    if (f32) {
+        const double il = k / (2.0 * 3.14159265358979323846);  // 1/lambda in turns per micron
+        const float hi = (float)il;
+        const float lo = (float)(il - (double)hi);
+        rs_f32c_kernel<<<grid, kThreads, 0, st>>>(static_cast<const float4*>(rec), npil, chunk_len,
+                                                  g, hi, lo, partial);
+    } else {
+        rs_f64_kernel<<<grid, kThreads, 0, st>>>(static_cast<const double4*>(rec), npil,
+                                                 chunk_len, g, k, partial);
+    }
+    timer_end(st);
+    rs_reduce_kernel<<<(int)((npix + 255) / 256), 256, 0, st>>>(
+        partial, nchunk, g, k, f32 ? 1 : 0, reinterpret_cast<double2*>(d_field), d_int);
+    count_launch(3);
+    CEL_CUDA(cudaGetLastError());
+    return CELERIS_OK;
+}
+
+int ff_adjoint(const double* d_px, const double* d_py, int npil, const Geom& g, double k,
+               const double* d_v, double* d_out, cudaStream_t st) {
+    const long npix = (long)g.nx * g.ny;
+    if (npil <= 0) return CELERIS_OK;
+    if (npix <= 0) {
+        CEL_CUDA(cudaMemsetAsync(d_out, 0, (size_t)npil * 2 * sizeof(double), st));
+        return CELERIS_OK;
+    }
+    const int ctas = (int)(((long)npil + kThreads * kAdjPPT - 1) / (kThreads * kAdjPPT));
+    int nchunk = 1, chunk_len = (int)npix;
+    plan_chunks(ctas, (int)npix, kTile64, 2, &nchunk, &chunk_len);
+    Workspace& ws = Workspace::for_stream(st);
+    const size_t rec_bytes = (size_t)npix * sizeof(double4);
+    const size_t part_bytes = (size_t)nchunk * npil * sizeof(double2);
+    CEL_TRY(ws.reserve(st, celeris_rt::align256(rec_bytes) + celeris_rt::align256(part_bytes)));
+    double4* rec = static_cast<double4*>(ws.take(rec_bytes));
+    double2* partial = static_cast<double2*>(ws.take(part_bytes));
+    ff_pack_pix<<<(int)((npix + 255) / 256), 256, 0, st>>>(g, reinterpret_cast<const double2*>(d_v), rec);
+    dim3 grid(ctas, nchunk);
+    timer_begin(st);
+    rs_adj_f64_kernel<<<grid, kThreads, 0, st>>>(rec, (int)npix, chunk_len, d_px, d_py, npil, g.z, k,
+                                                 partial);
+    timer_end(st);
+    chunk_sum_kernel<<<(npil + 255) / 256, 256, 0, st>>>(partial, nchunk, npil,
+                                                         reinterpret_cast<double2*>(d_out));
+    count_launch(3);
+    CEL_CUDA(cudaGetLastError());
+    return CELERIS_OK;
+}
+
+int ff_check(const double* d_px, const double* d_py, const double* d_pt, int npil, const Geom& g,
+             double k, const double* d_field, const int* d_idx, int ns, double* err_out,
+             cudaStream_t st) {
+    const long npix = (long)g.nx * g.ny;
+    *err_out = 0.0;
+    if (npil <= 0 || npix <= 0 || ns <= 0) return CELERIS_OK;
+    Workspace& ws = Workspace::for_stream(st);
+    const size_t rec_bytes = (size_t)npil * sizeof(double4);
+    CEL_TRY(ws.reserve(st, celeris_rt::align256(rec_bytes) + 256));
+    double4* rec = static_cast<double4*>(ws.take(rec_bytes));
+    unsigned long long* bits = static_cast<unsigned long long*>(ws.take(2 * sizeof(unsigned long long)));
+    CEL_CUDA(cudaMemsetAsync(bits, 0, 2 * sizeof(unsigned long long), st));
+    ff_pack_f64<<<(npil + 255) / 256, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt),
+                                                    npil, rec);
+    rs_check_kernel<<<ns, 256, 0, st>>>(rec, npil, g, k, reinterpret_cast<const double2*>(d_field),
+                                        d_idx, ns, bits);
+    abs_max_kernel<<<4 * sm_count(), 256, 0, st>>>(reinterpret_cast<const double2*>(d_field),
+                                                   (int)npix, bits + 1);
+    count_launch(3);
+    CEL_CUDA(cudaGetLastError());
+    unsigned long long h[2];
+    CEL_CUDA(cudaMemcpyAsync(h, bits, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CEL_CUDA(cudaStreamSynchronize(st));
+    double e, m;
+    std::memcpy(&e, &h[0], sizeof(double));
+    std::memcpy(&m, &h[1], sizeof(double));
+    *err_out = m > 0.0 ? e / m : e;
+    return check_status_and_reset();
+}
+
+// One non-blocking stream per host thread for the synchronous host-buffer calls.
+cudaStream_t thread_stream() {
+    thread_local cudaStream_t s = nullptr;
+    thread_local int dev = -1;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (!s || dev != cur) {
+        cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        dev = cur;
+    }
+    return s;
+}
+
+// Sample of pixel indices for the stated error: a strided lattice plus the
+// centre pixel.
+std::vector<int> sample_pixels(int nx, int ny, int want) {
+    std::vector<int> idx;
+    const long npix = (long)nx * ny;
+    if (npix <= want) {
+        for (int p = 0; p < npix; ++p) idx.push_back(p);
+        return idx;
+    }
+    const long stride = npix / want;
+    for (long p = stride / 2; p < npix && (int)idx.size() < want; p += stride) idx.push_back((int)p);
+    idx.push_back((ny / 2) * nx + nx / 2);
+    return idx;
+}
+
+// Host-buffer wrapper: stage inputs through pinned memory, run, copy back.
+int ff_host(int form, const double* px, const double* py, const double* pt, int npil,
+            const Geom& g, double k, double* field_out, double* int_out, double* err_out) {
+    CEL_TRY(celeris_rt::require_device());
+    const long npix = (long)g.nx * g.ny;
+    if (err_out) *err_out = 0.0;
+    if (npix <= 0) return CELERIS_OK;
+    if (npil < 0) return set_error(CELERIS_ERR_INVALID_ARG, "npil < 0");
+    if (npil > 0 && (!px || !py || !pt)) return set_error(CELERIS_ERR_INVALID_ARG, "NULL pillar arrays");
+    cudaStream_t st = thread_stream();
+    const bool want_err = (form == CELERIS_FORM_F32C) && err_out && npil > 0;
+    std::vector<int> sidx;
+    if (want_err) sidx = sample_pixels(g.nx, g.ny, 256);
+
+    const size_t in_bytes = (size_t)npil * 4 * sizeof(double);
+    const size_t fld_bytes = (size_t)npix * 2 * sizeof(double);
+    const size_t int_bytes = (size_t)npix * sizeof(double);
+    const size_t idx_bytes = sidx.size() * sizeof(int);
+    const size_t pin_bytes = celeris_rt::align256(in_bytes) + celeris_rt::align256(fld_bytes) +
+                             celeris_rt::align256(int_bytes) + celeris_rt::align256(idx_bytes);
+    char* pin = static_cast<char*>(celeris_rt::pinned_staging(pin_bytes));
+    if (!pin) return set_error(CELERIS_ERR_OOM, "pinned staging of %zu bytes failed", pin_bytes);
+
+    // Device I/O buffers live in their own persistent arena (separate from the
+    // scratch arena the kernels use on the same stream).
+    static thread_local void* d_io = nullptr;
+    static thread_local size_t d_io_cap = 0;
+    if (d_io_cap < pin_bytes) {
+        if (d_io) {
+            cudaStreamSynchronize(st);
+            cudaFree(d_io);
+        }
+        d_io = nullptr;
+        d_io_cap = 0;
+        CEL_CUDA(cudaMalloc(&d_io, pin_bytes));
+        d_io_cap = pin_bytes;
+    }
+    char* d = static_cast<char*>(d_io);
+    double* d_px = reinterpret_cast<double*>(d);
+    double* d_py = d_px + npil;
+    double* d_pt = d_py + npil;
+    double* d_fld = reinterpret_cast<double*>(d + celeris_rt::align256(in_bytes));
+    double* d_int = reinterpret_cast<double*>(d + celeris_rt::align256(in_bytes) +
+                                              celeris_rt::align256(fld_bytes));
+    int* d_idx = reinterpret_cast<int*>(d + celeris_rt::align256(in_bytes) +
+                                        celeris_rt::align256(fld_bytes) + celeris_rt::align256(int_bytes));
+    double* h_px = reinterpret_cast<double*>(pin);
+    if (npil > 0) {
+        std::memcpy(h_px, px, npil * sizeof(double));
+        std::memcpy(h_px + npil, py, npil * sizeof(double));
+        std::memcpy(h_px + 2 * npil, pt, npil * 2 * sizeof(double));
+        CEL_CUDA(cudaMemcpyAsync(d_px, h_px, in_bytes, cudaMemcpyHostToDevice, st));
+    }
+    if (want_err) {
+        int* h_idx = reinterpret_cast<int*>(pin + celeris_rt::align256(in_bytes) +
+                                            celeris_rt::align256(fld_bytes) + celeris_rt::align256(int_bytes));
+        std::memcpy(h_idx, sidx.data(), idx_bytes);
+        CEL_CUDA(cudaMemcpyAsync(d_idx, h_idx, idx_bytes, cudaMemcpyHostToDevice, st));
+    }
+    const bool need_field = field_out || want_err;
+    CEL_TRY(ff_run(form, d_px, d_py, d_pt, npil, g, k, need_field ? d_fld : nullptr,
+                   int_out ? d_int : nullptr, st));
+    double* h_fld = reinterpret_cast<double*>(pin + celeris_rt::align256(in_bytes));
+    double* h_int = reinterpret_cast<double*>(pin + celeris_rt::align256(in_bytes) + celeris_rt::align256(fld_bytes));
+    if (field_out) CEL_CUDA(cudaMemcpyAsync(h_fld, d_fld, fld_bytes, cudaMemcpyDeviceToHost, st));
+    if (int_out) CEL_CUDA(cudaMemcpyAsync(h_int, d_int, int_bytes, cudaMemcpyDeviceToHost, st));
+    if (want_err) {
+        CEL_TRY(ff_check(d_px, d_py, d_pt, npil, g, k, d_fld, d_idx, (int)sidx.size(), err_out, st));
+    }
+    CEL_CUDA(cudaStreamSynchronize(st));
+    CEL_TRY(check_status_and_reset());
+    if (field_out) std::memcpy(field_out, h_fld, fld_bytes);
+    if (int_out) std::memcpy(int_out, h_int, int_bytes);
+    return CELERIS_OK;
+}
+
+bool valid_form(int form) { return form == CELERIS_FORM_PLAIN_F64 || form == CELERIS_FORM_F32C; }
+
+}  // namespace
+
+extern "C" {
+
+int celeris_propagate_psf(const double* px, const double* py, const double* pt, int npil,
+                          double cx, double cy, double z, double k, int n, double half_window,
+                          double* out) {
+    if (n < 0) return set_error(CELERIS_ERR_INVALID_ARG, "n < 0");
+    if (n == 0) return CELERIS_OK;
+    if (!out) return set_error(CELERIS_ERR_INVALID_ARG, "out is NULL");
+    return ff_host(CELERIS_FORM_PLAIN_F64, px, py, pt, npil, psf_geom(cx, cy, z, n, half_window), k,
+                   nullptr, out, nullptr);
+}
+
+int celeris_propagate_zx(const double* px, const double* py, const double* pt, int npil,
+                         double xmin, double xmax, int nx, double zmin, double zmax, int nz,
+                         double k, double* out) {
+    if (nx <= 1 || nz <= 1) return set_error(CELERIS_ERR_INVALID_ARG, "nx, nz must be > 1");
+    if (!out) return set_error(CELERIS_ERR_INVALID_ARG, "out is NULL");
+    return ff_host(CELERIS_FORM_PLAIN_F64, px, py, pt, npil, zx_geom(xmin, xmax, nx, zmin, zmax, nz),
+                   k, nullptr, out, nullptr);
+}
+
+int celeris_rs_field(int form, const double* px, const double* py, const double* pt, int npil,
+                     double cx, double cy, double z, double k, int n, double half_window,
+                     double* field_out, double* intensity_out, double* err_out) {
+    if (!valid_form(form)) return set_error(CELERIS_ERR_INVALID_ARG, "unknown form %d", form);
+    if (n < 0) return set_error(CELERIS_ERR_INVALID_ARG, "n < 0");
+    if (n == 0) {
+        if (err_out) *err_out = 0.0;
+        return CELERIS_OK;
+    }
+    return ff_host(form, px, py, pt, npil, psf_geom(cx, cy, z, n, half_window), k, field_out,
+                   intensity_out, err_out);
+}
+
+int celeris_rs_field_dev(int form, const double* d_px, const double* d_py, const double* d_pt,
+                         int npil, double cx, double cy, double z, double k, int n,
+                         double half_window, double* d_field, double* d_intensity, void* stream) {
+    if (!valid_form(form)) return set_error(CELERIS_ERR_INVALID_ARG, "unknown form %d", form);
+    if (n < 0 || npil < 0) return set_error(CELERIS_ERR_INVALID_ARG, "negative size");
+    if (npil > 0 && (!d_px || !d_py || !d_pt)) return set_error(CELERIS_ERR_INVALID_ARG, "NULL pillar arrays");
+    CEL_TRY(celeris_rt::require_device());
+    return ff_run(form, d_px, d_py, d_pt, npil, psf_geom(cx, cy, z, n, half_window), k, d_field,
+                  d_intensity, static_cast<cudaStream_t>(stream));
+}
+
+int celeris_rs_adjoint_dev(int form, const double* d_px, const double* d_py, int npil, double cx,
+                           double cy, double z, double k, int n, double half_window,
+                           const double* d_v, double* d_out, void* stream) {
+    if (form != CELERIS_FORM_PLAIN_F64)
+        return set_error(CELERIS_ERR_INVALID_ARG, "adjoint: only the plain FP64 form is provided");
+    if (n < 0 || npil < 0) return set_error(CELERIS_ERR_INVALID_ARG, "negative size");
+    if (npil > 0 && (!d_px || !d_py || !d_out)) return set_error(CELERIS_ERR_INVALID_ARG, "NULL arrays");
+    if ((long)n * n > 0 && !d_v) return set_error(CELERIS_ERR_INVALID_ARG, "d_v is NULL");
+    CEL_TRY(celeris_rt::require_device());
+    return ff_adjoint(d_px, d_py, npil, psf_geom(cx, cy, z, n, half_window), k, d_v, d_out,
+                      static_cast<cudaStream_t>(stream));
+}
+
+int celeris_rs_check_dev(const double* d_px, const double* d_py, const double* d_pt, int npil,
+                         double cx, double cy, double z, double k, int n, double half_window,
+                         const double* d_field, const int* d_idx, int ns, double* err_out,
+                         void* stream) {
+    if (!err_out) return set_error(CELERIS_ERR_INVALID_ARG, "err_out is NULL");
+    if (n < 0 || npil < 0 || ns < 0) return set_error(CELERIS_ERR_INVALID_ARG, "negative size");
+    CEL_TRY(celeris_rt::require_device());
+    return ff_check(d_px, d_py, d_pt, npil, psf_geom(cx, cy, z, n, half_window), k, d_field, d_idx,
+                    ns, err_out, static_cast<cudaStream_t>(stream));
+}
+
+int celeris_set_kernel_timing(int on) {
+    g_time_kernels.store(on ? 1 : 0);
+    return CELERIS_OK;
+}
+
+int celeris_last_kernel_ms(double* ms) {
+    if (!ms) return set_error(CELERIS_ERR_INVALID_ARG, "ms is NULL");
+    if (!t_timer.pending) return set_error(CELERIS_ERR_INVALID_ARG, "no timed kernel recorded");
+    CEL_CUDA(cudaEventSynchronize(t_timer.b));
+    float v = 0.f;
+    CEL_CUDA(cudaEventElapsedTime(&v, t_timer.a, t_timer.b));
+    *ms = v;
+    return CELERIS_OK;
+}
+
+int celeris_sync_status(void* stream) {
+    CEL_TRY(celeris_rt::require_device());
+    CEL_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    return check_status_and_reset();
+}
+
+}  // extern "C"

@@ -1,0 +1,96 @@
+// Throughput probes: measured peaks of the pipes the far-field kernels are
+// bound by (MUFU transcendentals, FP32 FMA, FP64 FMA) on the current device.
+// Used by bench.py for the roofline denominators; not part of any result path.
+#include <cuda_runtime.h>
+
+#include "runtime.cuh"
+
+namespace {
+
+constexpr int kChains = 8;
+
+__global__ void probe_mufu(float seed, int iters, float* sink) {
+    float v[kChains];
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) v[c] = seed + 0.001f * (threadIdx.x + c);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int c = 0; c < kChains; ++c) {
+            float y;
+            asm volatile("sin.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(v[c]));
+            v[c] = y;
+        }
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) s += v[c];
+    if (s == 12345.678f) sink[0] = s;
+}
+
+__global__ void probe_ffma(float a, int iters, float* sink) {
+    float v[kChains];
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) v[c] = a + threadIdx.x * 1e-3f + c;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int c = 0; c < kChains; ++c) v[c] = fmaf(v[c], 0.9999f, 1e-4f);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) s += v[c];
+    if (s == 12345.678f) sink[0] = s;
+}
+
+__global__ void probe_dfma(double a, int iters, double* sink) {
+    double v[kChains];
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) v[c] = a + threadIdx.x * 1e-3 + c;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int c = 0; c < kChains; ++c) v[c] = fma(v[c], 0.9999, 1e-4);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) s += v[c];
+    if (s == 12345.678) sink[0] = s;
+}
+
+template <typename F>
+int time_probe(F launch, double ops, double* out_per_s) {
+    cudaEvent_t a, b;
+    CEL_CUDA(cudaEventCreate(&a));
+    CEL_CUDA(cudaEventCreate(&b));
+    launch();  // warm-up
+    CEL_CUDA(cudaEventRecord(a));
+    launch();
+    CEL_CUDA(cudaEventRecord(b));
+    CEL_CUDA(cudaEventSynchronize(b));
+    float ms = 0.f;
+    CEL_CUDA(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *out_per_s = ops / (ms * 1e-3);
+    return CELERIS_OK;
+}
+
+}  // namespace
+
+// New: measured op rates: MUFU sin.approx results/s, FP32 FMA/s, FP64 FMA/s.
+extern "C" int celeris_probe_peaks(double* mufu_per_s, double* ffma_per_s, double* dfma_per_s) {
+    CEL_TRY(celeris_rt::require_device());
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    void* sink = nullptr;
+    CEL_CUDA(cudaMalloc(&sink, 64));
+    const int blocks = sms * 8, threads = 256;
+    const int it_m = 4096, it_f = 16384, it_d = 4096;
+    const double thr = (double)blocks * threads * kChains;
+    CEL_TRY(time_probe([&] { probe_mufu<<<blocks, threads>>>(0.5f, it_m, (float*)sink); }, thr * it_m, mufu_per_s));
+    CEL_TRY(time_probe([&] { probe_ffma<<<blocks, threads>>>(0.5f, it_f, (float*)sink); }, thr * it_f, ffma_per_s));
+    CEL_TRY(time_probe([&] { probe_dfma<<<blocks, threads>>>(0.5, it_d, (double*)sink); }, thr * it_d, dfma_per_s));
+    celeris_rt::count_launch(6);
+    cudaFree(sink);
+    CEL_CUDA(cudaGetLastError());
+    return CELERIS_OK;
+}

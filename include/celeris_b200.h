@@ -1,0 +1,194 @@
+/*
+ * celeris_b200.h - C ABI of the B200-native CELERIS hot path.
+ *
+ * Two data-parallel paths sit behind this boundary:
+ *   1. the Rayleigh-Sommerfeld (RS) far-field sum over focal pixels x pillars
+ *        E(p) = sum_j t_j exp(i k R_pj) / R_pj,
+ *        R_pj = sqrt((fx_p - x_j)^2 + (fy_p - y_j)^2 + z_p^2)
+ *      (reference: src/celeris/cuda/propagate.cu:36-130 psf/zx kernels,
+ *       src/celeris/analysis/focal.cpp:205-238 propagate_pillars);
+ *   2. the 2D vectorial RCWA unit-cell solve (reference:
+ *      src/celeris/rcwa/rcwa2d.cpp:209-488 solve_rcwa_2d) and the library sweep
+ *      built on it (src/celeris/design/metalens.cpp:122-163).
+ *
+ * Conventions
+ *   - Every entry point returns an int status (CELERIS_OK == 0). On a non-zero
+ *     status celeris_last_error() returns a message for the calling thread.
+ *     There is no CPU fallback: without a CUDA device the far-field and RCWA
+ *     entry points return CELERIS_ERR_NO_DEVICE.
+ *   - Complex arrays are interleaved (re, im) doubles: the memory layout of
+ *     std::complex<double>[] and of numpy complex128.
+ *   - Host-buffer entry points ("drop-in" forms) are synchronous from the
+ *     caller's view, like the reference. *_dev entry points take device
+ *     pointers and a cudaStream_t (passed as void*, NULL = legacy default
+ *     stream) and are asynchronous with respect to the host.
+ *   - Focal grid: pixel (i, j), i = column, j = row, row-major index j*n + i,
+ *       fx = cx - W + i * step, fy = cy - W + j * step, step = 2W / (n - 1)
+ *     (propagate.cu:51-52, focal.cpp:223-226).
+ */
+#ifndef CELERIS_B200_H
+#define CELERIS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------- */
+#define CELERIS_OK 0
+#define CELERIS_ERR_NO_DEVICE 1     /* no CUDA device (reference: propagate_psf returns false) */
+#define CELERIS_ERR_INVALID_ARG 2   /* bad sizes / NULL pointers (reference: std::invalid_argument) */
+#define CELERIS_ERR_OOM 3           /* device or pinned allocation failed */
+#define CELERIS_ERR_CUDA 4          /* a CUDA runtime call or kernel failed */
+#define CELERIS_ERR_EIG_NOCONV 5    /* QR eigensolve hit its sweep cap (LAPACK info > 0) */
+#define CELERIS_ERR_TOO_LARGE 6     /* size beyond a documented limit */
+#define CELERIS_ERR_DEVICE_TIMEOUT 7 /* a bounded device-side wait ran out */
+#define CELERIS_ERR_SINGULAR 8      /* exactly singular pivot in an LU factorization */
+
+/* Far-field arithmetic forms. */
+#define CELERIS_FORM_PLAIN_F64 0 /* FP64 throughout, the reference CPU method (focal.cpp:229-233) */
+#define CELERIS_FORM_F32C 1      /* FP32 terms, FP64 k*z phase reduction, compensated accumulation */
+
+/* ---- device / diagnostics -------------------------------------------------- */
+
+/* replaces celeris::cuda::available() (src/celeris/cuda/propagate.hpp:20) */
+int celeris_available(void);
+/* replaces celeris::cuda::device_name() (src/celeris/cuda/propagate.hpp:21) */
+const char* celeris_device_name(void);
+/* New: message for the last non-zero status returned on this thread. */
+const char* celeris_last_error(void);
+/* New: ABI version (major * 10000 + minor * 100 + patch). */
+int celeris_abi_version(void);
+/* New: number of kernels this library launched since load (all threads). */
+uint64_t celeris_launch_count(void);
+/* New: release the per-device workspace arenas and pinned staging buffers. */
+int celeris_release_workspace(void);
+
+/* New: measured op rates of the current device (MUFU sin.approx results/s,
+ * FP32 FMA/s, FP64 FMA/s) from short probe kernels; roofline denominators. */
+int celeris_probe_peaks(double* mufu_per_s, double* ffma_per_s, double* dfma_per_s);
+/* New: when on != 0, the far-field entry points record CUDA events around
+ * their main kernel (on the stream it is launched on). */
+int celeris_set_kernel_timing(int on);
+/* New: duration in ms of the last timed main far-field kernel of this thread
+ * (waits for it). Returns CELERIS_ERR_INVALID_ARG if none was recorded. */
+int celeris_last_kernel_ms(double* ms);
+
+/* ---- far-field: host-buffer drop-ins --------------------------------------- */
+
+/* Drop-in for celeris::cuda::propagate_psf (src/celeris/cuda/propagate.hpp:27-30,
+ * propagate.cu:133-193). Writes |E|^2 on the n x n grid into out (n*n doubles).
+ * Computed in the plain FP64 form (the reference kernel is FP32; the plain form
+ * reproduces the reference CPU path focal.cpp:224-236 instead). npil == 0
+ * writes zeros (the reference then falls back to its CPU path, which returns
+ * zeros, focal.cpp:216). */
+int celeris_propagate_psf(const double* px, const double* py, const double* pt,
+                          int npil, double cx, double cy, double z, double k,
+                          int n, double half_window, double* out);
+
+/* Drop-in for celeris::cuda::propagate_zx (src/celeris/cuda/propagate.hpp:35-38,
+ * propagate.cu:195-253): |E|^2 on an nz x nx grid in the y = 0 plane, row = z
+ * index, fx = xmin + (xmax - xmin) * ix / (nx - 1), z = zmin + (zmax - zmin) *
+ * iz / (nz - 1) (the CPU form of throughfocus.cpp:105-118). Plain FP64. */
+int celeris_propagate_zx(const double* px, const double* py, const double* pt,
+                         int npil, double xmin, double xmax, int nx,
+                         double zmin, double zmax, int nz, double k,
+                         double* out);
+
+/* New: general far-field on host buffers (the e2e path). form selects
+ * CELERIS_FORM_*. field_out (2*n*n doubles, complex E) and intensity_out
+ * (n*n doubles, |E|^2) may each be NULL. For CELERIS_FORM_F32C, err_out (may
+ * be NULL) receives max_p |E_p - E64_p| / max_p |E_p| over a pixel sample
+ * re-evaluated in the FP64 form on the device: the error stated with the
+ * result. For the plain form *err_out = 0. */
+int celeris_rs_field(int form, const double* px, const double* py,
+                     const double* pt, int npil, double cx, double cy,
+                     double z, double k, int n, double half_window,
+                     double* field_out, double* intensity_out, double* err_out);
+
+/* ---- far-field: device-buffer forms ---------------------------------------- */
+
+/* New: far-field with inputs resident on the device. d_field (2*n*n doubles)
+ * and d_intensity (n*n) may each be NULL. stream: cudaStream_t or NULL. */
+int celeris_rs_field_dev(int form, const double* d_px, const double* d_py,
+                         const double* d_pt, int npil, double cx, double cy,
+                         double z, double k, int n, double half_window,
+                         double* d_field, double* d_intensity, void* stream);
+
+/* New: adjoint (conjugate-transpose, pixel -> pillar) RS sum on the same grid:
+ *   d_out[j] = sum_p conj(g_pj) * d_v[p],   g_pj = exp(i k R_pj) / R_pj.
+ * d_v: n*n complex, d_out: npil complex. This is the vector-Jacobian product of
+ * celeris_rs_field_dev w.r.t. the pillar transmissions t (PyTorch convention).
+ * The reference has no adjoint (its only gradient is central finite differences
+ * of RCWA, src/celeris/design/optimize.cpp:60-71). */
+int celeris_rs_adjoint_dev(int form, const double* d_px, const double* d_py,
+                           int npil, double cx, double cy, double z, double k,
+                           int n, double half_window, const double* d_v,
+                           double* d_out, void* stream);
+
+/* New: sampled FP64 check of a computed field. For the pixel indices d_idx[0..ns)
+ * recomputes E in the plain FP64 form and writes max|E - E64| over the sample
+ * divided by max over all n*n pixels of |E| into *err_out (host). Synchronous. */
+int celeris_rs_check_dev(const double* d_px, const double* d_py,
+                         const double* d_pt, int npil, double cx, double cy,
+                         double z, double k, int n, double half_window,
+                         const double* d_field, const int* d_idx, int ns,
+                         double* err_out, void* stream);
+
+/* New: synchronize `stream` and report a device-side failure (a bounded wait
+ * that ran out) recorded by an earlier asynchronous *_dev call. */
+int celeris_sync_status(void* stream);
+
+/* ---- RCWA ------------------------------------------------------------------ */
+
+/* Shapes (src/celeris/rcwa/rcwa2d.hpp:26-31). */
+#define CELERIS_SHAPE_RECT 0
+#define CELERIS_SHAPE_ELLIPSE 1
+#define CELERIS_SHAPE_CROSS 2
+#define CELERIS_SHAPE_RING 3
+
+/* One unit cell: one patterned layer between two half-spaces, normal or oblique
+ * incidence. All permittivities/indices are complex (re, im). Mirrors the
+ * arguments solve_rcwa_2d receives for a one-layer Rcwa2DStack
+ * (rcwa2d.hpp:114-124, metalens.cpp:141-147). */
+typedef struct celeris_rcwa_cell {
+    double period_x_um, period_y_um;
+    double wavelength_um, theta_rad, phi_rad;
+    double n_inc[2];      /* incident half-space index n + i k */
+    double n_sub[2];      /* substrate index */
+    double eps_pillar[2]; /* pillar permittivity eps = n^2 */
+    double eps_bg[2];     /* background permittivity */
+    double fill_x, fill_y, thickness_um;
+    double shape_param, rotation_rad;
+    int shape;            /* CELERIS_SHAPE_* */
+    int Mx, My;           /* harmonic half-counts: N = (2Mx+1)(2My+1) */
+    int grid;             /* Laurent raster size; <= 0: the reference's max(128, 8(2M+1)) (rcwa2d.cpp:337) */
+    int force_laurent;    /* 1: rasterize plain rectangles too (otherwise the analytic Li path, rcwa2d.cpp:280) */
+} celeris_rcwa_cell;
+
+/* Per-cell, per-polarization result (Rcwa2DResult, rcwa2d.hpp:84-94). */
+typedef struct celeris_rcwa_result {
+    double R, T, sum_de, de_t0, de_r0;
+    double tx0[2], ty0[2];
+} celeris_rcwa_result;
+
+/* Drop-in for celeris::solve_rcwa_2d on a one-layer stack (rcwa2d.cpp:209-488)
+ * with incident field (Ex0, Ey0). Synchronous, host buffers. */
+int celeris_solve_rcwa_2d(const celeris_rcwa_cell* cell, const double* Ex0,
+                          const double* Ey0, celeris_rcwa_result* out);
+
+/* New: batched uneven cells. Each cell is solved once (one eigensolve, one
+ * S-matrix) for BOTH the X (Ex0=1, Ey0=0) and Y (Ex0=0, Ey0=1) excitations;
+ * out receives 2*ncell results: out[2c] = X, out[2c+1] = Y. Cells are bucketed
+ * by harmonic count internally. info (ncell ints, may be NULL) receives 0 or the
+ * eigensolve failure code per cell. Synchronous, host buffers. */
+int celeris_rcwa_batch(const celeris_rcwa_cell* cells, int ncell,
+                       celeris_rcwa_result* out, int* info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CELERIS_B200_H */

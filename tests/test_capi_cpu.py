@@ -1,0 +1,58 @@
+"""CPU checks of the C ABI: the library loads, exports every declared symbol,
+and reports argument errors and the missing device with the documented codes
+(no compute is attempted without a GPU)."""
+import os
+import re
+import subprocess
+
+import pytest
+
+from celeris_b200 import capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    hdr = open(os.path.join(ROOT, "include", "celeris_b200.h")).read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    return sorted(set(re.findall(r"\b(celeris_[a-z0-9_]+)\s*\(", hdr)))
+
+
+def test_header_and_binding_agree():
+    assert declared_functions() == sorted(capi.EXPORTED)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = capi.load()
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", capi.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT (celeris_[a-z0-9_]+)$", out, flags=re.M))
+    assert set(declared_functions()) <= exported
+
+
+def test_abi_version_and_launch_counter():
+    lib = capi.load()
+    assert lib.celeris_abi_version() >= 10000
+    assert capi.launch_count() >= 0
+
+
+@pytest.mark.skipif(capi.load().celeris_available() != 0, reason="a device is present")
+def test_no_device_is_an_error_not_a_fallback():
+    import numpy as np
+
+    with pytest.raises(capi.CelerisError) as e:
+        capi.propagate_psf(np.zeros(3), np.zeros(3), np.ones(3, complex), 0, 0, 10.0, 1.0, 5, 1.0)
+    assert e.value.status == capi.ERR_NO_DEVICE
+
+
+def test_invalid_arguments_are_rejected_before_device_work():
+    import numpy as np
+
+    with pytest.raises(capi.CelerisError) as e:
+        capi.rs_field(np.zeros(3), np.zeros(3), np.ones(3, complex), 0, 0, 10.0, 1.0, 5, 1.0, form=7)
+    assert e.value.status == capi.ERR_INVALID_ARG
+    lib = capi.load()
+    st = lib.celeris_propagate_zx(None, None, None, 0, 0.0, 1.0, 1, 0.0, 1.0, 5, 1.0, None)
+    assert st == capi.ERR_INVALID_ARG
+    assert b"nx" in lib.celeris_last_error()

@@ -1,0 +1,157 @@
+"""Far-field parity on the GPU, through the C ABI.
+
+Plain FP64 form: within 1e-10 of the oracle relative to the peak |E| on the
+complex field (and on |E|^2), on the reference's golden vectors and on the full
+70,688-pillar x 161^2 metalens. Precision (FP32-compensated) form: within 1e-5
+of the FP64 result relative to the peak |E|, and its stated error (sampled FP64
+re-evaluation) is an honest upper-bound-sized figure.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from celeris_b200 import capi
+from celeris_b200.workloads import metalens_70k, metalens_785k, small_aperture
+from oracle import farfield as F
+
+pytestmark = pytest.mark.gpu
+
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "farfield_ref.npz"))
+CASES = sorted({k.split("/")[0] for k in GOLD.files})
+TOL_PLAIN = 1e-10  # relative to max |E|, complex field
+TOL_F32C = 1e-5    # relative to max |E|
+
+
+def case(name):
+    g = {k.split("/")[1]: GOLD[k] for k in GOLD.files if k.startswith(name + "/")}
+    wl, z, cx, cy, n, W, k = g["params"]
+    return g, float(wl), float(z), float(cx), float(cy), int(n), float(W), float(k)
+
+
+def rel_err(a, b):
+    return np.max(np.abs(a - b)) / np.max(np.abs(b))
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_plain_matches_golden(name):
+    g, wl, z, cx, cy, n, W, k = case(name)
+    E, I, _ = capi.rs_field(g["px"], g["py"], g["t"], cx, cy, z, k, n, W)
+    if n == 1:
+        return
+    assert rel_err(E, g["E"]) <= TOL_PLAIN
+    assert rel_err(I, g["I_ref"]) <= TOL_PLAIN
+    I2 = capi.propagate_psf(g["px"], g["py"], g["t"], cx, cy, z, k, n, W)
+    assert np.array_equal(I, I2)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_f32c_matches_golden(name):
+    g, wl, z, cx, cy, n, W, k = case(name)
+    E, I, err = capi.rs_field(g["px"], g["py"], g["t"], cx, cy, z, k, n, W, form=capi.FORM_F32C, want_err=True)
+    e = rel_err(E, g["E"])
+    assert e <= TOL_F32C
+    assert err <= TOL_F32C
+
+
+def test_ragged_sizes_and_edges():
+    for npil in (1, 2, 31, 255, 256, 257, 513, 1025):
+        a = small_aperture(npil, seed=npil)
+        for n in (2, 3, 5, 8, 33):
+            Eo = F.rs_field(a.px, a.py, a.t, 0.2, -0.1, a.focal_um, a.k, n, 2.5)
+            E, _, _ = capi.rs_field(a.px, a.py, a.t, 0.2, -0.1, a.focal_um, a.k, n, 2.5)
+            assert rel_err(E, Eo) <= TOL_PLAIN, (npil, n)
+            E32, _, _ = capi.rs_field(a.px, a.py, a.t, 0.2, -0.1, a.focal_um, a.k, n, 2.5, form=capi.FORM_F32C)
+            assert rel_err(E32, Eo) <= TOL_F32C, (npil, n)
+    # zero pillars: zeros, like the reference's CPU path (focal.cpp:216)
+    E, I, _ = capi.rs_field(np.zeros(0), np.zeros(0), np.zeros(0, complex), 0, 0, 10.0, 1.0, 6, 1.0)
+    assert np.all(E == 0) and np.all(I == 0)
+    # n == 1: the reference's step 2W/0 makes the coordinates NaN
+    E, I, _ = capi.rs_field(np.zeros(1), np.zeros(1), np.ones(1, complex), 0, 0, 10.0, 1.0, 1, 1.0)
+    assert np.isnan(I[0, 0])
+
+
+def test_metalens_70k_plain_and_f32c_full_grid():
+    ap, g = metalens_70k()
+    Eo = F.rs_field(ap.px, ap.py, ap.t, 0.0, 0.0, g.z_um, ap.k, g.n, g.half_window_um)
+    E, I, _ = capi.rs_field(ap.px, ap.py, ap.t, 0.0, 0.0, g.z_um, ap.k, g.n, g.half_window_um)
+    assert rel_err(E, Eo) <= TOL_PLAIN
+    assert rel_err(I, np.abs(Eo) ** 2) <= TOL_PLAIN
+    E32, _, err = capi.rs_field(ap.px, ap.py, ap.t, 0.0, 0.0, g.z_um, ap.k, g.n, g.half_window_um,
+                                form=capi.FORM_F32C, want_err=True)
+    e = rel_err(E32, Eo)
+    assert e <= TOL_F32C
+    assert err <= TOL_F32C
+    # the stated error is a sample of the true one: never above it (up to the
+    # FP64 form's own 1e-10-level difference from the oracle)
+    assert err <= e + 1e-9
+
+
+def test_metalens_785k_sampled_plain_and_full_f32c():
+    ap, g = metalens_785k()
+    n = g.n
+    E, _, _ = capi.rs_field(ap.px, ap.py, ap.t, 0.0, 0.0, g.z_um, ap.k, n, g.half_window_um, want_intensity=False)
+    rng = np.random.default_rng(0)
+    idx = np.unique(np.concatenate([rng.integers(0, n * n, 40), [(n // 2) * n + n // 2, 0, n * n - 1]])).astype(np.int32)
+    Eo = F.rs_pixels(ap.px, ap.py, ap.t, 0.0, 0.0, g.z_um, ap.k, n, g.half_window_um, idx)
+    peak = np.max(np.abs(E))
+    assert np.max(np.abs(E.reshape(-1)[idx] - Eo)) <= TOL_PLAIN * peak
+    E32, _, err = capi.rs_field(ap.px, ap.py, ap.t, 0.0, 0.0, g.z_um, ap.k, n, g.half_window_um,
+                                form=capi.FORM_F32C, want_intensity=False, want_err=True)
+    assert rel_err(E32, E) <= TOL_F32C
+    assert err <= TOL_F32C
+
+
+def test_zx_caustic_matches_oracle():
+    ap, g = metalens_70k()
+    sel = slice(0, None, 7)  # 10,099 pillars keep the CPU oracle quick
+    px, py, t = ap.px[sel], ap.py[sel], ap.t[sel]
+    args = (-4.0, 4.0, 41, 80.0, 120.0, 33, ap.k)
+    out = capi.propagate_zx(px, py, t, *args)
+    ref = F.rs_zx(px, py, t, *args)
+    assert rel_err(out, ref) <= TOL_PLAIN
+
+
+def test_adjoint_matches_oracle_and_transposes_forward():
+    import torch
+
+    from celeris_b200 import torch_ops as T
+
+    a = small_aperture(700, seed=9)
+    grid = T.FarFieldGrid(19, 3.0, a.focal_um, a.wavelength_um, 0.3, -0.2)
+    dev = torch.device("cuda")
+    px = torch.tensor(a.px, device=dev)
+    py = torch.tensor(a.py, device=dev)
+    rng = np.random.default_rng(3)
+    v = rng.normal(size=(19, 19)) + 1j * rng.normal(size=(19, 19))
+    out = T.rs_adjoint_dev(px, py, torch.tensor(v, device=dev), grid).cpu().numpy()
+    ref = F.rs_adjoint(a.px, a.py, grid.cx, grid.cy, grid.z, grid.k, grid.n, grid.W, v)
+    assert rel_err(out, ref) <= 1e-10
+    # <G t, v> == <t, G^H v> at the full metalens size
+    ap, g = metalens_70k()
+    grid = T.FarFieldGrid(g.n, g.half_window_um, g.z_um, ap.wavelength_um)
+    px, py = torch.tensor(ap.px, device=dev), torch.tensor(ap.py, device=dev)
+    t = torch.tensor(ap.t, device=dev)
+    v = torch.tensor(rng.normal(size=(g.n, g.n)) + 1j * rng.normal(size=(g.n, g.n)), device=dev)
+    lhs = torch.vdot(v.reshape(-1), T.rs_field_dev(px, py, t, grid).reshape(-1))
+    rhs = torch.vdot(T.rs_adjoint_dev(px, py, v, grid), t)
+    assert abs(complex(lhs - rhs)) <= 1e-11 * abs(complex(lhs))
+
+
+def test_device_api_matches_host_api_and_counts_launches():
+    import torch
+
+    from celeris_b200 import torch_ops as T
+
+    ap, g = metalens_70k()
+    dev = torch.device("cuda")
+    grid = T.FarFieldGrid(g.n, g.half_window_um, g.z_um, ap.wavelength_um)
+    before = capi.launch_count()
+    E = T.rs_field_dev(torch.tensor(ap.px, device=dev), torch.tensor(ap.py, device=dev),
+                       torch.tensor(ap.t, device=dev), grid)
+    torch.cuda.synchronize()
+    assert capi.launch_count() - before == 3
+    Eh, _, _ = capi.rs_field(ap.px, ap.py, ap.t, 0.0, 0.0, g.z_um, ap.k, g.n, g.half_window_um)
+    assert np.array_equal(E.cpu().numpy(), Eh)
+    capi.check(capi.load().celeris_sync_status(ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))

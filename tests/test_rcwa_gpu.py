@@ -1,0 +1,107 @@
+"""RCWA parity on the GPU, through the C ABI, against the oracle restatement of
+solve_rcwa_2d (rcwa2d.cpp:209-488): complex order-0 transmission within 1e-10
+relative, R and T within 1e-10, and R + T = 1 to 1e-10 for lossless cells.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from celeris_b200 import capi
+from oracle import rcwa as RO
+
+pytestmark = pytest.mark.gpu
+
+TOL_T = 1e-10
+TOL_RT = 1e-10
+
+
+def ref(cell: dict, Ex0, Ey0):
+    return RO.solve_cell(**cell, Ex0=Ex0, Ey0=Ey0)
+
+
+def check(got, want, lossless=True, tol=TOL_T):
+    for key in ("tx0", "ty0"):
+        scale = max(abs(want["tx0"]), abs(want["ty0"]))
+        assert abs(got[key] - want[key]) <= tol * scale, (key, got[key], want[key])
+    for key in ("R", "T", "de_t0", "de_r0"):
+        assert abs(got[key] - want[key]) <= TOL_RT, (key, got[key], want[key])
+    if lossless:
+        assert abs(got["R"] + got["T"] - 1.0) <= TOL_RT
+
+
+def library_cells():
+    """64 square pillars n=2.0 on n=1.46 in air, p=0.4, h=0.6, lambda=0.633,
+    widths 80..360 nm, M=3 (N=49, 2N=98)."""
+    w = np.linspace(0.080, 0.360, 64)
+    return [dict(period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46, eps_pillar=4.0, eps_bg=1.0,
+                 fill_x=float(x / 0.4), thickness_um=0.6, Mx=3) for x in w]
+
+
+def test_library_sweep_both_polarizations():
+    cells = library_cells()
+    res, info = capi.rcwa_batch([capi.rcwa_cell(**c) for c in cells])
+    assert np.all(info == 0)
+    for i, c in enumerate(cells[::7]):
+        k = 7 * i
+        check(res[2 * k], ref(c, 1.0, 0.0))
+        check(res[2 * k + 1], ref(c, 0.0, 1.0))
+
+
+MIXED = [
+    dict(name="rect_M4_global_eig", period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46, eps_pillar=4.0,
+         eps_bg=1.0, fill_x=0.55, thickness_um=0.6, Mx=4),
+    dict(name="rect_asym_M3", period_um=0.35, wavelength_um=0.532, n_inc=1.0, n_sub=1.4607, eps_pillar=2.45 ** 2,
+         eps_bg=1.0, fill_x=0.6, fill_y=0.3, thickness_um=0.6, Mx=3),
+    dict(name="circle_laurent_M3", period_um=0.4, wavelength_um=0.55, n_inc=1.0, n_sub=1.46, eps_pillar=2.2 ** 2,
+         eps_bg=1.0, fill_x=0.6, thickness_um=0.5, Mx=3, shape=capi.SHAPE_ELLIPSE),
+    dict(name="ring_laurent_M4", period_um=0.4, wavelength_um=0.6, n_inc=1.0, n_sub=1.46, eps_pillar=2.4 ** 2,
+         eps_bg=1.0, fill_x=0.8, thickness_um=0.7, Mx=4, shape=capi.SHAPE_RING, shape_param=0.5),
+    dict(name="cross_laurent_M2", period_um=0.35, wavelength_um=0.532, n_inc=1.0, n_sub=1.46, eps_pillar=6.0,
+         eps_bg=1.0, fill_x=0.8, thickness_um=0.6, Mx=2, shape=capi.SHAPE_CROSS, shape_param=0.4),
+    dict(name="square_forced_laurent_grid96", period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46,
+         eps_pillar=4.0, eps_bg=1.0, fill_x=0.5, thickness_um=0.6, Mx=3, force_laurent=1, grid=96),
+    dict(name="rotated_rect_M3", period_um=0.4, wavelength_um=0.6, n_inc=1.0, n_sub=1.46, eps_pillar=5.0,
+         eps_bg=1.0, fill_x=0.7, fill_y=0.3, thickness_um=0.6, Mx=3, rotation_rad=0.4),
+    dict(name="oblique_M3", period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46, eps_pillar=4.0,
+         eps_bg=1.0, fill_x=0.45, thickness_um=0.6, Mx=3, theta_rad=math.radians(12.0), phi_rad=math.radians(30.0)),
+    dict(name="anisotropic_orders_Mx3_My1", period_x_um=0.4, period_y_um=0.3, wavelength_um=0.633, n_inc=1.0,
+         n_sub=1.46, eps_pillar=4.0, eps_bg=1.0, fill_x=0.5, fill_y=0.6, thickness_um=0.5, Mx=3, My=1),
+    dict(name="zero_order_only_M0", period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46, eps_pillar=4.0,
+         eps_bg=1.0, fill_x=0.5, thickness_um=0.6, Mx=0),
+]
+LOSSY = dict(name="lossy_M3", period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46, eps_pillar=(2.0 + 0.05j) ** 2,
+             eps_bg=1.0, fill_x=0.5, thickness_um=0.6, Mx=3)
+
+
+@pytest.mark.parametrize("cell", MIXED + [LOSSY], ids=lambda c: c["name"])
+def test_mixed_cells_batch(cell):
+    res, info = capi.rcwa_batch([capi.rcwa_cell(**cell)])
+    assert info[0] == 0
+    lossless = cell is not LOSSY
+    check(res[0], ref(cell, 1.0, 0.0), lossless)
+    check(res[1], ref(cell, 0.0, 1.0), lossless)
+
+
+def test_uneven_batch_matches_single_cell_solves():
+    cells = [MIXED[i % len(MIXED)] for i in range(23)]
+    res, info = capi.rcwa_batch([capi.rcwa_cell(**c) for c in cells])
+    assert np.all(info == 0)
+    for i, c in enumerate(cells):
+        one = capi.solve_rcwa_2d(capi.rcwa_cell(**c), 1.0, 0.0)
+        assert abs(one["tx0"] - res[2 * i]["tx0"]) <= 1e-12 * abs(one["tx0"])
+
+
+def test_custom_excitation_single_cell():
+    c = MIXED[1]
+    Ex0, Ey0 = 0.6 + 0.2j, -0.3j
+    got = capi.solve_rcwa_2d(capi.rcwa_cell(**c), Ex0, Ey0)
+    check(got, ref(c, Ex0, Ey0))
+
+
+def test_invalid_arguments():
+    c = capi.rcwa_cell(**MIXED[0])
+    c.Mx = -1
+    with pytest.raises(capi.CelerisError) as e:
+        capi.solve_rcwa_2d(c)
+    assert e.value.status == capi.ERR_INVALID_ARG

@@ -262,6 +262,107 @@ def timed_steps(fn, steps, stream, flush):
     return ms, kms
 
 
+def rcwa_flops(cell):
+    """Algorithmic FP64 flops of one cell solve: 240 n^3 (n = 2N, diagonal-aware
+    count of the reference method: ep2 kp 4n^3, eigensolve 100n^3, interfaces
+    136n^3), plus n^3 for the Laurent inverse and the raster DFT."""
+    N = (2 * cell["Mx"] + 1) * (2 * cell.get("My", cell["Mx"]) + 1)
+    n = 2 * N
+    f = 240.0 * n ** 3
+    if cell.get("force_laurent") or cell.get("shape", 0) != 0:
+        ng = cell.get("grid") or max(128, 8 * (2 * cell["Mx"] + 1))
+        M4 = 4 * cell["Mx"] + 1
+        f += n ** 3 + 8.0 * ng * ng * M4 + 8.0 * M4 * M4 * ng
+    return f
+
+
+def _oracle_cell_time(cell):
+    import time as _t
+
+    from oracle import rcwa as RO
+
+    t0 = _t.perf_counter()
+    RO.solve_cell(**cell, Ex0=1.0, Ey0=0.0)
+    RO.solve_cell(**cell, Ex0=0.0, Ey0=1.0)  # the reference solves each polarization
+    return _t.perf_counter() - t0
+
+
+def rcwa_cpu_baseline(cells, budget_s=15.0):
+    """The oracle port (numpy/LAPACK zgeev, one BLAS thread per worker) over all
+    host cores, on a sample of the cells: per-M mean time -> whole-batch rate."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    os.environ.setdefault("MKL_NUM_THREADS", "1")
+    workers = os.cpu_count() or 1
+    byM = {}
+    for c in cells:
+        byM.setdefault(c["Mx"], []).append(c)
+    per = max(1, min(workers, 8))
+    sample = [c for M in sorted(byM) for c in byM[M][:per]]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with cf.ProcessPoolExecutor(max_workers=min(workers, len(sample)), mp_context=ctx) as ex:
+        times = list(ex.map(_oracle_cell_time, sample))
+    wall = time.perf_counter() - t0
+    tM = {}
+    for c, t in zip(sample, times):
+        tM.setdefault(c["Mx"], []).append(t)
+    total = sum(float(np.mean(tM[c["Mx"]])) for c in cells)
+    rate = len(cells) / (total / workers)
+    return {"value": rate, "unit": "cells/s", "cores": workers, "kind": "port",
+            "sample": f"{len(sample)} cells ({per} per M) solved twice (X, Y) by the numpy/LAPACK restatement of "
+                      f"solve_rcwa_2d, {workers} processes x 1 BLAS thread, {wall:.1f} s; per-M mean times "
+                      f"scaled to the whole batch"}
+
+
+def measure_rcwa(peaks, quick=False, with_cpu=True):
+    from celeris_b200 import capi
+    from celeris_b200.workloads import rcwa_library_64, rcwa_uneven_4096
+
+    out = {"metric": "RCWA cells/s (one cell = one geometry/wavelength solve, X and Y polarizations)",
+           "unit": "cells/s", "dtype": "f64 complex"}
+    p_fp64 = peaks["dfma_per_s"] * 2.0
+    lib = rcwa_library_64()
+    lc = [capi.rcwa_cell(**c) for c in lib]
+    capi.rcwa_batch(lc)
+    t = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        capi.rcwa_batch(lc)
+        t.append(time.perf_counter() - t0)
+    dt = float(np.median(t))
+    t0 = time.perf_counter()
+    for c in lc[:8]:
+        capi.solve_rcwa_2d(c)
+    per_cell = (time.perf_counter() - t0) / 8
+    fl = sum(rcwa_flops(c) for c in lib)
+    out["library_64_M3"] = {"value": 64 / dt, "ms": 1e3 * dt, "per_cell_launch_cells_s": 1.0 / per_cell,
+                            "batched_over_per_cell": per_cell / (dt / 64),
+                            "roofline": {"bound": "fp64", "achieved": fl / dt, "peak": p_fp64, "unit": "FLOP/s",
+                                         "frac": fl / dt / p_fp64}}
+    if not quick:
+        cells = rcwa_uneven_4096()
+        cc = [capi.rcwa_cell(**c) for c in cells]
+        t0 = time.perf_counter()
+        res, info = capi.rcwa_batch(cc)
+        dt2 = time.perf_counter() - t0
+        fl2 = sum(rcwa_flops(c) for c in cells)
+        out["uneven_4096_M3to7_grid256"] = {
+            "value": len(cells) / dt2, "s": dt2, "failed_cells": int(np.sum(info != 0)),
+            "max_abs_R_plus_T_minus_1": float(max(abs(r["R"] + r["T"] - 1.0) for r in res)),
+            "roofline": {"bound": "fp64", "achieved": fl2 / dt2, "peak": p_fp64, "unit": "FLOP/s",
+                         "frac": fl2 / dt2 / p_fp64}}
+        if with_cpu:
+            try:
+                out["cpu_baseline"] = rcwa_cpu_baseline(cells)
+            except Exception as exc:
+                out["cpu_baseline"] = {"unavailable": str(exc)[:200]}
+    return out
+
+
 def run_gpu(args):
     import torch
 
@@ -382,12 +483,7 @@ def run_gpu(args):
                   "api": "celeris_rs_field (C ABI, host buffers, F32C form, stated error on)",
                   "stated_error": stated, "ms_per_step": 1e3 * float(np.mean(e2e_t))}
     # ---- RCWA cells/s ------------------------------------------------------------
-    try:
-        from celeris_b200 import rcwa_bench
-
-        out["rcwa"] = rcwa_bench.measure(quick=args.quick)
-    except Exception as exc:  # RCWA kernels not built into this library yet
-        out["rcwa"] = {"unavailable": str(exc)[:200]}
+    out["rcwa"] = measure_rcwa(peaks, quick=args.quick, with_cpu=not args.no_cpu)
     # ---- CPU baseline: the reference's own far-field on this host --------------
     if not args.no_cpu:
         try:
@@ -406,6 +502,16 @@ def run_case(name, reps):
     from celeris_b200.workloads import metalens_70k, metalens_785k
 
     dev = torch.device("cuda")
+    if name.startswith("rcwa"):
+        # rcwa_M<m>_<ncell>: uneven-batch cells of one harmonic count
+        from celeris_b200.workloads import rcwa_uneven_4096
+
+        _, m, nc = name.split("_")
+        cells = [c for c in rcwa_uneven_4096() if c["Mx"] == int(m[1:])][: int(nc)]
+        for _ in range(reps):
+            capi.rcwa_batch([capi.rcwa_cell(**c) for c in cells])
+        print(json.dumps({"case": name, "reps": reps, "cells": len(cells)}))
+        return
     if name.startswith("ff785k"):
         ap, g = metalens_785k()
         n = int(name.split("_")[2]) if name.count("_") >= 2 else 256

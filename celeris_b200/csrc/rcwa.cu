@@ -688,7 +688,7 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
     int dev = 0, smem_optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const size_t kChunkBytes = (size_t)8 << 30;
+    const size_t kChunkBytes = (size_t)32 << 30;
     std::vector<celeris_rcwa_result> hres(cells.size() * nexc);
     std::vector<int> hinfo(cells.size(), 0);
     for (auto& kv : buckets) {

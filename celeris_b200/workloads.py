@@ -79,6 +79,42 @@ def metalens_785k(seed: int = 0):
     return ap, FocalGrid(1024, 20.0, 1000.0)
 
 
+def rcwa_library_64():
+    """Library sweep: square pillar n = 2.0 on n = 1.46 in air, period 400 nm,
+    height 600 nm, 64 widths uniformly 80-360 nm (fill = w / p), M = 3
+    (7 x 7 = 49 harmonics, 2N = 98), lambda 633 nm, normal incidence."""
+    w = np.linspace(0.080, 0.360, 64)
+    return [dict(period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46, eps_pillar=4.0, eps_bg=1.0,
+                 fill_x=float(x / 0.4), thickness_um=0.6, Mx=3) for x in w]
+
+
+SHAPES = ("square", "circle", "ring")
+
+
+def rcwa_uneven_4096(ncell: int = 4096, seed: int = 0, grid: int = 256):
+    """Uneven batch: shape uniform in {square, circle, ring (inner/outer 0.5)}
+    rasterised on a grid x grid permittivity raster (Laurent rule, squares
+    included), pillar index U[1.9, 2.6], fill U[0.15, 0.85], height
+    U[0.4, 0.9] um, lambda U[0.45, 0.70] um, M uniform in {3..7} ((2M+1)^2 =
+    49..225 harmonics, 2N = 98..450); substrate n = 1.46, air above and around,
+    period 400 nm."""
+    rng = np.random.default_rng(seed)
+    shape = rng.integers(0, 3, ncell)
+    npil = rng.uniform(1.9, 2.6, ncell)
+    fill = rng.uniform(0.15, 0.85, ncell)
+    h = rng.uniform(0.4, 0.9, ncell)
+    wl = rng.uniform(0.45, 0.70, ncell)
+    M = rng.integers(3, 8, ncell)
+    shape_code = {0: 0, 1: 1, 2: 3}  # celeris_b200.capi SHAPE_RECT / ELLIPSE / RING
+    cells = []
+    for i in range(ncell):
+        cells.append(dict(period_um=0.4, wavelength_um=float(wl[i]), n_inc=1.0, n_sub=1.46,
+                          eps_pillar=float(npil[i]) ** 2, eps_bg=1.0, fill_x=float(fill[i]),
+                          thickness_um=float(h[i]), Mx=int(M[i]), shape=shape_code[int(shape[i])],
+                          shape_param=0.5, grid=grid, force_laurent=1, name=SHAPES[int(shape[i])]))
+    return cells
+
+
 def small_aperture(npil: int = 257, seed: int = 1, spread_um: float = 8.0, wavelength_um: float = 0.55,
                    focal_um: float = 30.0):
     """Random pillars (ragged count) for quick parity checks."""

@@ -1,0 +1,228 @@
+// pybind11 module `_celeris`: the reference's Python surface for the hot path
+// (bindings/python/celeris_module.cpp:54-439 names and arguments), over the C++
+// host mirror in celeris.hpp. Maps are returned as numpy arrays like the
+// reference (PsfMap.intensity, MetalensDesign.fill_map).
+#include <pybind11/complex.h>
+#include <pybind11/numpy.h>
+#include <pybind11/pybind11.h>
+#include <pybind11/stl.h>
+
+#include "celeris.hpp"
+
+namespace py = pybind11;
+using namespace celeris;
+
+static py::array_t<double> to_2d(const std::vector<double>& v, int rows, int cols) {
+    py::array_t<double> a({rows, cols});
+    std::copy(v.begin(), v.end(), a.mutable_data());
+    return a;
+}
+
+static std::vector<double> from_square(const py::array_t<double>& arr, int& n) {
+    auto buf = py::array_t<double, py::array::c_style | py::array::forcecast>(arr);
+    if (buf.ndim() != 2 || buf.shape(0) != buf.shape(1))
+        throw std::runtime_error("freeform phase map must be a square 2D array");
+    n = static_cast<int>(buf.shape(0));
+    return std::vector<double>(buf.data(), buf.data() + static_cast<size_t>(n) * n);
+}
+
+PYBIND11_MODULE(_celeris, m) {
+    m.doc() = "CELERIS hot path on B200 (sm_100a kernels behind a C ABI): far-field RS sum and 2D RCWA.";
+
+    py::enum_<Pol>(m, "Pol").value("TE", Pol::TE).value("TM", Pol::TM);
+    py::enum_<MetaShape>(m, "MetaShape")
+        .value("Rectangle", MetaShape::Rectangle)
+        .value("Ellipse", MetaShape::Ellipse)
+        .value("Cross", MetaShape::Cross)
+        .value("Ring", MetaShape::Ring);
+    py::enum_<PhaseProfileKind>(m, "PhaseProfileKind")
+        .value("Focusing", PhaseProfileKind::Focusing)
+        .value("Quadratic", PhaseProfileKind::Quadratic)
+        .value("Vortex", PhaseProfileKind::Vortex)
+        .value("Deflector", PhaseProfileKind::Deflector)
+        .value("Axicon", PhaseProfileKind::Axicon)
+        .value("Freeform", PhaseProfileKind::Freeform);
+
+    py::class_<Material>(m, "Material")
+        .def_static("constant", &Material::constant, py::arg("n"), py::arg("name") = "constant")
+        .def_static("sellmeier", &Material::sellmeier, py::arg("bc_terms"), py::arg("name") = "sellmeier")
+        .def_static("tabulated", &Material::tabulated, py::arg("wavelength_um"), py::arg("n"), py::arg("k"),
+                    py::arg("name") = "tabulated")
+        .def("index", &Material::index, py::arg("wavelength_um"))
+        .def("permittivity", &Material::permittivity, py::arg("wavelength_um"))
+        .def_property_readonly("name", &Material::name)
+        .def("__repr__", [](const Material& x) { return "<celeris.Material '" + x.name() + "'>"; });
+
+    auto mats = m.def_submodule("materials", "Built-in published materials.");
+    mats.def("air", [] { return materials::air(); });
+    mats.def("bk7", [] { return materials::bk7(); });
+    mats.def("fused_silica", [] { return materials::fused_silica(); });
+    mats.def("silicon_nitride", [] { return materials::silicon_nitride(); });
+
+    py::class_<RectCell2D>(m, "RectCell2D")
+        .def(py::init([](Material pillar, Material background, double fx, double fy, double h, MetaShape shape,
+                         double param) { return RectCell2D{pillar, background, fx, fy, h, shape, param}; }),
+             py::arg("pillar"), py::arg("background"), py::arg("fill_x"), py::arg("fill_y"),
+             py::arg("thickness_um"), py::arg("shape") = MetaShape::Rectangle, py::arg("shape_param") = 0.5)
+        .def_static("homogeneous", &RectCell2D::homogeneous, py::arg("material"), py::arg("thickness_um"))
+        .def_readwrite("pillar", &RectCell2D::pillar)
+        .def_readwrite("background", &RectCell2D::background)
+        .def_readwrite("fill_x", &RectCell2D::fill_x)
+        .def_readwrite("fill_y", &RectCell2D::fill_y)
+        .def_readwrite("thickness_um", &RectCell2D::thickness_um)
+        .def_readwrite("shape", &RectCell2D::shape)
+        .def_readwrite("shape_param", &RectCell2D::shape_param)
+        .def_readwrite("rotation_rad", &RectCell2D::rotation_rad);
+
+    py::class_<Rcwa2DStack>(m, "Rcwa2DStack")
+        .def(py::init([](double px, double py_, std::vector<RectCell2D> layers) {
+                 return Rcwa2DStack{px, py_, std::move(layers)};
+             }),
+             py::arg("period_x_um"), py::arg("period_y_um"), py::arg("layers"))
+        .def_readwrite("period_x_um", &Rcwa2DStack::period_x_um)
+        .def_readwrite("period_y_um", &Rcwa2DStack::period_y_um)
+        .def_readwrite("layers", &Rcwa2DStack::layers);
+
+    py::class_<Rcwa2DResult>(m, "Rcwa2DResult")
+        .def_readonly("R", &Rcwa2DResult::R)
+        .def_readonly("T", &Rcwa2DResult::T)
+        .def_readonly("sum_de", &Rcwa2DResult::sum_de)
+        .def_readonly("de_t0", &Rcwa2DResult::de_t0)
+        .def_readonly("de_r0", &Rcwa2DResult::de_r0)
+        .def_readonly("tx0", &Rcwa2DResult::tx0)
+        .def_readonly("ty0", &Rcwa2DResult::ty0);
+
+    m.def("solve_rcwa_2d",
+          [](const Material& inc, const Rcwa2DStack& st, const Material& sub, double wl, double th, double ph,
+             cdouble ex, cdouble ey, int Mx, int My) { return solve_rcwa_2d(inc, st, sub, wl, th, ph, ex, ey, Mx, My); },
+          py::arg("incident"), py::arg("stack"), py::arg("substrate"), py::arg("wavelength_um"),
+          py::arg("theta_rad"), py::arg("phi_rad"), py::arg("Ex0"), py::arg("Ey0"), py::arg("Mx"), py::arg("My"));
+
+    py::class_<UnitCellLibrary>(m, "UnitCellLibrary")
+        .def(py::init<>())
+        .def_readwrite("period_um", &UnitCellLibrary::period_um)
+        .def_readwrite("wavelength_um", &UnitCellLibrary::wavelength_um)
+        .def_readwrite("thickness_um", &UnitCellLibrary::thickness_um)
+        .def_readwrite("fill", &UnitCellLibrary::fill)
+        .def_readwrite("phase", &UnitCellLibrary::phase)
+        .def_readwrite("amplitude", &UnitCellLibrary::amplitude)
+        .def("phase_span", &UnitCellLibrary::phase_span)
+        .def("coverage", &UnitCellLibrary::coverage)
+        .def("lookup", &UnitCellLibrary::lookup, py::arg("target_phase_rad"))
+        .def("lookup_weighted", &UnitCellLibrary::lookup_weighted, py::arg("target_phase_rad"),
+             py::arg("amplitude_weight"))
+        .def("transmission_for_fill", &UnitCellLibrary::transmission_for_fill, py::arg("fill"));
+
+    m.def("build_unit_cell_library", &build_unit_cell_library, py::arg("pillar"), py::arg("background"),
+          py::arg("incident"), py::arg("substrate"), py::arg("period_um"), py::arg("wavelength_um"),
+          py::arg("thickness_um"), py::arg("fill_min"), py::arg("fill_max"), py::arg("n_samples"), py::arg("M"),
+          py::arg("shape") = MetaShape::Rectangle, py::arg("shape_param") = 0.5);
+
+    py::class_<HeightSweepEntry>(m, "HeightSweepEntry")
+        .def_readonly("thickness_um", &HeightSweepEntry::thickness_um)
+        .def_readonly("coverage_deg", &HeightSweepEntry::coverage_deg)
+        .def_readonly("mean_transmittance", &HeightSweepEntry::mean_transmittance);
+    py::class_<HeightOptResult>(m, "HeightOptResult")
+        .def_readonly("best_thickness_um", &HeightOptResult::best_thickness_um)
+        .def_readonly("coverage_deg", &HeightOptResult::coverage_deg)
+        .def_readonly("mean_transmittance", &HeightOptResult::mean_transmittance)
+        .def_readonly("reached_target", &HeightOptResult::reached_target)
+        .def_readonly("coverage_target_deg", &HeightOptResult::coverage_target_deg)
+        .def_readonly("sweep", &HeightOptResult::sweep)
+        .def_readonly("best_library", &HeightOptResult::best_library);
+    m.def("optimize_height_for_2pi", &optimize_height_for_2pi, py::arg("pillar"), py::arg("background"),
+          py::arg("incident"), py::arg("substrate"), py::arg("period_um"), py::arg("wavelength_um"),
+          py::arg("thick_lo"), py::arg("thick_hi"), py::arg("n_heights"), py::arg("fill_min"), py::arg("fill_max"),
+          py::arg("fill_samples"), py::arg("M"), py::arg("coverage_target_deg") = 330.0,
+          py::arg("shape") = MetaShape::Rectangle, py::arg("shape_param") = 0.5);
+
+    py::class_<MetalensDesign>(m, "MetalensDesign")
+        .def_readonly("n_cells", &MetalensDesign::n_cells)
+        .def_readonly("period_um", &MetalensDesign::period_um)
+        .def_readonly("rms_phase_error_deg", &MetalensDesign::rms_phase_error_deg)
+        .def_readonly("mean_amplitude", &MetalensDesign::mean_amplitude)
+        .def_property_readonly("fill_map",
+                               [](const MetalensDesign& d) { return to_2d(d.fill_map, d.n_cells, d.n_cells); });
+
+    py::class_<PhaseProfile>(m, "PhaseProfile")
+        .def(py::init<>())
+        .def_readwrite("kind", &PhaseProfile::kind)
+        .def_readwrite("focal_length_um", &PhaseProfile::focal_length_um)
+        .def_readwrite("topological_charge", &PhaseProfile::topological_charge)
+        .def_readwrite("deflect_deg", &PhaseProfile::deflect_deg)
+        .def_readwrite("deflect_azimuth_deg", &PhaseProfile::deflect_azimuth_deg)
+        .def_readwrite("axicon_deg", &PhaseProfile::axicon_deg)
+        .def_readwrite("freeform_n", &PhaseProfile::freeform_n)
+        .def_readwrite("freeform_extent_um", &PhaseProfile::freeform_extent_um)
+        .def_property(
+            "freeform_phase",
+            [](const PhaseProfile& p) { return to_2d(p.freeform_phase_rad, p.freeform_n, p.freeform_n); },
+            [](PhaseProfile& p, const py::array_t<double>& a) {
+                int n = 0;
+                p.freeform_phase_rad = from_square(a, n);
+                p.freeform_n = n;
+            })
+        .def_static("focusing",
+                    [](double f) {
+                        PhaseProfile p;
+                        p.kind = PhaseProfileKind::Focusing;
+                        p.focal_length_um = f;
+                        return p;
+                    },
+                    py::arg("focal_length_um"));
+    m.def("phase_profile_value", &phase_profile_value, py::arg("profile"), py::arg("x"), py::arg("y"),
+          py::arg("wavelength_um"));
+    m.def("load_freeform_phase", &load_freeform_phase, py::arg("path"), py::arg("extent_um"));
+    m.def("design_metalens", py::overload_cast<const UnitCellLibrary&, double, double, double>(&design_metalens),
+          py::arg("lib"), py::arg("focal_length_um"), py::arg("diameter_um"), py::arg("amplitude_weight") = 0.25);
+    m.def("design_metalens",
+          py::overload_cast<const UnitCellLibrary&, const PhaseProfile&, double, double>(&design_metalens),
+          py::arg("lib"), py::arg("profile"), py::arg("diameter_um"), py::arg("amplitude_weight") = 0.25);
+
+    py::class_<PillarTarget>(m, "PillarTarget")
+        .def(py::init([](double wl, double ph, double w) { return PillarTarget{wl, ph, w}; }),
+             py::arg("wavelength_um"), py::arg("target_phase_rad"), py::arg("amplitude_weight") = 0.25)
+        .def_readwrite("wavelength_um", &PillarTarget::wavelength_um)
+        .def_readwrite("target_phase_rad", &PillarTarget::target_phase_rad)
+        .def_readwrite("amplitude_weight", &PillarTarget::amplitude_weight);
+    py::class_<OptimizedPillar>(m, "OptimizedPillar")
+        .def_readonly("fill", &OptimizedPillar::fill)
+        .def_readonly("thickness_um", &OptimizedPillar::thickness_um)
+        .def_readonly("achieved_phase_rad", &OptimizedPillar::achieved_phase_rad)
+        .def_readonly("achieved_amplitude", &OptimizedPillar::achieved_amplitude)
+        .def_readonly("loss", &OptimizedPillar::loss)
+        .def_readonly("iterations", &OptimizedPillar::iterations);
+    m.def("optimize_pillar", &optimize_pillar, py::arg("pillar"), py::arg("background"), py::arg("incident"),
+          py::arg("substrate"), py::arg("period_um"), py::arg("target"), py::arg("M"), py::arg("fill0"),
+          py::arg("thickness0"), py::arg("max_iters"));
+
+    py::class_<FocalAnalysis>(m, "FocalAnalysis")
+        .def_readonly("strehl", &FocalAnalysis::strehl)
+        .def_readonly("phase_strehl", &FocalAnalysis::phase_strehl)
+        .def_readonly("fwhm_um", &FocalAnalysis::fwhm_um)
+        .def_readonly("diffraction_limit_um", &FocalAnalysis::diffraction_limit_um)
+        .def_readonly("encircled_energy", &FocalAnalysis::encircled_energy);
+    m.def("analyze_focus", &analyze_focus, py::arg("lens"), py::arg("lib"), py::arg("focal_length_um"),
+          py::arg("wavelength_um"), py::arg("diameter_um"));
+
+    py::class_<PsfMap>(m, "PsfMap")
+        .def_readonly("n", &PsfMap::n)
+        .def_readonly("half_window_um", &PsfMap::half_window_um)
+        .def_property_readonly("intensity", [](const PsfMap& p) { return to_2d(p.intensity, p.n, p.n); });
+    m.def("compute_psf", &compute_psf, py::arg("lens"), py::arg("lib"), py::arg("focal_length_um"),
+          py::arg("wavelength_um"), py::arg("diameter_um"), py::arg("n"), py::arg("half_window_um"));
+    m.def("propagate_pillars", &propagate_pillars, py::arg("px"), py::arg("py"), py::arg("t"), py::arg("cx"),
+          py::arg("cy"), py::arg("z"), py::arg("wavelength_um"), py::arg("n"), py::arg("half_window_um"));
+
+    py::class_<FieldPsf>(m, "FieldPsf")
+        .def_readonly("psf", &FieldPsf::psf)
+        .def_readonly("angle_deg", &FieldPsf::angle_deg)
+        .def_readonly("cx_um", &FieldPsf::cx_um)
+        .def_readonly("rel_strehl", &FieldPsf::rel_strehl);
+    m.def("compute_psf_field", &compute_psf_field, py::arg("lens"), py::arg("lib"), py::arg("focal_length_um"),
+          py::arg("wavelength_um"), py::arg("diameter_um"), py::arg("angle_deg"), py::arg("n"),
+          py::arg("half_window_um"), py::arg("on_axis_peak") = 0.0);
+
+    m.def("cuda_available", &cuda::available);
+    m.def("cuda_device_name", &cuda::device_name);
+}

@@ -1,0 +1,207 @@
+// C++ host mirror of the reference's celeris:: interface for the hot path.
+//
+// Same names, argument meaning and error behaviour as the reference headers
+// (src/celeris/core.hpp, materials/material.hpp, rcwa/rcwa2d.hpp,
+// design/metalens.hpp, design/phase_profile.hpp, design/optimize.hpp,
+// analysis/focal.hpp, cuda/propagate.hpp), so a caller switches by relinking.
+// Every far-field and RCWA evaluation goes through the C ABI in
+// include/celeris_b200.h (sm_100a kernels); there is no CPU fallback, and a
+// non-zero status becomes std::runtime_error (std::invalid_argument where the
+// reference throws it).
+#pragma once
+
+#include <array>
+#include <complex>
+#include <functional>
+#include <string>
+#include <vector>
+
+namespace celeris {
+
+using cdouble = std::complex<double>;
+inline constexpr double pi = 3.14159265358979323846;
+enum class Pol { TE, TM };
+
+// ---- materials (material.hpp:19-66) -------------------------------------------
+class Material {
+public:
+    Material(std::function<cdouble(double)> dispersion, std::string name);
+    cdouble index(double wavelength_um) const { return dispersion_(wavelength_um); }
+    cdouble permittivity(double wavelength_um) const {
+        const cdouble n = index(wavelength_um);
+        return n * n;
+    }
+    const std::string& name() const { return name_; }
+    static Material constant(cdouble n, std::string name = "constant");
+    static Material sellmeier(std::vector<std::array<double, 2>> bc_terms, std::string name = "sellmeier");
+    static Material sellmeier_ri_formula1(std::vector<double> coeffs, std::string name = "formula1");
+    static Material tabulated(std::vector<double> wavelength_um, std::vector<double> n, std::vector<double> k,
+                              std::string name = "tabulated");
+
+private:
+    std::function<cdouble(double)> dispersion_;
+    std::string name_;
+};
+
+namespace materials {
+const Material& air();
+const Material& bk7();
+const Material& fused_silica();
+const Material& silicon_nitride();
+}  // namespace materials
+
+// ---- 2D RCWA (rcwa2d.hpp:26-124) ------------------------------------------------
+enum class MetaShape { Rectangle, Ellipse, Cross, Ring };
+
+struct RectCell2D {
+    Material pillar;
+    Material background;
+    double fill_x;
+    double fill_y;
+    double thickness_um;
+    MetaShape shape = MetaShape::Rectangle;
+    double shape_param = 0.5;
+    double rotation_rad = 0.0;
+    bool is_plain_rect() const { return shape == MetaShape::Rectangle && rotation_rad == 0.0; }
+    static RectCell2D homogeneous(Material m, double thickness_um) {
+        return RectCell2D{m, m, 1.0, 1.0, thickness_um, MetaShape::Rectangle, 0.5};
+    }
+};
+
+struct Rcwa2DStack {
+    double period_x_um;
+    double period_y_um;
+    std::vector<RectCell2D> layers;
+};
+
+struct Rcwa2DResult {
+    double R, T, sum_de, de_t0, de_r0;
+    cdouble tx0, ty0;
+};
+
+// One patterned layer between the incident and substrate half-spaces (the
+// metalens unit cell); stacks of more layers raise std::invalid_argument.
+Rcwa2DResult solve_rcwa_2d(const Material& incident, const Rcwa2DStack& stack, const Material& substrate,
+                           double wavelength_um, double theta_rad, double phi_rad, cdouble Ex0, cdouble Ey0,
+                           int Mx, int My);
+
+// New: both polarizations of many uneven cells in one batched launch sequence.
+struct CellSpec {
+    Rcwa2DStack stack;
+    Material incident;
+    Material substrate;
+    double wavelength_um;
+    int M;
+    int grid = 0;             // Laurent raster size (0: reference rule)
+    bool force_laurent = false;
+};
+std::vector<std::array<Rcwa2DResult, 2>> solve_rcwa_2d_batch(const std::vector<CellSpec>& cells);
+
+// ---- phase profiles (phase_profile.hpp) -----------------------------------------
+enum class PhaseProfileKind { Focusing, Quadratic, Vortex, Deflector, Axicon, Freeform };
+struct PhaseProfile {
+    PhaseProfileKind kind = PhaseProfileKind::Focusing;
+    double focal_length_um = 50.0;
+    int topological_charge = 1;
+    double deflect_deg = 10.0;
+    double deflect_azimuth_deg = 0.0;
+    double axicon_deg = 5.0;
+    std::vector<double> freeform_phase_rad;
+    int freeform_n = 0;
+    double freeform_extent_um = 0.0;
+};
+double phase_profile_value(const PhaseProfile& profile, double x, double y, double wavelength_um);
+PhaseProfile load_freeform_phase(const std::string& path, double extent_um);
+
+// ---- unit-cell library and lens design (metalens.hpp:21-135) ----------------------
+struct UnitCellLibrary {
+    double period_um = 0, wavelength_um = 0, thickness_um = 0;
+    std::vector<double> fill, phase, amplitude;
+    double phase_span() const;
+    double coverage() const;
+    int lookup(double target_phase_rad) const;
+    int lookup_weighted(double target_phase_rad, double amplitude_weight) const;
+    cdouble transmission_for_fill(double fill) const;
+};
+
+UnitCellLibrary build_unit_cell_library(const Material& pillar, const Material& background,
+                                        const Material& incident, const Material& substrate, double period_um,
+                                        double wavelength_um, double thickness_um, double fill_min,
+                                        double fill_max, int n_samples, int M,
+                                        MetaShape shape = MetaShape::Rectangle, double shape_param = 0.5);
+
+struct HeightSweepEntry {
+    double thickness_um, coverage_deg, mean_transmittance;
+};
+struct HeightOptResult {
+    double best_thickness_um = 0, coverage_deg = 0, mean_transmittance = 0;
+    bool reached_target = false;
+    double coverage_target_deg = 0;
+    std::vector<HeightSweepEntry> sweep;
+    UnitCellLibrary best_library;
+};
+HeightOptResult optimize_height_for_2pi(const Material& pillar, const Material& background,
+                                        const Material& incident, const Material& substrate, double period_um,
+                                        double wavelength_um, double thick_lo, double thick_hi, int n_heights,
+                                        double fill_min, double fill_max, int fill_samples, int M,
+                                        double coverage_target_deg = 330.0,
+                                        MetaShape shape = MetaShape::Rectangle, double shape_param = 0.5);
+
+struct MetalensDesign {
+    int n_cells = 0;
+    double period_um = 0;
+    std::vector<double> fill_map;
+    double rms_phase_error_deg = 0;
+    double mean_amplitude = 0;
+};
+MetalensDesign design_metalens(const UnitCellLibrary& lib, const PhaseProfile& profile, double diameter_um,
+                               double amplitude_weight = 0.25);
+MetalensDesign design_metalens(const UnitCellLibrary& lib, double focal_length_um, double diameter_um,
+                               double amplitude_weight = 0.25);
+
+// ---- reference inverse-design gradient (optimize.hpp) --------------------------------
+struct PillarTarget {
+    double wavelength_um, target_phase_rad, amplitude_weight;
+};
+struct OptimizedPillar {
+    double fill, thickness_um, achieved_phase_rad, achieved_amplitude, loss;
+    int iterations;
+};
+OptimizedPillar optimize_pillar(const Material& pillar, const Material& background, const Material& incident,
+                                const Material& substrate, double period_um, const PillarTarget& target, int M,
+                                double fill0, double thickness0, int max_iters);
+
+// ---- focal-plane analysis (focal.hpp:16-72) ------------------------------------------
+struct FocalAnalysis {
+    double strehl, phase_strehl, fwhm_um, diffraction_limit_um, encircled_energy;
+};
+struct PsfMap {
+    int n;
+    double half_window_um;
+    std::vector<double> intensity;
+};
+FocalAnalysis analyze_focus(const MetalensDesign& lens, const UnitCellLibrary& lib, double focal_length_um,
+                            double wavelength_um, double diameter_um);
+PsfMap compute_psf(const MetalensDesign& lens, const UnitCellLibrary& lib, double focal_length_um,
+                   double wavelength_um, double diameter_um, int n, double half_window_um);
+PsfMap propagate_pillars(const std::vector<double>& px, const std::vector<double>& py,
+                         const std::vector<cdouble>& t, double cx, double cy, double z, double wavelength_um,
+                         int n, double half_window_um);
+struct FieldPsf {
+    PsfMap psf;
+    double angle_deg, cx_um, rel_strehl;
+};
+FieldPsf compute_psf_field(const MetalensDesign& lens, const UnitCellLibrary& lib, double focal_length_um,
+                           double wavelength_um, double diameter_um, double angle_deg, int n,
+                           double half_window_um, double on_axis_peak = 0.0);
+
+namespace cuda {
+bool available();
+const char* device_name();
+bool propagate_psf(const double* px, const double* py, const std::complex<double>* pt, int npil, double cx,
+                   double cy, double z, double k, int n, double half_window, double* out);
+bool propagate_zx(const double* px, const double* py, const std::complex<double>* pt, int npil, double xmin,
+                  double xmax, int nx, double zmin, double zmax, int nz, double k, double* out);
+}  // namespace cuda
+
+}  // namespace celeris

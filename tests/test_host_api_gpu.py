@@ -1,0 +1,96 @@
+"""The reference's Python surface (C++ host mirror `_celeris`) on the GPU.
+
+Checks the drop-in calls against the oracle and against the reference's own
+known answers: selftest [9] (cli/selftest.cpp:376-438: library phase coverage
+> 300 deg, RMS phase error < 20 deg, FWHM within 0.1 um of lambda f / D,
+Strehl > 0.5) and the reference's compiled propagate_pillars.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import celeris_b200 as cel
+from oracle import farfield as F
+from oracle import rcwa as RO
+
+pytestmark = pytest.mark.gpu
+
+
+def test_build_unit_cell_library_matches_oracle():
+    n2 = cel.Material.constant(2.0 + 0j, "n2")
+    sub = cel.Material.constant(1.46 + 0j, "sub")
+    air = cel.materials.air()
+    lib = cel.build_unit_cell_library(n2, air, air, sub, 0.4, 0.633, 0.6, 0.2, 0.9, 16, 3)
+    assert len(lib.fill) == 16
+    for i in (0, 5, 15):
+        r = RO.solve_cell(period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46, eps_pillar=4.0, eps_bg=1.0,
+                          fill_x=lib.fill[i], thickness_um=0.6, Mx=3)
+        t = lib.amplitude[i] * np.exp(1j * lib.phase[i])
+        assert abs(t - r["tx0"]) <= 1e-10 * abs(r["tx0"])
+
+
+def test_solve_rcwa_2d_reference_signature_and_errors():
+    tio2 = cel.Material.constant(2.45 + 0j, "TiO2")
+    air = cel.materials.air()
+    fs = cel.materials.fused_silica()
+    stack = cel.Rcwa2DStack(0.35, 0.35, [cel.RectCell2D(tio2, air, 0.5, 0.5, 0.6)])
+    r = cel.solve_rcwa_2d(air, stack, fs, 0.532, 0.0, 0.0, 1.0, 0.0, 6, 6)
+    assert abs(r.sum_de - 1.0) < 1e-4  # selftest [8b] (selftest.cpp:330-345)
+    with pytest.raises(ValueError):
+        cel.solve_rcwa_2d(air, stack, fs, 0.532, 0.0, 0.0, 1.0, 0.0, -1, 6)
+    with pytest.raises(ValueError):
+        cel.solve_rcwa_2d(air, cel.Rcwa2DStack(0.35, 0.35, []), fs, 0.532, 0.0, 0.0, 1.0, 0.0, 3, 3)
+
+
+def test_selftest9_metalens_pipeline():
+    tio2 = cel.Material.constant(2.40 + 0j, "TiO2~")
+    air = cel.materials.air()
+    lib = cel.build_unit_cell_library(tio2, air, air, cel.materials.bk7(), 0.35, 0.532, 0.6, 0.08, 0.92, 18, 6)
+    assert lib.phase_span() * 180.0 / math.pi > 300.0
+    lens = cel.design_metalens(lib, 50.0, 20.0)
+    assert lens.rms_phase_error_deg < 20.0
+    foc = cel.analyze_focus(lens, lib, 50.0, 0.532, 20.0)
+    assert abs(foc.fwhm_um - foc.diffraction_limit_um) < 0.1
+    assert foc.strehl > 0.5
+    assert 0.0 < foc.encircled_energy <= 1.0
+    # compute_psf equals the oracle field of the same aperture
+    psf = cel.compute_psf(lens, lib, 50.0, 0.532, 20.0, 41, 3.0)
+    n = lens.n_cells
+    c = (n - 1) / 2.0
+    fm = lens.fill_map
+    px, py, t = [], [], []
+    for iy in range(n):
+        for ix in range(n):
+            x, y = (ix - c) * lens.period_um, (iy - c) * lens.period_um
+            if math.sqrt(x * x + y * y) > 10.0:
+                continue
+            px.append(x)
+            py.append(y)
+            t.append(lib.transmission_for_fill(fm[iy, ix]))
+    E = F.rs_field(np.array(px), np.array(py), np.array(t), 0.0, 0.0, 50.0, 2 * math.pi / 0.532, 41, 3.0)
+    I = np.abs(E) ** 2
+    assert np.max(np.abs(psf.intensity - I)) <= 1e-10 * I.max()
+
+
+def test_propagate_pillars_matches_reference_build():
+    if F.ref_lib() is None:
+        pytest.skip("oracle/_ref not built")
+    rng = np.random.default_rng(4)
+    px, py = rng.uniform(-6, 6, 500), rng.uniform(-6, 6, 500)
+    t = rng.uniform(0.6, 1, 500) * np.exp(1j * rng.uniform(0, 6.3, 500))
+    m = cel.propagate_pillars(list(px), list(py), list(t), 0.4, -0.2, 25.0, 0.55, 23, 2.0)
+    ref = F.ref_propagate_pillars(px, py, t, 0.4, -0.2, 25.0, 0.55, 23, 2.0)
+    assert np.max(np.abs(m.intensity - ref)) <= 1e-10 * ref.max()
+    empty = cel.propagate_pillars([], [], [], 0.0, 0.0, 10.0, 0.5, 5, 1.0)
+    assert np.all(empty.intensity == 0)
+
+
+def test_optimize_pillar_reduces_loss():
+    tio2 = cel.Material.constant(2.40 + 0j, "TiO2~")
+    air = cel.materials.air()
+    tgt = cel.PillarTarget(0.532, 1.0, 0.25)
+    r0 = cel.optimize_pillar(tio2, air, air, cel.materials.fused_silica(), 0.35, tgt, 3, 0.5, 0.6, 0)
+    r = cel.optimize_pillar(tio2, air, air, cel.materials.fused_silica(), 0.35, tgt, 3, 0.5, 0.6, 15)
+    assert r.loss <= r0.loss
+    assert 0.08 <= r.fill <= 0.92 and 0.2 <= r.thickness_um <= 1.0

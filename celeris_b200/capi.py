@@ -51,6 +51,7 @@ EXPORTED = [
     "celeris_propagate_zx", "celeris_rs_field", "celeris_rs_field_dev", "celeris_rs_adjoint_dev",
     "celeris_rs_check_dev", "celeris_sync_status", "celeris_solve_rcwa_2d", "celeris_rcwa_batch",
     "celeris_probe_peaks", "celeris_set_kernel_timing", "celeris_last_kernel_ms",
+    "celeris_probe_sincos",
 ]
 
 
@@ -114,6 +115,7 @@ def load(path: str = LIB_PATH):
         "celeris_rs_check_dev": (_I, [_V, _V, _V, _I, _D, _D, _D, _D, _I, _D, _V, _V, _I, _P, _V]),
         "celeris_sync_status": (_I, [_V]),
         "celeris_probe_peaks": (_I, [_P, _P, _P]),
+        "celeris_probe_sincos": (_I, [_D, _I, _P]),
         "celeris_set_kernel_timing": (_I, [_I]),
         "celeris_last_kernel_ms": (_I, [_P]),
         "celeris_solve_rcwa_2d": (_I, [ctypes.POINTER(RcwaCell), _P, _P, ctypes.POINTER(RcwaResult)]),

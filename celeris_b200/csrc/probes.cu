@@ -55,6 +55,28 @@ __global__ void probe_dfma(double a, int iters, double* sink) {
     if (s == 12345.678) sink[0] = s;
 }
 
+// Accuracy of sin.approx / cos.approx against FP64 sin/cos of the same FP32
+// argument, for arguments uniform in [-xmax, xmax]: max |error| and the mean
+// signed error (bias) of each.
+__global__ void probe_sincos_err(float xmax, int npts, double* acc) {
+    double ms = 0.0, mc = 0.0, bs = 0.0, bc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += gridDim.x * blockDim.x) {
+        const float x = xmax * (2.0f * ((float)i + 0.5f) / (float)npts - 1.0f);
+        float s, c;
+        asm("sin.approx.ftz.f32 %0, %1;" : "=f"(s) : "f"(x));
+        asm("cos.approx.ftz.f32 %0, %1;" : "=f"(c) : "f"(x));
+        const double es = (double)s - sin((double)x), ec = (double)c - cos((double)x);
+        ms = fmax(ms, fabs(es));
+        mc = fmax(mc, fabs(ec));
+        bs += es;
+        bc += ec;
+    }
+    atomicMax(reinterpret_cast<unsigned long long*>(acc + 0), (unsigned long long)__double_as_longlong(ms));
+    atomicMax(reinterpret_cast<unsigned long long*>(acc + 1), (unsigned long long)__double_as_longlong(mc));
+    atomicAdd(acc + 2, bs);
+    atomicAdd(acc + 3, bc);
+}
+
 template <typename F>
 int time_probe(F launch, double ops, double* out_per_s) {
     cudaEvent_t a, b;
@@ -74,6 +96,26 @@ int time_probe(F launch, double ops, double* out_per_s) {
 }
 
 }  // namespace
+
+// New: accuracy of the MUFU sine/cosine on [-xmax, xmax] (npts samples):
+// out = {max |sin err|, max |cos err|, mean sin err, mean cos err}.
+extern "C" int celeris_probe_sincos(double xmax, int npts, double* out) {
+    CEL_TRY(celeris_rt::require_device());
+    if (!out || npts <= 0) return celeris_rt::set_error(CELERIS_ERR_INVALID_ARG, "bad arguments");
+    double* d = nullptr;
+    CEL_CUDA(cudaMalloc(&d, 4 * sizeof(double)));
+    CEL_CUDA(cudaMemset(d, 0, 4 * sizeof(double)));
+    probe_sincos_err<<<592, 256>>>((float)xmax, npts, d);
+    celeris_rt::count_launch(1);
+    double h[4];
+    CEL_CUDA(cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost));
+    cudaFree(d);
+    out[0] = h[0];
+    out[1] = h[1];
+    out[2] = h[2] / npts;
+    out[3] = h[3] / npts;
+    return CELERIS_OK;
+}
 
 // New: measured op rates: MUFU sin.approx results/s, FP32 FMA/s, FP64 FMA/s.
 extern "C" int celeris_probe_peaks(double* mufu_per_s, double* ffma_per_s, double* dfma_per_s) {

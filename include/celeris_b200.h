@@ -69,6 +69,10 @@ int celeris_release_workspace(void);
 /* New: measured op rates of the current device (MUFU sin.approx results/s,
  * FP32 FMA/s, FP64 FMA/s) from short probe kernels; roofline denominators. */
 int celeris_probe_peaks(double* mufu_per_s, double* ffma_per_s, double* dfma_per_s);
+/* New: accuracy of the hardware sine/cosine (sin/cos.approx.f32) over
+ * [-xmax, xmax]: out[4] = {max |sin err|, max |cos err|, mean sin err,
+ * mean cos err} against FP64 sin/cos of the same FP32 arguments. */
+int celeris_probe_sincos(double xmax, int npts, double* out);
 /* New: when on != 0, the far-field entry points record CUDA events around
  * their main kernel (on the stream it is launched on). */
 int celeris_set_kernel_timing(int on);

@@ -51,7 +51,7 @@ EXPORTED = [
     "celeris_propagate_zx", "celeris_rs_field", "celeris_rs_field_dev", "celeris_rs_adjoint_dev",
     "celeris_rs_check_dev", "celeris_sync_status", "celeris_solve_rcwa_2d", "celeris_rcwa_batch",
     "celeris_probe_peaks", "celeris_set_kernel_timing", "celeris_last_kernel_ms",
-    "celeris_probe_sincos",
+    "celeris_rs_field_noalloc", "celeris_probe_sincos",
 ]
 
 
@@ -111,6 +111,7 @@ def load(path: str = LIB_PATH):
         "celeris_propagate_zx": (_I, [_P, _P, _P, _I, _D, _D, _I, _D, _D, _I, _D, _P]),
         "celeris_rs_field": (_I, [_I, _P, _P, _P, _I, _D, _D, _D, _D, _I, _D, _P, _P, _P]),
         "celeris_rs_field_dev": (_I, [_I, _V, _V, _V, _I, _D, _D, _D, _D, _I, _D, _V, _V, _V]),
+        "celeris_rs_field_noalloc": (_I, [_I, _V, _V, _V, _I, _D, _D, _D, _D, _I, _D, _V, _V, _V]),
         "celeris_rs_adjoint_dev": (_I, [_I, _V, _V, _I, _D, _D, _D, _D, _I, _D, _V, _V, _V]),
         "celeris_rs_check_dev": (_I, [_V, _V, _V, _I, _D, _D, _D, _D, _I, _D, _V, _V, _I, _P, _V]),
         "celeris_sync_status": (_I, [_V]),

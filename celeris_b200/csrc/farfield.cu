@@ -32,6 +32,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "runtime.cuh"
@@ -804,6 +805,94 @@ int ff_host(int form, const double* px, const double* py, const double* pt, int 
 
 bool valid_form(int form) { return form == CELERIS_FORM_PLAIN_F64 || form == CELERIS_FORM_F32C; }
 
+// ---- far-field without allocation ----------------------------------------------
+// Scratch for callers that cannot allocate device memory: the pillar records
+// and the per-chunk partial sums live in this fixed module-scope array, which
+// the CUDA runtime creates once per device when the library is loaded and keeps
+// until the process exits. Host code must not pass the symbol itself to a
+// kernel (on the host it names a shadow variable, not device memory); it passes
+// the device address obtained with cudaGetSymbolAddress below.
+constexpr size_t kNoAllocScratchBytes = (size_t)48 << 20;  // 48 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device; resolved on the
+// first call per device (with that device current) and cached.
+int noalloc_scratch(void** out) {
+    int dev = 0;
+    CEL_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return set_error(CELERIS_ERR_TOO_LARGE, "device index %d", dev);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) return celeris_rt::cuda_error(e, "cudaGetSymbolAddress(no-alloc scratch)");
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return CELERIS_OK;
+}
+
+int ff_run_noalloc(int form, const double* d_px, const double* d_py, const double* d_pt, int npil, const Geom& g,
+                   double k, double* d_field, double* d_int, cudaStream_t st) {
+    const long npix = (long)g.nx * g.ny;
+    if (npix <= 0) return CELERIS_OK;
+    if (npil == 0) {
+        if (d_field) CEL_CUDA(cudaMemsetAsync(d_field, 0, npix * 2 * sizeof(double), st));
+        if (d_int) CEL_CUDA(cudaMemsetAsync(d_int, 0, npix * sizeof(double), st));
+        return CELERIS_OK;
+    }
+    const bool f32 = (form == CELERIS_FORM_F32C);
+    const int ppt = f32 ? kPPT32 : kPPT64;
+    const int tile = f32 ? kTile32 : kTile64;
+    const long spr = (g.nx + ppt - 1) / ppt;
+    const int ctas_pix = (int)((spr * g.ny + kThreads - 1) / kThreads);
+    const size_t rec_bytes = celeris_rt::align256((size_t)npil * (f32 ? sizeof(float4) : sizeof(double4)));
+    const size_t part_one = (size_t)npix * sizeof(double2);
+    if (rec_bytes + part_one > kNoAllocScratchBytes)
+        return set_error(CELERIS_ERR_TOO_LARGE,
+                         "no-alloc far-field: %d pillars x %ld pixels need %zu bytes of scratch, limit %zu",
+                         npil, npix, rec_bytes + part_one, kNoAllocScratchBytes);
+    int nchunk = 1, chunk_len = npil;
+    plan_chunks(ctas_pix, npil, tile, f32 ? 3 : 2, &nchunk, &chunk_len);
+    // fewer chunks (longer ones) until the partial sums fit beside the records
+    const int ntiles = (npil + tile - 1) / tile;
+    while ((size_t)nchunk * part_one + rec_bytes > kNoAllocScratchBytes) {
+        const int tiles_per = (chunk_len / tile) + 1;
+        chunk_len = tiles_per * tile;
+        nchunk = (ntiles + tiles_per - 1) / tiles_per;
+    }
+    void* base = nullptr;
+    CEL_TRY(noalloc_scratch(&base));
+    void* rec = base;
+    double2* partial = reinterpret_cast<double2*>(static_cast<char*>(base) + rec_bytes);
+    const int pb = (npil + 255) / 256;
+    if (f32)
+        ff_pack_f32<<<pb, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil, g.ox, g.oy,
+                                        static_cast<float4*>(rec));
+    else
+        ff_pack_f64<<<pb, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil,
+                                        static_cast<double4*>(rec));
+    dim3 grid(ctas_pix, nchunk);
+    if (f32) {
+        const double il = k / (2.0 * 3.14159265358979323846);
+        const float hi = (float)il;
+        const float lo = (float)(il - (double)hi);
+        rs_f32c_kernel<<<grid, kThreads, 0, st>>>(static_cast<const float4*>(rec), npil, chunk_len, g, hi, lo,
+                                                  partial);
+    } else {
+        rs_f64_kernel<<<grid, kThreads, 0, st>>>(static_cast<const double4*>(rec), npil, chunk_len, g, k, partial);
+    }
+    rs_reduce_kernel<<<(int)((npix + 255) / 256), 256, 0, st>>>(partial, nchunk, g, k, f32 ? 1 : 0,
+                                                                 reinterpret_cast<double2*>(d_field), d_int);
+    count_launch(3);
+    CEL_CUDA(cudaGetLastError());
+    return CELERIS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -873,6 +962,17 @@ int celeris_rs_check_dev(const double* d_px, const double* d_py, const double* d
     CEL_TRY(celeris_rt::require_device());
     return ff_check(d_px, d_py, d_pt, npil, psf_geom(cx, cy, z, n, half_window), k, d_field, d_idx,
                     ns, err_out, static_cast<cudaStream_t>(stream));
+}
+
+int celeris_rs_field_noalloc(int form, const double* d_px, const double* d_py, const double* d_pt, int npil,
+                             double cx, double cy, double z, double k, int n, double half_window, double* d_field,
+                             double* d_intensity, void* stream) {
+    if (!valid_form(form)) return set_error(CELERIS_ERR_INVALID_ARG, "unknown form %d", form);
+    if (n < 0 || npil < 0) return set_error(CELERIS_ERR_INVALID_ARG, "negative size");
+    if (npil > 0 && (!d_px || !d_py || !d_pt)) return set_error(CELERIS_ERR_INVALID_ARG, "NULL pillar arrays");
+    CEL_TRY(celeris_rt::require_device());
+    return ff_run_noalloc(form, d_px, d_py, d_pt, npil, psf_geom(cx, cy, z, n, half_window), k, d_field,
+                          d_intensity, static_cast<cudaStream_t>(stream));
 }
 
 int celeris_set_kernel_timing(int on) {

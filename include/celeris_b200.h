@@ -121,6 +121,27 @@ int celeris_rs_field_dev(int form, const double* d_px, const double* d_py,
                          double z, double k, int n, double half_window,
                          double* d_field, double* d_intensity, void* stream);
 
+/* New, with no counterpart in the reference: the far-field of
+ * celeris_rs_field_dev for callers that cannot allocate device memory - for
+ * example a host whose memory pool already owns the GPU's free memory, or a
+ * latency-critical loop in which the device-wide synchronisation of
+ * cudaMalloc/cudaFree is not acceptable. It allocates nothing: its scratch (the
+ * pillar records and the per-chunk partial sums) is a fixed 48 MiB array that
+ * every GPU loading this library holds until the process exits. Inputs and
+ * outputs are the caller's device buffers, as for celeris_rs_field_dev.
+ * Limit: (16 B per pillar for CELERIS_FORM_F32C, 32 B for the plain form,
+ * rounded up to 256 B) + 16 B per focal pixel must fit in 48 MiB (the
+ * 785,456-pillar x 1024^2 metalens fits in both forms); larger requests return
+ * CELERIS_ERR_TOO_LARGE. The first call on each device looks up the array's
+ * device address (cudaGetSymbolAddress) and caches it; make that first call
+ * before any stream capture begins. All calls share the one array: calls whose
+ * kernels overlap on the GPU (different streams, or different host threads
+ * without ordering) race on it and must be serialised by the caller. */
+int celeris_rs_field_noalloc(int form, const double* d_px, const double* d_py,
+                             const double* d_pt, int npil, double cx, double cy,
+                             double z, double k, int n, double half_window,
+                             double* d_field, double* d_intensity, void* stream);
+
 /* New: adjoint (conjugate-transpose, pixel -> pillar) RS sum on the same grid:
  *   d_out[j] = sum_p conj(g_pj) * d_v[p],   g_pj = exp(i k R_pj) / R_pj.
  * d_v: n*n complex, d_out: npil complex. This is the vector-Jacobian product of

@@ -209,13 +209,47 @@ __device__ void blk_gemm(int m, int n, int k, cplx alpha, const cplx* A, int lda
     __syncthreads();
 }
 
+// ---- rank-1 update ----------------------------------------------------------------------
+// A[i][j] -= x[i] * y[j] (or * conj(y[j])) for i < rows, j < cols. Each thread
+// first loads kU elements of A, then updates and stores them, so kU loads per
+// thread are in flight at once (a load-use-store loop would wait on every load,
+// the compiler being unable to move loads past stores to the same array).
+// x and y are shared-memory vectors.
+constexpr int kU = 8;
+template <bool CONJ_Y>
+__device__ __forceinline__ void blk_rank1(int rows, int cols, cplx* A, int lda, const cplx* x, const cplx* y) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int total = rows * cols;
+    for (int e0 = tid; e0 < total; e0 += kU * nt) {
+        cplx v[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int e = e0 + u * nt;
+            if (e < total) v[u] = A[(size_t)(e / cols) * lda + (e % cols)];
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int e = e0 + u * nt;
+            if (e < total) {
+                const int i = e / cols, j = e % cols;
+                const cplx yy = CONJ_Y ? cconj(y[j]) : y[j];
+                A[(size_t)i * lda + j] = cfms(x[i], yy, v[u]);
+            }
+        }
+    }
+}
+
 // ---- LU ------------------------------------------------------------------------------
 // In-place LU with partial pivoting of the n x n matrix A. piv[k] = row swapped
 // with k at step k. Returns 0, or k+1 for the first exactly-zero pivot (the
-// factorization continues, like zgetrf).
-__device__ int blk_lu(int n, cplx* A, int lda, int* piv, RedScratch* rs) {
+// factorization continues, like zgetrf). stage: shared scratch of 2n complex
+// (the pivot column and row of each step, so the trailing update reads only
+// its own element from A).
+__device__ int blk_lu(int n, cplx* A, int lda, int* piv, RedScratch* rs, cplx* stage) {
     const int tid = threadIdx.x, nt = blockDim.x;
     int info = 0;
+    cplx* colk = stage;
+    cplx* rowk = stage + n;
     __syncthreads();
     for (int k = 0; k < n; ++k) {
         double best = -1.0;
@@ -244,21 +278,27 @@ __device__ int blk_lu(int n, cplx* A, int lda, int* piv, RedScratch* rs) {
             continue;
         }
         const cplx inv = cinv(akk);
-        for (int i = k + 1 + tid; i < n; i += nt) A[(size_t)i * lda + k] = cmul(A[(size_t)i * lda + k], inv);
-        __syncthreads();
         const int w = n - k - 1;
-        for (int e = tid; e < w * w; e += nt) {
-            const int i = k + 1 + e / w, j = k + 1 + e % w;
-            A[(size_t)i * lda + j] = cfms(A[(size_t)i * lda + k], A[(size_t)k * lda + j], A[(size_t)i * lda + j]);
+        for (int i = tid; i < w; i += nt) {
+            const cplx l = cmul(A[(size_t)(k + 1 + i) * lda + k], inv);
+            A[(size_t)(k + 1 + i) * lda + k] = l;
+            colk[i] = l;
+            rowk[i] = A[(size_t)k * lda + k + 1 + i];
         }
+        __syncthreads();
+        blk_rank1<false>(w, w, A + (size_t)(k + 1) * lda + k + 1, lda, colk, rowk);
         __syncthreads();
     }
     return info;
 }
 
 // B (n x nrhs, row-major, ldb) <- A^{-1} B using the factors of blk_lu.
-__device__ void blk_lu_solve(int n, const cplx* LU, int lda, const int* piv, int nrhs, cplx* B, int ldb) {
+// stage: shared scratch of n + nrhs complex.
+__device__ void blk_lu_solve(int n, const cplx* LU, int lda, const int* piv, int nrhs, cplx* B, int ldb,
+                             cplx* stage) {
     const int tid = threadIdx.x, nt = blockDim.x;
+    cplx* lcol = stage;
+    cplx* brow = stage + n;
     __syncthreads();
     // row interchanges in factorization order
     for (int k = 0; k < n; ++k) {
@@ -274,22 +314,49 @@ __device__ void blk_lu_solve(int n, const cplx* LU, int lda, const int* piv, int
     // forward: unit lower L
     for (int j = 0; j < n - 1; ++j) {
         const int w = n - j - 1;
-        for (int e = tid; e < w * nrhs; e += nt) {
-            const int i = j + 1 + e / nrhs, r = e % nrhs;
-            B[(size_t)i * ldb + r] = cfms(LU[(size_t)i * lda + j], B[(size_t)j * ldb + r], B[(size_t)i * ldb + r]);
-        }
+        for (int i = tid; i < w; i += nt) lcol[i] = LU[(size_t)(j + 1 + i) * lda + j];
+        for (int r = tid; r < nrhs; r += nt) brow[r] = B[(size_t)j * ldb + r];
+        __syncthreads();
+        blk_rank1<false>(w, nrhs, B + (size_t)(j + 1) * ldb, ldb, lcol, brow);
         __syncthreads();
     }
     // backward: U
     for (int j = n - 1; j >= 0; --j) {
         const cplx inv = cinv(LU[(size_t)j * lda + j]);
-        for (int r = tid; r < nrhs; r += nt) B[(size_t)j * ldb + r] = cmul(B[(size_t)j * ldb + r], inv);
-        __syncthreads();
-        for (int e = tid; e < j * nrhs; e += nt) {
-            const int i = e / nrhs, r = e % nrhs;
-            B[(size_t)i * ldb + r] = cfms(LU[(size_t)i * lda + j], B[(size_t)j * ldb + r], B[(size_t)i * ldb + r]);
+        for (int r = tid; r < nrhs; r += nt) {
+            const cplx x = cmul(B[(size_t)j * ldb + r], inv);
+            B[(size_t)j * ldb + r] = x;
+            brow[r] = x;
         }
+        for (int i = tid; i < j; i += nt) lcol[i] = LU[(size_t)i * lda + j];
         __syncthreads();
+        blk_rank1<false>(j, nrhs, B, ldb, lcol, brow);
+        __syncthreads();
+    }
+}
+
+// w[i] = beta * sum_j A[i][j] v[j] for i < rows, j < cols: one warp per group
+// of 4 rows, lanes over j, so every lane has 4 row loads in flight.
+__device__ __forceinline__ void blk_matvec_rows(int rows, int cols, const cplx* A, int lda, const cplx* v, cplx* w,
+                                                double beta, int warp, int lane, int nwarp) {
+    for (int i0 = 4 * warp; i0 < rows; i0 += 4 * nwarp) {
+        cplx acc[4] = {C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0)};
+        for (int j = lane; j < cols; j += 32) {
+            const cplx vj = v[j];
+            cplx h[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) h[r] = (i0 + r < rows) ? A[(size_t)(i0 + r) * lda + j] : C(0.0, 0.0);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[r] = cfma(h[r], vj, acc[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            for (int o = 16; o > 0; o >>= 1) {
+                acc[r].x += __shfl_down_sync(0xffffffffu, acc[r].x, o);
+                acc[r].y += __shfl_down_sync(0xffffffffu, acc[r].y, o);
+            }
+            if (lane == 0 && i0 + r < rows) w[i0 + r] = cscale(acc[r], beta);
+        }
     }
 }
 
@@ -326,69 +393,55 @@ __device__ void blk_hessenberg(int n, cplx* H, int ldh, cplx* Z, int ldz, cplx* 
         __syncthreads();
         // left: rows k+1.., columns k+1..n-1 (column k becomes alpha e1)
         for (int j = k + 1 + tid; j < n; j += nt) {
-            cplx acc = C(0.0, 0.0);
-            for (int i = 0; i < m; ++i) acc = cfma(cconj(v[i]), H[(size_t)(k + 1 + i) * ldh + j], acc);
-            w[j] = cscale(acc, beta);
+            const cplx* col = H + (size_t)(k + 1) * ldh + j;
+            cplx acc[4] = {C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0)};
+            int i = 0;
+            for (; i + 8 <= m; i += 8) {  // 8 loads in flight
+                cplx h[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) h[u] = col[(size_t)(i + u) * ldh];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) acc[u & 3] = cfma(cconj(v[i + u]), h[u], acc[u & 3]);
+            }
+            for (; i < m; ++i) acc[0] = cfma(cconj(v[i]), col[(size_t)i * ldh], acc[0]);
+            w[j] = cscale(cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3])), beta);
         }
         __syncthreads();
-        for (int e = tid; e < m * (n - k - 1); e += nt) {
-            const int i = e / (n - k - 1), j = k + 1 + e % (n - k - 1);
-            H[(size_t)(k + 1 + i) * ldh + j] = cfms(v[i], w[j], H[(size_t)(k + 1 + i) * ldh + j]);
-        }
+        blk_rank1<false>(m, n - k - 1, H + (size_t)(k + 1) * ldh + k + 1, ldh, v, w + k + 1);
         for (int i = tid; i < m; i += nt) H[(size_t)(k + 1 + i) * ldh + k] = (i == 0) ? alpha : C(0.0, 0.0);
         __syncthreads();
         // right: all rows, columns k+1..n-1: H <- H (I - beta v v^H)
-        for (int i = warp; i < n; i += nwarp) {
-            cplx acc = C(0.0, 0.0);
-            for (int j = lane; j < m; j += 32) acc = cfma(H[(size_t)i * ldh + k + 1 + j], v[j], acc);
-            for (int o = 16; o > 0; o >>= 1) {
-                acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
-                acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
-            }
-            if (lane == 0) w[i] = cscale(acc, beta);
-        }
+        blk_matvec_rows(n, m, H + k + 1, ldh, v, w, beta, warp, lane, nwarp);
         __syncthreads();
-        for (int e = tid; e < n * m; e += nt) {
-            const int i = e / m, j = e % m;
-            H[(size_t)i * ldh + k + 1 + j] = cfms(w[i], cconj(v[j]), H[(size_t)i * ldh + k + 1 + j]);
-        }
+        blk_rank1<true>(n, m, H + k + 1, ldh, w, v);
         __syncthreads();
         // Z <- Z (I - beta v v^H)
-        for (int i = warp; i < n; i += nwarp) {
-            cplx acc = C(0.0, 0.0);
-            for (int j = lane; j < m; j += 32) acc = cfma(Z[(size_t)i * ldz + k + 1 + j], v[j], acc);
-            for (int o = 16; o > 0; o >>= 1) {
-                acc.x += __shfl_down_sync(0xffffffffu, acc.x, o);
-                acc.y += __shfl_down_sync(0xffffffffu, acc.y, o);
-            }
-            if (lane == 0) w[i] = cscale(acc, beta);
-        }
+        blk_matvec_rows(n, m, Z + k + 1, ldz, v, w, beta, warp, lane, nwarp);
         __syncthreads();
-        for (int e = tid; e < n * m; e += nt) {
-            const int i = e / m, j = e % m;
-            Z[(size_t)i * ldz + k + 1 + j] = cfms(w[i], cconj(v[j]), Z[(size_t)i * ldz + k + 1 + j]);
-        }
+        blk_rank1<true>(n, m, Z + k + 1, ldz, w, v);
         __syncthreads();
     }
 }
 
 // ---- complex Schur by shifted QR ------------------------------------------------------
 // Givens G = [[c, s], [-conj(s), c]] with G [a; b] = [r; 0], c real.
+// c = |a| / r, s = a conj(b) / (|a| r), r = sqrt(|a|^2 + |b|^2), formed with
+// two reciprocal square roots (entries here are far from over/underflow).
 __device__ __forceinline__ void givens(cplx a, cplx b, double& c, cplx& s) {
-    const double aa = cabs(a), ab = cabs(b);
-    if (ab == 0.0) {
+    const double na = cnorm2(a), nb = cnorm2(b);
+    if (nb == 0.0) {
         c = 1.0;
         s = C(0.0, 0.0);
         return;
     }
-    if (aa == 0.0) {
+    if (na == 0.0) {
         c = 0.0;
-        s = cscale(cconj(b), 1.0 / ab);
+        s = cscale(cconj(b), rsqrt(nb));
         return;
     }
-    const double r = hypot(aa, ab);
-    c = aa / r;
-    s = cscale(cmul(cscale(a, 1.0 / aa), cconj(b)), 1.0 / r);
+    const double ia = rsqrt(na), ir = rsqrt(na + nb);
+    c = na * ia * ir;
+    s = cscale(cmul(a, cconj(b)), ia * ir);
 }
 
 // eigenvalue of [[a, b], [c, d]] closest to d
@@ -400,23 +453,79 @@ __device__ __forceinline__ cplx wilkinson(cplx a, cplx b, cplx c, cplx d) {
     return cabs1(csub(e1, d)) <= cabs1(csub(e2, d)) ? e1 : e2;
 }
 
+constexpr int QW = 16;  // bulge-chase window (rows/columns)
+constexpr int kMaxN = 1024;
+
 struct SchurShared {
-    int lo, hi, done, info;
-    double c[2];
-    cplx s[2];
+    cplx B[QW][QW + 1];  // the window block
+    double c[QW];        // rotations of the current window
+    cplx s[QW];
+    unsigned char flag[kMaxN];
+    int lo, hi, done, info, nsweep;
+    cplx shift;
 };
+
+// Apply the window's row rotations (rows ws+R0+t, ws+R0+t+1, t < nr) to the
+// column segment H[ws : ws+w, j] held in registers; rotation t is
+// [[c, s], [-conj(s), c]].
+template <int R0>
+__device__ __forceinline__ void rot_rows_col(cplx* col0, int ld, int w, int nr, const SchurShared* sh) {
+    cplx v[QW];
+#pragma unroll
+    for (int q = 0; q < QW; ++q)
+        if (q < w) v[q] = col0[(size_t)q * ld];
+#pragma unroll
+    for (int t = 0; t + R0 + 1 < QW; ++t) {
+        if (t < nr) {
+            const double c = sh->c[t];
+            const cplx s = sh->s[t];
+            const cplx x = v[R0 + t], y = v[R0 + t + 1];
+            v[R0 + t] = cfma(s, y, cscale(x, c));
+            v[R0 + t + 1] = cfma(cneg(cconj(s)), x, cscale(y, c));
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < QW; ++q)
+        if (q < w) col0[(size_t)q * ld] = v[q];
+}
+
+// Apply the window's column rotations (columns ws+R0+t, ws+R0+t+1) to the row
+// segment row0[0 : w] (one row of H above the window, or of Z): new col k =
+// c h_k + conj(s) h_{k+1}, new col k+1 = -s h_k + c h_{k+1}.
+template <int R0>
+__device__ __forceinline__ void rot_cols_row(cplx* row0, int w, int nr, const SchurShared* sh) {
+    cplx v[QW];
+#pragma unroll
+    for (int q = 0; q < QW; ++q)
+        if (q < w) v[q] = row0[q];
+#pragma unroll
+    for (int t = 0; t + R0 + 1 < QW; ++t) {
+        if (t < nr) {
+            const double c = sh->c[t];
+            const cplx s = sh->s[t];
+            const cplx x = v[R0 + t], y = v[R0 + t + 1];
+            v[R0 + t] = cfma(cconj(s), y, cscale(x, c));
+            v[R0 + t + 1] = cfma(cneg(s), x, cscale(y, c));
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < QW; ++q)
+        if (q < w) row0[q] = v[q];
+}
 
 // T <- Q^H H Q upper triangular, Z <- Z Q. Returns info (0, or hi+1 when the
 // sweep cap ran out with rows 0..hi unconverged).
 //
-// Each sweep chases one bulge down [lo, hi]. Thread 0 owns the near-diagonal
-// "corner" of every step k (column k-1 of rows k, k+1; the 2x2 block at
-// (k, k); row k+2 at columns k, k+1) and computes rotation k+1 from it, while
-// the other threads apply rotation k to the far parts (rows k, k+1 right of
-// column k+1; columns k, k+1 above row k; Z). The write sets are disjoint and
-// rotation k+1 depends only on the corner, so each step needs one barrier.
+// Each sweep chases one bulge down the active window [lo, hi] in blocks of at
+// most QW rows/columns: warp 0 performs the rotations of a block on a shared
+// copy of H[ws:we, ws:we] (warp-synchronous), recording them; then the whole
+// CTA applies the recorded rotations to the rest of rows ws..we-1 (columns
+// >= we), to the rest of columns ws..we-1 (rows < ws) and to Z, each thread
+// owning one column or row segment in registers. Consecutive blocks overlap by
+// the bulge column, so every entry a rotation reads is current when it is read.
 __device__ int blk_schur(int n, cplx* H, int ldh, cplx* Z, int ldz, SchurShared* sh, int max_sweeps_per_row) {
     const int tid = threadIdx.x, nt = blockDim.x;
+    const int warp = tid >> 5, lane = tid & 31;
     const double eps = 2.220446049250313e-16;
     const double smallnum = 2.2250738585072014e-308 * (n / eps);
     if (tid == 0) {
@@ -424,35 +533,30 @@ __device__ int blk_schur(int n, cplx* H, int ldh, cplx* Z, int ldz, SchurShared*
         sh->lo = 0;
         sh->done = 0;
         sh->info = 0;
+        sh->nsweep = 0;
     }
     __syncthreads();
-    int iter_row = 0;
+    int iter_row = 0;  // used by thread 0 only
     const long max_total = (long)max_sweeps_per_row * n;
     long total = 0;
     while (true) {
+        // negligible subdiagonals of [1, hi], in parallel
+        const int hi0 = sh->hi;
+        for (int i = 1 + tid; i <= hi0; i += nt) {
+            const double tst = cabs1(H[(size_t)(i - 1) * ldh + i - 1]) + cabs1(H[(size_t)i * ldh + i]);
+            sh->flag[i] = cabs1(H[(size_t)i * ldh + i - 1]) <= fmax(eps * tst, smallnum) ? 1 : 0;
+        }
+        __syncthreads();
         if (tid == 0) {
-            int hi = sh->hi;
-            while (hi > 0) {
-                const cplx sub = H[(size_t)hi * ldh + hi - 1];
-                const double tst = cabs1(H[(size_t)(hi - 1) * ldh + hi - 1]) + cabs1(H[(size_t)hi * ldh + hi]);
-                if (cabs1(sub) <= fmax(eps * tst, smallnum)) {
-                    H[(size_t)hi * ldh + hi - 1] = C(0.0, 0.0);
-                    --hi;
-                    iter_row = 0;
-                } else {
-                    break;
-                }
+            int hi = hi0;
+            while (hi > 0 && sh->flag[hi]) {
+                H[(size_t)hi * ldh + hi - 1] = C(0.0, 0.0);
+                --hi;
+                iter_row = 0;
             }
             int lo = hi;
-            while (lo > 0) {
-                const cplx sub = H[(size_t)lo * ldh + lo - 1];
-                const double tst = cabs1(H[(size_t)(lo - 1) * ldh + lo - 1]) + cabs1(H[(size_t)lo * ldh + lo]);
-                if (cabs1(sub) <= fmax(eps * tst, smallnum)) {
-                    H[(size_t)lo * ldh + lo - 1] = C(0.0, 0.0);
-                    break;
-                }
-                --lo;
-            }
+            while (lo > 0 && !sh->flag[lo]) --lo;
+            if (lo > 0) H[(size_t)lo * ldh + lo - 1] = C(0.0, 0.0);
             sh->hi = hi;
             sh->lo = lo;
             if (hi <= 0) {
@@ -463,76 +567,101 @@ __device__ int blk_schur(int n, cplx* H, int ldh, cplx* Z, int ldz, SchurShared*
             } else {
                 ++iter_row;
                 ++total;
-                cplx shift;
+                sh->nsweep = (int)total;
                 if (iter_row == 10 || iter_row == 30) {  // exceptional shift
                     const double e = fabs(H[(size_t)hi * ldh + hi - 1].x) +
                                      (hi >= 2 ? fabs(H[(size_t)(hi - 1) * ldh + hi - 2].x) : 0.0);
-                    shift = cadd(H[(size_t)hi * ldh + hi], C(e, 0.0));
+                    sh->shift = cadd(H[(size_t)hi * ldh + hi], C(e, 0.0));
                 } else {
-                    shift = wilkinson(H[(size_t)(hi - 1) * ldh + hi - 1], H[(size_t)(hi - 1) * ldh + hi],
-                                      H[(size_t)hi * ldh + hi - 1], H[(size_t)hi * ldh + hi]);
+                    sh->shift = wilkinson(H[(size_t)(hi - 1) * ldh + hi - 1], H[(size_t)(hi - 1) * ldh + hi],
+                                          H[(size_t)hi * ldh + hi - 1], H[(size_t)hi * ldh + hi]);
                 }
-                double c;
-                cplx s;
-                givens(csub(H[(size_t)lo * ldh + lo], shift), H[(size_t)(lo + 1) * ldh + lo], c, s);
-                sh->c[lo & 1] = c;
-                sh->s[lo & 1] = s;
             }
         }
         __syncthreads();
         if (sh->done) break;
         const int lo = sh->lo, hi = sh->hi;
-        for (int k = lo; k < hi; ++k) {
-            const double c = sh->c[k & 1];
-            const cplx s = sh->s[k & 1];
-            const cplx ms = cneg(cconj(s));  // row rotation, second row: -conj(s) x + c y
-            const cplx cs = cconj(s), ns = cneg(s);  // column rotation
-            if (tid == 0) {
-                // corner: bulge column k-1, 2x2 block, row k+2
-                if (k > lo) {
-                    const cplx a = H[(size_t)k * ldh + k - 1], b = H[(size_t)(k + 1) * ldh + k - 1];
-                    H[(size_t)k * ldh + k - 1] = cfma(s, b, cscale(a, c));
-                    H[(size_t)(k + 1) * ldh + k - 1] = C(0.0, 0.0);
-                }
-                cplx h00 = H[(size_t)k * ldh + k], h01 = H[(size_t)k * ldh + k + 1];
-                cplx h10 = H[(size_t)(k + 1) * ldh + k], h11 = H[(size_t)(k + 1) * ldh + k + 1];
-                const cplx r00 = cfma(s, h10, cscale(h00, c)), r01 = cfma(s, h11, cscale(h01, c));
-                const cplx r10 = cfma(ms, h00, cscale(h10, c)), r11 = cfma(ms, h01, cscale(h11, c));
-                H[(size_t)k * ldh + k] = cfma(cs, r01, cscale(r00, c));
-                H[(size_t)k * ldh + k + 1] = cfma(ns, r00, cscale(r01, c));
-                H[(size_t)(k + 1) * ldh + k] = cfma(cs, r11, cscale(r10, c));
-                H[(size_t)(k + 1) * ldh + k + 1] = cfma(ns, r10, cscale(r11, c));
-                if (k + 2 <= hi) {
-                    const cplx x = H[(size_t)(k + 2) * ldh + k], y = H[(size_t)(k + 2) * ldh + k + 1];
-                    H[(size_t)(k + 2) * ldh + k] = cfma(cs, y, cscale(x, c));
-                    H[(size_t)(k + 2) * ldh + k + 1] = cfma(ns, x, cscale(y, c));
-                }
-                if (k + 1 < hi) {  // next rotation annihilates the new bulge H[k+2][k]
-                    double c2;
-                    cplx s2;
-                    givens(H[(size_t)(k + 1) * ldh + k], H[(size_t)(k + 2) * ldh + k], c2, s2);
-                    sh->c[(k + 1) & 1] = c2;
-                    sh->s[(k + 1) & 1] = s2;
-                }
-            }
-            // far part of the row rotation: rows k, k+1, columns k+2..n-1
-            for (int j = k + 2 + tid; j < n; j += nt) {
-                const cplx x = H[(size_t)k * ldh + j], y = H[(size_t)(k + 1) * ldh + j];
-                H[(size_t)k * ldh + j] = cfma(s, y, cscale(x, c));
-                H[(size_t)(k + 1) * ldh + j] = cfma(ms, x, cscale(y, c));
-            }
-            // far part of the column rotation: rows 0..k-1, columns k, k+1
-            for (int i = tid; i < k; i += nt) {
-                const cplx x = H[(size_t)i * ldh + k], y = H[(size_t)i * ldh + k + 1];
-                H[(size_t)i * ldh + k] = cfma(cs, y, cscale(x, c));
-                H[(size_t)i * ldh + k + 1] = cfma(ns, x, cscale(y, c));
-            }
-            for (int i = tid; i < n; i += nt) {
-                const cplx x = Z[(size_t)i * ldz + k], y = Z[(size_t)i * ldz + k + 1];
-                Z[(size_t)i * ldz + k] = cfma(cs, y, cscale(x, c));
-                Z[(size_t)i * ldz + k + 1] = cfma(ns, x, cscale(y, c));
+        const cplx shift = sh->shift;
+        int k_next = lo;
+        bool first = true;
+        while (k_next < hi) {
+            const int ws = first ? lo : k_next - 1;
+            const int we = min(ws + QW, hi + 1);
+            const int k_last = (we == hi + 1) ? hi - 1 : we - 3;
+            const int w = we - ws;
+            const int r0 = k_next - ws;  // 0 for the first block of a sweep, else 1
+            const int nr = k_last - k_next + 1;
+            for (int e = tid; e < w * w; e += nt) {
+                const int r = e / w, cc = e % w;
+                sh->B[r][cc] = H[(size_t)(ws + r) * ldh + ws + cc];
             }
             __syncthreads();
+            if (warp == 0) {
+                for (int k = k_next; k <= k_last; ++k) {
+                    const int kk = k - ws;
+                    const bool start = first && k == lo;
+                    cplx a, b;
+                    if (start) {
+                        a = csub(sh->B[kk][kk], shift);
+                        b = sh->B[kk + 1][kk];
+                    } else {
+                        a = sh->B[kk][kk - 1];
+                        b = sh->B[kk + 1][kk - 1];
+                    }
+                    double c;
+                    cplx s;
+                    givens(a, b, c, s);
+                    const cplx ms = cneg(cconj(s)), cs = cconj(s), ns = cneg(s);
+                    const int jlo = start ? kk : kk - 1;
+                    for (int col = jlo + lane; col < w; col += 32) {
+                        const cplx x = sh->B[kk][col], y = sh->B[kk + 1][col];
+                        sh->B[kk][col] = cfma(s, y, cscale(x, c));
+                        sh->B[kk + 1][col] = cfma(ms, x, cscale(y, c));
+                    }
+                    __syncwarp();
+                    const int rmax = min(kk + 2, hi - ws);
+                    for (int row = lane; row <= rmax; row += 32) {
+                        const cplx x = sh->B[row][kk], y = sh->B[row][kk + 1];
+                        sh->B[row][kk] = cfma(cs, y, cscale(x, c));
+                        sh->B[row][kk + 1] = cfma(ns, x, cscale(y, c));
+                    }
+                    __syncwarp();
+                    if (lane == 0) {
+                        if (!start) sh->B[kk + 1][kk - 1] = C(0.0, 0.0);
+                        sh->c[k - k_next] = c;
+                        sh->s[k - k_next] = s;
+                    }
+                    __syncwarp();
+                }
+            }
+            __syncthreads();
+            for (int e = tid; e < w * w; e += nt) {
+                const int r = e / w, cc = e % w;
+                H[(size_t)(ws + r) * ldh + ws + cc] = sh->B[r][cc];
+            }
+            // deferred parts: rows ws..we-1 right of the block, columns ws..we-1
+            // above the block, and Z
+            const int nright = n - we, nabove = ws;
+            const int jobs = nright + nabove + n;
+            for (int e = tid; e < jobs; e += nt) {
+                if (e < nright) {
+                    cplx* col0 = H + (size_t)ws * ldh + we + e;
+                    if (r0 == 0)
+                        rot_rows_col<0>(col0, ldh, w, nr, sh);
+                    else
+                        rot_rows_col<1>(col0, ldh, w, nr, sh);
+                } else {
+                    cplx* row0 = (e < nright + nabove) ? H + (size_t)(e - nright) * ldh + ws
+                                                       : Z + (size_t)(e - nright - nabove) * ldz + ws;
+                    if (r0 == 0)
+                        rot_cols_row<0>(row0, w, nr, sh);
+                    else
+                        rot_cols_row<1>(row0, w, nr, sh);
+                }
+            }
+            __syncthreads();
+            k_next = k_last + 1;
+            first = false;
         }
     }
     const int info = sh->info;

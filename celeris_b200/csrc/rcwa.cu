@@ -24,6 +24,8 @@
 #include <math.h>
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <tuple>
@@ -69,6 +71,7 @@ struct Bucket {
     size_t s_nn, s_ns, s_NN, s_n;
     const cplx* phx;  // [(4Mx+1) x ng] centred DFT phase table (x)
     const cplx* phy;  // [(4My+1) x ng]
+    long long* dbg;   // optional per-cell stage clocks (CELERIS_RCWA_STAGE_CLOCKS=1), else NULL
 };
 
 __device__ __forceinline__ cplx* at(cplx* base, size_t stride, int c) { return base + stride * c; }
@@ -122,6 +125,7 @@ __global__ void __launch_bounds__(kRT) rcwa_fourier_rect(Bucket b) {
     cplx* ax = hx + nx * nx;
     cplx* hy = ax + nx * nx;
     cplx* ay = hy + ny * ny;
+    cplx* stg = ay + ny * ny;  // LU staging: 2 * max(nx, ny)
     const int tid = threadIdx.x, nt = blockDim.x;
     const cplx ep = c.eps_p, eb = c.eps_b;
     const cplx ipe = cinv(ep), ibe = cinv(eb);
@@ -142,10 +146,10 @@ __global__ void __launch_bounds__(kRT) rcwa_fourier_rect(Bucket b) {
         ay[e] = C(a == bb ? 1.0 : 0.0, 0.0);
     }
     __syncthreads();
-    blk_lu(nx, hx, nx, pv, &rs);
-    blk_lu_solve(nx, hx, nx, pv, nx, ax, nx);  // ax = Hx^{-1}
-    blk_lu(ny, hy, ny, pv, &rs);
-    blk_lu_solve(ny, hy, ny, pv, ny, ay, ny);  // ay = Hy^{-1}
+    blk_lu(nx, hx, nx, pv, &rs, stg);
+    blk_lu_solve(nx, hx, nx, pv, nx, ax, nx, stg);  // ax = Hx^{-1}
+    blk_lu(ny, hy, ny, pv, &rs, stg);
+    blk_lu_solve(ny, hy, ny, pv, ny, ay, ny, stg);  // ay = Hy^{-1}
     cplx* Einv = at(b.Einv, b.s_NN, cell);
     cplx* Exx = at(b.Exx, b.s_NN, cell);
     cplx* Eyy = at(b.Eyy, b.s_NN, cell);
@@ -279,9 +283,9 @@ __global__ void __launch_bounds__(kRT) rcwa_fourier_laurent(Bucket b) {
     }
     __syncthreads();
     int* piv = b.piv + b.s_n * cell;
-    const int info = blk_lu(N, lu, N, piv, &rs);
+    const int info = blk_lu(N, lu, N, piv, &rs, G1);  // G1 is dead: LU staging
     if (info != 0 && tid == 0) b.info[cell] = -info;
-    blk_lu_solve(N, lu, N, piv, N, Einv, N);  // Einv = epsT^{-1} (rcwa2d.cpp:203)
+    blk_lu_solve(N, lu, N, piv, N, Einv, N, G1);  // Einv = epsT^{-1} (rcwa2d.cpp:203)
 }
 
 // ---- M = ep2 kp - kkT -------------------------------------------------------------
@@ -328,34 +332,50 @@ __global__ void __launch_bounds__(kRT) rcwa_build_M(Bucket b, int laurent) {
 }
 
 // ---- eigensolve -----------------------------------------------------------------------
-// dynamic smem (SMEM variant): H [n*n] | v [n] | w [n]; otherwise v, w only.
+// Three kernels so that each gets its own register budget (the bulge chase
+// keeps 16-element row/column segments in registers). SMEM variants (n <= 112)
+// stage H in shared memory for the duration of the kernel.
+// dynamic smem: SMEM: H [n*n] | v [n] | w [n]; otherwise v [n] | w [n].
 template <bool SMEM>
-__global__ void __launch_bounds__(kRT) rcwa_eig(Bucket b) {
+__global__ void __launch_bounds__(kRT) rcwa_hess(Bucket b) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ RedScratch rs;
-    __shared__ SchurShared sh;
-    __shared__ GemmSmem gs;
     const int cell = blockIdx.x;
     const int n = b.n;
     const int tid = threadIdx.x, nt = blockDim.x;
     cplx* Hg = at(b.H, b.s_nn, cell);
-    cplx* Z = at(b.Z, b.s_nn, cell);
-    cplx* X = at(b.X, b.s_nn, cell);
-    cplx* H;
-    cplx* v;
+    cplx* H = SMEM ? reinterpret_cast<cplx*>(smem) : Hg;
+    cplx* v = SMEM ? H + (size_t)n * n : reinterpret_cast<cplx*>(smem);
     if (SMEM) {
-        H = reinterpret_cast<cplx*>(smem);
-        v = H + (size_t)n * n;
         for (int e = tid; e < n * n; e += nt) H[e] = Hg[e];
         __syncthreads();
-    } else {
-        H = Hg;
-        v = reinterpret_cast<cplx*>(smem);
     }
-    cplx* w = v + n;
-    blk_hessenberg(n, H, n, Z, n, v, w, &rs);
-    const int info = blk_schur(n, H, n, Z, n, &sh, kMaxSweepsPerRow);
-    if (tid == 0 && info != 0) b.info[b.ncell > 0 ? cell : 0] = info;
+    blk_hessenberg(n, H, n, at(b.Z, b.s_nn, cell), n, v, v + n, &rs);
+    if (SMEM) {
+        __syncthreads();
+        for (int e = tid; e < n * n; e += nt) Hg[e] = H[e];
+    }
+}
+
+// dynamic smem: SMEM: H [n*n]; otherwise none.
+template <bool SMEM>
+__global__ void __launch_bounds__(kRT) rcwa_schur(Bucket b) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ SchurShared sh;
+    const int cell = blockIdx.x;
+    const int n = b.n;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    cplx* Hg = at(b.H, b.s_nn, cell);
+    cplx* H = SMEM ? reinterpret_cast<cplx*>(smem) : Hg;
+    if (SMEM) {
+        for (int e = tid; e < n * n; e += nt) H[e] = Hg[e];
+        __syncthreads();
+    }
+    const int info = blk_schur(n, H, n, at(b.Z, b.s_nn, cell), n, &sh, kMaxSweepsPerRow);
+    if (tid == 0) {
+        if (info != 0) b.info[cell] = info;
+        if (b.dbg) b.dbg[8 * (size_t)cell + 6] = sh.nsweep;
+    }
     // eigenvalues -> q = branch(sqrt(lambda)) (rcwa2d.cpp:364)
     cplx* q1 = at(b.q1, b.s_n, cell);
     for (int i = tid; i < n; i += nt) {
@@ -363,12 +383,27 @@ __global__ void __launch_bounds__(kRT) rcwa_eig(Bucket b) {
         if (q.y < 0.0) q = cneg(q);
         q1[i] = q;
     }
-    blk_trevc(n, H, n, X, n);
-    blk_gemm(n, n, n, C(1.0, 0.0), Z, n, X, n, C(0.0, 0.0), at(b.W, b.s_nn, cell), n, &gs);
+    if (SMEM) {
+        __syncthreads();
+        for (int e = tid; e < n * n; e += nt) Hg[e] = H[e];
+    }
+}
+
+// eigenvectors of T, then W = Z X
+__global__ void __launch_bounds__(kRT) rcwa_vec(Bucket b) {
+    __shared__ GemmSmem gs;
+    const int cell = blockIdx.x;
+    const int n = b.n;
+    cplx* X = at(b.X, b.s_nn, cell);
+    blk_trevc(n, at(b.H, b.s_nn, cell), n, X, n);
+    blk_gemm(n, n, n, C(1.0, 0.0), at(b.Z, b.s_nn, cell), n, X, n, C(0.0, 0.0), at(b.W, b.s_nn, cell), n, &gs);
 }
 
 // ---- S-matrix, interface 0 --------------------------------------------------------------
+// dynamic smem: LU staging (2n + 2 complex)
 __global__ void __launch_bounds__(kRT) rcwa_smat1(Bucket b) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    cplx* stg = reinterpret_cast<cplx*>(smem);
     __shared__ GemmSmem gs;
     __shared__ RedScratch rs;
     const int cell = blockIdx.x;
@@ -440,13 +475,16 @@ __global__ void __launch_bounds__(kRT) rcwa_smat1(Bucket b) {
     }
     __syncthreads();
     int* piv = b.piv + b.s_n * cell;
-    const int info = blk_lu(n, T11lu, n, piv, &rs);
+    const int info = blk_lu(n, T11lu, n, piv, &rs, stg);
     if (info != 0 && tid == 0) b.info[cell] = -info;
-    blk_lu_solve(n, T11lu, n, piv, ld, S, ld);  // [S12 | u_X | u_Y]
+    blk_lu_solve(n, T11lu, n, piv, ld, S, ld, stg);  // [S12 | u_X | u_Y]
 }
 
 // ---- S-matrix, interface 1 + exterior amplitudes --------------------------------------------
+// dynamic smem: LU staging (2n + 2 complex)
 __global__ void __launch_bounds__(kRT) rcwa_smat2(Bucket b) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    cplx* stg = reinterpret_cast<cplx*>(smem);
     __shared__ GemmSmem gs;
     __shared__ RedScratch rs;
     const int cell = blockIdx.x;
@@ -464,10 +502,10 @@ __global__ void __launch_bounds__(kRT) rcwa_smat2(Bucket b) {
         Winv[e] = C(i == j ? 1.0 : 0.0, 0.0);
         Ainv[e] = C(i == j ? 1.0 : 0.0, 0.0);
     }
-    int info = blk_lu(n, W, n, piv, &rs);
-    blk_lu_solve(n, W, n, piv, n, Winv, n);
-    int info2 = blk_lu(n, A, n, piv, &rs);
-    blk_lu_solve(n, A, n, piv, n, Ainv, n);
+    int info = blk_lu(n, W, n, piv, &rs, stg);
+    blk_lu_solve(n, W, n, piv, n, Winv, n, stg);
+    int info2 = blk_lu(n, A, n, piv, &rs, stg);
+    blk_lu_solve(n, A, n, piv, n, Ainv, n, stg);
     if (tid == 0 && (info || info2)) b.info[cell] = -(info ? info : info2);
     // P' = diag(q1) A^{-1} kp2 diag(1/q2): T11' -> Winv, T12' -> Ainv (in place)
     const cplx ier = cinv(cmul(c.n_sub, c.n_sub));
@@ -503,9 +541,9 @@ __global__ void __launch_bounds__(kRT) rcwa_smat2(Bucket b) {
         const int i = e / 2, r = e % 2;
         x[e] = cmul(cexpi(cscale(q1[i], c.h)), S[(size_t)i * ld + n + r]);
     }
-    info = blk_lu(n, Bm, n, piv, &rs);
+    info = blk_lu(n, Bm, n, piv, &rs, stg);
     if (tid == 0 && info) b.info[cell] = -info;
-    blk_lu_solve(n, Bm, n, piv, 2, x, 2);  // x = aN (X, Y)
+    blk_lu_solve(n, Bm, n, piv, 2, x, 2, stg);  // x = aN (X, Y)
     // y = T12' x ; z = S12 y ; b0 = T12 (u + z) + T11 (D y)
     cplx* y = vec + 6 * (size_t)b.s_n;   // [n x 2]
     cplx* zz = vec + 8 * (size_t)b.s_n;  // [n x 2]
@@ -751,24 +789,69 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                 count_launch(3);
             } else {
                 const int nx = 2 * Mx + 1, ny = 2 * My + 1;
-                const size_t sm = (size_t)2 * (nx * nx + ny * ny) * sizeof(cplx);
+                const size_t sm = ((size_t)2 * (nx * nx + ny * ny) + 2 * std::max(nx, ny)) * sizeof(cplx);
                 CEL_CUDA(cudaFuncSetAttribute(rcwa_fourier_rect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
                 rcwa_fourier_rect<<<nc, kRT, sm, st>>>(b);
                 count_launch(1);
             }
+            // optional stage timing (diagnostics): CELERIS_RCWA_STAGE_CLOCKS=1
+            const bool prof = std::getenv("CELERIS_RCWA_STAGE_CLOCKS") != nullptr;
+            cudaEvent_t ev[8] = {};
+            long long* dbg = nullptr;
+            if (prof) {
+                for (auto& e : ev) cudaEventCreate(&e);
+                CEL_CUDA(cudaMalloc(&dbg, sizeof(long long) * 8 * nc));
+                CEL_CUDA(cudaMemsetAsync(dbg, 0, sizeof(long long) * 8 * nc, st));
+                b.dbg = dbg;
+                cudaEventRecord(ev[0], st);
+            }
             rcwa_build_M<<<nc, kRT, 0, st>>>(b, ng > 0 ? 1 : 0);
+            if (prof) cudaEventRecord(ev[1], st);
             if (n <= kSmemEigMaxN) {
                 const size_t sm = ((size_t)n * n + 2 * n) * sizeof(cplx);
-                CEL_CUDA(cudaFuncSetAttribute(rcwa_eig<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-                rcwa_eig<true><<<nc, kRT, sm, st>>>(b);
+                CEL_CUDA(cudaFuncSetAttribute(rcwa_hess<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                CEL_CUDA(cudaFuncSetAttribute(rcwa_schur<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                rcwa_hess<true><<<nc, kRT, sm, st>>>(b);
+                if (prof) cudaEventRecord(ev[6], st);
+                rcwa_schur<true><<<nc, kRT, sm, st>>>(b);
             } else {
-                rcwa_eig<false><<<nc, kRT, 2 * n * sizeof(cplx), st>>>(b);
+                rcwa_hess<false><<<nc, kRT, 2 * n * sizeof(cplx), st>>>(b);
+                if (prof) cudaEventRecord(ev[6], st);
+                rcwa_schur<false><<<nc, kRT, 0, st>>>(b);
             }
-            rcwa_smat1<<<nc, kRT, 0, st>>>(b);
-            rcwa_smat2<<<nc, kRT, 0, st>>>(b);
+            if (prof) cudaEventRecord(ev[7], st);
+            rcwa_vec<<<nc, kRT, 0, st>>>(b);
+            if (prof) cudaEventRecord(ev[2], st);
+            const size_t sm_stage = (size_t)(2 * n + 2) * sizeof(cplx);
+            CEL_CUDA(cudaFuncSetAttribute(rcwa_smat1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_stage));
+            CEL_CUDA(cudaFuncSetAttribute(rcwa_smat2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_stage));
+            rcwa_smat1<<<nc, kRT, sm_stage, st>>>(b);
+            if (prof) cudaEventRecord(ev[3], st);
+            rcwa_smat2<<<nc, kRT, sm_stage, st>>>(b);
+            if (prof) cudaEventRecord(ev[4], st);
             rcwa_epilogue<<<nc, kRT, 0, st>>>(b);
-            count_launch(5);
+            if (prof) cudaEventRecord(ev[5], st);
+            count_launch(7);
             CEL_CUDA(cudaGetLastError());
+            if (prof) {
+                CEL_CUDA(cudaStreamSynchronize(st));
+                float ms[5];
+                for (int q = 0; q < 5; ++q) cudaEventElapsedTime(&ms[q], ev[q], ev[q + 1]);
+                std::vector<long long> h(8 * nc);
+                cudaMemcpy(h.data(), dbg, sizeof(long long) * 8 * nc, cudaMemcpyDeviceToHost);
+                float mh = 0.f, msch = 0.f;
+                cudaEventElapsedTime(&mh, ev[1], ev[6]);
+                cudaEventElapsedTime(&msch, ev[6], ev[7]);
+                double sw = 0;
+                for (int i = 0; i < nc; ++i) sw += (double)h[8 * i + 6];
+                std::fprintf(stderr,
+                             "[rcwa stages] n=%d cells=%d ms: build_M %.2f eig %.2f (hess %.2f schur %.2f vec %.2f) "
+                             "smat1 %.2f smat2 %.2f epi %.2f | sweeps/cell %.1f\n",
+                             n, nc, ms[0], ms[1], mh, msch, ms[1] - mh - msch, ms[2], ms[3], ms[4], sw / nc);
+                cudaFree(dbg);
+                b.dbg = nullptr;
+                for (auto& e : ev) cudaEventDestroy(e);
+            }
             std::vector<celeris_rcwa_result> r(nc * nexc);
             std::vector<int> inf(nc);
             CEL_CUDA(cudaMemcpyAsync(r.data(), b.res, sizeof(celeris_rcwa_result) * nexc * nc, cudaMemcpyDeviceToHost, st));

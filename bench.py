@@ -81,14 +81,24 @@ def barrier(world):
 
 
 def max_over_ranks(world, x):
+    """Max of a per-rank scalar over all ranks (NCCL on GPUs, gloo on CPU)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def shard_center(rank, n, half_window_um):
+    """Window centre y of rank `rank`'s n-row tile: the tiles of ranks 0..N-1
+    are consecutive, disjoint row blocks of one taller focal window whose first
+    row sits at -half_window (weak scaling, pillars replicated)."""
+    step = 2.0 * half_window_um / (n - 1)
+    return rank * n * step
 
 
 # ---------------------------------------------------------------- clocks
@@ -150,9 +160,7 @@ def workload(rank):
 
     ap, g = metalens_785k()
     # rank r evaluates the r-th 1024-row tile of a taller focal window
-    step = 2.0 * g.half_window_um / (g.n - 1)
-    cy = rank * g.n * step
-    return ap, g, cy
+    return ap, g, shard_center(rank, g.n, g.half_window_um)
 
 
 def choose_cpu_sample(npil, seconds, rate_guess, threads):

@@ -51,7 +51,7 @@ EXPORTED = [
     "celeris_propagate_zx", "celeris_rs_field", "celeris_rs_field_dev", "celeris_rs_adjoint_dev",
     "celeris_rs_check_dev", "celeris_sync_status", "celeris_solve_rcwa_2d", "celeris_rcwa_batch",
     "celeris_probe_peaks", "celeris_set_kernel_timing", "celeris_last_kernel_ms",
-    "celeris_rs_field_noalloc", "celeris_probe_sincos",
+    "celeris_rs_field_noalloc", "celeris_probe_sincos", "celeris_rcwa_tuning_report",
 ]
 
 
@@ -121,6 +121,7 @@ def load(path: str = LIB_PATH):
         "celeris_last_kernel_ms": (_I, [_P]),
         "celeris_solve_rcwa_2d": (_I, [ctypes.POINTER(RcwaCell), _P, _P, ctypes.POINTER(RcwaResult)]),
         "celeris_rcwa_batch": (_I, [ctypes.POINTER(RcwaCell), _I, ctypes.POINTER(RcwaResult), _PI]),
+        "celeris_rcwa_tuning_report": (_I, [ctypes.c_char_p, _I]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -243,6 +244,12 @@ def solve_rcwa_2d(cell: RcwaCell, Ex0=1.0 + 0j, Ey0=0.0 + 0j) -> dict:
     out = RcwaResult()
     check(load().celeris_solve_rcwa_2d(ctypes.byref(cell), _dp(ex), _dp(ey), ctypes.byref(out)))
     return result_dict(out)
+
+
+def rcwa_tuning_report() -> str:
+    buf = ctypes.create_string_buffer(1 << 16)
+    check(load().celeris_rcwa_tuning_report(buf, len(buf)))
+    return buf.value.decode()
 
 
 def rcwa_batch(cells) -> tuple[list[dict], np.ndarray]:

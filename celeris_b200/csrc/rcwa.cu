@@ -28,6 +28,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
+#include <string>
 #include <tuple>
 #include <vector>
 
@@ -715,152 +717,434 @@ size_t laurent_smem(int Mx, int My, int ng) {
     return (mx4 * ng + mx4 * my4) * sizeof(cplx) + (size_t)ng * ng;
 }
 
+// ---- stage configuration and autotuning -------------------------------------------------
+// Every stage kernel runs with blockDim in {128, 256} (they are written for any
+// multiple of 32 >= 128). For each bucket shape (Mx, My, raster) the first batch
+// that meets it times every stage at both sizes on the bucket's own cells and
+// keeps the faster size per stage; the table lives for the process and can be
+// read with celeris_rcwa_tuning_report. CELERIS_RCWA_AUTOTUNE=0 disables it
+// (all stages at 256 threads).
+enum Stage { ST_FOURIER, ST_BUILD, ST_HESS, ST_SCHUR, ST_VEC, ST_SMAT1, ST_SMAT2, ST_EPI, ST_COUNT };
+const char* const kStageNames[ST_COUNT] = {"fourier", "build_M", "hessenberg", "schur", "eigvec",
+                                           "smat1", "smat2", "epilogue"};
+constexpr int kCand[2] = {128, 256};
+struct StageCfg {
+    int threads[ST_COUNT];
+};
+StageCfg uniform_cfg(int t) {
+    StageCfg c;
+    for (int i = 0; i < ST_COUNT; ++i) c.threads[i] = t;
+    return c;
+}
+
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, StageCfg>& tune_table() {
+    static auto* m = new std::map<std::tuple<int, int, int>, StageCfg>();
+    return *m;
+}
+bool tuning_enabled() {
+    const char* e = std::getenv("CELERIS_RCWA_AUTOTUNE");
+    return !(e && e[0] == '0');
+}
+
+struct BucketPlan {
+    int Mx, My, ng, N, n;
+    std::vector<int> ids;  // indices into the cell list
+    size_t per_cell = 0, bytes = 0;
+    Bucket b;
+};
+
+size_t per_cell_bytes(int n, int nexc) {
+    const int N = n / 2;
+    const size_t s_nn = (size_t)n * n, s_ns = (size_t)n * (n + 2), s_NN = (size_t)N * N, s_n = (size_t)n;
+    return celeris_rt::align256((11 * s_nn + s_ns + 3 * s_NN + 11 * s_n) * sizeof(cplx)) +
+           celeris_rt::align256(s_n * sizeof(int)) + 256 + celeris_rt::align256(sizeof(celeris_rcwa_result) * nexc) +
+           celeris_rt::align256(sizeof(CellDev)) + 14 * 256;
+}
+
+// Dynamic shared-memory limits are per kernel function, so they are set once
+// per wave to the largest need over its buckets (outside any capture).
+struct SmemNeeds {
+    size_t laurent = 0, rect = 0, hess_s = 0, smat = 0;
+    void add(int Mx, int My, int ng, int n) {
+        if (ng > 0) {
+            laurent = std::max(laurent, laurent_smem(Mx, My, ng));
+        } else {
+            const int nx = 2 * Mx + 1, ny = 2 * My + 1;
+            rect = std::max(rect, ((size_t)2 * (nx * nx + ny * ny) + 2 * std::max(nx, ny)) * sizeof(cplx));
+        }
+        if (n <= kSmemEigMaxN) hess_s = std::max(hess_s, ((size_t)n * n + 2 * n) * sizeof(cplx));
+        smat = std::max(smat, (size_t)(2 * n + 2) * sizeof(cplx));
+    }
+};
+
+int set_smem_limits(const SmemNeeds& s) {
+    if (s.laurent)
+        CEL_CUDA(cudaFuncSetAttribute(rcwa_fourier_laurent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.laurent));
+    if (s.rect)
+        CEL_CUDA(cudaFuncSetAttribute(rcwa_fourier_rect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.rect));
+    if (s.hess_s) {
+        CEL_CUDA(cudaFuncSetAttribute(rcwa_hess<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.hess_s));
+        CEL_CUDA(cudaFuncSetAttribute(rcwa_schur<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.hess_s));
+    }
+    if (s.smat) {
+        CEL_CUDA(cudaFuncSetAttribute(rcwa_smat1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smat));
+        CEL_CUDA(cudaFuncSetAttribute(rcwa_smat2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smat));
+    }
+    return CELERIS_OK;
+}
+
+// Launch the stage sequence of one bucket on `st`. ev (ST_COUNT + 1 events) is
+// optional: stage boundaries are recorded into it.
+void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEvent_t* ev) {
+    const int nc = b.ncell, n = b.n;
+    const int* T = cfg.threads;
+    if (ev) cudaEventRecord(ev[0], st);
+    cudaMemsetAsync(b.info, 0, sizeof(int) * nc, st);
+    if (b.ng > 0) {
+        const int Mx = b.Mx, My = b.My, ng = b.ng;
+        rcwa_phase_table<<<((4 * Mx + 1) * ng + 255) / 256, 256, 0, st>>>(ng, 2 * Mx, const_cast<cplx*>(b.phx));
+        rcwa_phase_table<<<((4 * My + 1) * ng + 255) / 256, 256, 0, st>>>(ng, 2 * My, const_cast<cplx*>(b.phy));
+        rcwa_fourier_laurent<<<nc, T[ST_FOURIER], laurent_smem(Mx, My, ng), st>>>(b);
+        count_launch(3);
+    } else {
+        const int nx = 2 * b.Mx + 1, ny = 2 * b.My + 1;
+        const size_t sm = ((size_t)2 * (nx * nx + ny * ny) + 2 * std::max(nx, ny)) * sizeof(cplx);
+        rcwa_fourier_rect<<<nc, T[ST_FOURIER], sm, st>>>(b);
+        count_launch(1);
+    }
+    if (ev) cudaEventRecord(ev[1], st);
+    rcwa_build_M<<<nc, T[ST_BUILD], 0, st>>>(b, b.ng > 0 ? 1 : 0);
+    if (ev) cudaEventRecord(ev[2], st);
+    if (n <= kSmemEigMaxN) {
+        const size_t sm = ((size_t)n * n + 2 * n) * sizeof(cplx);
+        rcwa_hess<true><<<nc, T[ST_HESS], sm, st>>>(b);
+        if (ev) cudaEventRecord(ev[3], st);
+        rcwa_schur<true><<<nc, T[ST_SCHUR], sm, st>>>(b);
+    } else {
+        rcwa_hess<false><<<nc, T[ST_HESS], 2 * n * sizeof(cplx), st>>>(b);
+        if (ev) cudaEventRecord(ev[3], st);
+        rcwa_schur<false><<<nc, T[ST_SCHUR], 0, st>>>(b);
+    }
+    if (ev) cudaEventRecord(ev[4], st);
+    rcwa_vec<<<nc, T[ST_VEC], 0, st>>>(b);
+    if (ev) cudaEventRecord(ev[5], st);
+    const size_t sm_stage = (size_t)(2 * n + 2) * sizeof(cplx);
+    rcwa_smat1<<<nc, T[ST_SMAT1], sm_stage, st>>>(b);
+    if (ev) cudaEventRecord(ev[6], st);
+    rcwa_smat2<<<nc, T[ST_SMAT2], sm_stage, st>>>(b);
+    if (ev) cudaEventRecord(ev[7], st);
+    rcwa_epilogue<<<nc, T[ST_EPI], 0, st>>>(b);
+    if (ev) cudaEventRecord(ev[8], st);
+    count_launch(7);
+}
+
+// Time each stage at every candidate size on (up to) the first 2 x SMs cells
+// of the bucket; keep the faster size per stage.
+int autotune(const BucketPlan& p, cudaStream_t st, StageCfg* out) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    Bucket t = p.b;
+    t.ncell = std::min(t.ncell, 2 * sms);
+    cudaEvent_t ev[ST_COUNT + 1];
+    for (auto& e : ev) CEL_CUDA(cudaEventCreate(&e));
+    float best[ST_COUNT];
+    StageCfg cfg = uniform_cfg(256);
+    for (int c = 0; c < 2; ++c) {
+        launch_bucket(t, uniform_cfg(kCand[c]), st, ev);
+        CEL_CUDA(cudaStreamSynchronize(st));
+        for (int s = 0; s < ST_COUNT; ++s) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[s], ev[s + 1]);
+            if (c == 0 || ms < best[s]) {
+                best[s] = ms;
+                cfg.threads[s] = kCand[c];
+            }
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    CEL_CUDA(cudaGetLastError());
+    *out = cfg;
+    return CELERIS_OK;
+}
+
+// Per-thread execution context: streams, pinned staging and the cached graph.
+struct BatchCtx {
+    cudaStream_t main = nullptr;
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> fork, join;
+    void* pinned = nullptr;
+    size_t pinned_cap = 0;
+    cudaGraphExec_t exec = nullptr;
+    std::string sig;
+    uint64_t nkern = 0;  // kernels per graph launch
+};
+thread_local BatchCtx t_ctx;
+
+int ensure_streams(int nb) {
+    BatchCtx& c = t_ctx;
+    if (!c.main) CEL_CUDA(cudaStreamCreateWithFlags(&c.main, cudaStreamNonBlocking));
+    while ((int)c.side.size() < nb) {
+        cudaStream_t s;
+        cudaEvent_t f, j;
+        CEL_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        CEL_CUDA(cudaEventCreateWithFlags(&f, cudaEventDisableTiming));
+        CEL_CUDA(cudaEventCreateWithFlags(&j, cudaEventDisableTiming));
+        c.side.push_back(s);
+        c.fork.push_back(f);
+        c.join.push_back(j);
+    }
+    return CELERIS_OK;
+}
+
 int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_out, int nexc) {
     CEL_TRY(celeris_rt::require_device());
-    thread_local cudaStream_t st = nullptr;
-    if (!st) CEL_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    // bucket by (Mx, My, ng)
-    std::map<std::tuple<int, int, int>, std::vector<int>> buckets;
-    for (int i = 0; i < (int)cells.size(); ++i)
-        buckets[std::make_tuple(cells[i].Mx, cells[i].My, cells[i].ng)].push_back(i);
+    // ---- plan: buckets by (Mx, My, raster), largest first so they start first
+    std::map<std::tuple<int, int, int>, std::vector<int>> by;
+    for (int i = 0; i < (int)cells.size(); ++i) by[std::make_tuple(cells[i].Mx, cells[i].My, cells[i].ng)].push_back(i);
+    std::vector<BucketPlan> plans;
+    CEL_TRY(ensure_streams(1));
     int dev = 0, smem_optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const size_t kChunkBytes = (size_t)32 << 30;
+    size_t free_b = 0, total_b = 0;
+    CEL_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    Workspace& ws0 = Workspace::for_stream(t_ctx.main);
+    const size_t budget = (size_t)(0.6 * (double)(free_b + ws0.capacity()));
+    for (auto& kv : by) {
+        BucketPlan p;
+        p.Mx = std::get<0>(kv.first);
+        p.My = std::get<1>(kv.first);
+        p.ng = std::get<2>(kv.first);
+        p.N = (2 * p.Mx + 1) * (2 * p.My + 1);
+        p.n = 2 * p.N;
+        if (p.ng > 0 && laurent_smem(p.Mx, p.My, p.ng) + 1024 > (size_t)smem_optin)
+            return set_error(CELERIS_ERR_TOO_LARGE, "raster %d with M=(%d,%d) exceeds shared memory", p.ng, p.Mx, p.My);
+        p.per_cell = per_cell_bytes(p.n, nexc);
+        // split buckets that alone exceed the budget
+        const size_t max_cells = std::max<size_t>(1, budget / std::max<size_t>(1, p.per_cell));
+        for (size_t c0 = 0; c0 < kv.second.size(); c0 += max_cells) {
+            BucketPlan q = p;
+            const size_t c1 = std::min(kv.second.size(), c0 + max_cells);
+            q.ids.assign(kv.second.begin() + c0, kv.second.begin() + c1);
+            q.bytes = q.per_cell * q.ids.size() +
+                      (q.ng > 0 ? celeris_rt::align256(((size_t)(4 * q.Mx + 1) + (4 * q.My + 1)) * q.ng * sizeof(cplx)) + 512
+                                : 0);
+            plans.push_back(q);
+        }
+    }
+    std::sort(plans.begin(), plans.end(), [](const BucketPlan& a, const BucketPlan& b) { return a.n > b.n; });
+    // ---- waves of buckets that fit the memory budget together
+    std::vector<std::vector<int>> waves;
+    size_t acc = 0;
+    for (int i = 0; i < (int)plans.size(); ++i) {
+        if (waves.empty() || acc + plans[i].bytes > budget) {
+            waves.emplace_back();
+            acc = 0;
+        }
+        waves.back().push_back(i);
+        acc += plans[i].bytes;
+    }
     std::vector<celeris_rcwa_result> hres(cells.size() * nexc);
     std::vector<int> hinfo(cells.size(), 0);
-    for (auto& kv : buckets) {
-        const int Mx = std::get<0>(kv.first), My = std::get<1>(kv.first), ng = std::get<2>(kv.first);
-        const int N = (2 * Mx + 1) * (2 * My + 1), n = 2 * N;
-        const std::vector<int>& ids = kv.second;
-        const size_t s_nn = (size_t)n * n, s_ns = (size_t)n * (n + 2), s_NN = (size_t)N * N, s_n = (size_t)n;
-        const size_t per_cell = (11 * s_nn + s_ns + 3 * s_NN + 11 * s_n) * sizeof(cplx) + s_n * sizeof(int) +
-                                sizeof(int) + sizeof(celeris_rcwa_result) * nexc + sizeof(CellDev) + 8 * 256;
-        const int chunk = (int)std::max<size_t>(1, std::min<size_t>(ids.size(), kChunkBytes / per_cell));
-        if (ng > 0 && laurent_smem(Mx, My, ng) > (size_t)smem_optin)
-            return set_error(CELERIS_ERR_TOO_LARGE, "raster %d with M=(%d,%d) exceeds shared memory", ng, Mx, My);
-        for (int c0 = 0; c0 < (int)ids.size(); c0 += chunk) {
-            const int nc = std::min(chunk, (int)ids.size() - c0);
-            Workspace& ws = Workspace::for_stream(st);
-            const size_t ph_bytes = ng > 0 ? ((size_t)(4 * Mx + 1) + (4 * My + 1)) * ng * sizeof(cplx) : 0;
-            const size_t total = per_cell * nc + ph_bytes + 64 * 256;
-            CEL_TRY(ws.reserve(st, total));
-            Bucket b;
+    const bool prof = std::getenv("CELERIS_RCWA_STAGE_CLOCKS") != nullptr;
+    for (const auto& wave : waves) {
+        CEL_TRY(ensure_streams((int)wave.size()));
+        BatchCtx& ctx = t_ctx;
+        cudaStream_t st = ctx.main;
+        Workspace& ws = Workspace::for_stream(st);
+        size_t need = 0, pin_need = 0;
+        for (int i : wave) {
+            need += plans[i].bytes + 4096;
+            pin_need += celeris_rt::align256(sizeof(CellDev) * plans[i].ids.size()) +
+                        celeris_rt::align256(sizeof(celeris_rcwa_result) * nexc * plans[i].ids.size()) +
+                        celeris_rt::align256(sizeof(int) * plans[i].ids.size());
+        }
+        void* old_base = ws.base();
+        CEL_TRY(ws.reserve(st, need));
+        if (ws.base() != old_base && ctx.exec) {  // the cached graph points at the old arena
+            cudaGraphExecDestroy(ctx.exec);
+            ctx.exec = nullptr;
+            ctx.sig.clear();
+        }
+        if (ctx.pinned_cap < pin_need) {
+            if (ctx.exec) {
+                cudaGraphExecDestroy(ctx.exec);
+                ctx.exec = nullptr;
+                ctx.sig.clear();
+            }
+            if (ctx.pinned) cudaFreeHost(ctx.pinned);
+            ctx.pinned = nullptr;
+            ctx.pinned_cap = 0;
+            CEL_CUDA(cudaHostAlloc(&ctx.pinned, pin_need, cudaHostAllocDefault));
+            ctx.pinned_cap = pin_need;
+        }
+        // ---- carve the arena and the pinned staging, fill the descriptors
+        char* pin = static_cast<char*>(ctx.pinned);
+        std::string sig = "n" + std::to_string(nexc);
+        std::vector<CellDev*> hdesc(wave.size());
+        std::vector<celeris_rcwa_result*> hres_pin(wave.size());
+        std::vector<int*> hinfo_pin(wave.size());
+        SmemNeeds needs;
+        for (size_t w = 0; w < wave.size(); ++w) {
+            BucketPlan& p = plans[wave[w]];
+            const int nc = (int)p.ids.size();
+            Bucket& b = p.b;
             std::memset(&b, 0, sizeof(b));
-            b.Mx = Mx;
-            b.My = My;
-            b.N = N;
-            b.n = n;
-            b.ng = ng;
+            b.Mx = p.Mx;
+            b.My = p.My;
+            b.N = p.N;
+            b.n = p.n;
+            b.ng = p.ng;
             b.ncell = nc;
-            b.s_nn = s_nn;
-            b.s_ns = s_ns;
-            b.s_NN = s_NN;
-            b.s_n = s_n;
-            auto take = [&](size_t bytes) { return ws.take(bytes); };
-            CellDev* dcells = static_cast<CellDev*>(take(sizeof(CellDev) * nc));
+            b.s_nn = (size_t)p.n * p.n;
+            b.s_ns = (size_t)p.n * (p.n + 2);
+            b.s_NN = (size_t)p.N * p.N;
+            b.s_n = (size_t)p.n;
+            CellDev* dcells = static_cast<CellDev*>(ws.take(sizeof(CellDev) * nc));
             b.cells = dcells;
             cplx** mats[] = {&b.H, &b.Z, &b.X, &b.W, &b.A, &b.T11, &b.T11lu, &b.T12, &b.Winv, &b.Ainv, &b.B};
-            for (cplx** m : mats) *m = static_cast<cplx*>(take(sizeof(cplx) * s_nn * nc));
-            b.S12 = static_cast<cplx*>(take(sizeof(cplx) * s_ns * nc));
-            b.Einv = static_cast<cplx*>(take(sizeof(cplx) * s_NN * nc));
-            b.Exx = static_cast<cplx*>(take(sizeof(cplx) * s_NN * nc));
-            b.Eyy = static_cast<cplx*>(take(sizeof(cplx) * s_NN * nc));
-            b.q1 = static_cast<cplx*>(take(sizeof(cplx) * s_n * nc));
-            b.vec = static_cast<cplx*>(take(sizeof(cplx) * 10 * s_n * nc));
-            b.piv = static_cast<int*>(take(sizeof(int) * s_n * nc));
-            b.info = static_cast<int*>(take(sizeof(int) * nc));
-            b.res = static_cast<celeris_rcwa_result*>(take(sizeof(celeris_rcwa_result) * nexc * nc));
-            std::vector<CellDev> hc(nc);
-            for (int i = 0; i < nc; ++i) hc[i] = cells[ids[c0 + i]].d;
-            CEL_CUDA(cudaMemcpyAsync(dcells, hc.data(), sizeof(CellDev) * nc, cudaMemcpyHostToDevice, st));
-            CEL_CUDA(cudaMemsetAsync(b.info, 0, sizeof(int) * nc, st));
-            if (ng > 0) {
-                cplx* phx = static_cast<cplx*>(take(sizeof(cplx) * (4 * Mx + 1) * ng));
-                cplx* phy = static_cast<cplx*>(take(sizeof(cplx) * (4 * My + 1) * ng));
-                rcwa_phase_table<<<((4 * Mx + 1) * ng + 255) / 256, 256, 0, st>>>(ng, 2 * Mx, phx);
-                rcwa_phase_table<<<((4 * My + 1) * ng + 255) / 256, 256, 0, st>>>(ng, 2 * My, phy);
-                b.phx = phx;
-                b.phy = phy;
-                const size_t sm = laurent_smem(Mx, My, ng);
-                CEL_CUDA(cudaFuncSetAttribute(rcwa_fourier_laurent, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)sm));
-                rcwa_fourier_laurent<<<nc, kRT, sm, st>>>(b);
-                count_launch(3);
-            } else {
-                const int nx = 2 * Mx + 1, ny = 2 * My + 1;
-                const size_t sm = ((size_t)2 * (nx * nx + ny * ny) + 2 * std::max(nx, ny)) * sizeof(cplx);
-                CEL_CUDA(cudaFuncSetAttribute(rcwa_fourier_rect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-                rcwa_fourier_rect<<<nc, kRT, sm, st>>>(b);
-                count_launch(1);
+            for (cplx** m : mats) *m = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_nn * nc));
+            b.S12 = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_ns * nc));
+            b.Einv = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_NN * nc));
+            b.Exx = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_NN * nc));
+            b.Eyy = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_NN * nc));
+            b.q1 = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_n * nc));
+            b.vec = static_cast<cplx*>(ws.take(sizeof(cplx) * 10 * b.s_n * nc));
+            b.piv = static_cast<int*>(ws.take(sizeof(int) * b.s_n * nc));
+            b.info = static_cast<int*>(ws.take(sizeof(int) * nc));
+            b.res = static_cast<celeris_rcwa_result*>(ws.take(sizeof(celeris_rcwa_result) * nexc * nc));
+            if (p.ng > 0) {
+                b.phx = static_cast<cplx*>(ws.take(sizeof(cplx) * (4 * p.Mx + 1) * p.ng));
+                b.phy = static_cast<cplx*>(ws.take(sizeof(cplx) * (4 * p.My + 1) * p.ng));
             }
-            // optional stage timing (diagnostics): CELERIS_RCWA_STAGE_CLOCKS=1
-            const bool prof = std::getenv("CELERIS_RCWA_STAGE_CLOCKS") != nullptr;
-            cudaEvent_t ev[8] = {};
-            long long* dbg = nullptr;
-            if (prof) {
-                for (auto& e : ev) cudaEventCreate(&e);
+            hdesc[w] = reinterpret_cast<CellDev*>(pin);
+            pin += celeris_rt::align256(sizeof(CellDev) * nc);
+            hres_pin[w] = reinterpret_cast<celeris_rcwa_result*>(pin);
+            pin += celeris_rt::align256(sizeof(celeris_rcwa_result) * nexc * nc);
+            hinfo_pin[w] = reinterpret_cast<int*>(pin);
+            pin += celeris_rt::align256(sizeof(int) * nc);
+            for (int i = 0; i < nc; ++i) hdesc[w][i] = cells[p.ids[i]].d;
+            needs.add(p.Mx, p.My, p.ng, p.n);
+            sig += "|" + std::to_string(p.Mx) + "," + std::to_string(p.My) + "," + std::to_string(p.ng) + "," +
+                   std::to_string(nc);
+        }
+        CEL_TRY(set_smem_limits(needs));
+        // ---- tune unseen bucket shapes (descriptors must be on the device)
+        std::vector<StageCfg> cfgs(wave.size(), uniform_cfg(256));
+        for (size_t w = 0; w < wave.size(); ++w) {
+            const BucketPlan& p = plans[wave[w]];
+            // key: shape and batch class (fewer than, or at least, one cell per SM)
+            int sms = 148;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            const auto key = std::make_tuple(p.Mx, p.My, 2 * p.ng + ((int)p.ids.size() >= sms ? 1 : 0));
+            bool have = false;
+            {
+                std::lock_guard<std::mutex> lk(g_tune_mu);
+                auto it = tune_table().find(key);
+                if (it != tune_table().end()) {
+                    cfgs[w] = it->second;
+                    have = true;
+                }
+            }
+            if (!have && tuning_enabled() && !prof) {
+                CEL_CUDA(cudaMemcpyAsync(const_cast<CellDev*>(p.b.cells), hdesc[w], sizeof(CellDev) * p.ids.size(),
+                                         cudaMemcpyHostToDevice, st));
+                CEL_TRY(autotune(p, st, &cfgs[w]));
+                std::lock_guard<std::mutex> lk(g_tune_mu);
+                tune_table()[key] = cfgs[w];
+            }
+            for (int s = 0; s < ST_COUNT; ++s) sig += (cfgs[w].threads[s] == 128 ? "a" : "b");
+        }
+        if (prof) {
+            // diagnostics: one bucket after the other, events per stage
+            for (size_t w = 0; w < wave.size(); ++w) {
+                BucketPlan& p = plans[wave[w]];
+                const int nc = (int)p.ids.size();
+                CEL_CUDA(cudaMemcpyAsync(const_cast<CellDev*>(p.b.cells), hdesc[w], sizeof(CellDev) * nc,
+                                         cudaMemcpyHostToDevice, st));
+                long long* dbg = nullptr;
                 CEL_CUDA(cudaMalloc(&dbg, sizeof(long long) * 8 * nc));
                 CEL_CUDA(cudaMemsetAsync(dbg, 0, sizeof(long long) * 8 * nc, st));
-                b.dbg = dbg;
-                cudaEventRecord(ev[0], st);
-            }
-            rcwa_build_M<<<nc, kRT, 0, st>>>(b, ng > 0 ? 1 : 0);
-            if (prof) cudaEventRecord(ev[1], st);
-            if (n <= kSmemEigMaxN) {
-                const size_t sm = ((size_t)n * n + 2 * n) * sizeof(cplx);
-                CEL_CUDA(cudaFuncSetAttribute(rcwa_hess<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-                CEL_CUDA(cudaFuncSetAttribute(rcwa_schur<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-                rcwa_hess<true><<<nc, kRT, sm, st>>>(b);
-                if (prof) cudaEventRecord(ev[6], st);
-                rcwa_schur<true><<<nc, kRT, sm, st>>>(b);
-            } else {
-                rcwa_hess<false><<<nc, kRT, 2 * n * sizeof(cplx), st>>>(b);
-                if (prof) cudaEventRecord(ev[6], st);
-                rcwa_schur<false><<<nc, kRT, 0, st>>>(b);
-            }
-            if (prof) cudaEventRecord(ev[7], st);
-            rcwa_vec<<<nc, kRT, 0, st>>>(b);
-            if (prof) cudaEventRecord(ev[2], st);
-            const size_t sm_stage = (size_t)(2 * n + 2) * sizeof(cplx);
-            CEL_CUDA(cudaFuncSetAttribute(rcwa_smat1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_stage));
-            CEL_CUDA(cudaFuncSetAttribute(rcwa_smat2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_stage));
-            rcwa_smat1<<<nc, kRT, sm_stage, st>>>(b);
-            if (prof) cudaEventRecord(ev[3], st);
-            rcwa_smat2<<<nc, kRT, sm_stage, st>>>(b);
-            if (prof) cudaEventRecord(ev[4], st);
-            rcwa_epilogue<<<nc, kRT, 0, st>>>(b);
-            if (prof) cudaEventRecord(ev[5], st);
-            count_launch(7);
-            CEL_CUDA(cudaGetLastError());
-            if (prof) {
+                p.b.dbg = dbg;
+                cudaEvent_t ev[ST_COUNT + 1];
+                for (auto& e : ev) cudaEventCreate(&e);
+                launch_bucket(p.b, cfgs[w], st, ev);
+                CEL_CUDA(cudaMemcpyAsync(hres_pin[w], p.b.res, sizeof(celeris_rcwa_result) * nexc * nc,
+                                         cudaMemcpyDeviceToHost, st));
+                CEL_CUDA(cudaMemcpyAsync(hinfo_pin[w], p.b.info, sizeof(int) * nc, cudaMemcpyDeviceToHost, st));
                 CEL_CUDA(cudaStreamSynchronize(st));
-                float ms[5];
-                for (int q = 0; q < 5; ++q) cudaEventElapsedTime(&ms[q], ev[q], ev[q + 1]);
                 std::vector<long long> h(8 * nc);
                 cudaMemcpy(h.data(), dbg, sizeof(long long) * 8 * nc, cudaMemcpyDeviceToHost);
-                float mh = 0.f, msch = 0.f;
-                cudaEventElapsedTime(&mh, ev[1], ev[6]);
-                cudaEventElapsedTime(&msch, ev[6], ev[7]);
                 double sw = 0;
                 for (int i = 0; i < nc; ++i) sw += (double)h[8 * i + 6];
-                std::fprintf(stderr,
-                             "[rcwa stages] n=%d cells=%d ms: build_M %.2f eig %.2f (hess %.2f schur %.2f vec %.2f) "
-                             "smat1 %.2f smat2 %.2f epi %.2f | sweeps/cell %.1f\n",
-                             n, nc, ms[0], ms[1], mh, msch, ms[1] - mh - msch, ms[2], ms[3], ms[4], sw / nc);
-                cudaFree(dbg);
-                b.dbg = nullptr;
+                std::string line = "[rcwa stages] n=" + std::to_string(p.n) + " cells=" + std::to_string(nc) + " ms:";
+                for (int s = 0; s < ST_COUNT; ++s) {
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, ev[s], ev[s + 1]);
+                    char buf[64];
+                    std::snprintf(buf, sizeof(buf), " %s %.2f", kStageNames[s], ms);
+                    line += buf;
+                }
+                char buf[64];
+                std::snprintf(buf, sizeof(buf), " | sweeps/cell %.1f\n", sw / nc);
+                std::fprintf(stderr, "%s%s", line.c_str(), buf);
                 for (auto& e : ev) cudaEventDestroy(e);
+                cudaFree(dbg);
+                p.b.dbg = nullptr;
             }
-            std::vector<celeris_rcwa_result> r(nc * nexc);
-            std::vector<int> inf(nc);
-            CEL_CUDA(cudaMemcpyAsync(r.data(), b.res, sizeof(celeris_rcwa_result) * nexc * nc, cudaMemcpyDeviceToHost, st));
-            CEL_CUDA(cudaMemcpyAsync(inf.data(), b.info, sizeof(int) * nc, cudaMemcpyDeviceToHost, st));
+        } else {
+            // ---- the whole wave as one CUDA graph: descriptors in, every bucket
+            // on its own stream (fork/join), results out; cached per shape.
+            if (!ctx.exec || ctx.sig != sig) {
+                if (ctx.exec) {
+                    cudaGraphExecDestroy(ctx.exec);
+                    ctx.exec = nullptr;
+                }
+                cudaGraph_t graph = nullptr;
+                CEL_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                celeris_rt::set_launch_counting(false);
+                uint64_t nk = 0;
+                for (size_t w = 0; w < wave.size(); ++w) {
+                    const BucketPlan& p = plans[wave[w]];
+                    const int nc = (int)p.ids.size();
+                    cudaStream_t bs = ctx.side[w];
+                    cudaEventRecord(ctx.fork[w], st);
+                    cudaStreamWaitEvent(bs, ctx.fork[w], 0);
+                    cudaMemcpyAsync(const_cast<CellDev*>(p.b.cells), hdesc[w], sizeof(CellDev) * nc,
+                                    cudaMemcpyHostToDevice, bs);
+                    launch_bucket(p.b, cfgs[w], bs, nullptr);
+                    nk += (p.ng > 0 ? 3 : 1) + 7;
+                    cudaMemcpyAsync(hres_pin[w], p.b.res, sizeof(celeris_rcwa_result) * nexc * nc,
+                                    cudaMemcpyDeviceToHost, bs);
+                    cudaMemcpyAsync(hinfo_pin[w], p.b.info, sizeof(int) * nc, cudaMemcpyDeviceToHost, bs);
+                    cudaEventRecord(ctx.join[w], bs);
+                    cudaStreamWaitEvent(st, ctx.join[w], 0);
+                }
+                const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+                celeris_rt::set_launch_counting(true);
+                if (ce != cudaSuccess) return celeris_rt::cuda_error(ce, "capture of the RCWA batch");
+                const cudaError_t ie = cudaGraphInstantiate(&ctx.exec, graph, 0);
+                cudaGraphDestroy(graph);
+                if (ie != cudaSuccess) {
+                    ctx.exec = nullptr;
+                    return celeris_rt::cuda_error(ie, "instantiate the RCWA batch graph");
+                }
+                ctx.sig = sig;
+                ctx.nkern = nk;
+            }
+            CEL_CUDA(cudaGraphLaunch(ctx.exec, st));
+            count_launch(ctx.nkern);
             CEL_CUDA(cudaStreamSynchronize(st));
-            for (int i = 0; i < nc; ++i) {
-                const int idx = cells[ids[c0 + i]].index;
-                for (int e = 0; e < nexc; ++e) hres[(size_t)idx * nexc + e] = r[(size_t)i * nexc + e];
-                hinfo[idx] = inf[i];
+        }
+        CEL_CUDA(cudaGetLastError());
+        for (size_t w = 0; w < wave.size(); ++w) {
+            const BucketPlan& p = plans[wave[w]];
+            for (int i = 0; i < (int)p.ids.size(); ++i) {
+                const int idx = cells[p.ids[i]].index;
+                for (int e = 0; e < nexc; ++e) hres[(size_t)idx * nexc + e] = hres_pin[w][(size_t)i * nexc + e];
+                hinfo[idx] = hinfo_pin[w][i];
             }
         }
     }
@@ -889,6 +1173,22 @@ int celeris_solve_rcwa_2d(const celeris_rcwa_cell* cell, const double* Ex0, cons
     CEL_TRY(validate(*cell));
     std::vector<HostCell> cells{make_cell(*cell, 0, Ex0[0], Ex0[1], Ey0[0], Ey0[1], 1)};
     return run_cells(cells, out, nullptr, 1);
+}
+
+int celeris_rcwa_tuning_report(char* buf, int len) {
+    if (!buf || len <= 0) return set_error(CELERIS_ERR_INVALID_ARG, "bad buffer");
+    std::string s;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (const auto& kv : tune_table()) {
+        s += "Mx=" + std::to_string(std::get<0>(kv.first)) + " My=" + std::to_string(std::get<1>(kv.first)) +
+             " grid=" + std::to_string(std::get<2>(kv.first) / 2) +
+             ((std::get<2>(kv.first) & 1) ? " batch>=SMs:" : " batch<SMs:");
+        for (int st = 0; st < ST_COUNT; ++st)
+            s += std::string(" ") + kStageNames[st] + "=" + std::to_string(kv.second.threads[st]);
+        s += "\n";
+    }
+    std::snprintf(buf, (size_t)len, "%s", s.c_str());
+    return CELERIS_OK;
 }
 
 int celeris_rcwa_batch(const celeris_rcwa_cell* cells, int ncell, celeris_rcwa_result* out, int* info) {

@@ -60,7 +60,13 @@ int require_device() {
     return CELERIS_OK;
 }
 
-void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+thread_local bool t_counting = true;
+
+void count_launch(uint64_t n) {
+    if (t_counting) g_launches.fetch_add(n, std::memory_order_relaxed);
+}
+
+void set_launch_counting(bool on) { t_counting = on; }
 
 int Workspace::reserve(cudaStream_t stream, size_t bytes) {
     off_ = 0;

@@ -33,7 +33,10 @@ int cuda_error(cudaError_t e, const char* where);
 int require_device();
 
 // ---- launch accounting ----------------------------------------------------
+// Kernels launched while the calling thread captures a CUDA graph are not
+// counted (set_launch_counting(false)); a graph launch counts its kernels.
 void count_launch(uint64_t n = 1);
+void set_launch_counting(bool on);
 
 // ---- workspace -------------------------------------------------------------
 // A bump allocator over one device buffer that belongs to (current device,

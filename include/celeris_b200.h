@@ -212,6 +212,12 @@ int celeris_solve_rcwa_2d(const celeris_rcwa_cell* cell, const double* Ex0,
 int celeris_rcwa_batch(const celeris_rcwa_cell* cells, int ncell,
                        celeris_rcwa_result* out, int* info);
 
+/* New: the autotuner's table (one line per bucket shape Mx, My, raster: the
+ * threads per CTA it chose for each RCWA stage), NUL-terminated into buf. The
+ * batch runs all buckets as one CUDA graph (one stream per bucket), captured on
+ * the first call for a given set of bucket shapes and replayed afterwards. */
+int celeris_rcwa_tuning_report(char* buf, int len);
+
 #ifdef __cplusplus
 }
 #endif

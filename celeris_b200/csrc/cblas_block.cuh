@@ -149,63 +149,108 @@ __device__ __forceinline__ int blk_argmax(double val, int idx, RedScratch* rs) {
 }
 
 // ---- GEMM -------------------------------------------------------------------------
-constexpr int GT = 32;  // output tile
-constexpr int GK = 16;  // k chunk
+// Register-tiled: the block is 16 x (NT/16) threads, each owning a 4 x 4 block of
+// outputs strided by 16 rows / NT/16 columns, so a 64 x (NT/4) output tile is
+// computed from k-chunks of GKC staged in shared memory. Per k step a thread reads
+// 4 A and 4 B values for 16 complex FMAs (shared-memory traffic a quarter of the
+// one-output-per-thread form). The next chunk is fetched into registers while the
+// current one is multiplied.
+constexpr int GM = 64;   // tile rows
+constexpr int GKC = 8;   // k chunk
 struct GemmSmem {
-    cplx a[GT][GK + 1];
-    cplx b[GK][GT + 1];
+    cplx a[GKC][GM + 1];  // A chunk transposed (k-major); +1 keeps the transposing store conflict-free
+    cplx b[GKC][64];
 };
 
-// C[m x n] = alpha * A[m x k] * B[k x n] + beta * C  (row-major). C may not alias A or B.
-__device__ void blk_gemm(int m, int n, int k, cplx alpha, const cplx* A, int lda, const cplx* B, int ldb,
-                         cplx beta, cplx* Cm, int ldc, GemmSmem* sm) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    // each thread owns outputs (r, c) of the tile with index tid + s*nt
-    const int per = (GT * GT + nt - 1) / nt;
-    __syncthreads();
-    for (int i0 = 0; i0 < m; i0 += GT) {
-        for (int j0 = 0; j0 < n; j0 += GT) {
-            cplx acc[8];
+template <int NT>
+__device__ __forceinline__ void gemm_tiles(int m, int n, int k, cplx alpha, const cplx* A, int lda, const cplx* B,
+                                           int ldb, cplx beta, cplx* Cm, int ldc, GemmSmem* sm) {
+    constexpr int TX = NT / 16, GN = 4 * TX, PA = GM * GKC / NT, PB = GKC * GN / NT;
+    const int tid = threadIdx.x;
+    const bool act = tid < NT;
+    const int ty = tid / TX, tx = tid % TX;
+    const int mt = (m + GM - 1) / GM, ntl = (n + GN - 1) / GN;
+    const bool use_beta = beta.x != 0.0 || beta.y != 0.0;
+    for (int t = 0; t < mt * ntl; ++t) {
+        const int i0 = (t / ntl) * GM, j0 = (t % ntl) * GN;
+        cplx acc[4][4];
 #pragma unroll
-            for (int s = 0; s < 8; ++s) acc[s] = C(0.0, 0.0);
-            for (int k0 = 0; k0 < k; k0 += GK) {
-                for (int e = tid; e < GT * GK; e += nt) {
-                    const int r = e / GK, c = e % GK;
-                    sm->a[r][c] = (i0 + r < m && k0 + c < k) ? A[(size_t)(i0 + r) * lda + k0 + c] : C(0.0, 0.0);
-                }
-                for (int e = tid; e < GK * GT; e += nt) {
-                    const int r = e / GT, c = e % GT;
-                    sm->b[r][c] = (k0 + r < k && j0 + c < n) ? B[(size_t)(k0 + r) * ldb + j0 + c] : C(0.0, 0.0);
-                }
-                __syncthreads();
+        for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int s = 0; s < 8; ++s) {
-                    if (s >= per) break;
-                    const int e = tid + s * nt;
-                    if (e >= GT * GT) break;
-                    const int r = e / GT, c = e % GT;
-                    cplx a = acc[s];
-#pragma unroll 4
-                    for (int kk = 0; kk < GK; ++kk) a = cfma(sm->a[r][kk], sm->b[kk][c], a);
-                    acc[s] = a;
-                }
-                __syncthreads();
+            for (int j = 0; j < 4; ++j) acc[i][j] = C(0.0, 0.0);
+        cplx ra[PA], rb[PB];
+        auto fetch = [&](int k0) {
+#pragma unroll
+            for (int s = 0; s < PA; ++s) {
+                const int e = tid + s * NT, r = e / GKC, c = e % GKC;
+                ra[s] = (act && i0 + r < m && k0 + c < k) ? A[(size_t)(i0 + r) * lda + k0 + c] : C(0.0, 0.0);
             }
 #pragma unroll
-            for (int s = 0; s < 8; ++s) {
-                if (s >= per) break;
-                const int e = tid + s * nt;
-                if (e >= GT * GT) break;
-                const int r = e / GT, c = e % GT;
-                if (i0 + r < m && j0 + c < n) {
-                    cplx* dst = &Cm[(size_t)(i0 + r) * ldc + j0 + c];
-                    cplx v = cmul(alpha, acc[s]);
-                    if (beta.x != 0.0 || beta.y != 0.0) v = cfma(beta, *dst, v);
-                    *dst = v;
+            for (int s = 0; s < PB; ++s) {
+                const int e = tid + s * NT, r = e / GN, c = e % GN;
+                rb[s] = (act && k0 + r < k && j0 + c < n) ? B[(size_t)(k0 + r) * ldb + j0 + c] : C(0.0, 0.0);
+            }
+        };
+        fetch(0);
+        for (int k0 = 0; k0 < k; k0 += GKC) {
+            if (act) {
+#pragma unroll
+                for (int s = 0; s < PA; ++s) {
+                    const int e = tid + s * NT;
+                    sm->a[e % GKC][e / GKC] = ra[s];
+                }
+#pragma unroll
+                for (int s = 0; s < PB; ++s) {
+                    const int e = tid + s * NT;
+                    sm->b[e / GN][e % GN] = rb[s];
+                }
+            }
+            __syncthreads();
+            if (k0 + GKC < k) fetch(k0 + GKC);
+            if (act) {
+#pragma unroll
+                for (int kk = 0; kk < GKC; ++kk) {
+                    cplx av[4], bv[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) av[i] = sm->a[kk][ty + 16 * i];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) bv[j] = sm->b[kk][tx + TX * j];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) acc[i][j] = cfma(av[i], bv[j], acc[i][j]);
+                }
+            }
+            __syncthreads();
+        }
+        if (act) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int r = i0 + ty + 16 * i;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int c = j0 + tx + TX * j;
+                    if (r < m && c < n) {
+                        cplx* dst = &Cm[(size_t)r * ldc + c];
+                        cplx v = cmul(alpha, acc[i][j]);
+                        if (use_beta) v = cfma(beta, *dst, v);
+                        *dst = v;
+                    }
                 }
             }
         }
     }
+}
+
+// C[m x n] = alpha * A[m x k] * B[k x n] + beta * C  (row-major). C may not alias A
+// or B. blockDim.x >= 128 (every kernel here runs 128 or 256 threads).
+__device__ void blk_gemm(int m, int n, int k, cplx alpha, const cplx* A, int lda, const cplx* B, int ldb,
+                         cplx beta, cplx* Cm, int ldc, GemmSmem* sm) {
+    __syncthreads();
+    if (blockDim.x >= 256)
+        gemm_tiles<256>(m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc, sm);
+    else
+        gemm_tiles<128>(m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc, sm);
     __syncthreads();
 }
 
@@ -357,6 +402,182 @@ __device__ __forceinline__ void blk_matvec_rows(int rows, int cols, const cplx* 
             }
             if (lane == 0 && i0 + r < rows) w[i0 + r] = cscale(acc[r], beta);
         }
+    }
+}
+
+// Two right-hand sides at once: w(i, r) (+)= sum_j A[i][j] v[j][r], r = 0, 1,
+// v row-major [cols][2] (shared memory), w(i, r) stored at w[i * wi + r * wr].
+// One warp per pair of rows, lanes over j (coalesced row reads).
+__device__ __forceinline__ void blk_matvec2(int rows, int cols, const cplx* A, int lda, const cplx* v, cplx* w,
+                                            size_t wi, size_t wr, bool accumulate) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int i0 = 2 * warp; i0 < rows; i0 += 2 * nwarp) {
+        cplx acc[2][2] = {{C(0.0, 0.0), C(0.0, 0.0)}, {C(0.0, 0.0), C(0.0, 0.0)}};
+        const bool two = i0 + 1 < rows;
+        for (int j = lane; j < cols; j += 32) {
+            const cplx v0 = v[2 * j], v1 = v[2 * j + 1];
+            const cplx a0 = A[(size_t)i0 * lda + j];
+            const cplx a1 = two ? A[(size_t)(i0 + 1) * lda + j] : C(0.0, 0.0);
+            acc[0][0] = cfma(a0, v0, acc[0][0]);
+            acc[0][1] = cfma(a0, v1, acc[0][1]);
+            acc[1][0] = cfma(a1, v0, acc[1][0]);
+            acc[1][1] = cfma(a1, v1, acc[1][1]);
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int r = 0; r < 2; ++r)
+                for (int o = 16; o > 0; o >>= 1) {
+                    acc[q][r].x += __shfl_down_sync(0xffffffffu, acc[q][r].x, o);
+                    acc[q][r].y += __shfl_down_sync(0xffffffffu, acc[q][r].y, o);
+                }
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                if (q == 1 && !two) break;
+#pragma unroll
+                for (int r = 0; r < 2; ++r) {
+                    cplx* dst = w + (size_t)(i0 + q) * wi + (size_t)r * wr;
+                    *dst = accumulate ? cadd(*dst, acc[q][r]) : acc[q][r];
+                }
+            }
+        }
+    }
+}
+
+// ---- blocked LU and solves ----------------------------------------------------------------
+// Column-wise triangular solves of a kb x kb diagonal block T (shared memory,
+// row-major kb x kb) against columns j0 .. j0+ncols-1 of the kb-row panel B: one
+// thread per column, in place (each thread rereads only what it wrote).
+__device__ __forceinline__ void trsm_unit_lower_cols(int kb, const cplx* T, cplx* B, int ldb, int j0, int ncols) {
+    for (int j = j0 + threadIdx.x; j < j0 + ncols; j += blockDim.x) {
+        cplx* col = B + j;
+        for (int r = 1; r < kb; ++r) {
+            cplx s = col[(size_t)r * ldb];
+            for (int c = 0; c < r; ++c) s = cfms(T[r * kb + c], col[(size_t)c * ldb], s);
+            col[(size_t)r * ldb] = s;
+        }
+    }
+}
+__device__ __forceinline__ void trsm_upper_cols(int kb, const cplx* T, cplx* B, int ldb, int j0, int ncols) {
+    for (int j = j0 + threadIdx.x; j < j0 + ncols; j += blockDim.x) {
+        cplx* col = B + j;
+        for (int r = kb - 1; r >= 0; --r) {
+            cplx s = col[(size_t)r * ldb];
+            for (int c = r + 1; c < kb; ++c) s = cfms(T[r * kb + c], col[(size_t)c * ldb], s);
+            col[(size_t)r * ldb] = cdiv(s, T[r * kb + r]);
+        }
+    }
+}
+
+// Right-looking LU with partial pivoting in panels of LNB columns: the panel is
+// factored with rank-1 steps (full rows swapped at once), the block row of U is
+// a small triangular solve, and the trailing matrix is updated by blk_gemm, so
+// the O(n^3) part is tiled through shared memory. Same pivot rule and same info
+// as blk_lu. stage: >= 2n + LNB*LNB complex of shared memory.
+constexpr int LNB = 16;
+
+__device__ int blk_lu_blocked(int n, cplx* A, int lda, int* piv, RedScratch* rs, cplx* stage, GemmSmem* gs) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    int info = 0;
+    cplx* colk = stage;
+    cplx* rowk = stage + n;
+    cplx* L11 = stage + 2 * n;
+    __syncthreads();
+    for (int k0 = 0; k0 < n; k0 += LNB) {
+        const int kb = min(LNB, n - k0);
+        for (int k = k0; k < k0 + kb; ++k) {
+            double best = -1.0;
+            int bi = k;
+            for (int i = k + tid; i < n; i += nt) {
+                const double v = cabs1(A[(size_t)i * lda + k]);
+                if (v > best) {
+                    best = v;
+                    bi = i;
+                }
+            }
+            const int p = blk_argmax(best, bi, rs);
+            if (tid == 0) piv[k] = p;
+            if (p != k) {
+                for (int j = tid; j < n; j += nt) {
+                    const cplx t = A[(size_t)k * lda + j];
+                    A[(size_t)k * lda + j] = A[(size_t)p * lda + j];
+                    A[(size_t)p * lda + j] = t;
+                }
+            }
+            __syncthreads();
+            const cplx akk = A[(size_t)k * lda + k];
+            const int m = n - k - 1, w = k0 + kb - 1 - k;  // rows below, panel columns right
+            if (akk.x == 0.0 && akk.y == 0.0) {
+                if (info == 0) info = k + 1;
+                __syncthreads();
+                continue;
+            }
+            const cplx inv = cinv(akk);
+            for (int i = tid; i < m; i += nt) {
+                const cplx l = cmul(A[(size_t)(k + 1 + i) * lda + k], inv);
+                A[(size_t)(k + 1 + i) * lda + k] = l;
+                colk[i] = l;
+            }
+            for (int j = tid; j < w; j += nt) rowk[j] = A[(size_t)k * lda + k + 1 + j];
+            __syncthreads();
+            if (w > 0) blk_rank1<false>(m, w, A + (size_t)(k + 1) * lda + k + 1, lda, colk, rowk);
+            __syncthreads();
+        }
+        const int r0 = k0 + kb, nr = n - r0;
+        if (nr <= 0) continue;
+        // U12 = L11^{-1} A12 (unit lower L11), one thread per column
+        for (int e = tid; e < kb * kb; e += nt) L11[e] = A[(size_t)(k0 + e / kb) * lda + k0 + e % kb];
+        __syncthreads();
+        trsm_unit_lower_cols(kb, L11, A + (size_t)k0 * lda, lda, r0, n - r0);
+        __syncthreads();
+        // A22 -= L21 U12
+        blk_gemm(nr, nr, kb, C(-1.0, 0.0), A + (size_t)r0 * lda + k0, lda, A + (size_t)k0 * lda + r0, lda,
+                 C(1.0, 0.0), A + (size_t)r0 * lda + r0, lda, gs);
+    }
+    return info;
+}
+
+// B (n x nrhs) <- A^{-1} B from the factors of blk_lu / blk_lu_blocked, by
+// block rows: a small triangular solve per block (one thread per RHS column)
+// and a blk_gemm update of the remaining rows. stage: >= LNB*LNB complex.
+__device__ void blk_lu_solve_blocked(int n, const cplx* LU, int lda, const int* piv, int nrhs, cplx* B, int ldb,
+                                     cplx* stage, GemmSmem* gs) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    cplx* Tkk = stage;
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        const int p = piv[k];
+        if (p != k)
+            for (int r = tid; r < nrhs; r += nt) {
+                const cplx t = B[(size_t)k * ldb + r];
+                B[(size_t)k * ldb + r] = B[(size_t)p * ldb + r];
+                B[(size_t)p * ldb + r] = t;
+            }
+        __syncthreads();
+    }
+    // forward: unit lower
+    for (int k0 = 0; k0 < n; k0 += LNB) {
+        const int kb = min(LNB, n - k0);
+        for (int e = tid; e < kb * kb; e += nt) Tkk[e] = LU[(size_t)(k0 + e / kb) * lda + k0 + e % kb];
+        __syncthreads();
+        trsm_unit_lower_cols(kb, Tkk, B + (size_t)k0 * ldb, ldb, 0, nrhs);
+        __syncthreads();
+        const int r0 = k0 + kb;
+        if (r0 < n)
+            blk_gemm(n - r0, nrhs, kb, C(-1.0, 0.0), LU + (size_t)r0 * lda + k0, lda, B + (size_t)k0 * ldb, ldb,
+                     C(1.0, 0.0), B + (size_t)r0 * ldb, ldb, gs);
+    }
+    // backward: upper (with diagonal)
+    const int nblk = (n + LNB - 1) / LNB;
+    for (int bI = nblk - 1; bI >= 0; --bI) {
+        const int k0 = bI * LNB, kb = min(LNB, n - k0);
+        for (int e = tid; e < kb * kb; e += nt) Tkk[e] = LU[(size_t)(k0 + e / kb) * lda + k0 + e % kb];
+        __syncthreads();
+        trsm_upper_cols(kb, Tkk, B + (size_t)k0 * ldb, ldb, 0, nrhs);
+        __syncthreads();
+        if (k0 > 0)
+            blk_gemm(k0, nrhs, kb, C(-1.0, 0.0), LU + k0, lda, B + (size_t)k0 * ldb, ldb, C(1.0, 0.0), B, ldb, gs);
     }
 }
 

@@ -63,7 +63,7 @@ struct CellDev {
 struct Bucket {
     int Mx, My, N, n, ng, ncell;
     const CellDev* cells;
-    cplx *H, *Z, *X, *W, *A, *T11, *T11lu, *T12, *S12, *Winv, *Ainv, *B;
+    cplx *H, *Z, *X, *W, *A, *T11, *T11lu, *T12, *S12;
     cplx *Einv, *Exx, *Eyy;
     cplx* q1;
     int* piv;
@@ -284,10 +284,13 @@ __global__ void __launch_bounds__(kRT) rcwa_fourier_laurent(Bucket b) {
         Einv[e] = C(r == col ? 1.0 : 0.0, 0.0);
     }
     __syncthreads();
+    // the raster, G1 and Ge are dead: the LU staging and GEMM tiles overlay them
+    cplx* stg = reinterpret_cast<cplx*>(smem);
+    GemmSmem* gs = reinterpret_cast<GemmSmem*>(stg + 2 * N + LNB * LNB);
     int* piv = b.piv + b.s_n * cell;
-    const int info = blk_lu(N, lu, N, piv, &rs, G1);  // G1 is dead: LU staging
+    const int info = blk_lu_blocked(N, lu, N, piv, &rs, stg, gs);
     if (info != 0 && tid == 0) b.info[cell] = -info;
-    blk_lu_solve(N, lu, N, piv, N, Einv, N, G1);  // Einv = epsT^{-1} (rcwa2d.cpp:203)
+    blk_lu_solve_blocked(N, lu, N, piv, N, Einv, N, stg, gs);  // Einv = epsT^{-1} (rcwa2d.cpp:203)
 }
 
 // ---- M = ep2 kp - kkT -------------------------------------------------------------
@@ -402,7 +405,7 @@ __global__ void __launch_bounds__(kRT) rcwa_vec(Bucket b) {
 }
 
 // ---- S-matrix, interface 0 --------------------------------------------------------------
-// dynamic smem: LU staging (2n + 2 complex)
+// dynamic smem: LU staging (2n + LNB^2 complex)
 __global__ void __launch_bounds__(kRT) rcwa_smat1(Bucket b) {
     extern __shared__ __align__(16) unsigned char smem[];
     cplx* stg = reinterpret_cast<cplx*>(smem);
@@ -477,13 +480,23 @@ __global__ void __launch_bounds__(kRT) rcwa_smat1(Bucket b) {
     }
     __syncthreads();
     int* piv = b.piv + b.s_n * cell;
-    const int info = blk_lu(n, T11lu, n, piv, &rs, stg);
+    const int info = blk_lu_blocked(n, T11lu, n, piv, &rs, stg, &gs);
     if (info != 0 && tid == 0) b.info[cell] = -info;
-    blk_lu_solve(n, T11lu, n, piv, ld, S, ld, stg);  // [S12 | u_X | u_Y]
+    blk_lu_solve_blocked(n, T11lu, n, piv, ld, S, ld, stg, &gs);  // [S12 | u_X | u_Y]
 }
 
 // ---- S-matrix, interface 1 + exterior amplitudes --------------------------------------------
-// dynamic smem: LU staging (2n + 2 complex)
+// The layer -> substrate interface in the reference's form (rcwa2d.cpp:394-410) is
+// T11' = (W^-1 + P')/2, T12' = (W^-1 - P')/2 with P' = diag(q1) A^-1 K, K the
+// substrate kp diag(1/kz) blocks; the exterior amplitudes solve
+// (T11' - D S12 T12') aN = D u, D = diag(exp(i q1 h)). With aN = W y the
+// inverse of W drops out: T11' aN = (y + Q y)/2, T12' aN = (y - Q y)/2 with
+// Q = diag(q1) A^-1 K W, so
+//     (I + Q - D S12 + D S12 Q) y = 2 D u,   aN = W y,   y2 = T12' aN = (y - Q y)/2,
+//     b0 = T12 (u + S12 y2) + T11 D y2.
+// One LU of A with n right-hand sides, one GEMM and one LU of the combined
+// matrix (instead of two inverses, a GEMM and an LU).
+// dynamic smem: staging (2n + LNB^2 complex)
 __global__ void __launch_bounds__(kRT) rcwa_smat2(Bucket b) {
     extern __shared__ __align__(16) unsigned char smem[];
     cplx* stg = reinterpret_cast<cplx*>(smem);
@@ -493,90 +506,79 @@ __global__ void __launch_bounds__(kRT) rcwa_smat2(Bucket b) {
     const CellDev c = b.cells[cell];
     const int N = b.N, n = b.n;
     const int tid = threadIdx.x, nt = blockDim.x;
-    cplx* W = at(b.W, b.s_nn, cell);
+    const cplx* W = at(b.W, b.s_nn, cell);
     cplx* A = at(b.A, b.s_nn, cell);
-    cplx* Winv = at(b.Winv, b.s_nn, cell);
-    cplx* Ainv = at(b.Ainv, b.s_nn, cell);
+    cplx* Q = at(b.H, b.s_nn, cell);   // K W, then Q (H, Z, X are dead after the eigenvectors)
+    cplx* SQ = at(b.Z, b.s_nn, cell);  // S12 Q
+    cplx* Cm = at(b.X, b.s_nn, cell);  // I + Q - D S12 + D S12 Q, then its LU
     const cplx* q1 = at(b.q1, b.s_n, cell);
     int* piv = b.piv + b.s_n * cell;
-    for (int e = tid; e < n * n; e += nt) {
-        const int i = e / n, j = e % n;
-        Winv[e] = C(i == j ? 1.0 : 0.0, 0.0);
-        Ainv[e] = C(i == j ? 1.0 : 0.0, 0.0);
-    }
-    int info = blk_lu(n, W, n, piv, &rs, stg);
-    blk_lu_solve(n, W, n, piv, n, Winv, n, stg);
-    int info2 = blk_lu(n, A, n, piv, &rs, stg);
-    blk_lu_solve(n, A, n, piv, n, Ainv, n, stg);
-    if (tid == 0 && (info || info2)) b.info[cell] = -(info ? info : info2);
-    // P' = diag(q1) A^{-1} kp2 diag(1/q2): T11' -> Winv, T12' -> Ainv (in place)
+    // K W: rows m and N+m mix through the substrate kp block of order m over kz_m
     const cplx ier = cinv(cmul(c.n_sub, c.n_sub));
     const cplx er = cmul(c.n_sub, c.n_sub);
-    for (int e = tid; e < n * N; e += nt) {
-        const int i = e / N, m = e % N;
+    for (int e = tid; e < N * n; e += nt) {
+        const int m = e / n, j = e % n;
         const cplx kx = kx_of(b, c, m), ky = ky_of(b, c, m);
         cplx ka, kb, kc, kd;
         kp_uniform(ier, c.omega, kx, ky, ka, kb, kc, kd);
         const cplx iq2 = cinv(kz_uniform(er, c.omega, kx, ky));
-        const cplx x0 = Ainv[(size_t)i * n + m], x1 = Ainv[(size_t)i * n + N + m];
-        const cplx pa = cmul(cmul(q1[i], cfma(x0, ka, cmul(x1, kc))), iq2);
-        const cplx pb = cmul(cmul(q1[i], cfma(x0, kb, cmul(x1, kd))), iq2);
-        const cplx wa = Winv[(size_t)i * n + m], wb = Winv[(size_t)i * n + N + m];
-        Winv[(size_t)i * n + m] = cscale(cadd(wa, pa), 0.5);
-        Winv[(size_t)i * n + N + m] = cscale(cadd(wb, pb), 0.5);
-        Ainv[(size_t)i * n + m] = cscale(csub(wa, pa), 0.5);
-        Ainv[(size_t)i * n + N + m] = cscale(csub(wb, pb), 0.5);
+        const cplx w0 = W[(size_t)m * n + j], w1 = W[(size_t)(N + m) * n + j];
+        Q[(size_t)m * n + j] = cmul(cfma(ka, w0, cmul(kb, w1)), iq2);
+        Q[(size_t)(N + m) * n + j] = cmul(cfma(kc, w0, cmul(kd, w1)), iq2);
     }
-    __syncthreads();
-    const cplx* T11p = Winv;
-    const cplx* T12p = Ainv;
+    int info = blk_lu_blocked(n, A, n, piv, &rs, stg, &gs);
+    blk_lu_solve_blocked(n, A, n, piv, n, Q, n, stg, &gs);  // A^-1 K W
+    if (tid == 0 && info) b.info[cell] = -info;
+    for (int e = tid; e < n * n; e += nt) Q[e] = cmul(q1[e / n], Q[e]);
     cplx* S = at(b.S12, b.s_ns, cell);
     const int ld = n + 2;
-    cplx* Bm = at(b.B, b.s_nn, cell);
-    // B = T11' - D (S12 T12')
-    blk_gemm(n, n, n, C(1.0, 0.0), S, ld, T12p, n, C(0.0, 0.0), Bm, n, &gs);
-    for (int e = tid; e < n * n; e += nt) Bm[e] = cfms(cexpi(cscale(q1[e / n], c.h)), Bm[e], T11p[e]);
-    // rhs = D u  (2 columns) into vec scratch [n x 2]
+    blk_gemm(n, n, n, C(1.0, 0.0), S, ld, Q, n, C(0.0, 0.0), SQ, n, &gs);
+    for (int e = tid; e < n * n; e += nt) {
+        const int i = e / n, j = e % n;
+        const cplx d = cexpi(cscale(q1[i], c.h));
+        cplx v = cadd(Q[e], cmul(d, csub(SQ[e], S[(size_t)i * ld + j])));
+        if (i == j) v.x += 1.0;
+        Cm[e] = v;
+    }
+    // rhs = 2 D u (2 columns) into vec scratch [n x 2]
     cplx* vec = at(b.vec, 10 * b.s_n, cell);
-    cplx* x = vec + 4 * (size_t)b.s_n;  // [n x 2] row-major
+    cplx* x = vec + 4 * (size_t)b.s_n;    // [n x 2] row-major: y
+    cplx* y2 = vec + 6 * (size_t)b.s_n;   // [n x 2]: Q y, then y2
+    cplx* zz = vec + 8 * (size_t)b.s_n;   // [n x 2]: u + S12 y2
     for (int e = tid; e < 2 * n; e += nt) {
         const int i = e / 2, r = e % 2;
-        x[e] = cmul(cexpi(cscale(q1[i], c.h)), S[(size_t)i * ld + n + r]);
+        x[e] = cscale(cmul(cexpi(cscale(q1[i], c.h)), S[(size_t)i * ld + n + r]), 2.0);
     }
-    info = blk_lu(n, Bm, n, piv, &rs, stg);
+    info = blk_lu_blocked(n, Cm, n, piv, &rs, stg, &gs);
     if (tid == 0 && info) b.info[cell] = -info;
-    blk_lu_solve(n, Bm, n, piv, 2, x, 2, stg);  // x = aN (X, Y)
-    // y = T12' x ; z = S12 y ; b0 = T12 (u + z) + T11 (D y)
-    cplx* y = vec + 6 * (size_t)b.s_n;   // [n x 2]
-    cplx* zz = vec + 8 * (size_t)b.s_n;  // [n x 2]
-    for (int e = tid; e < 2 * n; e += nt) {
-        const int i = e / 2, r = e % 2;
-        cplx s = C(0.0, 0.0);
-        for (int k = 0; k < n; ++k) s = cfma(T12p[(size_t)i * n + k], x[k * 2 + r], s);
-        y[e] = s;
-    }
-    __syncthreads();
-    for (int e = tid; e < 2 * n; e += nt) {
-        const int i = e / 2, r = e % 2;
-        cplx s = S[(size_t)i * ld + n + r];  // u
-        for (int k = 0; k < n; ++k) s = cfma(S[(size_t)i * ld + k], y[k * 2 + r], s);
-        zz[e] = s;  // u + S12 y
-    }
-    __syncthreads();
-    const cplx* T11 = at(b.T11, b.s_nn, cell);
-    const cplx* T12 = at(b.T12, b.s_nn, cell);
+    blk_lu_solve_blocked(n, Cm, n, piv, 2, x, 2, stg, &gs);  // x = y (X, Y)
     cplx* aN = vec;                      // [2][n]
     cplx* b0 = vec + 2 * (size_t)b.s_n;  // [2][n]
+    for (int e = tid; e < 2 * n; e += nt) stg[e] = x[e];
+    __syncthreads();
+    blk_matvec2(n, n, W, n, stg, aN, 1, b.s_n, false);  // aN = W y
+    blk_matvec2(n, n, Q, n, stg, y2, 2, 1, false);      // Q y
+    __syncthreads();
     for (int e = tid; e < 2 * n; e += nt) {
-        const int i = e / 2, r = e % 2;
-        cplx s = C(0.0, 0.0);
-        for (int k = 0; k < n; ++k) {
-            s = cfma(T12[(size_t)i * n + k], zz[k * 2 + r], s);
-            s = cfma(T11[(size_t)i * n + k], cmul(cexpi(cscale(q1[k], c.h)), y[k * 2 + r]), s);
-        }
-        b0[(size_t)r * b.s_n + i] = s;
-        aN[(size_t)r * b.s_n + i] = x[e];
+        const cplx v = cscale(csub(stg[e], y2[e]), 0.5);
+        y2[e] = v;
+        zz[e] = S[(size_t)(e / 2) * ld + n + (e % 2)];  // u
     }
+    __syncthreads();
+    for (int e = tid; e < 2 * n; e += nt) stg[e] = y2[e];
+    __syncthreads();
+    blk_matvec2(n, n, S, ld, stg, zz, 2, 1, true);  // u + S12 y2
+    __syncthreads();
+    // b0 = T12 zz + T11 (D y2)
+    const cplx* T11 = at(b.T11, b.s_nn, cell);
+    const cplx* T12 = at(b.T12, b.s_nn, cell);
+    for (int e = tid; e < 2 * n; e += nt) stg[e] = zz[e];
+    __syncthreads();
+    blk_matvec2(n, n, T12, n, stg, b0, 1, b.s_n, false);
+    __syncthreads();
+    for (int e = tid; e < 2 * n; e += nt) stg[e] = cmul(cexpi(cscale(q1[e / 2], c.h)), y2[e]);
+    __syncthreads();
+    blk_matvec2(n, n, T11, n, stg, b0, 1, b.s_n, true);
 }
 
 // ---- flux and order-0 field (rcwa2d.cpp:416-463) ---------------------------------------------
@@ -712,9 +714,14 @@ HostCell make_cell(const celeris_rcwa_cell& c, int index, double ex_re, double e
     return h;
 }
 
+// staging of blk_lu_blocked and the matvecs of the S-matrix kernels
+size_t lu_stage_bytes(int n) { return (size_t)(2 * n + LNB * LNB) * sizeof(cplx); }
+
 size_t laurent_smem(int Mx, int My, int ng) {
     const size_t mx4 = 4 * Mx + 1, my4 = 4 * My + 1;
-    return (mx4 * ng + mx4 * my4) * sizeof(cplx) + (size_t)ng * ng;
+    const int N = (2 * Mx + 1) * (2 * My + 1);
+    const size_t raster = (mx4 * ng + mx4 * my4) * sizeof(cplx) + (size_t)ng * ng;
+    return std::max(raster, lu_stage_bytes(N) + sizeof(GemmSmem));
 }
 
 // ---- stage configuration and autotuning -------------------------------------------------
@@ -757,7 +764,7 @@ struct BucketPlan {
 size_t per_cell_bytes(int n, int nexc) {
     const int N = n / 2;
     const size_t s_nn = (size_t)n * n, s_ns = (size_t)n * (n + 2), s_NN = (size_t)N * N, s_n = (size_t)n;
-    return celeris_rt::align256((11 * s_nn + s_ns + 3 * s_NN + 11 * s_n) * sizeof(cplx)) +
+    return celeris_rt::align256((8 * s_nn + s_ns + 3 * s_NN + 11 * s_n) * sizeof(cplx)) +
            celeris_rt::align256(s_n * sizeof(int)) + 256 + celeris_rt::align256(sizeof(celeris_rcwa_result) * nexc) +
            celeris_rt::align256(sizeof(CellDev)) + 14 * 256;
 }
@@ -774,7 +781,7 @@ struct SmemNeeds {
             rect = std::max(rect, ((size_t)2 * (nx * nx + ny * ny) + 2 * std::max(nx, ny)) * sizeof(cplx));
         }
         if (n <= kSmemEigMaxN) hess_s = std::max(hess_s, ((size_t)n * n + 2 * n) * sizeof(cplx));
-        smat = std::max(smat, (size_t)(2 * n + 2) * sizeof(cplx));
+        smat = std::max(smat, lu_stage_bytes(n));
     }
 };
 
@@ -829,7 +836,7 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
     if (ev) cudaEventRecord(ev[4], st);
     rcwa_vec<<<nc, T[ST_VEC], 0, st>>>(b);
     if (ev) cudaEventRecord(ev[5], st);
-    const size_t sm_stage = (size_t)(2 * n + 2) * sizeof(cplx);
+    const size_t sm_stage = lu_stage_bytes(n);
     rcwa_smat1<<<nc, T[ST_SMAT1], sm_stage, st>>>(b);
     if (ev) cudaEventRecord(ev[6], st);
     rcwa_smat2<<<nc, T[ST_SMAT2], sm_stage, st>>>(b);
@@ -1004,7 +1011,7 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
             b.s_n = (size_t)p.n;
             CellDev* dcells = static_cast<CellDev*>(ws.take(sizeof(CellDev) * nc));
             b.cells = dcells;
-            cplx** mats[] = {&b.H, &b.Z, &b.X, &b.W, &b.A, &b.T11, &b.T11lu, &b.T12, &b.Winv, &b.Ainv, &b.B};
+            cplx** mats[] = {&b.H, &b.Z, &b.X, &b.W, &b.A, &b.T11, &b.T11lu, &b.T12};
             for (cplx** m : mats) *m = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_nn * nc));
             b.S12 = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_ns * nc));
             b.Einv = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_NN * nc));

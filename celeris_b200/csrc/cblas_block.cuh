@@ -644,6 +644,159 @@ __device__ void blk_hessenberg(int n, cplx* H, int ldh, cplx* Z, int ldz, cplx* 
     }
 }
 
+// Blocked Householder reduction (panels of LNB columns, compact WY form).
+// Reflector P_j = I - b_j v_j v_j^H (b_j real, P_j Hermitian) as in
+// blk_hessenberg; a panel's product is Q = I - V T V^H with T upper triangular.
+// For each panel column the right update by the earlier reflectors uses
+// Y = A V T (A at the panel start), the left update applies Q_prev^H to that
+// column only, and Y gains A v_j by one matrix-vector product over the columns
+// right of it (untouched within the panel). After the panel the trailing
+// columns get A <- A - Y V^H, then A <- (I - V T^H V^H) A, and Z <- Z - (Z V T) V^H,
+// all by blk_gemm. Memory traffic per column is one read of the trailing
+// matrix (the product A v_j) plus 1/LNB of a few passes for the GEMMs, against
+// ~8 passes for rank-1 updates.
+// scratch (global, >= 5 * LNB * n complex); stage (shared, >= n + LNB^2 + 2 LNB complex).
+__device__ void blk_hessenberg_blocked(int n, cplx* H, int ldh, cplx* Z, int ldz, cplx* scratch, cplx* stage,
+                                       RedScratch* rs, GemmSmem* gs) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int warp = tid >> 5, lane = tid & 31, nwarp = nt >> 5;
+    constexpr int NB = LNB;
+    cplx* V = scratch;                    // [m x NB] (row r <-> index k+1+r)
+    cplx* VH = V + (size_t)NB * n;        // [NB x n]: conj(V)^T, leading dimension n
+    cplx* Y = VH + (size_t)NB * n;        // [n x NB]
+    cplx* Wt = Y + (size_t)NB * n;        // [NB x n]
+    cplx* P = Wt + (size_t)NB * n;        // [n x NB]
+    cplx* v = stage;                      // [n] current reflector (index i+1 .. n-1)
+    cplx* Tm = stage + n;                 // [NB x NB]
+    cplx* u = Tm + NB * NB;               // [NB]
+    cplx* wv = u + NB;                    // [NB]
+    for (int e = tid; e < n * n; e += nt) {
+        const int i = e / n, j = e % n;
+        Z[(size_t)i * ldz + j] = C(i == j ? 1.0 : 0.0, 0.0);
+    }
+    __syncthreads();
+    for (int k = 0; k + 2 < n; k += NB) {
+        const int kb = min(NB, n - 2 - k);
+        const int m = n - k - 1;
+        for (int e = tid; e < m * NB; e += nt) V[e] = C(0.0, 0.0);
+        for (int e = tid; e < NB * NB; e += nt) Tm[e] = C(0.0, 0.0);
+        __syncthreads();
+        for (int j = 0; j < kb; ++j) {
+            const int i = k + j;
+            if (j > 0) {
+                // (1) column i <- column i of A Q_prev:  H[:, i] -= Y[:, :j] conj(V[j-1, :j])
+                for (int r = tid; r < n; r += nt) {
+                    cplx s = H[(size_t)r * ldh + i];
+                    for (int l = 0; l < j; ++l) s = csub(s, cmul(Y[(size_t)r * NB + l], cconj(V[(size_t)(j - 1) * NB + l])));
+                    H[(size_t)r * ldh + i] = s;
+                }
+                __syncthreads();
+                // (2) rows k+1.. of column i <- Q_prev^H b = b - V T^H (V^H b)
+                for (int l = warp; l < j; l += nwarp) {
+                    cplx s = C(0.0, 0.0);
+                    for (int r = l + lane; r < m; r += 32)
+                        s = cfma(cconj(V[(size_t)r * NB + l]), H[(size_t)(k + 1 + r) * ldh + i], s);
+                    for (int o = 16; o > 0; o >>= 1) {
+                        s.x += __shfl_down_sync(0xffffffffu, s.x, o);
+                        s.y += __shfl_down_sync(0xffffffffu, s.y, o);
+                    }
+                    if (lane == 0) u[l] = s;
+                }
+                __syncthreads();
+                if (tid < j) {  // wv = T^H u (T upper: (T^H)[l][p] = conj(T[p][l]), p <= l)
+                    cplx s = C(0.0, 0.0);
+                    for (int p = 0; p <= tid; ++p) s = cfma(cconj(Tm[p * NB + tid]), u[p], s);
+                    wv[tid] = s;
+                }
+                __syncthreads();
+                for (int r = tid; r < m; r += nt) {
+                    cplx s = H[(size_t)(k + 1 + r) * ldh + i];
+                    for (int l = 0; l < j; ++l) s = csub(s, cmul(V[(size_t)r * NB + l], wv[l]));
+                    H[(size_t)(k + 1 + r) * ldh + i] = s;
+                }
+                __syncthreads();
+            }
+            // (3) reflector from x = H[i+1:, i]
+            const int mx = n - i - 1;
+            double s2 = 0.0;
+            for (int r = tid; r < mx; r += nt) s2 += cnorm2(H[(size_t)(i + 1 + r) * ldh + i]);
+            const double xnorm2 = blk_sum(s2, rs);
+            const cplx x0 = H[(size_t)(i + 1) * ldh + i];
+            const double tail = xnorm2 - cnorm2(x0);
+            double beta = 0.0;
+            cplx alpha = x0, v0 = C(0.0, 0.0);
+            if (tail > 0.0) {
+                const double xn = sqrt(xnorm2), ax0 = cabs(x0);
+                const cplx ph = ax0 > 0.0 ? cscale(x0, 1.0 / ax0) : C(1.0, 0.0);
+                alpha = cscale(ph, -xn);
+                v0 = csub(x0, alpha);
+                beta = 2.0 / (tail + cnorm2(v0));
+            }
+            for (int r = tid; r < mx; r += nt) {
+                const cplx vr = beta == 0.0 ? C(0.0, 0.0) : (r == 0 ? v0 : H[(size_t)(i + 1 + r) * ldh + i]);
+                v[r] = vr;
+                V[(size_t)(j + r) * NB + j] = vr;
+            }
+            __syncthreads();
+            for (int r = tid; r < mx; r += nt) H[(size_t)(i + 1 + r) * ldh + i] = (r == 0) ? alpha : C(0.0, 0.0);
+            // (4) u = V_prev^H v_j; Y[:, j] = beta (A v_j - Y_prev u); T[:j, j] = -beta T_prev u
+            for (int l = warp; l < j; l += nwarp) {
+                cplx s = C(0.0, 0.0);
+                for (int r = j + lane; r < m; r += 32) s = cfma(cconj(V[(size_t)r * NB + l]), v[r - j], s);
+                for (int o = 16; o > 0; o >>= 1) {
+                    s.x += __shfl_down_sync(0xffffffffu, s.x, o);
+                    s.y += __shfl_down_sync(0xffffffffu, s.y, o);
+                }
+                if (lane == 0) u[l] = s;
+            }
+            blk_matvec_rows(n, mx, H + i + 1, ldh, v, P, 1.0, warp, lane, nwarp);  // P[:n] as a vector
+            __syncthreads();
+            if (tid < j) {
+                cplx s = C(0.0, 0.0);
+                for (int p = tid; p < j; ++p) s = cfma(Tm[tid * NB + p], u[p], s);
+                wv[tid] = cscale(s, -beta);
+            }
+            for (int r = tid; r < n; r += nt) {
+                cplx s = P[r];
+                for (int l = 0; l < j; ++l) s = csub(s, cmul(Y[(size_t)r * NB + l], u[l]));
+                Y[(size_t)r * NB + j] = cscale(s, beta);
+            }
+            __syncthreads();
+            if (tid < j) Tm[tid * NB + j] = wv[tid];
+            if (tid == 0) Tm[j * NB + j] = C(beta, 0.0);
+            __syncthreads();
+        }
+        for (int e = tid; e < NB * m; e += nt) {
+            const int l = e / m, r = e % m;
+            VH[(size_t)l * n + r] = l < kb ? cconj(V[(size_t)r * NB + l]) : C(0.0, 0.0);
+        }
+        // (5) trailing columns c >= k+kb  (V row kb-1 <-> index k+kb)
+        const int c0 = k + kb, nc = n - c0;
+        if (nc > 0) {
+            blk_gemm(n, nc, kb, C(-1.0, 0.0), Y, NB, VH + (kb - 1), n, C(1.0, 0.0), H + c0, ldh, gs);  // A -= Y V^H
+            blk_gemm(kb, nc, m, C(1.0, 0.0), VH, n, H + (size_t)(k + 1) * ldh + c0, ldh, C(0.0, 0.0), Wt, n, gs);
+            for (int c = tid; c < nc; c += nt) {  // Wt <- T^H Wt, rows from the bottom up
+                for (int l = kb - 1; l >= 0; --l) {
+                    cplx s = C(0.0, 0.0);
+                    for (int p = 0; p <= l; ++p) s = cfma(cconj(Tm[p * NB + l]), Wt[(size_t)p * n + c], s);
+                    Wt[(size_t)l * n + c] = s;
+                }
+            }
+            blk_gemm(m, nc, kb, C(-1.0, 0.0), V, NB, Wt, n, C(1.0, 0.0), H + (size_t)(k + 1) * ldh + c0, ldh, gs);
+        }
+        // Z[:, k+1:] <- Z[:, k+1:] - (Z V T) V^H
+        blk_gemm(n, kb, m, C(1.0, 0.0), Z + k + 1, ldz, V, NB, C(0.0, 0.0), P, NB, gs);
+        for (int r = tid; r < n; r += nt) {  // P <- P T, columns from the right
+            for (int l = kb - 1; l >= 0; --l) {
+                cplx s = C(0.0, 0.0);
+                for (int p = 0; p <= l; ++p) s = cfma(P[(size_t)r * NB + p], Tm[p * NB + l], s);
+                P[(size_t)r * NB + l] = s;
+            }
+        }
+        blk_gemm(n, m, kb, C(-1.0, 0.0), P, NB, VH, n, C(1.0, 0.0), Z + k + 1, ldz, gs);
+    }
+}
+
 // ---- complex Schur by shifted QR ------------------------------------------------------
 // Givens G = [[c, s], [-conj(s), c]] with G [a; b] = [r; 0], c real.
 // c = |a| / r, s = a conj(b) / (|a| r), r = sqrt(|a|^2 + |b|^2), formed with

@@ -340,7 +340,9 @@ __global__ void __launch_bounds__(kRT) rcwa_build_M(Bucket b, int laurent) {
 // Three kernels so that each gets its own register budget (the bulge chase
 // keeps 16-element row/column segments in registers). SMEM variants (n <= 112)
 // stage H in shared memory for the duration of the kernel.
-// dynamic smem: SMEM: H [n*n] | v [n] | w [n]; otherwise v [n] | w [n].
+// dynamic smem: SMEM: H [n*n] | v [n] | w [n] (rank-1 updates on the shared
+// copy); otherwise the staging of blk_hessenberg_blocked (scratch in X, which
+// is free until the eigenvectors).
 template <bool SMEM>
 __global__ void __launch_bounds__(kRT) rcwa_hess(Bucket b) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -349,16 +351,18 @@ __global__ void __launch_bounds__(kRT) rcwa_hess(Bucket b) {
     const int n = b.n;
     const int tid = threadIdx.x, nt = blockDim.x;
     cplx* Hg = at(b.H, b.s_nn, cell);
-    cplx* H = SMEM ? reinterpret_cast<cplx*>(smem) : Hg;
-    cplx* v = SMEM ? H + (size_t)n * n : reinterpret_cast<cplx*>(smem);
-    if (SMEM) {
+    if constexpr (SMEM) {
+        cplx* H = reinterpret_cast<cplx*>(smem);
+        cplx* v = H + (size_t)n * n;
         for (int e = tid; e < n * n; e += nt) H[e] = Hg[e];
         __syncthreads();
-    }
-    blk_hessenberg(n, H, n, at(b.Z, b.s_nn, cell), n, v, v + n, &rs);
-    if (SMEM) {
+        blk_hessenberg(n, H, n, at(b.Z, b.s_nn, cell), n, v, v + n, &rs);
         __syncthreads();
         for (int e = tid; e < n * n; e += nt) Hg[e] = H[e];
+    } else {
+        __shared__ GemmSmem gs;
+        blk_hessenberg_blocked(n, Hg, n, at(b.Z, b.s_nn, cell), n, at(b.X, b.s_nn, cell),
+                               reinterpret_cast<cplx*>(smem), &rs, &gs);
     }
 }
 
@@ -714,6 +718,9 @@ HostCell make_cell(const celeris_rcwa_cell& c, int index, double ex_re, double e
     return h;
 }
 
+// staging of blk_hessenberg_blocked
+size_t hess_stage_bytes(int n) { return (size_t)(n + LNB * LNB + 2 * LNB) * sizeof(cplx); }
+
 // staging of blk_lu_blocked and the matvecs of the S-matrix kernels
 size_t lu_stage_bytes(int n) { return (size_t)(2 * n + LNB * LNB) * sizeof(cplx); }
 
@@ -829,7 +836,7 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
         if (ev) cudaEventRecord(ev[3], st);
         rcwa_schur<true><<<nc, T[ST_SCHUR], sm, st>>>(b);
     } else {
-        rcwa_hess<false><<<nc, T[ST_HESS], 2 * n * sizeof(cplx), st>>>(b);
+        rcwa_hess<false><<<nc, T[ST_HESS], hess_stage_bytes(n), st>>>(b);
         if (ev) cudaEventRecord(ev[3], st);
         rcwa_schur<false><<<nc, T[ST_SCHUR], 0, st>>>(b);
     }

@@ -34,6 +34,7 @@
 #include <vector>
 
 #include "cblas_block.cuh"
+#include "schur_aed.cuh"
 #include "runtime.cuh"
 
 namespace {
@@ -366,24 +367,31 @@ __global__ void __launch_bounds__(kRT) rcwa_hess(Bucket b) {
     }
 }
 
-// dynamic smem: SMEM: H [n*n]; otherwise none.
+// dynamic smem: SMEM: H [n*n] (windowed single-shift QR on the shared copy);
+// otherwise the AedShared block of the multishift/AED Schur form.
 template <bool SMEM>
 __global__ void __launch_bounds__(kRT) rcwa_schur(Bucket b) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ SchurShared sh;
     const int cell = blockIdx.x;
     const int n = b.n;
     const int tid = threadIdx.x, nt = blockDim.x;
     cplx* Hg = at(b.H, b.s_nn, cell);
     cplx* H = SMEM ? reinterpret_cast<cplx*>(smem) : Hg;
-    if (SMEM) {
+    int info, nsweep;
+    if constexpr (SMEM) {
+        __shared__ SchurShared sh;
         for (int e = tid; e < n * n; e += nt) H[e] = Hg[e];
         __syncthreads();
+        info = blk_schur(n, H, n, at(b.Z, b.s_nn, cell), n, &sh, kMaxSweepsPerRow);
+        nsweep = sh.nsweep;
+    } else {
+        AedShared* sh = reinterpret_cast<AedShared*>(smem);
+        info = blk_schur_aed(n, H, n, at(b.Z, b.s_nn, cell), n, sh);
+        nsweep = sh->nsweep;
     }
-    const int info = blk_schur(n, H, n, at(b.Z, b.s_nn, cell), n, &sh, kMaxSweepsPerRow);
     if (tid == 0) {
         if (info != 0) b.info[cell] = info;
-        if (b.dbg) b.dbg[8 * (size_t)cell + 6] = sh.nsweep;
+        if (b.dbg) b.dbg[8 * (size_t)cell + 6] = nsweep;
     }
     // eigenvalues -> q = branch(sqrt(lambda)) (rcwa2d.cpp:364)
     cplx* q1 = at(b.q1, b.s_n, cell);
@@ -780,6 +788,7 @@ size_t per_cell_bytes(int n, int nexc) {
 // per wave to the largest need over its buckets (outside any capture).
 struct SmemNeeds {
     size_t laurent = 0, rect = 0, hess_s = 0, smat = 0;
+    bool aed = false;
     void add(int Mx, int My, int ng, int n) {
         if (ng > 0) {
             laurent = std::max(laurent, laurent_smem(Mx, My, ng));
@@ -788,6 +797,7 @@ struct SmemNeeds {
             rect = std::max(rect, ((size_t)2 * (nx * nx + ny * ny) + 2 * std::max(nx, ny)) * sizeof(cplx));
         }
         if (n <= kSmemEigMaxN) hess_s = std::max(hess_s, ((size_t)n * n + 2 * n) * sizeof(cplx));
+        else aed = true;
         smat = std::max(smat, lu_stage_bytes(n));
     }
 };
@@ -797,6 +807,9 @@ int set_smem_limits(const SmemNeeds& s) {
         CEL_CUDA(cudaFuncSetAttribute(rcwa_fourier_laurent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.laurent));
     if (s.rect)
         CEL_CUDA(cudaFuncSetAttribute(rcwa_fourier_rect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.rect));
+    if (s.aed)
+        CEL_CUDA(cudaFuncSetAttribute(rcwa_schur<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sizeof(AedShared)));
     if (s.hess_s) {
         CEL_CUDA(cudaFuncSetAttribute(rcwa_hess<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.hess_s));
         CEL_CUDA(cudaFuncSetAttribute(rcwa_schur<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.hess_s));
@@ -838,7 +851,7 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
     } else {
         rcwa_hess<false><<<nc, T[ST_HESS], hess_stage_bytes(n), st>>>(b);
         if (ev) cudaEventRecord(ev[3], st);
-        rcwa_schur<false><<<nc, T[ST_SCHUR], 0, st>>>(b);
+        rcwa_schur<false><<<nc, T[ST_SCHUR], sizeof(AedShared), st>>>(b);
     }
     if (ev) cudaEventRecord(ev[4], st);
     rcwa_vec<<<nc, T[ST_VEC], 0, st>>>(b);

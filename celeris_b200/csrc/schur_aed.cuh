@@ -1,0 +1,590 @@
+// Complex Schur decomposition for large n (one CTA per cell): small-bulge
+// multishift QR with aggressive early deflation (AED), the scheme of LAPACK's
+// xLAQR0/xLAQR3/xLAQR5 restated for one thread block:
+//
+//  * AED: the trailing NW x NW window of the active block is brought to Schur
+//    form in shared memory (one warp, single-shift QR, unitary U accumulated).
+//    Eigenvalues whose spike entry s * conj(U[0][j]) is negligible deflate;
+//    the others are moved to the top of the window by adjacent swaps, the spike
+//    is reflected back to a multiple of e1 and the undeflated part is reduced
+//    to Hessenberg form again. The undeflated eigenvalues become the shifts.
+//  * Sweep: up to NSH single-shift bulges are chased down the active block as
+//    a chain (bulges two rows apart, all moved one row per step: first every
+//    row rotation, then every column rotation, one warp per bulge). The chain
+//    advances through windows of at most WMAX rows/columns held in shared
+//    memory; each window's rotations are accumulated into one unitary U.
+//  * Every window (AED, sweep or a whole small block) reaches the rest of the
+//    matrix once, as dense products with U (rows right of the window,
+//    columns above it, and Z), tiled through shared memory.
+//
+// The rows and columns outside the window are therefore read and written once
+// per window instead of once per rotation block of a single-shift sweep; the
+// work moves from memory-bound rotations to compute-bound small products.
+#pragma once
+
+#include "cblas_block.cuh"
+
+namespace cb {
+
+constexpr int WMAX = 64;   // window size (rows/columns)
+constexpr int NSH = 16;    // shifts per sweep
+constexpr int NWIN = 32;   // AED window
+constexpr int NSMALL = 64; // active blocks up to this size are finished in shared memory
+constexpr int FT = 32;     // far-update tile (rows or columns)
+
+struct AedShared {
+    cplx B[WMAX][WMAX + 1];  // window
+    cplx U[WMAX][WMAX];      // accumulated unitary of the window
+    cplx tile[FT][WMAX];     // far-update staging
+    cplx sh[NWIN];           // undeflated eigenvalues of the last AED
+    cplx vec[WMAX];          // Householder vector
+    double rc[NSH + 1];      // rotations of one chain step
+    cplx rs[NSH + 1];
+    int plan_k[NSH + 1];     // global position of each move of the step
+    int plan_intro[NSH + 1]; // shift index for an introduction, -1 for a chase move
+    int pos[NSH];            // bulge positions (-2 not introduced, -1 gone)
+    unsigned char flag[kMaxN];
+    int lo, hi, done, info, nsweep, nsu, nd, nplan, nxt, win_end, ws, we, it;
+    cplx shift[NSH];
+};
+
+// ---- warp-level helpers on shared matrices ------------------------------------------------
+// rows r, r+1 over columns [c0, c1): G = [[c, s], [-conj s, c]] from the left
+__device__ __forceinline__ void wrot_rows(cplx* B, int ld, int r, double c, cplx s, int c0, int c1, int lane) {
+    const cplx ms = cneg(cconj(s));
+    for (int col = c0 + lane; col < c1; col += 32) {
+        const cplx x = B[r * ld + col], y = B[(r + 1) * ld + col];
+        B[r * ld + col] = cfma(s, y, cscale(x, c));
+        B[(r + 1) * ld + col] = cfma(ms, x, cscale(y, c));
+    }
+}
+// columns k, k+1 over rows [r0, r1): M <- M G^H
+__device__ __forceinline__ void wrot_cols(cplx* B, int ld, int k, double c, cplx s, int r0, int r1, int lane) {
+    const cplx cs = cconj(s), ns = cneg(s);
+    for (int row = r0 + lane; row < r1; row += 32) {
+        const cplx x = B[row * ld + k], y = B[row * ld + k + 1];
+        B[row * ld + k] = cfma(cs, y, cscale(x, c));
+        B[row * ld + k + 1] = cfma(ns, x, cscale(y, c));
+    }
+}
+
+// Single-shift QR of the m x m upper Hessenberg matrix B (shared, ld) to upper
+// triangular form, U <- U Q (rows [0, mu)). One warp. Returns 0, or the
+// (1-based) row where the iteration cap ran out.
+__device__ int warp_schur_small(int m, cplx* B, int ld, cplx* U, int ldu, int mu, int lane) {
+    const double eps = 2.220446049250313e-16;
+    const double smallnum = 2.2250738585072014e-308 * (m / eps);
+    int hi = m - 1, it = 0, total = 0;
+    const int max_total = 30 * m;
+    while (hi > 0) {
+        // l = largest index in [1, hi] with a negligible subdiagonal (0 if none)
+        int l = 0;
+        for (int base = hi; base >= 1 && l == 0; base -= 32) {
+            const int i = base - lane;
+            bool f = false;
+            if (i >= 1) {
+                const double tst = cabs1(B[(i - 1) * ld + i - 1]) + cabs1(B[i * ld + i]);
+                f = cabs1(B[i * ld + i - 1]) <= fmax(eps * tst, smallnum);
+            }
+            const unsigned msk = __ballot_sync(0xffffffffu, f);
+            if (msk) l = base - (__ffs(msk) - 1);
+        }
+        __syncwarp();
+        if (l > 0 && lane == 0) B[l * ld + l - 1] = C(0.0, 0.0);
+        __syncwarp();
+        if (l == hi) {
+            --hi;
+            it = 0;
+            continue;
+        }
+        if (++total > max_total) return hi + 1;
+        ++it;
+        cplx shift;
+        if (it == 10 || it == 20) {
+            shift = cadd(B[hi * ld + hi], C(0.75 * fabs(B[hi * ld + hi - 1].x) + fabs(B[hi * ld + hi - 1].y), 0.0));
+        } else {
+            shift = wilkinson(B[(hi - 1) * ld + hi - 1], B[(hi - 1) * ld + hi], B[hi * ld + hi - 1], B[hi * ld + hi]);
+        }
+        for (int k = l; k < hi; ++k) {
+            cplx a, b;
+            if (k == l) {
+                a = csub(B[l * ld + l], shift);
+                b = B[(l + 1) * ld + l];
+            } else {
+                a = B[k * ld + k - 1];
+                b = B[(k + 1) * ld + k - 1];
+            }
+            double c;
+            cplx s;
+            givens(a, b, c, s);
+            __syncwarp();
+            wrot_rows(B, ld, k, c, s, k == l ? l : k - 1, m, lane);
+            __syncwarp();
+            if (k > l && lane == 0) B[(k + 1) * ld + k - 1] = C(0.0, 0.0);
+            wrot_cols(B, ld, k, c, s, 0, min(k + 2, hi) + 1, lane);
+            wrot_cols(U, ldu, k, c, s, 0, mu, lane);
+            __syncwarp();
+        }
+    }
+    return 0;
+}
+
+// Householder reflector from x (length len, shared) : returns beta (0 when x is
+// already a multiple of e1) and leaves v in x (v0 = x0 - alpha), alpha out.
+// P = I - beta v v^H is Hermitian and unitary with P x = alpha e1. One warp.
+__device__ double warp_reflector(cplx* x, int len, cplx& alpha, int lane) {
+    double s2 = 0.0;
+    for (int i = lane; i < len; i += 32) s2 += cnorm2(x[i]);
+    for (int o = 16; o > 0; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    const cplx x0 = x[0];
+    const double tail = s2 - cnorm2(x0);
+    __syncwarp();
+    if (!(tail > 0.0)) {
+        alpha = x0;
+        return 0.0;
+    }
+    const double xn = sqrt(s2), ax0 = cabs(x0);
+    const cplx ph = ax0 > 0.0 ? cscale(x0, 1.0 / ax0) : C(1.0, 0.0);
+    alpha = cscale(ph, -xn);
+    const cplx v0 = csub(x0, alpha);
+    if (lane == 0) x[0] = v0;
+    __syncwarp();
+    return 2.0 / (tail + cnorm2(v0));
+}
+
+// M[r0:r0+len, c0:c1] <- P M (P = I - beta v v^H), lanes over columns
+__device__ __forceinline__ void wrefl_left(cplx* M, int ld, int r0, int len, int c0, int c1, const cplx* v,
+                                           double beta, int lane) {
+    for (int col = c0 + lane; col < c1; col += 32) {
+        cplx w = C(0.0, 0.0);
+        for (int i = 0; i < len; ++i) w = cfma(cconj(v[i]), M[(r0 + i) * ld + col], w);
+        w = cscale(w, beta);
+        for (int i = 0; i < len; ++i) M[(r0 + i) * ld + col] = cfms(v[i], w, M[(r0 + i) * ld + col]);
+    }
+}
+// M[r0:r1, c0:c0+len] <- M P, lanes over rows
+__device__ __forceinline__ void wrefl_right(cplx* M, int ld, int r0, int r1, int c0, int len, const cplx* v,
+                                            double beta, int lane) {
+    for (int row = r0 + lane; row < r1; row += 32) {
+        cplx w = C(0.0, 0.0);
+        for (int i = 0; i < len; ++i) w = cfma(M[row * ld + c0 + i], v[i], w);
+        w = cscale(w, beta);
+        for (int i = 0; i < len; ++i) M[row * ld + c0 + i] = cfms(w, cconj(v[i]), M[row * ld + c0 + i]);
+    }
+}
+
+// ---- far updates: the window's unitary applied to the rest of the matrix ------------------
+// X[r0:r0+w, c0:c1] <- U^H X  (U w x w in shared memory); the staged tile is
+// k-major [w][FT] so that a warp reads 8 consecutive entries of one row.
+__device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const cplx (*U)[WMAX], cplx* tile) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int cb = c0; cb < c1; cb += FT) {
+        const int nc = min(FT, c1 - cb);
+        for (int e = tid; e < w * FT; e += nt) {
+            const int k = e / FT, c = e % FT;
+            tile[e] = c < nc ? X[(size_t)(r0 + k) * ld + cb + c] : C(0.0, 0.0);
+        }
+        __syncthreads();
+        for (int q = tid; q < 256; q += nt) {
+            const int ty = q >> 3, tx = q & 7;  // rows ty, ty+32; columns tx + 8j
+            cplx acc[2][4];
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[a][j] = C(0.0, 0.0);
+            for (int k = 0; k < w; ++k) {
+                const cplx u0 = cconj(U[k][ty]);
+                const cplx u1 = cconj(U[k][ty + 32]);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const cplx t = tile[k * FT + tx + 8 * j];
+                    acc[0][j] = cfma(u0, t, acc[0][j]);
+                    acc[1][j] = cfma(u1, t, acc[1][j]);
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                const int r = ty + 32 * a;
+                if (r >= w) continue;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int c = tx + 8 * j;
+                    if (c < nc) X[(size_t)(r0 + r) * ld + cb + c] = acc[a][j];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// X[r0:r1, c0:c0+w] <- X U
+__device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const cplx (*U)[WMAX], cplx (*tile)[WMAX]) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int rb = r0; rb < r1; rb += FT) {
+        const int nr = min(FT, r1 - rb);
+        for (int e = tid; e < FT * w; e += nt) {
+            const int r = e / w, k = e % w;
+            tile[r][k] = r < nr ? X[(size_t)(rb + r) * ld + c0 + k] : C(0.0, 0.0);
+        }
+        __syncthreads();
+        for (int q = tid; q < 256; q += nt) {
+            const int ty = q >> 4, tx = q & 15;  // rows ty, ty+16; columns tx + 16j
+            cplx acc[2][4];
+#pragma unroll
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[a][j] = C(0.0, 0.0);
+            for (int k = 0; k < w; ++k) {
+                const cplx t0 = tile[ty][k], t1 = tile[ty + 16][k];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const cplx u = U[k][tx + 16 * j];
+                    acc[0][j] = cfma(t0, u, acc[0][j]);
+                    acc[1][j] = cfma(t1, u, acc[1][j]);
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                const int r = ty + 16 * a;
+                if (r >= nr) continue;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int c = tx + 16 * j;
+                    if (c < w) X[(size_t)(rb + r) * ld + c0 + c] = acc[a][j];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Window [ws, we) of H <- U^H (.) U everywhere outside the window, given that
+// the window itself was already transformed in shared memory: rows ws..we-1 to
+// the right (columns we..n-1), columns ws..we-1 above (rows 0..ws-1), and Z.
+__device__ void far_all(int n, cplx* H, int ldh, cplx* Z, int ldz, int ws, int we, AedShared* sh) {
+    const int w = we - ws;
+    if (we < n) far_left(H, ldh, ws, w, we, n, sh->U, &sh->tile[0][0]);
+    if (ws > 0) far_right(H, ldh, 0, ws, ws, w, sh->U, sh->tile);
+    far_right(Z, ldz, 0, n, ws, w, sh->U, sh->tile);
+}
+
+__device__ void load_window(const cplx* H, int ldh, int ws, int w, AedShared* sh) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e = tid; e < w * w; e += nt) {
+        const int r = e / w, c = e % w;
+        sh->B[r][c] = H[(size_t)(ws + r) * ldh + ws + c];
+        sh->U[r][c] = C(r == c ? 1.0 : 0.0, 0.0);
+    }
+    __syncthreads();
+}
+
+// mask: write exact zeros below the subdiagonal (a finished Hessenberg or
+// triangular window); a sweep window is stored as it is (it holds bulges).
+__device__ void store_window(cplx* H, int ldh, int ws, int w, const AedShared* sh, bool mask) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e = tid; e < w * w; e += nt) {
+        const int r = e / w, c = e % w;
+        H[(size_t)(ws + r) * ldh + ws + c] = (mask && r > c + 1) ? C(0.0, 0.0) : sh->B[r][c];
+    }
+}
+
+// ---- aggressive early deflation ---------------------------------------------------------------
+// Window [kwtop, hi] of the active block [lo, hi]. Sets sh->nd (deflated count)
+// and sh->nsu / sh->sh[0..nsu) (undeflated eigenvalues, the shifts).
+__device__ void aed(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, AedShared* sh) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const double eps = 2.220446049250313e-16;
+    const double smallnum = 2.2250738585072014e-308 * (n / eps);
+    const int kwtop = max(lo, hi - NWIN + 1), jw = hi - kwtop + 1;
+    const cplx s = kwtop > lo ? H[(size_t)kwtop * ldh + kwtop - 1] : C(0.0, 0.0);
+    load_window(H, ldh, kwtop, jw, sh);
+    cplx* B = &sh->B[0][0];
+    cplx* U = &sh->U[0][0];
+    constexpr int ldb = WMAX + 1, ldu = WMAX;
+    if (warp == 0) {
+        const int info = warp_schur_small(jw, B, ldb, U, ldu, jw, lane);
+        int nsu = jw, ilst = 0;
+        if (info == 0) {
+            while (nsu > ilst) {
+                double foo = cabs1(B[(nsu - 1) * ldb + nsu - 1]);
+                if (foo == 0.0) foo = cabs1(s);
+                if (cabs1(s) * cabs1(U[nsu - 1]) <= fmax(smallnum, eps * foo)) {
+                    --nsu;  // deflatable: stays at the bottom
+                } else {
+                    for (int k = nsu - 2; k >= ilst; --k) {  // move it up to ilst
+                        double c;
+                        cplx sn;
+                        givens(B[k * ldb + k + 1], csub(B[(k + 1) * ldb + k + 1], B[k * ldb + k]), c, sn);
+                        __syncwarp();
+                        wrot_rows(B, ldb, k, c, sn, k, jw, lane);
+                        __syncwarp();
+                        wrot_cols(B, ldb, k, c, sn, 0, k + 2, lane);
+                        wrot_cols(U, ldu, k, c, sn, 0, jw, lane);
+                        __syncwarp();
+                        if (lane == 0) B[(k + 1) * ldb + k] = C(0.0, 0.0);
+                        __syncwarp();
+                    }
+                    ++ilst;
+                }
+                __syncwarp();
+            }
+        }
+        for (int i = lane; i < nsu; i += 32) sh->sh[i] = B[i * ldb + i];
+        if (lane == 0) {
+            sh->nsu = nsu;
+            sh->nd = jw - nsu;
+        }
+        __syncwarp();
+        if (s.x != 0.0 || s.y != 0.0) {
+            if (nsu > 0) {
+                // spike w = s conj(U[0, :nsu]) -> alpha e1
+                for (int i = lane; i < nsu; i += 32) sh->vec[i] = cmul(s, cconj(U[i]));
+                __syncwarp();
+                cplx alpha;
+                const double beta = warp_reflector(sh->vec, nsu, alpha, lane);
+                if (beta != 0.0) {
+                    wrefl_left(B, ldb, 0, nsu, 0, jw, sh->vec, beta, lane);
+                    __syncwarp();
+                    wrefl_right(B, ldb, 0, nsu, 0, nsu, sh->vec, beta, lane);
+                    wrefl_right(U, ldu, 0, jw, 0, nsu, sh->vec, beta, lane);
+                    __syncwarp();
+                }
+                // back to Hessenberg: columns 0 .. nsu-3 of the undeflated block
+                for (int j = 0; j + 2 < nsu; ++j) {
+                    const int len = nsu - j - 1;
+                    for (int i = lane; i < len; i += 32) sh->vec[i] = B[(j + 1 + i) * ldb + j];
+                    __syncwarp();
+                    cplx al;
+                    const double bt = warp_reflector(sh->vec, len, al, lane);
+                    if (bt != 0.0) {
+                        wrefl_left(B, ldb, j + 1, len, j + 1, jw, sh->vec, bt, lane);
+                        __syncwarp();
+                        for (int i = lane; i < len; i += 32) B[(j + 1 + i) * ldb + j] = i == 0 ? al : C(0.0, 0.0);
+                        wrefl_right(B, ldb, 0, nsu, j + 1, len, sh->vec, bt, lane);
+                        wrefl_right(U, ldu, 0, jw, j + 1, len, sh->vec, bt, lane);
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+    }
+    __syncthreads();
+    const int nsu = sh->nsu;
+    store_window(H, ldh, kwtop, jw, sh, true);
+    if (kwtop > lo) {
+        for (int i = tid; i < jw; i += blockDim.x)
+            H[(size_t)(kwtop + i) * ldh + kwtop - 1] = (i == 0 && nsu > 0) ? cmul(s, cconj(sh->U[0][0])) : C(0.0, 0.0);
+    }
+    far_all(n, H, ldh, Z, ldz, kwtop, hi + 1, sh);
+}
+
+// ---- one multishift sweep over the active block [lo, hi] with nsh shifts ----------------------
+__device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, int nsh, AedShared* sh) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+    constexpr int ldb = WMAX + 1, ldu = WMAX;
+    cplx* B = &sh->B[0][0];
+    cplx* U = &sh->U[0][0];
+    if (tid == 0) {
+        for (int b = 0; b < nsh; ++b) sh->pos[b] = -2;
+        sh->nxt = 0;
+        sh->ws = lo;
+        sh->we = min(lo + WMAX, hi + 1);
+    }
+    __syncthreads();
+    for (int guard = 0; guard < n / 4 + 32; ++guard) {  // a sweep takes about n / 30 windows
+        const int ws = sh->ws, we = sh->we, w = we - ws;
+        load_window(H, ldh, ws, w, sh);
+        for (int step = 0; step < 4 * WMAX; ++step) {
+            if (tid == 0) {
+                int np = 0, last = -1, lead = -1;
+                for (int b = 0; b < sh->nxt; ++b)
+                    if (sh->pos[b] >= 0) {
+                        if (lead < 0) lead = b;
+                        last = b;
+                    }
+                bool intro = ws == lo && sh->nxt < nsh && (last < 0 || sh->pos[last] >= lo + 2) &&
+                             (lo + 2 <= we - 1 || lo + 1 == hi);
+                bool go = true;
+                if (lead >= 0) {
+                    const int p = sh->pos[lead];
+                    go = p <= we - 3 || (we == hi + 1 && p <= hi - 1);
+                } else {
+                    go = intro;
+                }
+                if (go) {
+                    for (int b = 0; b < sh->nxt; ++b) {
+                        const int p = sh->pos[b];
+                        if (p < 0) continue;
+                        sh->plan_k[np] = p;
+                        sh->plan_intro[np] = -1;
+                        ++np;
+                        sh->pos[b] = p + 1 <= hi - 1 ? p + 1 : -1;
+                    }
+                    if (intro) {
+                        sh->plan_k[np] = lo;
+                        sh->plan_intro[np] = sh->nxt;
+                        ++np;
+                        sh->pos[sh->nxt] = lo + 1 <= hi - 1 ? lo + 1 : -1;
+                        sh->nxt += 1;
+                    }
+                }
+                sh->nplan = np;
+            }
+            __syncthreads();
+            const int np = sh->nplan;
+            if (np == 0) break;
+            // phase 1: row rotations
+            for (int t = warp; t < np; t += nwarp) {
+                const int k = sh->plan_k[t] - ws, si = sh->plan_intro[t];
+                cplx a, bb;
+                if (si >= 0) {
+                    a = csub(B[k * ldb + k], sh->shift[si]);
+                    bb = B[(k + 1) * ldb + k];
+                } else {
+                    a = B[k * ldb + k - 1];
+                    bb = B[(k + 1) * ldb + k - 1];
+                }
+                double c;
+                cplx s;
+                givens(a, bb, c, s);
+                __syncwarp();
+                wrot_rows(B, ldb, k, c, s, si >= 0 ? k : k - 1, w, lane);
+                __syncwarp();
+                if (lane == 0) {
+                    if (si < 0) B[(k + 1) * ldb + k - 1] = C(0.0, 0.0);
+                    sh->rc[t] = c;
+                    sh->rs[t] = s;
+                }
+            }
+            __syncthreads();
+            // phase 2: column rotations
+            for (int t = warp; t < np; t += nwarp) {
+                const int p = sh->plan_k[t], k = p - ws;
+                const double c = sh->rc[t];
+                const cplx s = sh->rs[t];
+                wrot_cols(B, ldb, k, c, s, 0, min(p + 2, hi) - ws + 1, lane);
+                wrot_cols(U, ldu, k, c, s, 0, w, lane);
+            }
+            __syncthreads();
+        }
+        store_window(H, ldh, ws, w, sh, false);
+        far_all(n, H, ldh, Z, ldz, ws, we, sh);  // begins and ends with barriers
+        if (tid == 0) {
+            int last = -1;
+            for (int b = 0; b < sh->nxt; ++b)
+                if (sh->pos[b] >= 0) last = b;
+            if (last < 0 && sh->nxt >= nsh) {
+                sh->win_end = 1;
+            } else {
+                sh->win_end = 0;
+                const int nws = last >= 0 ? sh->pos[last] - 1 : lo;
+                sh->ws = nws;
+                sh->we = min(nws + WMAX, hi + 1);
+            }
+        }
+        __syncthreads();
+        if (sh->win_end) break;
+    }
+}
+
+// T <- Q^H H Q upper triangular, Z <- Z Q, for n > NSMALL. Returns info (0, or
+// the 1-based row where the iteration cap ran out).
+__device__ int blk_schur_aed(int n, cplx* H, int ldh, cplx* Z, int ldz, AedShared* sh) {
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    const double eps = 2.220446049250313e-16;
+    const double smallnum = 2.2250738585072014e-308 * (n / eps);
+    if (tid == 0) {
+        sh->hi = n - 1;
+        sh->lo = 0;
+        sh->done = 0;
+        sh->info = 0;
+        sh->nsweep = 0;
+        sh->it = 0;
+    }
+    __syncthreads();
+    const int max_iter = 2 * n + 100;  // AED + sweep iterations (about n / 4 are typical)
+    for (int iter = 0; iter < max_iter; ++iter) {
+        const int hi0 = sh->hi;
+        for (int i = 1 + tid; i <= hi0; i += nt) {
+            const double tst = cabs1(H[(size_t)(i - 1) * ldh + i - 1]) + cabs1(H[(size_t)i * ldh + i]);
+            sh->flag[i] = cabs1(H[(size_t)i * ldh + i - 1]) <= fmax(eps * tst, smallnum) ? 1 : 0;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            int hi = hi0;
+            while (hi > 0 && sh->flag[hi]) {
+                H[(size_t)hi * ldh + hi - 1] = C(0.0, 0.0);
+                --hi;
+                sh->it = 0;
+            }
+            int lo = hi;
+            while (lo > 0 && !sh->flag[lo]) --lo;
+            if (lo > 0) H[(size_t)lo * ldh + lo - 1] = C(0.0, 0.0);
+            sh->hi = hi;
+            sh->lo = lo;
+            sh->done = hi <= 0 ? 1 : 0;
+        }
+        __syncthreads();
+        if (sh->done) break;
+        const int lo = sh->lo, hi = sh->hi, L = hi - lo + 1;
+        if (L <= NSMALL) {
+            // the whole block in shared memory
+            load_window(H, ldh, lo, L, sh);
+            if (warp == 0) {
+                const int info = warp_schur_small(L, &sh->B[0][0], WMAX + 1, &sh->U[0][0], WMAX, L, lane);
+                if (lane == 0 && info) sh->info = lo + info;
+            }
+            __syncthreads();
+            store_window(H, ldh, lo, L, sh, true);
+            far_all(n, H, ldh, Z, ldz, lo, hi + 1, sh);
+            if (tid == 0) {
+                sh->hi = lo - 1;
+                sh->it = 0;
+                sh->nsweep += 1;
+                if (sh->info) sh->done = 1;
+            }
+            __syncthreads();
+            if (sh->done) break;
+            if (sh->hi <= 0) break;
+            continue;
+        }
+        aed(n, H, ldh, Z, ldz, lo, hi, sh);
+        if (tid == 0) {
+            const int nd = sh->nd;
+            sh->hi = hi - nd;
+            sh->it = nd > 0 ? 0 : sh->it + 1;
+            sh->nsweep += 1;
+            // sweep unless AED deflated at least 14% of its window
+            int nsh = 0;
+            const int L2 = sh->hi - lo + 1;
+            if ((nd == 0 || 100 * nd <= 14 * NWIN) && L2 > NSMALL) {
+                const int nsu = sh->nsu;
+                if (sh->it > 0 && sh->it % 6 == 0) {  // exceptional shifts
+                    nsh = NSH;
+                    for (int i = 0; i < nsh; ++i) {
+                        const int r = sh->hi - i;
+                        const cplx sub = H[(size_t)r * ldh + r - 1];
+                        sh->shift[i] = cadd(H[(size_t)r * ldh + r], C(0.75 * cabs1(sub), 0.0));
+                    }
+                } else if (nsu >= 2) {
+                    nsh = min(NSH, nsu);
+                    for (int i = 0; i < nsh; ++i) sh->shift[i] = sh->sh[i];
+                } else {
+                    nsh = 2;
+                    for (int i = 0; i < nsh; ++i) sh->shift[i] = H[(size_t)(sh->hi - i) * ldh + sh->hi - i];
+                }
+            }
+            sh->nplan = nsh;  // reused as the shift count of the sweep
+        }
+        __syncthreads();
+        const int nsh = sh->nplan;
+        if (nsh > 0) chain_sweep(n, H, ldh, Z, ldz, lo, sh->hi, nsh, sh);
+        if (iter == max_iter - 1 && tid == 0) sh->info = sh->hi + 1;
+        __syncthreads();
+    }
+    const int info = sh->info;
+    __syncthreads();
+    return info;
+}
+
+}  // namespace cb

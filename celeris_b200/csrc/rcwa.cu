@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(kRT) rcwa_schur(Bucket b) {
         nsweep = sh.nsweep;
     } else {
         AedShared* sh = reinterpret_cast<AedShared*>(smem);
-        info = blk_schur_aed(n, H, n, at(b.Z, b.s_nn, cell), n, sh);
+        info = blk_schur_aed(n, H, n, at(b.Z, b.s_nn, cell), n, sh, b.dbg ? b.dbg + 8 * (size_t)cell : nullptr);
         nsweep = sh->nsweep;
     }
     if (tid == 0) {
@@ -797,7 +797,7 @@ struct SmemNeeds {
             rect = std::max(rect, ((size_t)2 * (nx * nx + ny * ny) + 2 * std::max(nx, ny)) * sizeof(cplx));
         }
         if (n <= kSmemEigMaxN) hess_s = std::max(hess_s, ((size_t)n * n + 2 * n) * sizeof(cplx));
-        else aed = true;
+        aed = true;
         smat = std::max(smat, lu_stage_bytes(n));
     }
 };
@@ -847,7 +847,7 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
         const size_t sm = ((size_t)n * n + 2 * n) * sizeof(cplx);
         rcwa_hess<true><<<nc, T[ST_HESS], sm, st>>>(b);
         if (ev) cudaEventRecord(ev[3], st);
-        rcwa_schur<true><<<nc, T[ST_SCHUR], sm, st>>>(b);
+        rcwa_schur<false><<<nc, T[ST_SCHUR], sizeof(AedShared), st>>>(b);
     } else {
         rcwa_hess<false><<<nc, T[ST_HESS], hess_stage_bytes(n), st>>>(b);
         if (ev) cudaEventRecord(ev[3], st);
@@ -1104,8 +1104,11 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                 CEL_CUDA(cudaStreamSynchronize(st));
                 std::vector<long long> h(8 * nc);
                 cudaMemcpy(h.data(), dbg, sizeof(long long) * 8 * nc, cudaMemcpyDeviceToHost);
-                double sw = 0;
-                for (int i = 0; i < nc; ++i) sw += (double)h[8 * i + 6];
+                double sw = 0, ph[5] = {0, 0, 0, 0, 0};
+                for (int i = 0; i < nc; ++i) {
+                    sw += (double)h[8 * i + 6];
+                    for (int q = 0; q < 5; ++q) ph[q] += (double)h[8 * i + q];
+                }
                 std::string line = "[rcwa stages] n=" + std::to_string(p.n) + " cells=" + std::to_string(nc) + " ms:";
                 for (int s = 0; s < ST_COUNT; ++s) {
                     float ms = 0.f;
@@ -1115,8 +1118,11 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                     line += buf;
                 }
                 char buf[64];
-                std::snprintf(buf, sizeof(buf), " | sweeps/cell %.1f\n", sw / nc);
-                std::fprintf(stderr, "%s%s", line.c_str(), buf);
+                std::snprintf(buf, sizeof(buf), " | sweeps/cell %.1f", sw / nc);
+                char buf2[160];
+                std::snprintf(buf2, sizeof(buf2), " | schur Mcycles/cell: aed %.2f aed_far %.2f sweep %.2f sweep_far %.2f small %.2f\n",
+                              ph[0] / nc * 1e-6, ph[1] / nc * 1e-6, ph[2] / nc * 1e-6, ph[3] / nc * 1e-6, ph[4] / nc * 1e-6);
+                std::fprintf(stderr, "%s%s%s", line.c_str(), buf, buf2);
                 for (auto& e : ev) cudaEventDestroy(e);
                 cudaFree(dbg);
                 p.b.dbg = nullptr;

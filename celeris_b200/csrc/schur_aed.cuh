@@ -33,18 +33,15 @@ constexpr int NSMALL = 64; // active blocks up to this size are finished in shar
 constexpr int FT = 32;     // far-update tile (rows or columns)
 
 struct AedShared {
-    cplx B[WMAX][WMAX + 1];  // window
+    cplx B[WMAX][WMAX + 1];  // window; during far updates two tile buffers of WMAX * FT
     cplx U[WMAX][WMAX];      // accumulated unitary of the window
-    cplx tile[FT][WMAX];     // far-update staging
     cplx sh[NWIN];           // undeflated eigenvalues of the last AED
     cplx vec[WMAX];          // Householder vector
-    double rc[NSH + 1];      // rotations of one chain step
-    cplx rs[NSH + 1];
-    int plan_k[NSH + 1];     // global position of each move of the step
-    int plan_intro[NSH + 1]; // shift index for an introduction, -1 for a chase move
+    double rc[NSH];          // rotations of one chain step, per bulge
+    cplx rs[NSH];
     int pos[NSH];            // bulge positions (-2 not introduced, -1 gone)
     unsigned char flag[kMaxN];
-    int lo, hi, done, info, nsweep, nsu, nd, nplan, nxt, win_end, ws, we, it;
+    int lo, hi, done, info, nsweep, nsu, nd, nshift, nxt, win_end, ws, we, it;
     cplx shift[NSH];
 };
 
@@ -174,17 +171,46 @@ __device__ __forceinline__ void wrefl_right(cplx* M, int ld, int r0, int r1, int
 }
 
 // ---- far updates: the window's unitary applied to the rest of the matrix ------------------
-// X[r0:r0+w, c0:c1] <- U^H X  (U w x w in shared memory); the staged tile is
-// k-major [w][FT] so that a warp reads 8 consecutive entries of one row.
-__device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const cplx (*U)[WMAX], cplx* tile) {
+// Tiles of FT rows or columns stream through two shared buffers with cp.async
+// (16-byte copies, zero-filled past the edge): the next tile is in flight
+// while the current one is multiplied. The buffers overlay the window B, which
+// is dead during the far updates.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    const int sz = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+constexpr int FBUF = WMAX * FT;  // complex entries per tile buffer
+
+// X[r0:r0+w, c0:c1] <- U^H X  (U w x w in shared memory). Tile t holds columns
+// c0 + t*FT .. as [w][FT] (k-major: a warp reads 8 consecutive entries).
+__device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const cplx (*U)[WMAX], cplx* buf) {
     const int tid = threadIdx.x, nt = blockDim.x;
-    for (int cb = c0; cb < c1; cb += FT) {
-        const int nc = min(FT, c1 - cb);
+    const int ntile = (c1 - c0 + FT - 1) / FT;
+    auto issue = [&](int t) {
+        const int cb = c0 + t * FT, nc = min(FT, c1 - cb);
+        cplx* dst = buf + (t & 1) * FBUF;
         for (int e = tid; e < w * FT; e += nt) {
             const int k = e / FT, c = e % FT;
-            tile[e] = c < nc ? X[(size_t)(r0 + k) * ld + cb + c] : C(0.0, 0.0);
+            cp_async16(dst + e, X + (size_t)(r0 + k) * ld + cb + (c < nc ? c : 0), c < nc);
+        }
+        cp_async_commit();
+    };
+    issue(0);
+    for (int t = 0; t < ntile; ++t) {
+        if (t + 1 < ntile) {
+            issue(t + 1);
+            cp_async_wait1();
+        } else {
+            cp_async_wait0();
         }
         __syncthreads();
+        const cplx* tile = buf + (t & 1) * FBUF;
+        const int cb = c0 + t * FT, nc = min(FT, c1 - cb);
         for (int q = tid; q < 256; q += nt) {
             const int ty = q >> 3, tx = q & 7;  // rows ty, ty+32; columns tx + 8j
             cplx acc[2][4];
@@ -192,14 +218,15 @@ __device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const c
             for (int a = 0; a < 2; ++a)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) acc[a][j] = C(0.0, 0.0);
+#pragma unroll 4
             for (int k = 0; k < w; ++k) {
                 const cplx u0 = cconj(U[k][ty]);
                 const cplx u1 = cconj(U[k][ty + 32]);
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    const cplx t = tile[k * FT + tx + 8 * j];
-                    acc[0][j] = cfma(u0, t, acc[0][j]);
-                    acc[1][j] = cfma(u1, t, acc[1][j]);
+                    const cplx tv = tile[k * FT + tx + 8 * j];
+                    acc[0][j] = cfma(u0, tv, acc[0][j]);
+                    acc[1][j] = cfma(u1, tv, acc[1][j]);
                 }
             }
 #pragma unroll
@@ -217,16 +244,30 @@ __device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const c
     }
 }
 
-// X[r0:r1, c0:c0+w] <- X U
-__device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const cplx (*U)[WMAX], cplx (*tile)[WMAX]) {
+// X[r0:r1, c0:c0+w] <- X U. Tile t holds rows r0 + t*FT .. as [FT][w] (ld WMAX).
+__device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const cplx (*U)[WMAX], cplx* buf) {
     const int tid = threadIdx.x, nt = blockDim.x;
-    for (int rb = r0; rb < r1; rb += FT) {
-        const int nr = min(FT, r1 - rb);
+    const int ntile = (r1 - r0 + FT - 1) / FT;
+    auto issue = [&](int t) {
+        const int rb = r0 + t * FT, nr = min(FT, r1 - rb);
+        cplx* dst = buf + (t & 1) * FBUF;
         for (int e = tid; e < FT * w; e += nt) {
             const int r = e / w, k = e % w;
-            tile[r][k] = r < nr ? X[(size_t)(rb + r) * ld + c0 + k] : C(0.0, 0.0);
+            cp_async16(dst + r * WMAX + k, X + (size_t)(rb + (r < nr ? r : 0)) * ld + c0 + k, r < nr);
+        }
+        cp_async_commit();
+    };
+    issue(0);
+    for (int t = 0; t < ntile; ++t) {
+        if (t + 1 < ntile) {
+            issue(t + 1);
+            cp_async_wait1();
+        } else {
+            cp_async_wait0();
         }
         __syncthreads();
+        const cplx* tile = buf + (t & 1) * FBUF;
+        const int rb = r0 + t * FT, nr = min(FT, r1 - rb);
         for (int q = tid; q < 256; q += nt) {
             const int ty = q >> 4, tx = q & 15;  // rows ty, ty+16; columns tx + 16j
             cplx acc[2][4];
@@ -234,8 +275,9 @@ __device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const 
             for (int a = 0; a < 2; ++a)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) acc[a][j] = C(0.0, 0.0);
+#pragma unroll 4
             for (int k = 0; k < w; ++k) {
-                const cplx t0 = tile[ty][k], t1 = tile[ty + 16][k];
+                const cplx t0 = tile[ty * WMAX + k], t1 = tile[(ty + 16) * WMAX + k];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const cplx u = U[k][tx + 16 * j];
@@ -261,11 +303,14 @@ __device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const 
 // Window [ws, we) of H <- U^H (.) U everywhere outside the window, given that
 // the window itself was already transformed in shared memory: rows ws..we-1 to
 // the right (columns we..n-1), columns ws..we-1 above (rows 0..ws-1), and Z.
+// The tile buffers overlay B: the window must be stored before the call.
 __device__ void far_all(int n, cplx* H, int ldh, cplx* Z, int ldz, int ws, int we, AedShared* sh) {
     const int w = we - ws;
-    if (we < n) far_left(H, ldh, ws, w, we, n, sh->U, &sh->tile[0][0]);
-    if (ws > 0) far_right(H, ldh, 0, ws, ws, w, sh->U, sh->tile);
-    far_right(Z, ldz, 0, n, ws, w, sh->U, sh->tile);
+    cplx* buf = &sh->B[0][0];
+    __syncthreads();
+    if (we < n) far_left(H, ldh, ws, w, we, n, sh->U, buf);
+    if (ws > 0) far_right(H, ldh, 0, ws, ws, w, sh->U, buf);
+    far_right(Z, ldz, 0, n, ws, w, sh->U, buf);
 }
 
 __device__ void load_window(const cplx* H, int ldh, int ws, int w, AedShared* sh) {
@@ -291,8 +336,9 @@ __device__ void store_window(cplx* H, int ldh, int ws, int w, const AedShared* s
 // ---- aggressive early deflation ---------------------------------------------------------------
 // Window [kwtop, hi] of the active block [lo, hi]. Sets sh->nd (deflated count)
 // and sh->nsu / sh->sh[0..nsu) (undeflated eigenvalues, the shifts).
-__device__ void aed(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, AedShared* sh) {
+__device__ void aed(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, AedShared* sh, long long* prof) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const long long t0 = clock64();
     const double eps = 2.220446049250313e-16;
     const double smallnum = 2.2250738585072014e-308 * (n / eps);
     const int kwtop = max(lo, hi - NWIN + 1), jw = hi - kwtop + 1;
@@ -369,6 +415,7 @@ __device__ void aed(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, A
         }
     }
     __syncthreads();
+    const long long t1 = clock64();
     const int nsu = sh->nsu;
     store_window(H, ldh, kwtop, jw, sh, true);
     if (kwtop > lo) {
@@ -376,10 +423,25 @@ __device__ void aed(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, A
             H[(size_t)(kwtop + i) * ldh + kwtop - 1] = (i == 0 && nsu > 0) ? cmul(s, cconj(sh->U[0][0])) : C(0.0, 0.0);
     }
     far_all(n, H, ldh, Z, ldz, kwtop, hi + 1, sh);
+    if (prof && tid == 0) {
+        prof[0] += t1 - t0;
+        prof[1] += clock64() - t1;
+    }
 }
 
 // ---- one multishift sweep over the active block [lo, hi] with nsh shifts ----------------------
-__device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, int nsh, AedShared* sh) {
+// All bulges move in lockstep, so the moves of every step follow from the
+// positions at the start of a window: in the first window (ws = lo) bulge b is
+// introduced at step 2b and sits at lo + t - 2b before step t > 2b; later
+// windows introduce nothing and bulge b sits at pos[b] + t until it leaves the
+// block (its last move starts at hi - 1). A window runs while the leading
+// bulge's move stays inside it (its rows reach p + 2 <= we - 1), or, in the
+// window that ends at hi, until every bulge has left.
+static_assert(WMAX - 2 > 2 * (NSH - 1), "the first window introduces every bulge");
+static_assert(2 * WMAX * FT <= WMAX * (WMAX + 1), "tile buffers overlay the window");
+
+__device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, int nsh, AedShared* sh,
+                            long long* prof) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
     constexpr int ldb = WMAX + 1, ldu = WMAX;
     cplx* B = &sh->B[0][0];
@@ -393,52 +455,42 @@ __device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, i
     __syncthreads();
     for (int guard = 0; guard < n / 4 + 32; ++guard) {  // a sweep takes about n / 30 windows
         const int ws = sh->ws, we = sh->we, w = we - ws;
-        load_window(H, ldh, ws, w, sh);
-        for (int step = 0; step < 4 * WMAX; ++step) {
-            if (tid == 0) {
-                int np = 0, last = -1, lead = -1;
-                for (int b = 0; b < sh->nxt; ++b)
-                    if (sh->pos[b] >= 0) {
-                        if (lead < 0) lead = b;
-                        last = b;
-                    }
-                bool intro = ws == lo && sh->nxt < nsh && (last < 0 || sh->pos[last] >= lo + 2) &&
-                             (lo + 2 <= we - 1 || lo + 1 == hi);
-                bool go = true;
-                if (lead >= 0) {
-                    const int p = sh->pos[lead];
-                    go = p <= we - 3 || (we == hi + 1 && p <= hi - 1);
-                } else {
-                    go = intro;
+        const bool first = sh->nxt == 0;
+        int S;
+        if (first) {
+            S = we - 2 - lo;  // we < hi + 1 here: the block is longer than a window
+        } else {
+            int plead = -1, plast = 1 << 30;
+            for (int b = 0; b < nsh; ++b) {
+                const int p = sh->pos[b];
+                if (p >= 0) {
+                    plead = max(plead, p);
+                    plast = min(plast, p);
                 }
-                if (go) {
-                    for (int b = 0; b < sh->nxt; ++b) {
-                        const int p = sh->pos[b];
-                        if (p < 0) continue;
-                        sh->plan_k[np] = p;
-                        sh->plan_intro[np] = -1;
-                        ++np;
-                        sh->pos[b] = p + 1 <= hi - 1 ? p + 1 : -1;
-                    }
-                    if (intro) {
-                        sh->plan_k[np] = lo;
-                        sh->plan_intro[np] = sh->nxt;
-                        ++np;
-                        sh->pos[sh->nxt] = lo + 1 <= hi - 1 ? lo + 1 : -1;
-                        sh->nxt += 1;
-                    }
-                }
-                sh->nplan = np;
             }
-            __syncthreads();
-            const int np = sh->nplan;
-            if (np == 0) break;
-            // phase 1: row rotations
-            for (int t = warp; t < np; t += nwarp) {
-                const int k = sh->plan_k[t] - ws, si = sh->plan_intro[t];
+            S = (we == hi + 1) ? hi - plast : we - 2 - plead;
+        }
+        const long long t0 = clock64();
+        load_window(H, ldh, ws, w, sh);
+        for (int t = 0; t < S; ++t) {
+            // phase 1: row rotations (one warp per bulge)
+            for (int b = warp; b < nsh; b += nwarp) {
+                int p;
+                bool intro = false;
+                if (first) {
+                    if (t < 2 * b) continue;
+                    intro = t == 2 * b;
+                    p = intro ? lo : lo + t - 2 * b;
+                } else {
+                    const int p0 = sh->pos[b];
+                    if (p0 < 0) continue;
+                    p = p0 + t;
+                    if (p > hi - 1) continue;
+                }
+                const int k = p - ws;
                 cplx a, bb;
-                if (si >= 0) {
-                    a = csub(B[k * ldb + k], sh->shift[si]);
+                if (intro) {
+                    a = csub(B[k * ldb + k], sh->shift[b]);
                     bb = B[(k + 1) * ldb + k];
                 } else {
                     a = B[k * ldb + k - 1];
@@ -448,38 +500,62 @@ __device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, i
                 cplx s;
                 givens(a, bb, c, s);
                 __syncwarp();
-                wrot_rows(B, ldb, k, c, s, si >= 0 ? k : k - 1, w, lane);
+                wrot_rows(B, ldb, k, c, s, intro ? k : k - 1, w, lane);
                 __syncwarp();
                 if (lane == 0) {
-                    if (si < 0) B[(k + 1) * ldb + k - 1] = C(0.0, 0.0);
-                    sh->rc[t] = c;
-                    sh->rs[t] = s;
+                    if (!intro) B[(k + 1) * ldb + k - 1] = C(0.0, 0.0);
+                    sh->rc[b] = c;
+                    sh->rs[b] = s;
                 }
             }
             __syncthreads();
             // phase 2: column rotations
-            for (int t = warp; t < np; t += nwarp) {
-                const int p = sh->plan_k[t], k = p - ws;
-                const double c = sh->rc[t];
-                const cplx s = sh->rs[t];
+            for (int b = warp; b < nsh; b += nwarp) {
+                int p;
+                if (first) {
+                    if (t < 2 * b) continue;
+                    p = t == 2 * b ? lo : lo + t - 2 * b;
+                } else {
+                    const int p0 = sh->pos[b];
+                    if (p0 < 0) continue;
+                    p = p0 + t;
+                    if (p > hi - 1) continue;
+                }
+                const int k = p - ws;
+                const double c = sh->rc[b];
+                const cplx s = sh->rs[b];
                 wrot_cols(B, ldb, k, c, s, 0, min(p + 2, hi) - ws + 1, lane);
                 wrot_cols(U, ldu, k, c, s, 0, w, lane);
             }
             __syncthreads();
         }
+        const long long t1 = clock64();
         store_window(H, ldh, ws, w, sh, false);
         far_all(n, H, ldh, Z, ldz, ws, we, sh);  // begins and ends with barriers
+        if (prof && tid == 0) {
+            prof[2] += t1 - t0;
+            prof[3] += clock64() - t1;
+        }
         if (tid == 0) {
-            int last = -1;
-            for (int b = 0; b < sh->nxt; ++b)
-                if (sh->pos[b] >= 0) last = b;
-            if (last < 0 && sh->nxt >= nsh) {
+            int plast = 1 << 30;
+            for (int b = 0; b < nsh; ++b) {
+                int p;
+                if (first) {
+                    p = 2 * b < S ? lo + S - 2 * b : -2;
+                } else {
+                    p = sh->pos[b] >= 0 ? sh->pos[b] + S : -1;
+                }
+                if (p > hi - 1) p = -1;
+                sh->pos[b] = p;
+                if (p >= 0) plast = min(plast, p);
+            }
+            sh->nxt = nsh;
+            if (plast == 1 << 30) {
                 sh->win_end = 1;
             } else {
                 sh->win_end = 0;
-                const int nws = last >= 0 ? sh->pos[last] - 1 : lo;
-                sh->ws = nws;
-                sh->we = min(nws + WMAX, hi + 1);
+                sh->ws = plast - 1;
+                sh->we = min(plast - 1 + WMAX, hi + 1);
             }
         }
         __syncthreads();
@@ -487,9 +563,9 @@ __device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, i
     }
 }
 
-// T <- Q^H H Q upper triangular, Z <- Z Q, for n > NSMALL. Returns info (0, or
-// the 1-based row where the iteration cap ran out).
-__device__ int blk_schur_aed(int n, cplx* H, int ldh, cplx* Z, int ldz, AedShared* sh) {
+// prof (optional, per cell): clock64 sums of [AED local, AED far, sweep local,
+// sweep far, small blocks].
+__device__ int blk_schur_aed(int n, cplx* H, int ldh, cplx* Z, int ldz, AedShared* sh, long long* prof) {
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     const double eps = 2.220446049250313e-16;
     const double smallnum = 2.2250738585072014e-308 * (n / eps);
@@ -529,6 +605,7 @@ __device__ int blk_schur_aed(int n, cplx* H, int ldh, cplx* Z, int ldz, AedShare
         const int lo = sh->lo, hi = sh->hi, L = hi - lo + 1;
         if (L <= NSMALL) {
             // the whole block in shared memory
+            const long long t0 = clock64();
             load_window(H, ldh, lo, L, sh);
             if (warp == 0) {
                 const int info = warp_schur_small(L, &sh->B[0][0], WMAX + 1, &sh->U[0][0], WMAX, L, lane);
@@ -537,6 +614,7 @@ __device__ int blk_schur_aed(int n, cplx* H, int ldh, cplx* Z, int ldz, AedShare
             __syncthreads();
             store_window(H, ldh, lo, L, sh, true);
             far_all(n, H, ldh, Z, ldz, lo, hi + 1, sh);
+            if (prof && tid == 0) prof[4] += clock64() - t0;
             if (tid == 0) {
                 sh->hi = lo - 1;
                 sh->it = 0;
@@ -548,7 +626,7 @@ __device__ int blk_schur_aed(int n, cplx* H, int ldh, cplx* Z, int ldz, AedShare
             if (sh->hi <= 0) break;
             continue;
         }
-        aed(n, H, ldh, Z, ldz, lo, hi, sh);
+        aed(n, H, ldh, Z, ldz, lo, hi, sh, prof);
         if (tid == 0) {
             const int nd = sh->nd;
             sh->hi = hi - nd;
@@ -574,11 +652,11 @@ __device__ int blk_schur_aed(int n, cplx* H, int ldh, cplx* Z, int ldz, AedShare
                     for (int i = 0; i < nsh; ++i) sh->shift[i] = H[(size_t)(sh->hi - i) * ldh + sh->hi - i];
                 }
             }
-            sh->nplan = nsh;  // reused as the shift count of the sweep
+            sh->nshift = nsh;  // reused as the shift count of the sweep
         }
         __syncthreads();
-        const int nsh = sh->nplan;
-        if (nsh > 0) chain_sweep(n, H, ldh, Z, ldz, lo, sh->hi, nsh, sh);
+        const int nsh = sh->nshift;
+        if (nsh > 0) chain_sweep(n, H, ldh, Z, ldz, lo, sh->hi, nsh, sh, prof);
         if (iter == max_iter - 1 && tid == 0) sh->info = sh->hi + 1;
         __syncthreads();
     }

@@ -726,6 +726,22 @@ HostCell make_cell(const celeris_rcwa_cell& c, int index, double ex_re, double e
     return h;
 }
 
+// Shared memory of the Schur kernel: two CTAs fit per SM with sizeof(AedShared);
+// a launch with no more cells than SMs asks for more than half an SM's shared
+// memory so that the cells spread one per SM instead of pairing up.
+constexpr size_t kSchurSmemOneCta = 120 * 1024;
+static_assert(sizeof(AedShared) <= kSchurSmemOneCta, "Schur shared block");
+size_t schur_smem(int ncell) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 1;
+    }
+    return ncell <= sms ? kSchurSmemOneCta : sizeof(AedShared);
+}
+
 // staging of blk_hessenberg_blocked
 size_t hess_stage_bytes(int n) { return (size_t)(n + LNB * LNB + 2 * LNB) * sizeof(cplx); }
 
@@ -809,7 +825,7 @@ int set_smem_limits(const SmemNeeds& s) {
         CEL_CUDA(cudaFuncSetAttribute(rcwa_fourier_rect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.rect));
     if (s.aed)
         CEL_CUDA(cudaFuncSetAttribute(rcwa_schur<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sizeof(AedShared)));
+                                      (int)kSchurSmemOneCta));
     if (s.hess_s) {
         CEL_CUDA(cudaFuncSetAttribute(rcwa_hess<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.hess_s));
         CEL_CUDA(cudaFuncSetAttribute(rcwa_schur<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.hess_s));
@@ -847,11 +863,11 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
         const size_t sm = ((size_t)n * n + 2 * n) * sizeof(cplx);
         rcwa_hess<true><<<nc, T[ST_HESS], sm, st>>>(b);
         if (ev) cudaEventRecord(ev[3], st);
-        rcwa_schur<false><<<nc, T[ST_SCHUR], sizeof(AedShared), st>>>(b);
+        rcwa_schur<false><<<nc, T[ST_SCHUR], schur_smem(nc), st>>>(b);
     } else {
         rcwa_hess<false><<<nc, T[ST_HESS], hess_stage_bytes(n), st>>>(b);
         if (ev) cudaEventRecord(ev[3], st);
-        rcwa_schur<false><<<nc, T[ST_SCHUR], sizeof(AedShared), st>>>(b);
+        rcwa_schur<false><<<nc, T[ST_SCHUR], schur_smem(nc), st>>>(b);
     }
     if (ev) cudaEventRecord(ev[4], st);
     rcwa_vec<<<nc, T[ST_VEC], 0, st>>>(b);
@@ -1104,10 +1120,10 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                 CEL_CUDA(cudaStreamSynchronize(st));
                 std::vector<long long> h(8 * nc);
                 cudaMemcpy(h.data(), dbg, sizeof(long long) * 8 * nc, cudaMemcpyDeviceToHost);
-                double sw = 0, ph[5] = {0, 0, 0, 0, 0};
+                double sw = 0, ph[6] = {0, 0, 0, 0, 0, 0};
                 for (int i = 0; i < nc; ++i) {
                     sw += (double)h[8 * i + 6];
-                    for (int q = 0; q < 5; ++q) ph[q] += (double)h[8 * i + q];
+                    for (int q = 0; q < 6; ++q) ph[q] += (double)h[8 * i + q];
                 }
                 std::string line = "[rcwa stages] n=" + std::to_string(p.n) + " cells=" + std::to_string(nc) + " ms:";
                 for (int s = 0; s < ST_COUNT; ++s) {
@@ -1120,8 +1136,9 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                 char buf[64];
                 std::snprintf(buf, sizeof(buf), " | sweeps/cell %.1f", sw / nc);
                 char buf2[160];
-                std::snprintf(buf2, sizeof(buf2), " | schur Mcycles/cell: aed %.2f aed_far %.2f sweep %.2f sweep_far %.2f small %.2f\n",
-                              ph[0] / nc * 1e-6, ph[1] / nc * 1e-6, ph[2] / nc * 1e-6, ph[3] / nc * 1e-6, ph[4] / nc * 1e-6);
+                std::snprintf(buf2, sizeof(buf2), " | schur Mcycles/cell: aed %.2f (qr %.2f) aed_far %.2f sweep %.2f sweep_far %.2f small %.2f\n",
+                              ph[0] / nc * 1e-6, ph[5] / nc * 1e-6, ph[1] / nc * 1e-6, ph[2] / nc * 1e-6, ph[3] / nc * 1e-6,
+                              ph[4] / nc * 1e-6);
                 std::fprintf(stderr, "%s%s%s", line.c_str(), buf, buf2);
                 for (auto& e : ev) cudaEventDestroy(e);
                 cudaFree(dbg);

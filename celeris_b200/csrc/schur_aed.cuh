@@ -26,11 +26,14 @@
 
 namespace cb {
 
-constexpr int WMAX = 64;   // window size (rows/columns)
-constexpr int NSH = 16;    // shifts per sweep
-constexpr int NWIN = 32;   // AED window
-constexpr int NSMALL = 64; // active blocks up to this size are finished in shared memory
-constexpr int FT = 32;     // far-update tile (rows or columns)
+// WMAX = 56 keeps the shared block near 104 KB, so two cells share an SM and
+// one cell's latency-bound phases (AED, rotation steps) overlap the other's
+// products; with 16 shifts a window still advances the chain by 23 rows.
+constexpr int WMAX = 56;     // window size (rows/columns)
+constexpr int NSH = 16;      // shifts per sweep
+constexpr int NWIN = 24;     // AED window
+constexpr int NSMALL = WMAX; // active blocks up to this size are finished in shared memory
+constexpr int FT = 28;       // far-update tile (rows or columns)
 
 struct AedShared {
     cplx B[WMAX][WMAX + 1];  // window; during far updates two tile buffers of WMAX * FT
@@ -211,31 +214,36 @@ __device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const c
         __syncthreads();
         const cplx* tile = buf + (t & 1) * FBUF;
         const int cb = c0 + t * FT, nc = min(FT, c1 - cb);
-        for (int q = tid; q < 256; q += nt) {
-            const int ty = q >> 3, tx = q & 7;  // rows ty, ty+32; columns tx + 8j
+        // thread grid (WMAX/2) x (FT/4), each thread rows ty, ty + WMAX/2 and
+        // columns tx + j FT/4 (j < 4): every slot is a real output of a full tile
+        constexpr int R2 = WMAX / 2, C4 = FT / 4;
+        for (int q = tid; q < R2 * C4; q += nt) {
+            const int ty = q / C4, tx = q % C4;
+            if (ty >= w) continue;
             cplx acc[2][4];
 #pragma unroll
             for (int a = 0; a < 2; ++a)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) acc[a][j] = C(0.0, 0.0);
+            const bool two = ty + R2 < w;
 #pragma unroll 4
             for (int k = 0; k < w; ++k) {
                 const cplx u0 = cconj(U[k][ty]);
-                const cplx u1 = cconj(U[k][ty + 32]);
+                const cplx u1 = two ? cconj(U[k][ty + R2]) : C(0.0, 0.0);
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    const cplx tv = tile[k * FT + tx + 8 * j];
+                    const cplx tv = tile[k * FT + tx + C4 * j];
                     acc[0][j] = cfma(u0, tv, acc[0][j]);
                     acc[1][j] = cfma(u1, tv, acc[1][j]);
                 }
             }
 #pragma unroll
             for (int a = 0; a < 2; ++a) {
-                const int r = ty + 32 * a;
+                const int r = ty + R2 * a;
                 if (r >= w) continue;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    const int c = tx + 8 * j;
+                    const int c = tx + C4 * j;
                     if (c < nc) X[(size_t)(r0 + r) * ld + cb + c] = acc[a][j];
                 }
             }
@@ -268,8 +276,11 @@ __device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const 
         __syncthreads();
         const cplx* tile = buf + (t & 1) * FBUF;
         const int rb = r0 + t * FT, nr = min(FT, r1 - rb);
-        for (int q = tid; q < 256; q += nt) {
-            const int ty = q >> 4, tx = q & 15;  // rows ty, ty+16; columns tx + 16j
+        // thread grid (FT/2) x (WMAX/4): rows ty, ty + FT/2, columns tx + j WMAX/4
+        constexpr int R2 = FT / 2, C4 = WMAX / 4;
+        for (int q = tid; q < R2 * C4; q += nt) {
+            const int ty = q / C4, tx = q % C4;
+            if (ty >= nr || tx >= w) continue;
             cplx acc[2][4];
 #pragma unroll
             for (int a = 0; a < 2; ++a)
@@ -277,21 +288,21 @@ __device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const 
                 for (int j = 0; j < 4; ++j) acc[a][j] = C(0.0, 0.0);
 #pragma unroll 4
             for (int k = 0; k < w; ++k) {
-                const cplx t0 = tile[ty * WMAX + k], t1 = tile[(ty + 16) * WMAX + k];
+                const cplx t0 = tile[ty * WMAX + k], t1 = tile[(ty + R2) * WMAX + k];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    const cplx u = U[k][tx + 16 * j];
+                    const cplx u = U[k][tx + C4 * j];
                     acc[0][j] = cfma(t0, u, acc[0][j]);
                     acc[1][j] = cfma(t1, u, acc[1][j]);
                 }
             }
 #pragma unroll
             for (int a = 0; a < 2; ++a) {
-                const int r = ty + 16 * a;
+                const int r = ty + R2 * a;
                 if (r >= nr) continue;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    const int c = tx + 16 * j;
+                    const int c = tx + C4 * j;
                     if (c < w) X[(size_t)(rb + r) * ld + c0 + c] = acc[a][j];
                 }
             }
@@ -348,7 +359,9 @@ __device__ void aed(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, A
     cplx* U = &sh->U[0][0];
     constexpr int ldb = WMAX + 1, ldu = WMAX;
     if (warp == 0) {
+        const long long ts0 = clock64();
         const int info = warp_schur_small(jw, B, ldb, U, ldu, jw, lane);
+        if (prof && lane == 0) prof[5] += clock64() - ts0;
         int nsu = jw, ilst = 0;
         if (info == 0) {
             while (nsu > ilst) {
@@ -439,6 +452,7 @@ __device__ void aed(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, A
 // window that ends at hi, until every bulge has left.
 static_assert(WMAX - 2 > 2 * (NSH - 1), "the first window introduces every bulge");
 static_assert(2 * WMAX * FT <= WMAX * (WMAX + 1), "tile buffers overlay the window");
+static_assert(WMAX % 4 == 0 && FT % 4 == 0, "far-update thread grids");
 
 __device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, int nsh, AedShared* sh,
                             long long* prof) {

@@ -354,12 +354,21 @@ def measure_rcwa(peaks, quick=False, with_cpu=True):
     if not quick:
         cells = rcwa_uneven_4096()
         cc = [capi.rcwa_cell(**c) for c in cells]
+        # first call: tunes the CTA sizes of new bucket shapes and captures the
+        # batch graph; later calls with the same shapes replay it
         t0 = time.perf_counter()
         res, info = capi.rcwa_batch(cc)
-        dt2 = time.perf_counter() - t0
+        first = time.perf_counter() - t0
+        warm = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            res, info = capi.rcwa_batch(cc)
+            warm.append(time.perf_counter() - t0)
+        dt2 = min(warm)
         fl2 = sum(rcwa_flops(c) for c in cells)
         out["uneven_4096_M3to7_grid256"] = {
-            "value": len(cells) / dt2, "s": dt2, "failed_cells": int(np.sum(info != 0)),
+            "value": len(cells) / dt2, "s": dt2, "first_call_s": first,
+            "first_call_cells_s": len(cells) / first, "failed_cells": int(np.sum(info != 0)),
             "max_abs_R_plus_T_minus_1": float(max(abs(r["R"] + r["T"] - 1.0) for r in res)),
             "roofline": {"bound": "fp64", "achieved": fl2 / dt2, "peak": p_fp64, "unit": "FLOP/s",
                          "frac": fl2 / dt2 / p_fp64}}
@@ -491,7 +500,10 @@ def run_gpu(args):
                   "api": "celeris_rs_field (C ABI, host buffers, F32C form, stated error on)",
                   "stated_error": stated, "ms_per_step": 1e3 * float(np.mean(e2e_t))}
     # ---- RCWA cells/s ------------------------------------------------------------
+    rclk = ClockSampler(local)
+    rclk.start()
     out["rcwa"] = measure_rcwa(peaks, quick=args.quick, with_cpu=not args.no_cpu)
+    out["rcwa"]["clocks"] = rclk.stop()
     # ---- CPU baseline: the reference's own far-field on this host --------------
     if not args.no_cpu:
         try:

@@ -170,74 +170,88 @@ __device__ __forceinline__ void gemm_tiles(int m, int n, int k, cplx alpha, cons
     const bool act = tid < NT;
     const int ty = tid / TX, tx = tid % TX;
     const int mt = (m + GM - 1) / GM, ntl = (n + GN - 1) / GN;
+    const int nk = (k + GKC - 1) / GKC;
+    const int total = mt * ntl * nk;  // (tile, k-chunk) steps, fetched one step ahead
+    if (total == 0) return;
     const bool use_beta = beta.x != 0.0 || beta.y != 0.0;
-    for (int t = 0; t < mt * ntl; ++t) {
+    cplx acc[4][4];
+    cplx ra[PA], rb[PB];
+    // A is staged pre-multiplied by alpha, and the accumulators start from
+    // beta C, so C is read at the start of a tile (its latency overlaps the
+    // tile's first fetch) and the epilogue only stores.
+    auto fetch = [&](int g) {
+        const int t = g / nk, k0 = (g - t * nk) * GKC;
         const int i0 = (t / ntl) * GM, j0 = (t % ntl) * GN;
-        cplx acc[4][4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int s = 0; s < PA; ++s) {
+            const int e = tid + s * NT, r = e / GKC, c = e % GKC;
+            ra[s] = (act && i0 + r < m && k0 + c < k) ? A[(size_t)(i0 + r) * lda + k0 + c] : C(0.0, 0.0);
+        }
 #pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = C(0.0, 0.0);
-        cplx ra[PA], rb[PB];
-        auto fetch = [&](int k0) {
+        for (int s = 0; s < PB; ++s) {
+            const int e = tid + s * NT, r = e / GN, c = e % GN;
+            rb[s] = (act && k0 + r < k && j0 + c < n) ? B[(size_t)(k0 + r) * ldb + j0 + c] : C(0.0, 0.0);
+        }
+    };
+    auto init_acc = [&](int t) {
+        const int i0 = (t / ntl) * GM, j0 = (t % ntl) * GN;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int r = i0 + ty + 16 * i;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int c = j0 + tx + TX * j;
+                acc[i][j] = (use_beta && act && r < m && c < n) ? cmul(beta, Cm[(size_t)r * ldc + c]) : C(0.0, 0.0);
+            }
+        }
+    };
+    init_acc(0);
+    fetch(0);
+    for (int g = 0; g < total; ++g) {
+        if (act) {
 #pragma unroll
             for (int s = 0; s < PA; ++s) {
-                const int e = tid + s * NT, r = e / GKC, c = e % GKC;
-                ra[s] = (act && i0 + r < m && k0 + c < k) ? A[(size_t)(i0 + r) * lda + k0 + c] : C(0.0, 0.0);
+                const int e = tid + s * NT;
+                sm->a[e % GKC][e / GKC] = cmul(alpha, ra[s]);
             }
 #pragma unroll
             for (int s = 0; s < PB; ++s) {
-                const int e = tid + s * NT, r = e / GN, c = e % GN;
-                rb[s] = (act && k0 + r < k && j0 + c < n) ? B[(size_t)(k0 + r) * ldb + j0 + c] : C(0.0, 0.0);
+                const int e = tid + s * NT;
+                sm->b[e / GN][e % GN] = rb[s];
             }
-        };
-        fetch(0);
-        for (int k0 = 0; k0 < k; k0 += GKC) {
-            if (act) {
-#pragma unroll
-                for (int s = 0; s < PA; ++s) {
-                    const int e = tid + s * NT;
-                    sm->a[e % GKC][e / GKC] = ra[s];
-                }
-#pragma unroll
-                for (int s = 0; s < PB; ++s) {
-                    const int e = tid + s * NT;
-                    sm->b[e / GN][e % GN] = rb[s];
-                }
-            }
-            __syncthreads();
-            if (k0 + GKC < k) fetch(k0 + GKC);
-            if (act) {
-#pragma unroll
-                for (int kk = 0; kk < GKC; ++kk) {
-                    cplx av[4], bv[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) av[i] = sm->a[kk][ty + 16 * i];
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) bv[j] = sm->b[kk][tx + TX * j];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) acc[i][j] = cfma(av[i], bv[j], acc[i][j]);
-                }
-            }
-            __syncthreads();
         }
+        __syncthreads();
+        if (g + 1 < total) fetch(g + 1);
         if (act) {
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                const int r = i0 + ty + 16 * i;
+            for (int kk = 0; kk < GKC; ++kk) {
+                cplx av[4], bv[4];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int c = j0 + tx + TX * j;
-                    if (r < m && c < n) {
-                        cplx* dst = &Cm[(size_t)r * ldc + c];
-                        cplx v = cmul(alpha, acc[i][j]);
-                        if (use_beta) v = cfma(beta, *dst, v);
-                        *dst = v;
+                for (int i = 0; i < 4; ++i) av[i] = sm->a[kk][ty + 16 * i];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) bv[j] = sm->b[kk][tx + TX * j];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = cfma(av[i], bv[j], acc[i][j]);
+            }
+        }
+        __syncthreads();
+        const int t = g / nk;
+        if (g - t * nk == nk - 1) {  // last chunk of tile t: store it, start the next
+            if (act) {
+                const int i0 = (t / ntl) * GM, j0 = (t % ntl) * GN;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int r = i0 + ty + 16 * i;
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int c = j0 + tx + TX * j;
+                        if (r < m && c < n) Cm[(size_t)r * ldc + c] = acc[i][j];
                     }
                 }
             }
+            if (g + 1 < total) init_acc(t + 1);
         }
     }
 }
@@ -386,6 +400,7 @@ __device__ __forceinline__ void blk_matvec_rows(int rows, int cols, const cplx* 
                                                 double beta, int warp, int lane, int nwarp) {
     for (int i0 = 4 * warp; i0 < rows; i0 += 4 * nwarp) {
         cplx acc[4] = {C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0)};
+#pragma unroll 2
         for (int j = lane; j < cols; j += 32) {
             const cplx vj = v[j];
             cplx h[4];
@@ -414,6 +429,7 @@ __device__ __forceinline__ void blk_matvec2(int rows, int cols, const cplx* A, i
     for (int i0 = 2 * warp; i0 < rows; i0 += 2 * nwarp) {
         cplx acc[2][2] = {{C(0.0, 0.0), C(0.0, 0.0)}, {C(0.0, 0.0), C(0.0, 0.0)}};
         const bool two = i0 + 1 < rows;
+#pragma unroll 2
         for (int j = lane; j < cols; j += 32) {
             const cplx v0 = v[2 * j], v1 = v[2 * j + 1];
             const cplx a0 = A[(size_t)i0 * lda + j];

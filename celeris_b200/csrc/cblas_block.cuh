@@ -8,14 +8,15 @@
 // barrier, so consecutive calls compose without extra synchronization.
 //
 // Routines (all O(n^3) work is spread over the block; loops are bounded):
-//   blk_gemm        C = alpha A B + beta C (smem-staged 32x32 tiles)
+//   blk_gemm        C = alpha A B + beta C (register-tiled, smem-staged k chunks)
 //   blk_lu          partial-pivot LU in place (LAPACK zgetrf semantics: pivot =
-//                   first max |re|+|im| in the column)
+//                   first max |re|+|im| in the column); blk_lu_blocked: panels
+//                   of LNB columns with GEMM trailing updates, same pivots
 //   blk_lu_solve    X = A^{-1} B from the LU factors, any number of RHS
+//                   (blk_lu_solve_blocked: block rows with GEMM updates)
 //   blk_hessenberg  Householder reduction to upper Hessenberg, Z accumulated
-//   blk_schur       complex single-shift QR (Wilkinson shift, deflation on
-//                   negligible subdiagonals, exceptional shifts) to upper
-//                   triangular T, Z updated; sweep cap -> info > 0
+//                   (blk_hessenberg_blocked: compact-WY panels, GEMM updates)
+//   givens, wilkinson  rotation and shift helpers of the Schur form (schur_aed.cuh)
 //   blk_trevc       right eigenvectors of triangular T by back substitution
 #pragma once
 
@@ -843,221 +844,7 @@ __device__ __forceinline__ cplx wilkinson(cplx a, cplx b, cplx c, cplx d) {
     return cabs1(csub(e1, d)) <= cabs1(csub(e2, d)) ? e1 : e2;
 }
 
-constexpr int QW = 16;  // bulge-chase window (rows/columns)
-constexpr int kMaxN = 1024;
-
-struct SchurShared {
-    cplx B[QW][QW + 1];  // the window block
-    double c[QW];        // rotations of the current window
-    cplx s[QW];
-    unsigned char flag[kMaxN];
-    int lo, hi, done, info, nsweep;
-    cplx shift;
-};
-
-// Apply the window's row rotations (rows ws+R0+t, ws+R0+t+1, t < nr) to the
-// column segment H[ws : ws+w, j] held in registers; rotation t is
-// [[c, s], [-conj(s), c]].
-template <int R0>
-__device__ __forceinline__ void rot_rows_col(cplx* col0, int ld, int w, int nr, const SchurShared* sh) {
-    cplx v[QW];
-#pragma unroll
-    for (int q = 0; q < QW; ++q)
-        if (q < w) v[q] = col0[(size_t)q * ld];
-#pragma unroll
-    for (int t = 0; t + R0 + 1 < QW; ++t) {
-        if (t < nr) {
-            const double c = sh->c[t];
-            const cplx s = sh->s[t];
-            const cplx x = v[R0 + t], y = v[R0 + t + 1];
-            v[R0 + t] = cfma(s, y, cscale(x, c));
-            v[R0 + t + 1] = cfma(cneg(cconj(s)), x, cscale(y, c));
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < QW; ++q)
-        if (q < w) col0[(size_t)q * ld] = v[q];
-}
-
-// Apply the window's column rotations (columns ws+R0+t, ws+R0+t+1) to the row
-// segment row0[0 : w] (one row of H above the window, or of Z): new col k =
-// c h_k + conj(s) h_{k+1}, new col k+1 = -s h_k + c h_{k+1}.
-template <int R0>
-__device__ __forceinline__ void rot_cols_row(cplx* row0, int w, int nr, const SchurShared* sh) {
-    cplx v[QW];
-#pragma unroll
-    for (int q = 0; q < QW; ++q)
-        if (q < w) v[q] = row0[q];
-#pragma unroll
-    for (int t = 0; t + R0 + 1 < QW; ++t) {
-        if (t < nr) {
-            const double c = sh->c[t];
-            const cplx s = sh->s[t];
-            const cplx x = v[R0 + t], y = v[R0 + t + 1];
-            v[R0 + t] = cfma(cconj(s), y, cscale(x, c));
-            v[R0 + t + 1] = cfma(cneg(s), x, cscale(y, c));
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < QW; ++q)
-        if (q < w) row0[q] = v[q];
-}
-
-// T <- Q^H H Q upper triangular, Z <- Z Q. Returns info (0, or hi+1 when the
-// sweep cap ran out with rows 0..hi unconverged).
-//
-// Each sweep chases one bulge down the active window [lo, hi] in blocks of at
-// most QW rows/columns: warp 0 performs the rotations of a block on a shared
-// copy of H[ws:we, ws:we] (warp-synchronous), recording them; then the whole
-// CTA applies the recorded rotations to the rest of rows ws..we-1 (columns
-// >= we), to the rest of columns ws..we-1 (rows < ws) and to Z, each thread
-// owning one column or row segment in registers. Consecutive blocks overlap by
-// the bulge column, so every entry a rotation reads is current when it is read.
-__device__ int blk_schur(int n, cplx* H, int ldh, cplx* Z, int ldz, SchurShared* sh, int max_sweeps_per_row) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int warp = tid >> 5, lane = tid & 31;
-    const double eps = 2.220446049250313e-16;
-    const double smallnum = 2.2250738585072014e-308 * (n / eps);
-    if (tid == 0) {
-        sh->hi = n - 1;
-        sh->lo = 0;
-        sh->done = 0;
-        sh->info = 0;
-        sh->nsweep = 0;
-    }
-    __syncthreads();
-    int iter_row = 0;  // used by thread 0 only
-    const long max_total = (long)max_sweeps_per_row * n;
-    long total = 0;
-    while (true) {
-        // negligible subdiagonals of [1, hi], in parallel
-        const int hi0 = sh->hi;
-        for (int i = 1 + tid; i <= hi0; i += nt) {
-            const double tst = cabs1(H[(size_t)(i - 1) * ldh + i - 1]) + cabs1(H[(size_t)i * ldh + i]);
-            sh->flag[i] = cabs1(H[(size_t)i * ldh + i - 1]) <= fmax(eps * tst, smallnum) ? 1 : 0;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            int hi = hi0;
-            while (hi > 0 && sh->flag[hi]) {
-                H[(size_t)hi * ldh + hi - 1] = C(0.0, 0.0);
-                --hi;
-                iter_row = 0;
-            }
-            int lo = hi;
-            while (lo > 0 && !sh->flag[lo]) --lo;
-            if (lo > 0) H[(size_t)lo * ldh + lo - 1] = C(0.0, 0.0);
-            sh->hi = hi;
-            sh->lo = lo;
-            if (hi <= 0) {
-                sh->done = 1;
-            } else if (total >= max_total) {
-                sh->done = 1;
-                sh->info = hi + 1;
-            } else {
-                ++iter_row;
-                ++total;
-                sh->nsweep = (int)total;
-                if (iter_row == 10 || iter_row == 30) {  // exceptional shift
-                    const double e = fabs(H[(size_t)hi * ldh + hi - 1].x) +
-                                     (hi >= 2 ? fabs(H[(size_t)(hi - 1) * ldh + hi - 2].x) : 0.0);
-                    sh->shift = cadd(H[(size_t)hi * ldh + hi], C(e, 0.0));
-                } else {
-                    sh->shift = wilkinson(H[(size_t)(hi - 1) * ldh + hi - 1], H[(size_t)(hi - 1) * ldh + hi],
-                                          H[(size_t)hi * ldh + hi - 1], H[(size_t)hi * ldh + hi]);
-                }
-            }
-        }
-        __syncthreads();
-        if (sh->done) break;
-        const int lo = sh->lo, hi = sh->hi;
-        const cplx shift = sh->shift;
-        int k_next = lo;
-        bool first = true;
-        while (k_next < hi) {
-            const int ws = first ? lo : k_next - 1;
-            const int we = min(ws + QW, hi + 1);
-            const int k_last = (we == hi + 1) ? hi - 1 : we - 3;
-            const int w = we - ws;
-            const int r0 = k_next - ws;  // 0 for the first block of a sweep, else 1
-            const int nr = k_last - k_next + 1;
-            for (int e = tid; e < w * w; e += nt) {
-                const int r = e / w, cc = e % w;
-                sh->B[r][cc] = H[(size_t)(ws + r) * ldh + ws + cc];
-            }
-            __syncthreads();
-            if (warp == 0) {
-                for (int k = k_next; k <= k_last; ++k) {
-                    const int kk = k - ws;
-                    const bool start = first && k == lo;
-                    cplx a, b;
-                    if (start) {
-                        a = csub(sh->B[kk][kk], shift);
-                        b = sh->B[kk + 1][kk];
-                    } else {
-                        a = sh->B[kk][kk - 1];
-                        b = sh->B[kk + 1][kk - 1];
-                    }
-                    double c;
-                    cplx s;
-                    givens(a, b, c, s);
-                    const cplx ms = cneg(cconj(s)), cs = cconj(s), ns = cneg(s);
-                    const int jlo = start ? kk : kk - 1;
-                    for (int col = jlo + lane; col < w; col += 32) {
-                        const cplx x = sh->B[kk][col], y = sh->B[kk + 1][col];
-                        sh->B[kk][col] = cfma(s, y, cscale(x, c));
-                        sh->B[kk + 1][col] = cfma(ms, x, cscale(y, c));
-                    }
-                    __syncwarp();
-                    const int rmax = min(kk + 2, hi - ws);
-                    for (int row = lane; row <= rmax; row += 32) {
-                        const cplx x = sh->B[row][kk], y = sh->B[row][kk + 1];
-                        sh->B[row][kk] = cfma(cs, y, cscale(x, c));
-                        sh->B[row][kk + 1] = cfma(ns, x, cscale(y, c));
-                    }
-                    __syncwarp();
-                    if (lane == 0) {
-                        if (!start) sh->B[kk + 1][kk - 1] = C(0.0, 0.0);
-                        sh->c[k - k_next] = c;
-                        sh->s[k - k_next] = s;
-                    }
-                    __syncwarp();
-                }
-            }
-            __syncthreads();
-            for (int e = tid; e < w * w; e += nt) {
-                const int r = e / w, cc = e % w;
-                H[(size_t)(ws + r) * ldh + ws + cc] = sh->B[r][cc];
-            }
-            // deferred parts: rows ws..we-1 right of the block, columns ws..we-1
-            // above the block, and Z
-            const int nright = n - we, nabove = ws;
-            const int jobs = nright + nabove + n;
-            for (int e = tid; e < jobs; e += nt) {
-                if (e < nright) {
-                    cplx* col0 = H + (size_t)ws * ldh + we + e;
-                    if (r0 == 0)
-                        rot_rows_col<0>(col0, ldh, w, nr, sh);
-                    else
-                        rot_rows_col<1>(col0, ldh, w, nr, sh);
-                } else {
-                    cplx* row0 = (e < nright + nabove) ? H + (size_t)(e - nright) * ldh + ws
-                                                       : Z + (size_t)(e - nright - nabove) * ldz + ws;
-                    if (r0 == 0)
-                        rot_cols_row<0>(row0, w, nr, sh);
-                    else
-                        rot_cols_row<1>(row0, w, nr, sh);
-                }
-            }
-            __syncthreads();
-            k_next = k_last + 1;
-            first = false;
-        }
-    }
-    const int info = sh->info;
-    __syncthreads();
-    return info;
-}
+constexpr int kMaxN = 1024;  // largest matrix order (deflation flags are per row)
 
 // ---- eigenvectors of the triangular Schur factor ----------------------------------------
 // X (n x n, row-major) <- right eigenvectors of upper-triangular T: column k

@@ -47,7 +47,6 @@ using celeris_rt::Workspace;
 constexpr double PI = 3.14159265358979323846;
 constexpr int kRT = 256;            // threads per CTA
 constexpr int kSmemEigMaxN = 112;   // eigensolve in shared memory up to this n
-constexpr int kMaxSweepsPerRow = 30;
 
 struct CellDev {
     double omega;  // k0 = 2 pi / lambda (c = 1 units, omega = k0)
@@ -367,31 +366,19 @@ __global__ void __launch_bounds__(kRT) rcwa_hess(Bucket b) {
     }
 }
 
-// dynamic smem: SMEM: H [n*n] (windowed single-shift QR on the shared copy);
-// otherwise the AedShared block of the multishift/AED Schur form.
-template <bool SMEM>
-__global__ void __launch_bounds__(kRT) rcwa_schur(Bucket b) {
+// Schur form by multishift QR with aggressive early deflation (schur_aed.cuh).
+// dynamic smem: AedShared.
+__global__ void __launch_bounds__(kSchurThreads, 2) rcwa_schur(Bucket b) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int cell = blockIdx.x;
     const int n = b.n;
     const int tid = threadIdx.x, nt = blockDim.x;
-    cplx* Hg = at(b.H, b.s_nn, cell);
-    cplx* H = SMEM ? reinterpret_cast<cplx*>(smem) : Hg;
-    int info, nsweep;
-    if constexpr (SMEM) {
-        __shared__ SchurShared sh;
-        for (int e = tid; e < n * n; e += nt) H[e] = Hg[e];
-        __syncthreads();
-        info = blk_schur(n, H, n, at(b.Z, b.s_nn, cell), n, &sh, kMaxSweepsPerRow);
-        nsweep = sh.nsweep;
-    } else {
-        AedShared* sh = reinterpret_cast<AedShared*>(smem);
-        info = blk_schur_aed(n, H, n, at(b.Z, b.s_nn, cell), n, sh, b.dbg ? b.dbg + 8 * (size_t)cell : nullptr);
-        nsweep = sh->nsweep;
-    }
+    cplx* H = at(b.H, b.s_nn, cell);
+    AedShared* sh = reinterpret_cast<AedShared*>(smem);
+    const int info = blk_schur_aed(n, H, n, at(b.Z, b.s_nn, cell), n, sh, b.dbg ? b.dbg + 8 * (size_t)cell : nullptr);
     if (tid == 0) {
         if (info != 0) b.info[cell] = info;
-        if (b.dbg) b.dbg[8 * (size_t)cell + 6] = nsweep;
+        if (b.dbg) b.dbg[8 * (size_t)cell + 6] = sh->nsweep;
     }
     // eigenvalues -> q = branch(sqrt(lambda)) (rcwa2d.cpp:364)
     cplx* q1 = at(b.q1, b.s_n, cell);
@@ -399,10 +386,6 @@ __global__ void __launch_bounds__(kRT) rcwa_schur(Bucket b) {
         cplx q = csqrt_p(H[(size_t)i * n + i]);
         if (q.y < 0.0) q = cneg(q);
         q1[i] = q;
-    }
-    if (SMEM) {
-        __syncthreads();
-        for (int e = tid; e < n * n; e += nt) Hg[e] = H[e];
     }
 }
 
@@ -824,11 +807,10 @@ int set_smem_limits(const SmemNeeds& s) {
     if (s.rect)
         CEL_CUDA(cudaFuncSetAttribute(rcwa_fourier_rect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.rect));
     if (s.aed)
-        CEL_CUDA(cudaFuncSetAttribute(rcwa_schur<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CEL_CUDA(cudaFuncSetAttribute(rcwa_schur, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kSchurSmemOneCta));
     if (s.hess_s) {
         CEL_CUDA(cudaFuncSetAttribute(rcwa_hess<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.hess_s));
-        CEL_CUDA(cudaFuncSetAttribute(rcwa_schur<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.hess_s));
     }
     if (s.smat) {
         CEL_CUDA(cudaFuncSetAttribute(rcwa_smat1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smat));
@@ -863,11 +845,11 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
         const size_t sm = ((size_t)n * n + 2 * n) * sizeof(cplx);
         rcwa_hess<true><<<nc, T[ST_HESS], sm, st>>>(b);
         if (ev) cudaEventRecord(ev[3], st);
-        rcwa_schur<false><<<nc, T[ST_SCHUR], schur_smem(nc), st>>>(b);
+        rcwa_schur<<<nc, kSchurThreads, schur_smem(nc), st>>>(b);
     } else {
         rcwa_hess<false><<<nc, T[ST_HESS], hess_stage_bytes(n), st>>>(b);
         if (ev) cudaEventRecord(ev[3], st);
-        rcwa_schur<false><<<nc, T[ST_SCHUR], schur_smem(nc), st>>>(b);
+        rcwa_schur<<<nc, kSchurThreads, schur_smem(nc), st>>>(b);
     }
     if (ev) cudaEventRecord(ev[4], st);
     rcwa_vec<<<nc, T[ST_VEC], 0, st>>>(b);

@@ -34,6 +34,10 @@ constexpr int NSH = 16;      // shifts per sweep
 constexpr int NWIN = 24;     // AED window
 constexpr int NSMALL = WMAX; // active blocks up to this size are finished in shared memory
 constexpr int FT = 28;       // far-update tile (rows or columns)
+constexpr int MR = 2;        // rows of the per-thread output block of the far updates
+// Threads of the Schur kernel: 196 of them, (WMAX / MR) x (FT / 4), carry the far
+// updates; two CTAs of 256 threads and <= 128 registers share an SM.
+constexpr int kSchurThreads = 256;
 
 struct AedShared {
     cplx B[WMAX][WMAX + 1];  // window; during far updates two tile buffers of WMAX * FT
@@ -214,32 +218,32 @@ __device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const c
         __syncthreads();
         const cplx* tile = buf + (t & 1) * FBUF;
         const int cb = c0 + t * FT, nc = min(FT, c1 - cb);
-        // thread grid (WMAX/2) x (FT/4), each thread rows ty, ty + WMAX/2 and
-        // columns tx + j FT/4 (j < 4): every slot is a real output of a full tile
-        constexpr int R2 = WMAX / 2, C4 = FT / 4;
-        for (int q = tid; q < R2 * C4; q += nt) {
+        // thread grid (WMAX/MR) x (FT/4): rows ty + i WMAX/MR (i < MR), columns
+        // tx + j FT/4 (j < 4); every slot is a real output of a full tile
+        constexpr int RS = WMAX / MR, C4 = FT / 4;
+        for (int q = tid; q < RS * C4; q += nt) {
             const int ty = q / C4, tx = q % C4;
             if (ty >= w) continue;
-            cplx acc[2][4];
+            cplx acc[MR][4];
 #pragma unroll
-            for (int a = 0; a < 2; ++a)
+            for (int a = 0; a < MR; ++a)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) acc[a][j] = C(0.0, 0.0);
-            const bool two = ty + R2 < w;
 #pragma unroll 4
             for (int k = 0; k < w; ++k) {
-                const cplx u0 = cconj(U[k][ty]);
-                const cplx u1 = two ? cconj(U[k][ty + R2]) : C(0.0, 0.0);
+                cplx u[MR];
+#pragma unroll
+                for (int a = 0; a < MR; ++a) u[a] = ty + RS * a < w ? cconj(U[k][ty + RS * a]) : C(0.0, 0.0);
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const cplx tv = tile[k * FT + tx + C4 * j];
-                    acc[0][j] = cfma(u0, tv, acc[0][j]);
-                    acc[1][j] = cfma(u1, tv, acc[1][j]);
+#pragma unroll
+                    for (int a = 0; a < MR; ++a) acc[a][j] = cfma(u[a], tv, acc[a][j]);
                 }
             }
 #pragma unroll
-            for (int a = 0; a < 2; ++a) {
-                const int r = ty + R2 * a;
+            for (int a = 0; a < MR; ++a) {
+                const int r = ty + RS * a;
                 if (r >= w) continue;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
@@ -252,16 +256,20 @@ __device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const c
     }
 }
 
-// X[r0:r1, c0:c0+w] <- X U. Tile t holds rows r0 + t*FT .. as [FT][w] (ld WMAX).
+// X[r0:r1, c0:c0+w] <- X U. Tile t holds rows r0 + t*FT .. as [FT][w] with
+// row stride TS = WMAX + 1: WMAX complex is a multiple of 128 bytes, so without
+// the pad the rows a warp reads at once would sit in the same banks.
+constexpr int TS = WMAX + 1;
+constexpr int FBUF_R = FT * TS;
 __device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const cplx (*U)[WMAX], cplx* buf) {
     const int tid = threadIdx.x, nt = blockDim.x;
     const int ntile = (r1 - r0 + FT - 1) / FT;
     auto issue = [&](int t) {
         const int rb = r0 + t * FT, nr = min(FT, r1 - rb);
-        cplx* dst = buf + (t & 1) * FBUF;
+        cplx* dst = buf + (t & 1) * FBUF_R;
         for (int e = tid; e < FT * w; e += nt) {
             const int r = e / w, k = e % w;
-            cp_async16(dst + r * WMAX + k, X + (size_t)(rb + (r < nr ? r : 0)) * ld + c0 + k, r < nr);
+            cp_async16(dst + r * TS + k, X + (size_t)(rb + (r < nr ? r : 0)) * ld + c0 + k, r < nr);
         }
         cp_async_commit();
     };
@@ -274,31 +282,33 @@ __device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const 
             cp_async_wait0();
         }
         __syncthreads();
-        const cplx* tile = buf + (t & 1) * FBUF;
+        const cplx* tile = buf + (t & 1) * FBUF_R;
         const int rb = r0 + t * FT, nr = min(FT, r1 - rb);
-        // thread grid (FT/2) x (WMAX/4): rows ty, ty + FT/2, columns tx + j WMAX/4
-        constexpr int R2 = FT / 2, C4 = WMAX / 4;
-        for (int q = tid; q < R2 * C4; q += nt) {
+        // thread grid (FT/MR) x (WMAX/4): rows ty + i FT/MR, columns tx + j WMAX/4
+        constexpr int RS = FT / MR, C4 = WMAX / 4;
+        for (int q = tid; q < RS * C4; q += nt) {
             const int ty = q / C4, tx = q % C4;
             if (ty >= nr || tx >= w) continue;
-            cplx acc[2][4];
+            cplx acc[MR][4];
 #pragma unroll
-            for (int a = 0; a < 2; ++a)
+            for (int a = 0; a < MR; ++a)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) acc[a][j] = C(0.0, 0.0);
 #pragma unroll 4
             for (int k = 0; k < w; ++k) {
-                const cplx t0 = tile[ty * WMAX + k], t1 = tile[(ty + R2) * WMAX + k];
+                cplx tv[MR];
+#pragma unroll
+                for (int a = 0; a < MR; ++a) tv[a] = tile[(ty + RS * a) * TS + k];
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     const cplx u = U[k][tx + C4 * j];
-                    acc[0][j] = cfma(t0, u, acc[0][j]);
-                    acc[1][j] = cfma(t1, u, acc[1][j]);
+#pragma unroll
+                    for (int a = 0; a < MR; ++a) acc[a][j] = cfma(tv[a], u, acc[a][j]);
                 }
             }
 #pragma unroll
-            for (int a = 0; a < 2; ++a) {
-                const int r = ty + R2 * a;
+            for (int a = 0; a < MR; ++a) {
+                const int r = ty + RS * a;
                 if (r >= nr) continue;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
@@ -451,7 +461,8 @@ __device__ void aed(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, A
 // bulge's move stays inside it (its rows reach p + 2 <= we - 1), or, in the
 // window that ends at hi, until every bulge has left.
 static_assert(WMAX - 2 > 2 * (NSH - 1), "the first window introduces every bulge");
-static_assert(2 * WMAX * FT <= WMAX * (WMAX + 1), "tile buffers overlay the window");
+static_assert(2 * WMAX * FT <= WMAX * (WMAX + 1) && 2 * FBUF_R <= WMAX * (WMAX + 1),
+              "tile buffers overlay the window");
 static_assert(WMAX % 4 == 0 && FT % 4 == 0, "far-update thread grids");
 
 __device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, int nsh, AedShared* sh,

@@ -52,6 +52,7 @@ EXPORTED = [
     "celeris_rs_check_dev", "celeris_sync_status", "celeris_solve_rcwa_2d", "celeris_rcwa_batch",
     "celeris_probe_peaks", "celeris_set_kernel_timing", "celeris_last_kernel_ms",
     "celeris_rs_field_noalloc", "celeris_probe_sincos", "celeris_rcwa_tuning_report",
+    "celeris_probe_dmma",
 ]
 
 
@@ -116,6 +117,7 @@ def load(path: str = LIB_PATH):
         "celeris_rs_check_dev": (_I, [_V, _V, _V, _I, _D, _D, _D, _D, _I, _D, _V, _V, _I, _P, _V]),
         "celeris_sync_status": (_I, [_V]),
         "celeris_probe_peaks": (_I, [_P, _P, _P]),
+        "celeris_probe_dmma": (_I, [_P]),
         "celeris_probe_sincos": (_I, [_D, _I, _P]),
         "celeris_set_kernel_timing": (_I, [_I]),
         "celeris_last_kernel_ms": (_I, [_P]),
@@ -165,7 +167,10 @@ def probe_peaks() -> dict:
     """Measured MUFU / FP32-FMA / FP64-FMA op rates of the current device."""
     a, b, c = (np.zeros(1) for _ in range(3))
     check(load().celeris_probe_peaks(_dp(a), _dp(b), _dp(c)))
-    return {"mufu_per_s": float(a[0]), "ffma_per_s": float(b[0]), "dfma_per_s": float(c[0])}
+    d = np.zeros(1)
+    check(load().celeris_probe_dmma(_dp(d)))
+    return {"mufu_per_s": float(a[0]), "ffma_per_s": float(b[0]), "dfma_per_s": float(c[0]),
+            "dmma_fma_per_s": float(d[0])}
 
 
 def set_kernel_timing(on: bool):

@@ -8,7 +8,7 @@
 // barrier, so consecutive calls compose without extra synchronization.
 //
 // Routines (all O(n^3) work is spread over the block; loops are bounded):
-//   blk_gemm        C = alpha A B + beta C (register-tiled, smem-staged k chunks)
+//   blk_gemm        C = alpha A B + beta C (FP64 tensor-core DMMA, smem-staged k chunks)
 //   blk_lu          partial-pivot LU in place (LAPACK zgetrf semantics: pivot =
 //                   first max |re|+|im| in the column); blk_lu_blocked: panels
 //                   of LNB columns with GEMM trailing updates, same pivots
@@ -150,12 +150,14 @@ __device__ __forceinline__ int blk_argmax(double val, int idx, RedScratch* rs) {
 }
 
 // ---- GEMM -------------------------------------------------------------------------
-// Register-tiled: the block is 16 x (NT/16) threads, each owning a 4 x 4 block of
-// outputs strided by 16 rows / NT/16 columns, so a 64 x (NT/4) output tile is
-// computed from k-chunks of GKC staged in shared memory. Per k step a thread reads
-// 4 A and 4 B values for 16 complex FMAs (shared-memory traffic a quarter of the
-// one-output-per-thread form). The next chunk is fetched into registers while the
-// current one is multiplied.
+// FP64 tensor cores: mma.sync.m8n8k4 (DMMA). The CTA computes a 64 x (NT/4)
+// output tile from k-chunks of GKC staged in shared memory; each warp owns a
+// 32 x 16 block = 4 x 2 tiles of 8 x 8. A complex product over a k-step of 4
+// is four real DMMAs per tile: Re += Ar Br + (-Ai) Bi, Im += Ar Bi + Ai Br.
+// Fragment layout of m8n8k4 (g = lane / 4, t = lane % 4): A[g][t] (row-major
+// 8 x 4), B[t][g] (column-major 4 x 8), C[g][2t], C[g][2t + 1].
+// The next chunk is fetched into registers while the current one is multiplied,
+// in one pipeline over all (tile, chunk) steps.
 constexpr int GM = 64;   // tile rows
 constexpr int GKC = 8;   // k chunk
 struct GemmSmem {
@@ -163,25 +165,30 @@ struct GemmSmem {
     cplx b[GKC][64];
 };
 
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
 template <int NT>
 __device__ __forceinline__ void gemm_tiles(int m, int n, int k, cplx alpha, const cplx* A, int lda, const cplx* B,
                                            int ldb, cplx beta, cplx* Cm, int ldc, GemmSmem* sm) {
-    constexpr int TX = NT / 16, GN = 4 * TX, PA = GM * GKC / NT, PB = GKC * GN / NT;
+    constexpr int GN = NT / 4, PA = GM * GKC / NT, PB = GKC * GN / NT;
+    constexpr int WC = GN / 16;  // warps across the columns (4 or 2); 2 across the rows
     const int tid = threadIdx.x;
     const bool act = tid < NT;
-    const int ty = tid / TX, tx = tid % TX;
+    const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
+    const int wr = (warp / WC) * 32, wc = (warp % WC) * 16;  // warp block origin in the tile
     const int mt = (m + GM - 1) / GM, ntl = (n + GN - 1) / GN;
     const int nk = (k + GKC - 1) / GKC;
     const int total = mt * ntl * nk;  // (tile, k-chunk) steps, fetched one step ahead
     if (total == 0) return;
     const bool use_beta = beta.x != 0.0 || beta.y != 0.0;
-    cplx acc[4][4];
+    double cr[4][2][2], ci[4][2][2];  // [row tile][col tile][2 per thread]
     cplx ra[PA], rb[PB];
-    // A is staged pre-multiplied by alpha, and the accumulators start from
-    // beta C, so C is read at the start of a tile (its latency overlaps the
-    // tile's first fetch) and the epilogue only stores.
-    auto fetch = [&](int g) {
-        const int t = g / nk, k0 = (g - t * nk) * GKC;
+    auto fetch = [&](int gi) {
+        const int t = gi / nk, k0 = (gi - t * nk) * GKC;
         const int i0 = (t / ntl) * GM, j0 = (t % ntl) * GN;
 #pragma unroll
         for (int s = 0; s < PA; ++s) {
@@ -194,26 +201,33 @@ __device__ __forceinline__ void gemm_tiles(int m, int n, int k, cplx alpha, cons
             rb[s] = (act && k0 + r < k && j0 + c < n) ? B[(size_t)(k0 + r) * ldb + j0 + c] : C(0.0, 0.0);
         }
     };
+    // accumulators start from beta C: C is read at the start of a tile
     auto init_acc = [&](int t) {
         const int i0 = (t / ntl) * GM, j0 = (t % ntl) * GN;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const int r = i0 + ty + 16 * i;
+            const int r = i0 + wr + 8 * i + g;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int c = j0 + tx + TX * j;
-                acc[i][j] = (use_beta && act && r < m && c < n) ? cmul(beta, Cm[(size_t)r * ldc + c]) : C(0.0, 0.0);
+            for (int j = 0; j < 2; ++j) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int c = j0 + wc + 8 * j + 2 * t4 + h;
+                    cplx v = C(0.0, 0.0);
+                    if (use_beta && act && r < m && c < n) v = cmul(beta, Cm[(size_t)r * ldc + c]);
+                    cr[i][j][h] = v.x;
+                    ci[i][j][h] = v.y;
+                }
             }
         }
     };
     init_acc(0);
     fetch(0);
-    for (int g = 0; g < total; ++g) {
+    for (int gi = 0; gi < total; ++gi) {
         if (act) {
 #pragma unroll
             for (int s = 0; s < PA; ++s) {
                 const int e = tid + s * NT;
-                sm->a[e % GKC][e / GKC] = cmul(alpha, ra[s]);
+                sm->a[e % GKC][e / GKC] = cmul(alpha, ra[s]);  // A staged pre-multiplied by alpha
             }
 #pragma unroll
             for (int s = 0; s < PB; ++s) {
@@ -222,37 +236,54 @@ __device__ __forceinline__ void gemm_tiles(int m, int n, int k, cplx alpha, cons
             }
         }
         __syncthreads();
-        if (g + 1 < total) fetch(g + 1);
+        if (gi + 1 < total) fetch(gi + 1);
         if (act) {
 #pragma unroll
-            for (int kk = 0; kk < GKC; ++kk) {
-                cplx av[4], bv[4];
+            for (int ks = 0; ks < GKC; ks += 4) {
+                double ar[4], ai[4], nai[4], br[2], bi[2];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) av[i] = sm->a[kk][ty + 16 * i];
+                for (int i = 0; i < 4; ++i) {
+                    const cplx v = sm->a[ks + t4][wr + 8 * i + g];
+                    ar[i] = v.x;
+                    ai[i] = v.y;
+                    nai[i] = -v.y;
+                }
 #pragma unroll
-                for (int j = 0; j < 4; ++j) bv[j] = sm->b[kk][tx + TX * j];
+                for (int j = 0; j < 2; ++j) {
+                    const cplx v = sm->b[ks + t4][wc + 8 * j + g];
+                    br[j] = v.x;
+                    bi[j] = v.y;
+                }
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) acc[i][j] = cfma(av[i], bv[j], acc[i][j]);
+                    for (int j = 0; j < 2; ++j) {
+                        dmma(cr[i][j][0], cr[i][j][1], ar[i], br[j]);
+                        dmma(cr[i][j][0], cr[i][j][1], nai[i], bi[j]);
+                        dmma(ci[i][j][0], ci[i][j][1], ar[i], bi[j]);
+                        dmma(ci[i][j][0], ci[i][j][1], ai[i], br[j]);
+                    }
             }
         }
         __syncthreads();
-        const int t = g / nk;
-        if (g - t * nk == nk - 1) {  // last chunk of tile t: store it, start the next
+        const int t = gi / nk;
+        if (gi - t * nk == nk - 1) {  // last chunk of tile t: store it, start the next
             if (act) {
                 const int i0 = (t / ntl) * GM, j0 = (t % ntl) * GN;
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
-                    const int r = i0 + ty + 16 * i;
+                    const int r = i0 + wr + 8 * i + g;
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int c = j0 + tx + TX * j;
-                        if (r < m && c < n) Cm[(size_t)r * ldc + c] = acc[i][j];
+                    for (int j = 0; j < 2; ++j) {
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int c = j0 + wc + 8 * j + 2 * t4 + h;
+                            if (r < m && c < n) Cm[(size_t)r * ldc + c] = C(cr[i][j][h], ci[i][j][h]);
+                        }
                     }
                 }
             }
-            if (g + 1 < total) init_acc(t + 1);
+            if (gi + 1 < total) init_acc(t + 1);
         }
     }
 }

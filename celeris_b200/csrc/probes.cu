@@ -55,6 +55,26 @@ __global__ void probe_dfma(double a, int iters, double* sink) {
     if (s == 12345.678) sink[0] = s;
 }
 
+// FP64 tensor cores: kChains independent m8n8k4 accumulators per warp.
+__global__ void probe_dmma(double a, int iters, double* sink) {
+    const int lane = threadIdx.x & 31;
+    double c0[kChains], c1[kChains];
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) c0[c] = c1[c] = 0.001 * (lane + c);
+    const double x = a + 1e-3 * lane, y = 0.999;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int c = 0; c < kChains; ++c)
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                         : "+d"(c0[c]), "+d"(c1[c])
+                         : "d"(x), "d"(y));
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) s += c0[c] + c1[c];
+    if (s == 12345.678) sink[0] = s;
+}
+
 // Accuracy of sin.approx / cos.approx against FP64 sin/cos of the same FP32
 // argument, for arguments uniform in [-xmax, xmax]: max |error| and the mean
 // signed error (bias) of each.
@@ -114,6 +134,24 @@ extern "C" int celeris_probe_sincos(double xmax, int npts, double* out) {
     out[1] = h[1];
     out[2] = h[2] / npts;
     out[3] = h[3] / npts;
+    return CELERIS_OK;
+}
+
+// New: FP64 FMA/s of the tensor cores (mma.sync m8n8k4 f64, 256 FMA per warp op).
+extern "C" int celeris_probe_dmma(double* fma_per_s) {
+    CEL_TRY(celeris_rt::require_device());
+    if (!fma_per_s) return celeris_rt::set_error(CELERIS_ERR_INVALID_ARG, "null output");
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    void* sink = nullptr;
+    CEL_CUDA(cudaMalloc(&sink, 64));
+    const int blocks = sms * 8, threads = 256, iters = 2048;
+    const double fmas = (double)blocks * (threads / 32) * kChains * iters * 256.0;
+    CEL_TRY(time_probe([&] { probe_dmma<<<blocks, threads>>>(0.5, iters, (double*)sink); }, fmas, fma_per_s));
+    celeris_rt::count_launch(2);
+    cudaFree(sink);
+    CEL_CUDA(cudaGetLastError());
     return CELERIS_OK;
 }
 

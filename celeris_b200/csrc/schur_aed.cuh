@@ -33,10 +33,9 @@ constexpr int WMAX = 56;     // window size (rows/columns)
 constexpr int NSH = 16;      // shifts per sweep
 constexpr int NWIN = 24;     // AED window
 constexpr int NSMALL = WMAX; // active blocks up to this size are finished in shared memory
-constexpr int FT = 28;       // far-update tile (rows or columns)
-constexpr int MR = 2;        // rows of the per-thread output block of the far updates
-// Threads of the Schur kernel: 196 of them, (WMAX / MR) x (FT / 4), carry the far
-// updates; two CTAs of 256 threads and <= 128 registers share an SM.
+constexpr int FT = 24;       // far-update tile (rows or columns), a multiple of the 8-wide DMMA tile
+// Threads of the Schur kernel: two CTAs of 256 threads and <= 128 registers
+// share an SM; WMAX / 8 = 7 warps carry the far-update products.
 constexpr int kSchurThreads = 256;
 
 struct AedShared {
@@ -218,38 +217,35 @@ __device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const c
         __syncthreads();
         const cplx* tile = buf + (t & 1) * FBUF;
         const int cb = c0 + t * FT, nc = min(FT, c1 - cb);
-        // thread grid (WMAX/MR) x (FT/4): rows ty + i WMAX/MR (i < MR), columns
-        // tx + j FT/4 (j < 4); every slot is a real output of a full tile
-        constexpr int RS = WMAX / MR, C4 = FT / 4;
-        for (int q = tid; q < RS * C4; q += nt) {
-            const int ty = q / C4, tx = q % C4;
-            if (ty >= w) continue;
-            cplx acc[MR][4];
+        // DMMA: warp i < WMAX/8 owns output rows 8i..8i+7 and all FT/8 column
+        // tiles; A = U^H (A[g][t] = conj U[k][8i+g]), B = the staged tile
+        const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
+        if (warp < WMAX / 8 && 8 * warp < w) {
+            const int row = 8 * warp + g;
+            double cr[FT / 8][2], ci[FT / 8][2];
 #pragma unroll
-            for (int a = 0; a < MR; ++a)
+            for (int j = 0; j < FT / 8; ++j) cr[j][0] = cr[j][1] = ci[j][0] = ci[j][1] = 0.0;
+            for (int ks = 0; ks < w; ks += 4) {
+                const int kk = ks + t4;
+                const cplx uv = (kk < w && row < w) ? U[kk][row] : C(0.0, 0.0);
+                const double ar = uv.x, ai = -uv.y, nai = uv.y;  // conj(U)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[a][j] = C(0.0, 0.0);
-#pragma unroll 4
-            for (int k = 0; k < w; ++k) {
-                cplx u[MR];
-#pragma unroll
-                for (int a = 0; a < MR; ++a) u[a] = ty + RS * a < w ? cconj(U[k][ty + RS * a]) : C(0.0, 0.0);
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const cplx tv = tile[k * FT + tx + C4 * j];
-#pragma unroll
-                    for (int a = 0; a < MR; ++a) acc[a][j] = cfma(u[a], tv, acc[a][j]);
+                for (int j = 0; j < FT / 8; ++j) {
+                    const cplx bv = kk < w ? tile[kk * FT + 8 * j + g] : C(0.0, 0.0);
+                    dmma(cr[j][0], cr[j][1], ar, bv.x);
+                    dmma(cr[j][0], cr[j][1], nai, bv.y);
+                    dmma(ci[j][0], ci[j][1], ar, bv.y);
+                    dmma(ci[j][0], ci[j][1], ai, bv.x);
                 }
             }
+            if (row < w) {
 #pragma unroll
-            for (int a = 0; a < MR; ++a) {
-                const int r = ty + RS * a;
-                if (r >= w) continue;
+                for (int j = 0; j < FT / 8; ++j)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int c = tx + C4 * j;
-                    if (c < nc) X[(size_t)(r0 + r) * ld + cb + c] = acc[a][j];
-                }
+                    for (int h = 0; h < 2; ++h) {
+                        const int c = 8 * j + 2 * t4 + h;
+                        if (c < nc) X[(size_t)(r0 + row) * ld + cb + c] = C(cr[j][h], ci[j][h]);
+                    }
             }
         }
         __syncthreads();
@@ -284,36 +280,34 @@ __device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const 
         __syncthreads();
         const cplx* tile = buf + (t & 1) * FBUF_R;
         const int rb = r0 + t * FT, nr = min(FT, r1 - rb);
-        // thread grid (FT/MR) x (WMAX/4): rows ty + i FT/MR, columns tx + j WMAX/4
-        constexpr int RS = FT / MR, C4 = WMAX / 4;
-        for (int q = tid; q < RS * C4; q += nt) {
-            const int ty = q / C4, tx = q % C4;
-            if (ty >= nr || tx >= w) continue;
-            cplx acc[MR][4];
+        // DMMA: warp j < WMAX/8 owns output columns 8j..8j+7 and all FT/8 row
+        // tiles; A = the staged rows, B = U
+        const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
+        if (warp < WMAX / 8 && 8 * warp < w) {
+            const int col = 8 * warp + g;
+            double cr[FT / 8][2], ci[FT / 8][2];
 #pragma unroll
-            for (int a = 0; a < MR; ++a)
+            for (int i = 0; i < FT / 8; ++i) cr[i][0] = cr[i][1] = ci[i][0] = ci[i][1] = 0.0;
+            for (int ks = 0; ks < w; ks += 4) {
+                const int kk = ks + t4;
+                const cplx uv = (kk < w && col < w) ? U[kk][col] : C(0.0, 0.0);
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[a][j] = C(0.0, 0.0);
-#pragma unroll 4
-            for (int k = 0; k < w; ++k) {
-                cplx tv[MR];
-#pragma unroll
-                for (int a = 0; a < MR; ++a) tv[a] = tile[(ty + RS * a) * TS + k];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const cplx u = U[k][tx + C4 * j];
-#pragma unroll
-                    for (int a = 0; a < MR; ++a) acc[a][j] = cfma(tv[a], u, acc[a][j]);
+                for (int i = 0; i < FT / 8; ++i) {
+                    const cplx av = kk < w ? tile[(8 * i + g) * TS + kk] : C(0.0, 0.0);
+                    dmma(cr[i][0], cr[i][1], av.x, uv.x);
+                    dmma(cr[i][0], cr[i][1], -av.y, uv.y);
+                    dmma(ci[i][0], ci[i][1], av.x, uv.y);
+                    dmma(ci[i][0], ci[i][1], av.y, uv.x);
                 }
             }
 #pragma unroll
-            for (int a = 0; a < MR; ++a) {
-                const int r = ty + RS * a;
+            for (int i = 0; i < FT / 8; ++i) {
+                const int r = 8 * i + g;
                 if (r >= nr) continue;
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int c = tx + C4 * j;
-                    if (c < w) X[(size_t)(rb + r) * ld + c0 + c] = acc[a][j];
+                for (int h = 0; h < 2; ++h) {
+                    const int c = 8 * warp + 2 * t4 + h;
+                    if (c < w) X[(size_t)(rb + r) * ld + c0 + c] = C(cr[i][h], ci[i][h]);
                 }
             }
         }
@@ -463,7 +457,7 @@ __device__ void aed(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, A
 static_assert(WMAX - 2 > 2 * (NSH - 1), "the first window introduces every bulge");
 static_assert(2 * WMAX * FT <= WMAX * (WMAX + 1) && 2 * FBUF_R <= WMAX * (WMAX + 1),
               "tile buffers overlay the window");
-static_assert(WMAX % 4 == 0 && FT % 4 == 0, "far-update thread grids");
+static_assert(WMAX % 8 == 0 && FT % 8 == 0 && WMAX / 8 <= kSchurThreads / 32, "far-update DMMA tiles");
 
 __device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, int nsh, AedShared* sh,
                             long long* prof) {

@@ -69,6 +69,9 @@ int celeris_release_workspace(void);
 /* New: measured op rates of the current device (MUFU sin.approx results/s,
  * FP32 FMA/s, FP64 FMA/s) from short probe kernels; roofline denominators. */
 int celeris_probe_peaks(double* mufu_per_s, double* ffma_per_s, double* dfma_per_s);
+/* New: FP64 FMA/s of the tensor cores (mma.sync m8n8k4 f64) of the current
+ * device from a short probe kernel; roofline denominator of the RCWA products. */
+int celeris_probe_dmma(double* fma_per_s);
 /* New: accuracy of the hardware sine/cosine (sin/cos.approx.f32) over
  * [-xmax, xmax]: out[4] = {max |sin err|, max |cos err|, mean sin err,
  * mean cos err} against FP64 sin/cos of the same FP32 arguments. */

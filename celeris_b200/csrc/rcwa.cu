@@ -46,6 +46,7 @@ using celeris_rt::Workspace;
 
 constexpr double PI = 3.14159265358979323846;
 constexpr int kRT = 256;            // threads per CTA
+constexpr int kDbgSlots = 16;       // diagnostic counters per cell
 constexpr int kSmemEigMaxN = 112;   // eigensolve in shared memory up to this n
 
 struct CellDev {
@@ -73,7 +74,7 @@ struct Bucket {
     size_t s_nn, s_ns, s_NN, s_n;
     const cplx* phx;  // [(4Mx+1) x ng] centred DFT phase table (x)
     const cplx* phy;  // [(4My+1) x ng]
-    long long* dbg;   // optional per-cell stage clocks (CELERIS_RCWA_STAGE_CLOCKS=1), else NULL
+    long long* dbg;   // optional per-cell counters, kDbgSlots each (CELERIS_RCWA_STAGE_CLOCKS=1), else NULL
 };
 
 __device__ __forceinline__ cplx* at(cplx* base, size_t stride, int c) { return base + stride * c; }
@@ -375,10 +376,10 @@ __global__ void __launch_bounds__(kSchurThreads, 2) rcwa_schur(Bucket b) {
     const int tid = threadIdx.x, nt = blockDim.x;
     cplx* H = at(b.H, b.s_nn, cell);
     AedShared* sh = reinterpret_cast<AedShared*>(smem);
-    const int info = blk_schur_aed(n, H, n, at(b.Z, b.s_nn, cell), n, sh, b.dbg ? b.dbg + 8 * (size_t)cell : nullptr);
+    const int info = blk_schur_aed(n, H, n, at(b.Z, b.s_nn, cell), n, sh, b.dbg ? b.dbg + kDbgSlots * (size_t)cell : nullptr);
     if (tid == 0) {
         if (info != 0) b.info[cell] = info;
-        if (b.dbg) b.dbg[8 * (size_t)cell + 6] = sh->nsweep;
+        if (b.dbg) b.dbg[kDbgSlots * (size_t)cell + 6] = sh->nsweep;
     }
     // eigenvalues -> q = branch(sqrt(lambda)) (rcwa2d.cpp:364)
     cplx* q1 = at(b.q1, b.s_n, cell);
@@ -1090,8 +1091,8 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                 CEL_CUDA(cudaMemcpyAsync(const_cast<CellDev*>(p.b.cells), hdesc[w], sizeof(CellDev) * nc,
                                          cudaMemcpyHostToDevice, st));
                 long long* dbg = nullptr;
-                CEL_CUDA(cudaMalloc(&dbg, sizeof(long long) * 8 * nc));
-                CEL_CUDA(cudaMemsetAsync(dbg, 0, sizeof(long long) * 8 * nc, st));
+                CEL_CUDA(cudaMalloc(&dbg, sizeof(long long) * kDbgSlots * nc));
+                CEL_CUDA(cudaMemsetAsync(dbg, 0, sizeof(long long) * kDbgSlots * nc, st));
                 p.b.dbg = dbg;
                 cudaEvent_t ev[ST_COUNT + 1];
                 for (auto& e : ev) cudaEventCreate(&e);
@@ -1100,12 +1101,12 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                                          cudaMemcpyDeviceToHost, st));
                 CEL_CUDA(cudaMemcpyAsync(hinfo_pin[w], p.b.info, sizeof(int) * nc, cudaMemcpyDeviceToHost, st));
                 CEL_CUDA(cudaStreamSynchronize(st));
-                std::vector<long long> h(8 * nc);
-                cudaMemcpy(h.data(), dbg, sizeof(long long) * 8 * nc, cudaMemcpyDeviceToHost);
-                double sw = 0, ph[6] = {0, 0, 0, 0, 0, 0};
+                std::vector<long long> h(kDbgSlots * nc);
+                cudaMemcpy(h.data(), dbg, sizeof(long long) * kDbgSlots * nc, cudaMemcpyDeviceToHost);
+                double sw = 0, ph[kDbgSlots] = {};
                 for (int i = 0; i < nc; ++i) {
-                    sw += (double)h[8 * i + 6];
-                    for (int q = 0; q < 6; ++q) ph[q] += (double)h[8 * i + q];
+                    sw += (double)h[kDbgSlots * i + 6];
+                    for (int q = 0; q < kDbgSlots; ++q) ph[q] += (double)h[kDbgSlots * i + q];
                 }
                 std::string line = "[rcwa stages] n=" + std::to_string(p.n) + " cells=" + std::to_string(nc) + " ms:";
                 for (int s = 0; s < ST_COUNT; ++s) {
@@ -1118,9 +1119,9 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                 char buf[64];
                 std::snprintf(buf, sizeof(buf), " | sweeps/cell %.1f", sw / nc);
                 char buf2[160];
-                std::snprintf(buf2, sizeof(buf2), " | schur Mcycles/cell: aed %.2f (qr %.2f) aed_far %.2f sweep %.2f sweep_far %.2f small %.2f\n",
-                              ph[0] / nc * 1e-6, ph[5] / nc * 1e-6, ph[1] / nc * 1e-6, ph[2] / nc * 1e-6, ph[3] / nc * 1e-6,
-                              ph[4] / nc * 1e-6);
+                std::snprintf(buf2, sizeof(buf2), " | schur Mcycles/cell: aed %.2f (qr %.2f, %.0f rot) aed_far %.2f sweep %.2f (%.0f steps) sweep_far %.2f small %.2f\n",
+                              ph[0] / nc * 1e-6, ph[5] / nc * 1e-6, ph[8] / nc, ph[1] / nc * 1e-6, ph[2] / nc * 1e-6,
+                              ph[7] / nc, ph[3] / nc * 1e-6, ph[4] / nc * 1e-6);
                 std::fprintf(stderr, "%s%s%s", line.c_str(), buf, buf2);
                 for (auto& e : ev) cudaEventDestroy(e);
                 cudaFree(dbg);

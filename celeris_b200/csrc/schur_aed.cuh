@@ -40,7 +40,7 @@ constexpr int kSchurThreads = 256;
 
 struct AedShared {
     cplx B[WMAX][WMAX + 1];  // window; during far updates two tile buffers of WMAX * FT
-    cplx U[WMAX][WMAX];      // accumulated unitary of the window
+    cplx U[WMAX][WMAX + 1];  // accumulated unitary of the window (+1: column walks spread over the banks)
     cplx sh[NWIN];           // undeflated eigenvalues of the last AED
     cplx vec[WMAX];          // Householder vector
     double rc[NSH];          // rotations of one chain step, per bulge
@@ -74,7 +74,8 @@ __device__ __forceinline__ void wrot_cols(cplx* B, int ld, int k, double c, cplx
 // Single-shift QR of the m x m upper Hessenberg matrix B (shared, ld) to upper
 // triangular form, U <- U Q (rows [0, mu)). One warp. Returns 0, or the
 // (1-based) row where the iteration cap ran out.
-__device__ int warp_schur_small(int m, cplx* B, int ld, cplx* U, int ldu, int mu, int lane) {
+__device__ int warp_schur_small(int m, cplx* B, int ld, cplx* U, int ldu, int mu, int lane,
+                                 long long* nrot = nullptr) {
     const double eps = 2.220446049250313e-16;
     const double smallnum = 2.2250738585072014e-308 * (m / eps);
     int hi = m - 1, it = 0, total = 0;
@@ -108,6 +109,7 @@ __device__ int warp_schur_small(int m, cplx* B, int ld, cplx* U, int ldu, int mu
         } else {
             shift = wilkinson(B[(hi - 1) * ld + hi - 1], B[(hi - 1) * ld + hi], B[hi * ld + hi - 1], B[hi * ld + hi]);
         }
+        if (nrot && lane == 0) *nrot += hi - l;
         for (int k = l; k < hi; ++k) {
             cplx a, b;
             if (k == l) {
@@ -194,7 +196,7 @@ constexpr int FBUF = WMAX * FT;  // complex entries per tile buffer
 
 // X[r0:r0+w, c0:c1] <- U^H X  (U w x w in shared memory). Tile t holds columns
 // c0 + t*FT .. as [w][FT] (k-major: a warp reads 8 consecutive entries).
-__device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const cplx (*U)[WMAX], cplx* buf) {
+__device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const cplx (*U)[WMAX + 1], cplx* buf) {
     const int tid = threadIdx.x, nt = blockDim.x;
     const int ntile = (c1 - c0 + FT - 1) / FT;
     auto issue = [&](int t) {
@@ -257,7 +259,7 @@ __device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const c
 // the pad the rows a warp reads at once would sit in the same banks.
 constexpr int TS = WMAX + 1;
 constexpr int FBUF_R = FT * TS;
-__device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const cplx (*U)[WMAX], cplx* buf) {
+__device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const cplx (*U)[WMAX + 1], cplx* buf) {
     const int tid = threadIdx.x, nt = blockDim.x;
     const int ntile = (r1 - r0 + FT - 1) / FT;
     auto issue = [&](int t) {
@@ -361,10 +363,10 @@ __device__ void aed(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, A
     load_window(H, ldh, kwtop, jw, sh);
     cplx* B = &sh->B[0][0];
     cplx* U = &sh->U[0][0];
-    constexpr int ldb = WMAX + 1, ldu = WMAX;
+    constexpr int ldb = WMAX + 1, ldu = WMAX + 1;
     if (warp == 0) {
         const long long ts0 = clock64();
-        const int info = warp_schur_small(jw, B, ldb, U, ldu, jw, lane);
+        const int info = warp_schur_small(jw, B, ldb, U, ldu, jw, lane, prof ? prof + 8 : nullptr);
         if (prof && lane == 0) prof[5] += clock64() - ts0;
         int nsu = jw, ilst = 0;
         if (info == 0) {
@@ -462,7 +464,7 @@ static_assert(WMAX % 8 == 0 && FT % 8 == 0 && WMAX / 8 <= kSchurThreads / 32, "f
 __device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, int nsh, AedShared* sh,
                             long long* prof) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
-    constexpr int ldb = WMAX + 1, ldu = WMAX;
+    constexpr int ldb = WMAX + 1, ldu = WMAX + 1;
     cplx* B = &sh->B[0][0];
     cplx* U = &sh->U[0][0];
     if (tid == 0) {
@@ -554,6 +556,7 @@ __device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, i
         if (prof && tid == 0) {
             prof[2] += t1 - t0;
             prof[3] += clock64() - t1;
+            prof[7] += S;
         }
         if (tid == 0) {
             int plast = 1 << 30;
@@ -583,7 +586,7 @@ __device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, i
 }
 
 // prof (optional, per cell): clock64 sums of [AED local, AED far, sweep local,
-// sweep far, small blocks].
+// sweep far, small blocks, AED QR], [7] chain steps, [8] AED QR rotations.
 __device__ int blk_schur_aed(int n, cplx* H, int ldh, cplx* Z, int ldz, AedShared* sh, long long* prof) {
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     const double eps = 2.220446049250313e-16;
@@ -627,7 +630,7 @@ __device__ int blk_schur_aed(int n, cplx* H, int ldh, cplx* Z, int ldz, AedShare
             const long long t0 = clock64();
             load_window(H, ldh, lo, L, sh);
             if (warp == 0) {
-                const int info = warp_schur_small(L, &sh->B[0][0], WMAX + 1, &sh->U[0][0], WMAX, L, lane);
+                const int info = warp_schur_small(L, &sh->B[0][0], WMAX + 1, &sh->U[0][0], WMAX + 1, L, lane);
                 if (lane == 0 && info) sh->info = lo + info;
             }
             __syncthreads();

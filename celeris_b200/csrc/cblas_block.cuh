@@ -432,7 +432,7 @@ __device__ __forceinline__ void blk_matvec_rows(int rows, int cols, const cplx* 
                                                 double beta, int warp, int lane, int nwarp) {
     for (int i0 = 4 * warp; i0 < rows; i0 += 4 * nwarp) {
         cplx acc[4] = {C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0)};
-#pragma unroll 2
+#pragma unroll 4
         for (int j = lane; j < cols; j += 32) {
             const cplx vj = v[j];
             cplx h[4];
@@ -880,9 +880,14 @@ constexpr int kMaxN = 1024;  // largest matrix order (deflation flags are per ro
 // ---- eigenvectors of the triangular Schur factor ----------------------------------------
 // X (n x n, row-major) <- right eigenvectors of upper-triangular T: column k
 // solves (T - t_kk I) x = 0 with x_k = 1, x_i = 0 for i > k (ztrevc's back
-// substitution, with tiny denominators replaced by smin). Columns are then
-// scaled to unit max |re|+|im|.
-__device__ void blk_trevc(int n, const cplx* T, int ldt, cplx* X, int ldx) {
+// substitution, with tiny denominators replaced by smin = max(eps |t_kk|, tiny)).
+// Rows are solved bottom-up in blocks of TB: the coupling of a block to the rows
+// below it, S = T[block, below] X[below, below], is one GEMM (tensor cores);
+// inside the block one thread per column k finishes the substitution with its
+// own shift t_kk. Columns are then scaled to unit max |re|+|im|.
+// S: scratch of TB x n complex (global).
+constexpr int TB = 64;
+__device__ void blk_trevc(int n, const cplx* T, int ldt, cplx* X, int ldx, cplx* S, GemmSmem* gs) {
     const int tid = threadIdx.x, nt = blockDim.x;
     const double eps = 2.220446049250313e-16;
     const double tiny = 2.2250738585072014e-308 / eps;
@@ -891,24 +896,30 @@ __device__ void blk_trevc(int n, const cplx* T, int ldt, cplx* X, int ldx) {
         X[(size_t)i * ldx + k] = C(i == k ? 1.0 : 0.0, 0.0);
     }
     __syncthreads();
-    for (int k = tid; k < n; k += nt) {
-        const cplx lam = T[(size_t)k * ldt + k];
-        const double smin = fmax(eps * cabs1(lam), tiny);
-        double xmax = 1.0;
-        for (int i = k - 1; i >= 0; --i) {
-            cplx acc = C(0.0, 0.0);
-            for (int j = i + 1; j <= k; ++j) acc = cfma(T[(size_t)i * ldt + j], X[(size_t)j * ldx + k], acc);
-            cplx den = csub(T[(size_t)i * ldt + i], lam);
-            if (cabs1(den) < smin) den = C(smin, 0.0);
-            const cplx xi = cneg(cdiv(acc, den));
-            X[(size_t)i * ldx + k] = xi;
-            xmax = fmax(xmax, cabs1(xi));
-            if (xmax > 1e100) {  // rescale the partial vector to avoid overflow
-                const double sc = 1.0 / xmax;
-                for (int j = i; j <= k; ++j) X[(size_t)j * ldx + k] = cscale(X[(size_t)j * ldx + k], sc);
-                xmax = 1.0;
+    for (int r0 = ((n - 1) / TB) * TB; r0 >= 0; r0 -= TB) {
+        const int r1 = min(n, r0 + TB);
+        const bool below = r1 < n;
+        // S[i - r0][k - r1] = sum_{j >= r1} T[i][j] X[j][k]   (k >= r1; zero for k < r1)
+        if (below)
+            blk_gemm(r1 - r0, n - r1, n - r1, C(1.0, 0.0), T + (size_t)r0 * ldt + r1, ldt, X + (size_t)r1 * ldx + r1,
+                     ldx, C(0.0, 0.0), S, n, gs);
+        for (int k = r0 + 1 + tid; k < n; k += nt) {
+            const cplx lam = T[(size_t)k * ldt + k];
+            const double smin = fmax(eps * cabs1(lam), tiny);
+            const int jmax = min(r1 - 1, k);
+            for (int i = min(r1, k) - 1; i >= r0; --i) {
+                cplx acc = (below && k >= r1) ? S[(size_t)(i - r0) * n + (k - r1)] : C(0.0, 0.0);
+                for (int j = i + 1; j <= jmax; ++j) acc = cfma(T[(size_t)i * ldt + j], X[(size_t)j * ldx + k], acc);
+                cplx den = csub(T[(size_t)i * ldt + i], lam);
+                if (cabs1(den) < smin) den = C(smin, 0.0);
+                X[(size_t)i * ldx + k] = cneg(cdiv(acc, den));
             }
         }
+        __syncthreads();
+    }
+    for (int k = tid; k < n; k += nt) {
+        double xmax = 0.0;
+        for (int j = 0; j <= k; ++j) xmax = fmax(xmax, cabs1(X[(size_t)j * ldx + k]));
         const double sc = 1.0 / xmax;
         for (int j = 0; j <= k; ++j) X[(size_t)j * ldx + k] = cscale(X[(size_t)j * ldx + k], sc);
     }

@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(kRT) rcwa_vec(Bucket b) {
     const int cell = blockIdx.x;
     const int n = b.n;
     cplx* X = at(b.X, b.s_nn, cell);
-    blk_trevc(n, at(b.H, b.s_nn, cell), n, X, n);
+    blk_trevc(n, at(b.H, b.s_nn, cell), n, X, n, at(b.A, b.s_nn, cell), &gs);  // A is free until smat1
     blk_gemm(n, n, n, C(1.0, 0.0), at(b.Z, b.s_nn, cell), n, X, n, C(0.0, 0.0), at(b.W, b.s_nn, cell), n, &gs);
 }
 

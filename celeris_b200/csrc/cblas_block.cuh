@@ -151,18 +151,29 @@ __device__ __forceinline__ int blk_argmax(double val, int idx, RedScratch* rs) {
 
 // ---- GEMM -------------------------------------------------------------------------
 // FP64 tensor cores: mma.sync.m8n8k4 (DMMA). The CTA computes a 64 x (NT/4)
-// output tile from k-chunks of GKC staged in shared memory; each warp owns a
-// 32 x 16 block = 4 x 2 tiles of 8 x 8. A complex product over a k-step of 4
-// is four real DMMAs per tile: Re += Ar Br + (-Ai) Bi, Im += Ar Bi + Ai Br.
-// Fragment layout of m8n8k4 (g = lane / 4, t = lane % 4): A[g][t] (row-major
-// 8 x 4), B[t][g] (column-major 4 x 8), C[g][2t], C[g][2t + 1].
-// The next chunk is fetched into registers while the current one is multiplied,
-// in one pipeline over all (tile, chunk) steps.
+// output tile from k-chunks of GKC; each warp owns a 32 x 16 block = 4 x 2 tiles
+// of 8 x 8. A complex product over a k-step of 4 is four real DMMAs per tile:
+// Re += Ar Br + (-Ai) Bi, Im += Ar Bi + Ai Br. Fragment layout of m8n8k4
+// (g = lane / 4, t = lane % 4): A[g][t] (row-major 8 x 4), B[t][g] (column-major
+// 4 x 8), C[g][2t], C[g][2t + 1].
+// Chunks stream into two shared buffers with cp.async (16-byte copies,
+// zero-filled past the edges): chunk g+1 is in flight while chunk g is
+// multiplied, in one pipeline over all (tile, chunk) steps. The accumulators
+// start from (beta / alpha) C and the tile is stored as alpha * acc.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    const int sz = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 constexpr int GM = 64;   // tile rows
 constexpr int GKC = 8;   // k chunk
 struct GemmSmem {
-    cplx a[GKC][GM + 1];  // A chunk transposed (k-major); +1 keeps the transposing store conflict-free
-    cplx b[GKC][64];
+    cplx a[2][GM][GKC + 1];  // A chunks, row-major; +1 spreads a fragment's rows over the banks
+    cplx b[2][GKC][64];      // B chunks
 };
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
@@ -174,7 +185,7 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 template <int NT>
 __device__ __forceinline__ void gemm_tiles(int m, int n, int k, cplx alpha, const cplx* A, int lda, const cplx* B,
                                            int ldb, cplx beta, cplx* Cm, int ldc, GemmSmem* sm) {
-    constexpr int GN = NT / 4, PA = GM * GKC / NT, PB = GKC * GN / NT;
+    constexpr int GN = NT / 4;
     constexpr int WC = GN / 16;  // warps across the columns (4 or 2); 2 across the rows
     const int tid = threadIdx.x;
     const bool act = tid < NT;
@@ -182,26 +193,28 @@ __device__ __forceinline__ void gemm_tiles(int m, int n, int k, cplx alpha, cons
     const int wr = (warp / WC) * 32, wc = (warp % WC) * 16;  // warp block origin in the tile
     const int mt = (m + GM - 1) / GM, ntl = (n + GN - 1) / GN;
     const int nk = (k + GKC - 1) / GKC;
-    const int total = mt * ntl * nk;  // (tile, k-chunk) steps, fetched one step ahead
+    const int total = mt * ntl * nk;  // (tile, k-chunk) steps
     if (total == 0) return;
     const bool use_beta = beta.x != 0.0 || beta.y != 0.0;
+    const cplx ab = use_beta ? cdiv(beta, alpha) : C(0.0, 0.0);
     double cr[4][2][2], ci[4][2][2];  // [row tile][col tile][2 per thread]
-    cplx ra[PA], rb[PB];
-    auto fetch = [&](int gi) {
+    auto issue = [&](int gi) {
         const int t = gi / nk, k0 = (gi - t * nk) * GKC;
-        const int i0 = (t / ntl) * GM, j0 = (t % ntl) * GN;
-#pragma unroll
-        for (int s = 0; s < PA; ++s) {
-            const int e = tid + s * NT, r = e / GKC, c = e % GKC;
-            ra[s] = (act && i0 + r < m && k0 + c < k) ? A[(size_t)(i0 + r) * lda + k0 + c] : C(0.0, 0.0);
+        const int i0 = (t / ntl) * GM, j0 = (t % ntl) * GN, buf = gi & 1;
+        if (act) {
+            for (int e = tid; e < GM * GKC; e += NT) {
+                const int r = e / GKC, c = e % GKC;
+                const bool v = i0 + r < m && k0 + c < k;
+                cp_async16(&sm->a[buf][r][c], v ? A + (size_t)(i0 + r) * lda + k0 + c : A, v);
+            }
+            for (int e = tid; e < GKC * GN; e += NT) {
+                const int r = e / GN, c = e % GN;
+                const bool v = k0 + r < k && j0 + c < n;
+                cp_async16(&sm->b[buf][r][c], v ? B + (size_t)(k0 + r) * ldb + j0 + c : B, v);
+            }
         }
-#pragma unroll
-        for (int s = 0; s < PB; ++s) {
-            const int e = tid + s * NT, r = e / GN, c = e % GN;
-            rb[s] = (act && k0 + r < k && j0 + c < n) ? B[(size_t)(k0 + r) * ldb + j0 + c] : C(0.0, 0.0);
-        }
+        cp_async_commit();
     };
-    // accumulators start from beta C: C is read at the start of a tile
     auto init_acc = [&](int t) {
         const int i0 = (t / ntl) * GM, j0 = (t % ntl) * GN;
 #pragma unroll
@@ -213,7 +226,7 @@ __device__ __forceinline__ void gemm_tiles(int m, int n, int k, cplx alpha, cons
                 for (int h = 0; h < 2; ++h) {
                     const int c = j0 + wc + 8 * j + 2 * t4 + h;
                     cplx v = C(0.0, 0.0);
-                    if (use_beta && act && r < m && c < n) v = cmul(beta, Cm[(size_t)r * ldc + c]);
+                    if (use_beta && act && r < m && c < n) v = cmul(ab, Cm[(size_t)r * ldc + c]);
                     cr[i][j][h] = v.x;
                     ci[i][j][h] = v.y;
                 }
@@ -221,36 +234,30 @@ __device__ __forceinline__ void gemm_tiles(int m, int n, int k, cplx alpha, cons
         }
     };
     init_acc(0);
-    fetch(0);
+    issue(0);
     for (int gi = 0; gi < total; ++gi) {
-        if (act) {
-#pragma unroll
-            for (int s = 0; s < PA; ++s) {
-                const int e = tid + s * NT;
-                sm->a[e % GKC][e / GKC] = cmul(alpha, ra[s]);  // A staged pre-multiplied by alpha
-            }
-#pragma unroll
-            for (int s = 0; s < PB; ++s) {
-                const int e = tid + s * NT;
-                sm->b[e / GN][e % GN] = rb[s];
-            }
+        if (gi + 1 < total) {
+            issue(gi + 1);
+            cp_async_wait1();
+        } else {
+            cp_async_wait0();
         }
         __syncthreads();
-        if (gi + 1 < total) fetch(gi + 1);
         if (act) {
+            const int buf = gi & 1;
 #pragma unroll
             for (int ks = 0; ks < GKC; ks += 4) {
                 double ar[4], ai[4], nai[4], br[2], bi[2];
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
-                    const cplx v = sm->a[ks + t4][wr + 8 * i + g];
+                    const cplx v = sm->a[buf][wr + 8 * i + g][ks + t4];
                     ar[i] = v.x;
                     ai[i] = v.y;
                     nai[i] = -v.y;
                 }
 #pragma unroll
                 for (int j = 0; j < 2; ++j) {
-                    const cplx v = sm->b[ks + t4][wc + 8 * j + g];
+                    const cplx v = sm->b[buf][ks + t4][wc + 8 * j + g];
                     br[j] = v.x;
                     bi[j] = v.y;
                 }
@@ -265,7 +272,7 @@ __device__ __forceinline__ void gemm_tiles(int m, int n, int k, cplx alpha, cons
                     }
             }
         }
-        __syncthreads();
+        __syncthreads();  // buffer gi & 1 is refilled by the issue of step gi + 2
         const int t = gi / nk;
         if (gi - t * nk == nk - 1) {  // last chunk of tile t: store it, start the next
             if (act) {
@@ -278,7 +285,7 @@ __device__ __forceinline__ void gemm_tiles(int m, int n, int k, cplx alpha, cons
 #pragma unroll
                         for (int h = 0; h < 2; ++h) {
                             const int c = j0 + wc + 8 * j + 2 * t4 + h;
-                            if (r < m && c < n) Cm[(size_t)r * ldc + c] = C(cr[i][j][h], ci[i][j][h]);
+                            if (r < m && c < n) Cm[(size_t)r * ldc + c] = cmul(alpha, C(cr[i][j][h], ci[i][j][h]));
                         }
                     }
                 }

@@ -787,7 +787,7 @@ size_t per_cell_bytes(int n, int nexc) {
 // Dynamic shared-memory limits are per kernel function, so they are set once
 // per wave to the largest need over its buckets (outside any capture).
 struct SmemNeeds {
-    size_t laurent = 0, rect = 0, hess_s = 0, smat = 0;
+    size_t laurent = 0, rect = 0, hess_s = 0, hess_g = 0, smat = 0;
     bool aed = false;
     void add(int Mx, int My, int ng, int n) {
         if (ng > 0) {
@@ -797,6 +797,7 @@ struct SmemNeeds {
             rect = std::max(rect, ((size_t)2 * (nx * nx + ny * ny) + 2 * std::max(nx, ny)) * sizeof(cplx));
         }
         if (n <= kSmemEigMaxN) hess_s = std::max(hess_s, ((size_t)n * n + 2 * n) * sizeof(cplx));
+        else hess_g = std::max(hess_g, hess_stage_bytes(n));
         aed = true;
         smat = std::max(smat, lu_stage_bytes(n));
     }
@@ -810,6 +811,8 @@ int set_smem_limits(const SmemNeeds& s) {
     if (s.aed)
         CEL_CUDA(cudaFuncSetAttribute(rcwa_schur, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)kSchurSmemOneCta));
+    if (s.hess_g)
+        CEL_CUDA(cudaFuncSetAttribute(rcwa_hess<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.hess_g));
     if (s.hess_s) {
         CEL_CUDA(cudaFuncSetAttribute(rcwa_hess<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.hess_s));
     }

@@ -183,15 +183,6 @@ __device__ __forceinline__ void wrefl_right(cplx* M, int ld, int r0, int r1, int
 // (16-byte copies, zero-filled past the edge): the next tile is in flight
 // while the current one is multiplied. The buffers overlay the window B, which
 // is dead during the far updates.
-__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    const int sz = valid ? 16 : 0;
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(sz) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
 constexpr int FBUF = WMAX * FT;  // complex entries per tile buffer
 
 // X[r0:r0+w, c0:c1] <- U^H X  (U w x w in shared memory). Tile t holds columns

@@ -55,7 +55,7 @@ def loss_and_grad(spline, grid, w0, px, py):
     E = T.rs_field(spline(w), px, py, grid)
     L = T.encircled_energy_loss(E, grid, 1.0)
     L.backward()
-    return float(L), w.grad.cpu().numpy(), E.detach().cpu().numpy()
+    return float(L.detach()), w.grad.cpu().numpy(), E.detach().cpu().numpy()
 
 
 def fd_oracle(ap, g, spline, w0, idx, h=1e-6):

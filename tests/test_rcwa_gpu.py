@@ -88,6 +88,26 @@ def test_mixed_cells_batch(cell):
     check(res[1], ref(cell, 0.0, 1.0), lossless)
 
 
+LARGE = [
+    dict(name="rect_M7_n450", period_um=0.4, wavelength_um=0.6, n_inc=1.0, n_sub=1.46, eps_pillar=2.3 ** 2,
+         eps_bg=1.0, fill_x=0.62, thickness_um=0.8, Mx=7),
+    dict(name="circle_laurent_M7_grid256", period_um=0.45, wavelength_um=0.55, n_inc=1.0, n_sub=1.46,
+         eps_pillar=2.1 ** 2, eps_bg=1.0, fill_x=0.7, thickness_um=0.6, Mx=7, shape=capi.SHAPE_ELLIPSE, grid=256),
+    dict(name="rect_M10_n882", period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46, eps_pillar=4.0,
+         eps_bg=1.0, fill_x=0.5, thickness_um=0.6, Mx=10),
+]
+
+
+@pytest.mark.parametrize("cell", LARGE, ids=lambda c: c["name"])
+def test_large_cells(cell):
+    """The orders the eigensolve, LU and shared-memory limits meet beyond the
+    library sizes: 2N = 450 (Li rule and Laurent rule) and 2N = 882."""
+    res, info = capi.rcwa_batch([capi.rcwa_cell(**cell)])
+    assert info[0] == 0
+    check(res[0], ref(cell, 1.0, 0.0))
+    check(res[1], ref(cell, 0.0, 1.0))
+
+
 def test_uneven_batch_matches_single_cell_solves():
     cells = [MIXED[i % len(MIXED)] for i in range(23)]
     res, info = capi.rcwa_batch([capi.rcwa_cell(**c) for c in cells])

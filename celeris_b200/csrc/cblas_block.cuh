@@ -711,8 +711,10 @@ __device__ void blk_hessenberg(int n, cplx* H, int ldh, cplx* Z, int ldz, cplx* 
 // matrix (the product A v_j) plus 1/LNB of a few passes for the GEMMs, against
 // ~8 passes for rank-1 updates.
 // scratch (global, >= 5 * LNB * n complex); stage (shared, >= n + LNB^2 + 2 LNB complex).
+// prof (optional): clock64 sums [0] column steps without the matrix-vector
+// product, [1] the products A v_j, [2] the trailing and Z updates.
 __device__ void blk_hessenberg_blocked(int n, cplx* H, int ldh, cplx* Z, int ldz, cplx* scratch, cplx* stage,
-                                       RedScratch* rs, GemmSmem* gs) {
+                                       RedScratch* rs, GemmSmem* gs, long long* prof = nullptr) {
     const int tid = threadIdx.x, nt = blockDim.x;
     const int warp = tid >> 5, lane = tid & 31, nwarp = nt >> 5;
     constexpr int NB = LNB;
@@ -736,6 +738,7 @@ __device__ void blk_hessenberg_blocked(int n, cplx* H, int ldh, cplx* Z, int ldz
         for (int e = tid; e < m * NB; e += nt) V[e] = C(0.0, 0.0);
         for (int e = tid; e < NB * NB; e += nt) Tm[e] = C(0.0, 0.0);
         __syncthreads();
+        const long long tc0 = clock64();
         for (int j = 0; j < kb; ++j) {
             const int i = k + j;
             if (j > 0) {
@@ -804,8 +807,10 @@ __device__ void blk_hessenberg_blocked(int n, cplx* H, int ldh, cplx* Z, int ldz
                 }
                 if (lane == 0) u[l] = s;
             }
+            const long long tm0 = clock64();
             blk_matvec_rows(n, mx, H + i + 1, ldh, v, P, 1.0, warp, lane, nwarp);  // P[:n] as a vector
             __syncthreads();
+            if (prof && tid == 0) prof[1] += clock64() - tm0;
             if (tid < j) {
                 cplx s = C(0.0, 0.0);
                 for (int p = tid; p < j; ++p) s = cfma(Tm[tid * NB + p], u[p], s);
@@ -821,6 +826,8 @@ __device__ void blk_hessenberg_blocked(int n, cplx* H, int ldh, cplx* Z, int ldz
             if (tid == 0) Tm[j * NB + j] = C(beta, 0.0);
             __syncthreads();
         }
+        if (prof && tid == 0) prof[0] += clock64() - tc0;
+        const long long tg0 = clock64();
         for (int e = tid; e < NB * m; e += nt) {
             const int l = e / m, r = e % m;
             VH[(size_t)l * n + r] = l < kb ? cconj(V[(size_t)r * NB + l]) : C(0.0, 0.0);
@@ -849,6 +856,7 @@ __device__ void blk_hessenberg_blocked(int n, cplx* H, int ldh, cplx* Z, int ldz
             }
         }
         blk_gemm(n, m, kb, C(-1.0, 0.0), P, NB, VH, n, C(1.0, 0.0), Z + k + 1, ldz, gs);
+        if (prof && tid == 0) prof[2] += clock64() - tg0;
     }
 }
 

@@ -363,7 +363,8 @@ __global__ void __launch_bounds__(kRT) rcwa_hess(Bucket b) {
     } else {
         __shared__ GemmSmem gs;
         blk_hessenberg_blocked(n, Hg, n, at(b.Z, b.s_nn, cell), n, at(b.X, b.s_nn, cell),
-                               reinterpret_cast<cplx*>(smem), &rs, &gs);
+                               reinterpret_cast<cplx*>(smem), &rs, &gs,
+                               b.dbg ? b.dbg + kDbgSlots * (size_t)cell + 9 : nullptr);
     }
 }
 
@@ -1121,10 +1122,12 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                 }
                 char buf[64];
                 std::snprintf(buf, sizeof(buf), " | sweeps/cell %.1f", sw / nc);
-                char buf2[160];
-                std::snprintf(buf2, sizeof(buf2), " | schur Mcycles/cell: aed %.2f (qr %.2f, %.0f rot) aed_far %.2f sweep %.2f (%.0f steps) sweep_far %.2f small %.2f\n",
+                char buf2[320];
+                std::snprintf(buf2, sizeof(buf2), " | schur Mcycles/cell: aed %.2f (qr %.2f, %.0f rot) aed_far %.2f sweep %.2f (%.0f steps) sweep_far %.2f small %.2f"
+                              " | hess Mcycles/cell: columns %.2f (matvec %.2f) updates %.2f\n",
                               ph[0] / nc * 1e-6, ph[5] / nc * 1e-6, ph[8] / nc, ph[1] / nc * 1e-6, ph[2] / nc * 1e-6,
-                              ph[7] / nc, ph[3] / nc * 1e-6, ph[4] / nc * 1e-6);
+                              ph[7] / nc, ph[3] / nc * 1e-6, ph[4] / nc * 1e-6, ph[9] / nc * 1e-6, ph[10] / nc * 1e-6,
+                              ph[11] / nc * 1e-6);
                 std::fprintf(stderr, "%s%s%s", line.c_str(), buf, buf2);
                 for (auto& e : ev) cudaEventDestroy(e);
                 cudaFree(dbg);

@@ -295,12 +295,86 @@ __device__ __forceinline__ void gemm_tiles(int m, int n, int k, cplx alpha, cons
     }
 }
 
+// Warp-tiled product for small inner dimension or a thin output (k <= 32, m <= 16
+// or n <= 16: the rank-16 updates of the blocked LU, solves and Hessenberg, and
+// the 16-wide products of the compact WY form). Each warp owns 16 x (8 TN)
+// output blocks, round-robin, and streams its A rows and B columns straight from
+// memory into DMMA fragments, so the eight warps keep eight tiles' loads in
+// flight instead of one CTA-wide tile's.
+template <int TN>
+__device__ __forceinline__ void gemm_warps(int m, int n, int k, cplx alpha, const cplx* A, int lda, const cplx* B,
+                                           int ldb, cplx beta, cplx* Cm, int ldc) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int mt = (m + 15) / 16, ntl = (n + 8 * TN - 1) / (8 * TN);
+    const bool use_beta = beta.x != 0.0 || beta.y != 0.0;
+    const cplx ab = use_beta ? cdiv(beta, alpha) : C(0.0, 0.0);
+    for (int t = warp; t < mt * ntl; t += nwarp) {
+        const int r0 = (t / ntl) * 16, c0 = (t % ntl) * (8 * TN);
+        double cr[2][TN][2], ci[2][TN][2];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int r = r0 + 8 * i + g;
+#pragma unroll
+            for (int j = 0; j < TN; ++j)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int c = c0 + 8 * j + 2 * t4 + h;
+                    cplx v = C(0.0, 0.0);
+                    if (use_beta && r < m && c < n) v = cmul(ab, Cm[(size_t)r * ldc + c]);
+                    cr[i][j][h] = v.x;
+                    ci[i][j][h] = v.y;
+                }
+        }
+#pragma unroll 4
+        for (int k0 = 0; k0 < k; k0 += 4) {
+            const int kk = k0 + t4;
+            cplx a[2], b[TN];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int r = r0 + 8 * i + g;
+                a[i] = (r < m && kk < k) ? A[(size_t)r * lda + kk] : C(0.0, 0.0);
+            }
+#pragma unroll
+            for (int j = 0; j < TN; ++j) {
+                const int c = c0 + 8 * j + g;
+                b[j] = (kk < k && c < n) ? B[(size_t)kk * ldb + c] : C(0.0, 0.0);
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < TN; ++j) {
+                    dmma(cr[i][j][0], cr[i][j][1], a[i].x, b[j].x);
+                    dmma(cr[i][j][0], cr[i][j][1], -a[i].y, b[j].y);
+                    dmma(ci[i][j][0], ci[i][j][1], a[i].x, b[j].y);
+                    dmma(ci[i][j][0], ci[i][j][1], a[i].y, b[j].x);
+                }
+        }
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int r = r0 + 8 * i + g;
+            if (r >= m) continue;
+#pragma unroll
+            for (int j = 0; j < TN; ++j)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int c = c0 + 8 * j + 2 * t4 + h;
+                    if (c < n) Cm[(size_t)r * ldc + c] = cmul(alpha, C(cr[i][j][h], ci[i][j][h]));
+                }
+        }
+    }
+}
+
 // C[m x n] = alpha * A[m x k] * B[k x n] + beta * C  (row-major). C may not alias A
 // or B. blockDim.x >= 128 (every kernel here runs 128 or 256 threads).
 __device__ void blk_gemm(int m, int n, int k, cplx alpha, const cplx* A, int lda, const cplx* B, int ldb,
                          cplx beta, cplx* Cm, int ldc, GemmSmem* sm) {
     __syncthreads();
-    if (blockDim.x >= 256)
+    if (n <= 16)
+        gemm_warps<2>(m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc);
+    else if (k <= 32 || m <= 16)
+        gemm_warps<4>(m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc);
+    else if (blockDim.x >= 256)
         gemm_tiles<256>(m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc, sm);
     else
         gemm_tiles<128>(m, n, k, alpha, A, lda, B, ldb, beta, Cm, ldc, sm);

@@ -49,6 +49,7 @@ struct AedShared {
     unsigned char flag[kMaxN];
     int lo, hi, done, info, nsweep, nsu, nd, nshift, nxt, win_end, ws, we, it;
     cplx shift[NSH];
+    unsigned umask[WMAX / 8];  // bit q of umask[c]: block U[4q..4q+3][8c..8c+7] has a non-zero
 };
 
 // ---- warp-level helpers on shared matrices ------------------------------------------------
@@ -187,7 +188,8 @@ constexpr int FBUF = WMAX * FT;  // complex entries per tile buffer
 
 // X[r0:r0+w, c0:c1] <- U^H X  (U w x w in shared memory). Tile t holds columns
 // c0 + t*FT .. as [w][FT] (k-major: a warp reads 8 consecutive entries).
-__device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const cplx (*U)[WMAX + 1], cplx* buf) {
+__device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const cplx (*U)[WMAX + 1], cplx* buf,
+                         const unsigned* umask) {
     const int tid = threadIdx.x, nt = blockDim.x;
     const int ntile = (c1 - c0 + FT - 1) / FT;
     auto issue = [&](int t) {
@@ -215,10 +217,12 @@ __device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const c
         const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
         if (warp < WMAX / 8 && 8 * warp < w) {
             const int row = 8 * warp + g;
+            const unsigned mk = umask[warp];
             double cr[FT / 8][2], ci[FT / 8][2];
 #pragma unroll
             for (int j = 0; j < FT / 8; ++j) cr[j][0] = cr[j][1] = ci[j][0] = ci[j][1] = 0.0;
             for (int ks = 0; ks < w; ks += 4) {
+                if (!((mk >> (ks >> 2)) & 1u)) continue;  // this 8 x 4 block of U is zero
                 const int kk = ks + t4;
                 const cplx uv = (kk < w && row < w) ? U[kk][row] : C(0.0, 0.0);
                 const double ar = uv.x, ai = -uv.y, nai = uv.y;  // conj(U)
@@ -250,7 +254,8 @@ __device__ void far_left(cplx* X, int ld, int r0, int w, int c0, int c1, const c
 // the pad the rows a warp reads at once would sit in the same banks.
 constexpr int TS = WMAX + 1;
 constexpr int FBUF_R = FT * TS;
-__device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const cplx (*U)[WMAX + 1], cplx* buf) {
+__device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const cplx (*U)[WMAX + 1], cplx* buf,
+                          const unsigned* umask) {
     const int tid = threadIdx.x, nt = blockDim.x;
     const int ntile = (r1 - r0 + FT - 1) / FT;
     auto issue = [&](int t) {
@@ -278,10 +283,12 @@ __device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const 
         const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
         if (warp < WMAX / 8 && 8 * warp < w) {
             const int col = 8 * warp + g;
+            const unsigned mk = umask[warp];
             double cr[FT / 8][2], ci[FT / 8][2];
 #pragma unroll
             for (int i = 0; i < FT / 8; ++i) cr[i][0] = cr[i][1] = ci[i][0] = ci[i][1] = 0.0;
             for (int ks = 0; ks < w; ks += 4) {
+                if (!((mk >> (ks >> 2)) & 1u)) continue;  // this 4 x 8 block of U is zero
                 const int kk = ks + t4;
                 const cplx uv = (kk < w && col < w) ? U[kk][col] : C(0.0, 0.0);
 #pragma unroll
@@ -312,13 +319,32 @@ __device__ void far_right(cplx* X, int ld, int r0, int r1, int c0, int w, const 
 // the window itself was already transformed in shared memory: rows ws..we-1 to
 // the right (columns we..n-1), columns ws..we-1 above (rows 0..ws-1), and Z.
 // The tile buffers overlay B: the window must be stored before the call.
-__device__ void far_all(int n, cplx* H, int ldh, cplx* Z, int ldz, int ws, int we, AedShared* sh) {
+// The window unitary of a sweep is banded (a chain of adjacent-column rotations
+// that moves down the window): a bitmap of its non-zero 4 x 8 blocks lets the
+// products skip the zero ones (rotations keep structural zeros exactly zero).
+// banded: the window comes from a sweep (AED and small-block windows are dense).
+__device__ void far_all(int n, cplx* H, int ldh, cplx* Z, int ldz, int ws, int we, AedShared* sh,
+                        bool banded = false) {
+    const int tid = threadIdx.x, nt = blockDim.x;
     const int w = we - ws;
     cplx* buf = &sh->B[0][0];
+    if (tid < WMAX / 8) sh->umask[tid] = banded ? 0u : ~0u;
     __syncthreads();
-    if (we < n) far_left(H, ldh, ws, w, we, n, sh->U, buf);
-    if (ws > 0) far_right(H, ldh, 0, ws, ws, w, sh->U, buf);
-    far_right(Z, ldz, 0, n, ws, w, sh->U, buf);
+    const int nkq = (w + 3) / 4, njc = (w + 7) / 8;
+    for (int e = tid; banded && e < nkq * njc; e += nt) {
+        const int kq = e / njc, jc = e % njc;
+        bool nz = false;
+        for (int r = 4 * kq; r < min(4 * kq + 4, w); ++r)
+            for (int c = 8 * jc; c < min(8 * jc + 8, w); ++c) {
+                const cplx u = sh->U[r][c];
+                nz = nz || u.x != 0.0 || u.y != 0.0;
+            }
+        if (nz) atomicOr(&sh->umask[jc], 1u << kq);
+    }
+    __syncthreads();
+    if (we < n) far_left(H, ldh, ws, w, we, n, sh->U, buf, sh->umask);
+    if (ws > 0) far_right(H, ldh, 0, ws, ws, w, sh->U, buf, sh->umask);
+    far_right(Z, ldz, 0, n, ws, w, sh->U, buf, sh->umask);
 }
 
 __device__ void load_window(const cplx* H, int ldh, int ws, int w, AedShared* sh) {
@@ -450,7 +476,8 @@ __device__ void aed(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, A
 static_assert(WMAX - 2 > 2 * (NSH - 1), "the first window introduces every bulge");
 static_assert(2 * WMAX * FT <= WMAX * (WMAX + 1) && 2 * FBUF_R <= WMAX * (WMAX + 1),
               "tile buffers overlay the window");
-static_assert(WMAX % 8 == 0 && FT % 8 == 0 && WMAX / 8 <= kSchurThreads / 32, "far-update DMMA tiles");
+static_assert(WMAX % 8 == 0 && FT % 8 == 0 && WMAX / 8 <= kSchurThreads / 32 && WMAX / 4 <= 32,
+              "far-update DMMA tiles and block bitmap");
 
 __device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, int nsh, AedShared* sh,
                             long long* prof) {
@@ -543,7 +570,7 @@ __device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, i
         }
         const long long t1 = clock64();
         store_window(H, ldh, ws, w, sh, false);
-        far_all(n, H, ldh, Z, ldz, ws, we, sh);  // begins and ends with barriers
+        far_all(n, H, ldh, Z, ldz, ws, we, sh, true);  // begins and ends with barriers
         if (prof && tid == 0) {
             prof[2] += t1 - t0;
             prof[3] += clock64() - t1;

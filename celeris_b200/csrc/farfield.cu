@@ -51,7 +51,7 @@ constexpr int kTile64 = 256;  // pillars (or pixels) per stage, 32 B records -> 
 constexpr int kTile32 = 512;  // pillars per stage, 16 B records -> 8 KB
 constexpr int kStages = 4;
 constexpr int kPPT64 = 2;     // pixels per thread, plain form
-constexpr int kPPT32 = 8;     // pixels per thread, precision form (per-pillar loads and dy shared by 8 terms)
+constexpr int kPPT32 = 12;    // pixels per thread, precision form (per-pillar record load and dy shared by 12 terms)
 constexpr int kAdjPPT = 2;    // pillars per thread, adjoint
 
 enum { GEOM_PSF = 0, GEOM_ZX = 1 };

@@ -223,6 +223,51 @@ PYBIND11_MODULE(_celeris, m) {
           py::arg("wavelength_um"), py::arg("diameter_um"), py::arg("angle_deg"), py::arg("n"),
           py::arg("half_window_um"), py::arg("on_axis_peak") = 0.0);
 
+    py::class_<ThroughFocus>(m, "ThroughFocus")
+        .def_property_readonly("z_um", [](const ThroughFocus& t) { return py::array_t<float>(t.z_um.size(), t.z_um.data()); })
+        .def_property_readonly("intensity",
+                               [](const ThroughFocus& t) { return py::array_t<float>(t.intensity.size(), t.intensity.data()); })
+        .def_readonly("z_peak_um", &ThroughFocus::z_peak_um)
+        .def_readonly("dof_um", &ThroughFocus::dof_um)
+        .def_readonly("caustic_nx", &ThroughFocus::caustic_nx)
+        .def_readonly("caustic_nz", &ThroughFocus::caustic_nz)
+        .def_readonly("caustic_xmin", &ThroughFocus::caustic_xmin)
+        .def_readonly("caustic_xmax", &ThroughFocus::caustic_xmax)
+        .def_readonly("caustic_zmin", &ThroughFocus::caustic_zmin)
+        .def_readonly("caustic_zmax", &ThroughFocus::caustic_zmax)
+        .def_property_readonly("caustic", [](const ThroughFocus& t) {
+            py::array_t<float> a({t.caustic_nz, t.caustic_nx});
+            std::copy(t.caustic.begin(), t.caustic.end(), a.mutable_data());
+            return a;
+        });
+    m.def("analyze_through_focus", &analyze_through_focus, py::arg("lens"), py::arg("lib"),
+          py::arg("focal_length_um"), py::arg("wavelength_um"), py::arg("diameter_um"));
+
+    py::class_<FieldPoint>(m, "FieldPoint")
+        .def_readonly("angle_deg", &FieldPoint::angle_deg)
+        .def_readonly("rel_strehl", &FieldPoint::rel_strehl)
+        .def_readonly("spot_shift_um", &FieldPoint::spot_shift_um);
+    m.def("analyze_field_of_view", &analyze_field_of_view, py::arg("lens"), py::arg("lib"),
+          py::arg("focal_length_um"), py::arg("wavelength_um"), py::arg("diameter_um"), py::arg("angles_deg"));
+    m.def("analyze_wide_fov", &analyze_wide_fov, py::arg("lens"), py::arg("lib"), py::arg("focal_length_um"),
+          py::arg("wavelength_um"), py::arg("lens_diameter_um"), py::arg("stop_diameter_um"),
+          py::arg("stop_distance_um"), py::arg("angles_deg"));
+    py::class_<FieldGridPoint>(m, "FieldGridPoint")
+        .def_readonly("theta_x_deg", &FieldGridPoint::theta_x_deg)
+        .def_readonly("theta_y_deg", &FieldGridPoint::theta_y_deg)
+        .def_readonly("rel_strehl", &FieldGridPoint::rel_strehl)
+        .def_readonly("fwhm_x_um", &FieldGridPoint::fwhm_x_um)
+        .def_readonly("fwhm_y_um", &FieldGridPoint::fwhm_y_um)
+        .def_readonly("cx_um", &FieldGridPoint::cx_um)
+        .def_readonly("cy_um", &FieldGridPoint::cy_um);
+    py::class_<FieldGrid>(m, "FieldGrid")
+        .def_readonly("n", &FieldGrid::n)
+        .def_readonly("max_angle_deg", &FieldGrid::max_angle_deg)
+        .def_readonly("points", &FieldGrid::points);
+    m.def("analyze_field_grid", &analyze_field_grid, py::arg("lens"), py::arg("lib"), py::arg("focal_length_um"),
+          py::arg("wavelength_um"), py::arg("diameter_um"), py::arg("max_angle_deg"), py::arg("n_half"),
+          py::arg("psf_n"));
+
     m.def("cuda_available", &cuda::available);
     m.def("cuda_device_name", &cuda::device_name);
 }

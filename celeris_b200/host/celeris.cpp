@@ -115,6 +115,43 @@ std::vector<double> psf_gpu(const std::vector<Cell>& cells, double cx, double cy
     return out;
 }
 
+// |E|^2 on an x-z slice (y = 0) of the plain FP64 form: row = z, column = x.
+std::vector<double> zx_gpu(const std::vector<Cell>& cells, double xmin, double xmax, int nx, double zmin,
+                           double zmax, int nz, double k) {
+    std::vector<double> px(cells.size()), py(cells.size()), pt(2 * cells.size());
+    for (size_t c = 0; c < cells.size(); ++c) {
+        px[c] = cells[c].x;
+        py[c] = cells[c].y;
+        pt[2 * c] = cells[c].t.real();
+        pt[2 * c + 1] = cells[c].t.imag();
+    }
+    std::vector<double> out(static_cast<size_t>(nx) * nz, 0.0);
+    if (cells.empty()) return out;
+    check(celeris_propagate_zx(px.data(), py.data(), pt.data(), static_cast<int>(cells.size()), xmin, xmax, nx,
+                               zmin, zmax, nz, k, out.data()),
+          "propagate_zx");
+    return out;
+}
+
+// Peak |E|^2 and the x of its pixel on an NG x NG grid centred at (xc, 0): the
+// search of field.cpp:48-75 / 106-134 (first maximum in row-major order, strict >).
+std::pair<double, double> peak_on_grid(const std::vector<Cell>& cells, double xc, double W, double z, double k) {
+    constexpr int NG = 81;
+    double best = 0.0, best_x = xc;
+    if (cells.empty()) return {best, best_x};
+    const std::vector<double> I = psf_gpu(cells, xc, 0.0, z, k, NG, W);
+    const double step = 2.0 * W / (NG - 1);
+    for (int j = 0; j < NG; ++j)
+        for (int i = 0; i < NG; ++i) {
+            const double v = I[static_cast<size_t>(j) * NG + i];
+            if (v > best) {
+                best = v;
+                best_x = (xc - W) + i * step;
+            }
+        }
+    return {best, best_x};
+}
+
 }  // namespace
 
 // ---- materials ---------------------------------------------------------------------
@@ -623,6 +660,174 @@ FieldPsf compute_psf_field(const MetalensDesign& lens, const UnitCellLibrary& li
     for (double v : out.psf.intensity) peak = std::max(peak, v);
     out.rel_strehl = on_axis_peak > 0 ? peak / on_axis_peak : 1.0;
     return out;
+}
+
+// ---- through-focus (throughfocus.cpp:15-135) -------------------------------------------------
+ThroughFocus analyze_through_focus(const MetalensDesign& lens, const UnitCellLibrary& lib, double focal_length_um,
+                                   double wavelength_um, double diameter_um) {
+    const double R = diameter_um / 2.0;
+    const double k = 2.0 * pi / wavelength_um;
+    const std::vector<Cell> cells = aperture_cells(lens, lib, diameter_um);
+    // scan window around the nominal focus, widened for low NA (throughfocus.cpp:45-49)
+    const double na = std::sin(std::atan(R / focal_length_um));
+    const double half = std::max(2.0 * wavelength_um / (na * na + 1e-6), 0.25 * focal_length_um);
+    const double zlo = std::max(0.1 * focal_length_um, focal_length_um - half);
+    const double zhi = focal_length_um + half;
+    const int N = 161;
+    ThroughFocus tf;
+    // on-axis intensities: an x-z slice with both columns at x = 0
+    const std::vector<double> onaxis = zx_gpu(cells, 0.0, 0.0, 2, zlo, zhi, N, k);
+    std::vector<double> I(N);
+    double peak = 0.0;
+    for (int i = 0; i < N; ++i) {
+        I[i] = onaxis[static_cast<size_t>(i) * 2];
+        peak = std::max(peak, I[i]);
+        tf.z_um.push_back(static_cast<float>(zlo + (zhi - zlo) * i / (N - 1)));
+    }
+    if (peak <= 0) peak = 1;
+    int ipk = 0;
+    for (int i = 0; i < N; ++i) {
+        tf.intensity.push_back(static_cast<float>(I[i] / peak));
+        if (I[i] > I[ipk]) ipk = i;
+    }
+    tf.z_peak_um = tf.z_um[ipk];
+    const double half_lvl = peak / 2.0;  // depth of focus: axial FWHM (throughfocus.cpp:70-75)
+    int lo = -1, hi = -1;
+    for (int i = 0; i < N; ++i)
+        if (I[i] >= half_lvl) {
+            if (lo < 0) lo = i;
+            hi = i;
+        }
+    tf.dof_um = (hi > lo && lo >= 0) ? (tf.z_um[hi] - tf.z_um[lo]) : 0.0;
+    // x-z caustic on the GPU grid of the reference (201 x 201, throughfocus.cpp:80-100)
+    const double dl = wavelength_um * focal_length_um / std::max(diameter_um, 1e-6);
+    const double Wx = std::max(8.0 * dl, 3.0);
+    tf.caustic_xmin = -Wx;
+    tf.caustic_xmax = Wx;
+    tf.caustic_zmin = zlo;
+    tf.caustic_zmax = zhi;
+    tf.caustic_nx = tf.caustic_nz = 201;
+    const std::vector<double> cmap = zx_gpu(cells, -Wx, Wx, 201, zlo, zhi, 201, k);
+    double cpeak = 0.0;
+    for (double v : cmap) cpeak = std::max(cpeak, v);
+    if (cpeak <= 0) cpeak = 1.0;
+    tf.caustic.resize(cmap.size());
+    for (size_t i = 0; i < cmap.size(); ++i) tf.caustic[i] = static_cast<float>(cmap[i] / cpeak);
+    return tf;
+}
+
+// ---- off-axis analyses (field.cpp) --------------------------------------------------------------
+std::vector<FieldPoint> analyze_field_of_view(const MetalensDesign& lens, const UnitCellLibrary& lib,
+                                              double focal_length_um, double wavelength_um, double diameter_um,
+                                              const std::vector<double>& angles_deg) {
+    const double k = 2.0 * pi / wavelength_um;
+    const double dl = wavelength_um * focal_length_um / diameter_um;
+    // peak within the window spanning the f sin and f tan spot predictions (field.cpp:35-57)
+    auto peak_near = [&](double theta, double xc) {
+        const double s = std::sin(theta);
+        const double W = std::max(3.0 * dl, 2.0) + std::abs(focal_length_um * std::tan(theta) - focal_length_um * s);
+        return peak_on_grid(aperture_cells(lens, lib, diameter_um, k * s), xc, W, focal_length_um, k);
+    };
+    const double on_axis_peak = peak_near(0.0, 0.0).first;
+    std::vector<FieldPoint> out;
+    for (double ang : angles_deg) {
+        const double theta = ang * pi / 180.0;
+        const auto pk = peak_near(theta, focal_length_um * std::tan(theta));
+        out.push_back({ang, on_axis_peak > 0 ? pk.first / on_axis_peak : 0.0, pk.second});
+    }
+    return out;
+}
+
+std::vector<FieldPoint> analyze_wide_fov(const MetalensDesign& lens, const UnitCellLibrary& lib,
+                                         double focal_length_um, double wavelength_um, double lens_diameter_um,
+                                         double stop_diameter_um, double stop_distance_um,
+                                         const std::vector<double>& angles_deg) {
+    const double k = 2.0 * pi / wavelength_um;
+    const double R_stop = stop_diameter_um / 2.0;
+    const double dl_stop = wavelength_um * focal_length_um / stop_diameter_um;
+    const std::vector<Cell> all = aperture_cells(lens, lib, lens_diameter_um);
+    // only the cells under the decentred stop patch are lit (field.cpp:101-134)
+    auto peak = [&](double theta, double x_patch) {
+        const double s = std::sin(theta);
+        const double x_sin = focal_length_um * s, x_tan = focal_length_um * std::tan(theta);
+        const double xc = 0.5 * (x_sin + x_tan);
+        const double W = std::max(3.0 * dl_stop, 2.0) + 0.5 * std::abs(x_tan - x_sin);
+        std::vector<Cell> lit;
+        for (const Cell& c : all) {
+            const double dx = c.x - x_patch, dy = c.y;
+            if (dx * dx + dy * dy > R_stop * R_stop) continue;
+            lit.push_back({c.x, c.y, c.t * std::polar(1.0, k * s * c.x)});
+        }
+        return peak_on_grid(lit, xc, W, focal_length_um, k);
+    };
+    const double on_axis_peak = peak(0.0, 0.0).first;
+    std::vector<FieldPoint> out;
+    for (double ang : angles_deg) {
+        const double theta = ang * pi / 180.0;
+        const auto pk = peak(theta, stop_distance_um * std::tan(theta));
+        out.push_back({ang, on_axis_peak > 0 ? pk.first / on_axis_peak : 0.0, pk.second});
+    }
+    return out;
+}
+
+FieldGrid analyze_field_grid(const MetalensDesign& lens, const UnitCellLibrary& lib, double focal_length_um,
+                             double wavelength_um, double diameter_um, double max_angle_deg, int n_half, int psf_n) {
+    const double k = 2.0 * pi / wavelength_um;
+    const double dl = wavelength_um * focal_length_um / diameter_um;  // field.cpp:178-181
+    const double W = std::max(6.0 * dl, 4.0);
+    const double step = 2.0 * W / (psf_n - 1);
+    struct Spot {
+        double peak, fwhm_x, fwhm_y;
+    };
+    // peak and tangential/sagittal FWHM of one tilted-illumination PSF (field.cpp:183-211)
+    auto spot_at = [&](double tx, double ty, double cx, double cy) -> Spot {
+        std::vector<Cell> cells = aperture_cells(lens, lib, diameter_um);
+        const double sx = std::sin(tx), sy = std::sin(ty);
+        for (Cell& c : cells) c.t *= std::polar(1.0, k * (sx * c.x + sy * c.y));
+        const std::vector<double> I = psf_gpu(cells, cx, cy, focal_length_um, k, psf_n, W);
+        int pix = 0, piy = 0;
+        double best = -1.0;
+        for (int j = 0; j < psf_n; ++j)
+            for (int i = 0; i < psf_n; ++i) {
+                const double v = I[static_cast<size_t>(j) * psf_n + i];
+                if (v > best) {
+                    best = v;
+                    pix = i;
+                    piy = j;
+                }
+            }
+        const double half = best / 2.0;
+        auto fwhm_along = [&](bool horizontal) {
+            int lo = -1, hi = -1;
+            for (int s = 0; s < psf_n; ++s) {
+                const size_t idx = horizontal ? static_cast<size_t>(piy) * psf_n + s : static_cast<size_t>(s) * psf_n + pix;
+                if (I[idx] >= half) {
+                    if (lo < 0) lo = s;
+                    hi = s;
+                }
+            }
+            return (hi > lo && lo >= 0) ? (hi - lo) * step : 0.0;
+        };
+        return {best, fwhm_along(true), fwhm_along(false)};
+    };
+    const Spot on_axis = spot_at(0.0, 0.0, 0.0, 0.0);
+    const double ref = on_axis.peak > 0 ? on_axis.peak : 1.0;
+    FieldGrid g;
+    g.n = 2 * n_half + 1;
+    g.max_angle_deg = max_angle_deg;
+    g.points.reserve(static_cast<size_t>(g.n) * g.n);
+    for (int jy = -n_half; jy <= n_half; ++jy) {
+        const double ang_y = n_half > 0 ? max_angle_deg * jy / n_half : 0.0;
+        const double ty = ang_y * pi / 180.0;
+        for (int jx = -n_half; jx <= n_half; ++jx) {
+            const double ang_x = n_half > 0 ? max_angle_deg * jx / n_half : 0.0;
+            const double tx = ang_x * pi / 180.0;
+            const double cx = focal_length_um * std::tan(tx), cy = focal_length_um * std::tan(ty);
+            const Spot s = spot_at(tx, ty, cx, cy);
+            g.points.push_back({ang_x, ang_y, s.peak / ref, s.fwhm_x, s.fwhm_y, cx, cy});
+        }
+    }
+    return g;
 }
 
 namespace cuda {

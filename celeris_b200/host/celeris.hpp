@@ -195,6 +195,48 @@ FieldPsf compute_psf_field(const MetalensDesign& lens, const UnitCellLibrary& li
                            double wavelength_um, double diameter_um, double angle_deg, int n,
                            double half_window_um, double on_axis_peak = 0.0);
 
+// ---- through-focus and off-axis analyses (callers of the far field) ----------------------
+// throughfocus.hpp:13-35: on-axis z scan (161 points) + x-z caustic (201 x 201 on the GPU).
+struct ThroughFocus {
+    std::vector<float> z_um;
+    std::vector<float> intensity;
+    double z_peak_um = 0;
+    double dof_um = 0;
+    int caustic_nx = 0, caustic_nz = 0;
+    double caustic_xmin = 0, caustic_xmax = 0;
+    double caustic_zmin = 0, caustic_zmax = 0;
+    std::vector<float> caustic;
+};
+ThroughFocus analyze_through_focus(const MetalensDesign& lens, const UnitCellLibrary& lib, double focal_length_um,
+                                   double wavelength_um, double diameter_um);
+
+// field.hpp:9-47: tilted-illumination focal spots.
+struct FieldPoint {
+    double angle_deg;
+    double rel_strehl;
+    double spot_shift_um;
+};
+std::vector<FieldPoint> analyze_field_of_view(const MetalensDesign& lens, const UnitCellLibrary& lib,
+                                              double focal_length_um, double wavelength_um, double diameter_um,
+                                              const std::vector<double>& angles_deg);
+std::vector<FieldPoint> analyze_wide_fov(const MetalensDesign& lens, const UnitCellLibrary& lib,
+                                         double focal_length_um, double wavelength_um, double lens_diameter_um,
+                                         double stop_diameter_um, double stop_distance_um,
+                                         const std::vector<double>& angles_deg);
+struct FieldGridPoint {
+    double theta_x_deg, theta_y_deg;
+    double rel_strehl;
+    double fwhm_x_um, fwhm_y_um;
+    double cx_um, cy_um;
+};
+struct FieldGrid {
+    int n = 0;
+    double max_angle_deg = 0;
+    std::vector<FieldGridPoint> points;
+};
+FieldGrid analyze_field_grid(const MetalensDesign& lens, const UnitCellLibrary& lib, double focal_length_um,
+                             double wavelength_um, double diameter_um, double max_angle_deg, int n_half, int psf_n);
+
 namespace cuda {
 bool available();
 const char* device_name();

@@ -112,3 +112,61 @@ def ref_propagate_pillars(px, py, t, cx, cy, z, wavelength_um, n, half_window):
 def ref_threads():
     r = ref_lib()
     return None if r is None else int(r.ref_hardware_threads())
+
+
+# ---- the reference's own analyses (field.cpp, throughfocus.cpp) on a lens given
+# as arrays: n_cells, period, fill_map [n_cells^2], library fill/phase/amplitude.
+def _lens_args(lens_n, period, fill_map, lib_fill, lib_phase, lib_amp, lib_wl):
+    fm, lf, lp, la = (_f64(np.ravel(a)) for a in (fill_map, lib_fill, lib_phase, lib_amp))
+    keep = (fm, lf, lp, la)
+    args = [ctypes.c_int(lens_n), _D(period), _dp(fm), ctypes.c_int(len(lf)), _dp(lf), _dp(lp), _dp(la), _D(lib_wl)]
+    return args, keep
+
+
+def _ref_or_raise():
+    r = ref_lib()
+    if r is None:
+        raise FileNotFoundError("oracle/_ref/libref_farfield.so not built")
+    return r
+
+
+def ref_through_focus(lens_args, f, wl, D):
+    """celeris::analyze_through_focus (throughfocus.cpp:15-78, CPU): z, normalized
+    on-axis intensity, z_peak, depth of focus."""
+    r = _ref_or_raise()
+    args, keep = _lens_args(*lens_args)
+    z = np.zeros(161, dtype=np.float32)
+    I = np.zeros(161, dtype=np.float32)
+    sc = np.zeros(2)
+    fp = ctypes.POINTER(ctypes.c_float)
+    r.ref_through_focus(*args, _D(f), _D(wl), _D(D), z.ctypes.data_as(fp), I.ctypes.data_as(fp), _dp(sc))
+    return z, I, sc[0], sc[1]
+
+
+def ref_field_of_view(lens_args, f, wl, D, angles):
+    r = _ref_or_raise()
+    args, keep = _lens_args(*lens_args)
+    a = _f64(angles)
+    out = np.zeros((len(a), 3))
+    r.ref_field_of_view(*args, _D(f), _D(wl), _D(D), _dp(a), ctypes.c_int(len(a)), _dp(out))
+    return out
+
+
+def ref_wide_fov(lens_args, f, wl, D_lens, D_stop, stop_dist, angles):
+    r = _ref_or_raise()
+    args, keep = _lens_args(*lens_args)
+    a = _f64(angles)
+    out = np.zeros((len(a), 3))
+    r.ref_wide_fov(*args, _D(f), _D(wl), _D(D_lens), _D(D_stop), _D(stop_dist), _dp(a), ctypes.c_int(len(a)),
+                   _dp(out))
+    return out
+
+
+def ref_field_grid(lens_args, f, wl, D, max_angle, n_half, psf_n):
+    r = _ref_or_raise()
+    args, keep = _lens_args(*lens_args)
+    n = 2 * n_half + 1
+    out = np.zeros((n * n, 7))
+    r.ref_field_grid(*args, _D(f), _D(wl), _D(D), _D(max_angle), ctypes.c_int(n_half), ctypes.c_int(psf_n),
+                     _dp(out))
+    return out

@@ -52,7 +52,7 @@ EXPORTED = [
     "celeris_rs_check_dev", "celeris_sync_status", "celeris_solve_rcwa_2d", "celeris_rcwa_batch",
     "celeris_probe_peaks", "celeris_set_kernel_timing", "celeris_last_kernel_ms",
     "celeris_rs_field_noalloc", "celeris_probe_sincos", "celeris_rcwa_tuning_report",
-    "celeris_probe_dmma",
+    "celeris_probe_dmma", "celeris_solve_rcwa_2d_stack", "celeris_rcwa_stack_batch",
 ]
 
 
@@ -124,6 +124,8 @@ def load(path: str = LIB_PATH):
         "celeris_solve_rcwa_2d": (_I, [ctypes.POINTER(RcwaCell), _P, _P, ctypes.POINTER(RcwaResult)]),
         "celeris_rcwa_batch": (_I, [ctypes.POINTER(RcwaCell), _I, ctypes.POINTER(RcwaResult), _PI]),
         "celeris_rcwa_tuning_report": (_I, [ctypes.c_char_p, _I]),
+        "celeris_solve_rcwa_2d_stack": (_I, [ctypes.POINTER(RcwaCell), _I, _P, _P, ctypes.POINTER(RcwaResult)]),
+        "celeris_rcwa_stack_batch": (_I, [ctypes.POINTER(RcwaCell), _PI, _I, ctypes.POINTER(RcwaResult), _PI]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -265,3 +267,27 @@ def rcwa_batch(cells) -> tuple[list[dict], np.ndarray]:
     info = np.zeros(n, dtype=np.int32)
     check(load().celeris_rcwa_batch(arr, n, out, info.ctypes.data_as(_PI)))
     return [result_dict(out[i]) for i in range(2 * n)], info
+
+
+def solve_rcwa_2d_stack(layers, Ex0=1.0 + 0j, Ey0=0.0 + 0j) -> dict:
+    """Multi-layer stack (layers[0] next to the incident half-space)."""
+    n = len(layers)
+    arr = (RcwaCell * n)(*layers)
+    ex = np.array([complex(Ex0).real, complex(Ex0).imag])
+    ey = np.array([complex(Ey0).real, complex(Ey0).imag])
+    out = RcwaResult()
+    check(load().celeris_solve_rcwa_2d_stack(arr, n, _dp(ex), _dp(ey), ctypes.byref(out)))
+    return result_dict(out)
+
+
+def rcwa_stack_batch(stacks) -> tuple[list[dict], np.ndarray]:
+    """Batched stacks (a list of layer lists); returns ([X, Y] results per stack flattened, info)."""
+    flat = [c for st in stacks for c in st]
+    start = np.zeros(len(stacks) + 1, dtype=np.int32)
+    start[1:] = np.cumsum([len(st) for st in stacks])
+    arr = (RcwaCell * max(len(flat), 1))(*flat)
+    out = (RcwaResult * max(2 * len(stacks), 1))()
+    info = np.zeros(max(len(stacks), 1), dtype=np.int32)
+    check(load().celeris_rcwa_stack_batch(arr, start.ctypes.data_as(_PI), len(stacks), out,
+                                          info.ctypes.data_as(_PI)))
+    return [result_dict(out[i]) for i in range(2 * len(stacks))], info[:len(stacks)]

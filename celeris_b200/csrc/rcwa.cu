@@ -578,6 +578,237 @@ __global__ void __launch_bounds__(kRT) rcwa_smat2(Bucket b) {
     blk_matvec2(n, n, T11, n, stg, b0, 1, b.s_n, true);
 }
 
+// ---- multi-layer stacks ----------------------------------------------------------------------
+// A stack is its incident half-space, nl patterned layers and the substrate. The
+// layers run through the single-layer stages up to the eigenvectors as separate
+// cells; rcwa_layer_out keeps each layer's region data (phi = W, kp phi = A,
+// q, thickness) in a layer store; rcwa_stack_smat then runs the reference's
+// S-matrix recursion over the nl + 1 interfaces (rcwa2d.cpp:376-401) for the two
+// excitation columns (bN = 0, so only S11 a0 and S21 a0 are needed, with S12 and
+// S22 kept whole for the recursion).
+struct StackDev {
+    int nl;     // patterned layers
+    int slot0;  // first layer's slot in the layer store (layers are consecutive)
+};
+struct StackBucket {
+    int Mx, My, N, n, nstack;
+    const CellDev* cells;  // shared parameters of each stack (its first layer's descriptor)
+    const StackDev* stacks;
+    cplx *LW, *LA, *Lq;    // layer store: W [n*n], A [n*n], q [n] per slot
+    const double* Lh;      // thickness per slot
+    cplx *S12, *S22, *Q, *P, *X, *Y, *Z1;  // per stack, n*n each
+    cplx* vec;             // per stack 10n: aN_X, aN_Y, b0_X, b0_Y | u [n x 2] | w [n x 2] | unused [n x 2]
+    int* piv;
+    int* info;
+    size_t s_nn, s_n;
+};
+
+// Region data of one layer for the recursion: A = kp W (the operator of
+// rcwa2d.cpp:344-349 applied to the eigenvectors), copied with W, q and the
+// thickness into the layer store. Z and X are free after the eigenvectors.
+__global__ void __launch_bounds__(kRT) rcwa_layer_out(Bucket b, cplx* LW, cplx* LA, cplx* Lq, double* Lh,
+                                                      const int* slot) {
+    __shared__ GemmSmem gs;
+    const int cell = blockIdx.x;
+    const CellDev c = b.cells[cell];
+    const int N = b.N, n = b.n;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const double w2 = c.omega * c.omega;
+    const cplx* W = at(b.W, b.s_nn, cell);
+    const cplx* Einv = at(b.Einv, b.s_NN, cell);
+    cplx* V = at(b.Z, b.s_nn, cell);
+    cplx* U = at(b.X, b.s_nn, cell);
+    const int sl = slot[cell];
+    cplx* Wo = LW + b.s_nn * sl;
+    cplx* Ao = LA + b.s_nn * sl;
+    // V = Jk^T W = Kx W_bottom - Ky W_top; U = Einv V
+    for (int e = tid; e < N * n; e += nt) {
+        const int i = e / n, j = e % n;
+        V[e] = cfma(kx_of(b, c, i), W[(size_t)(N + i) * n + j], cneg(cmul(ky_of(b, c, i), W[(size_t)i * n + j])));
+    }
+    blk_gemm(N, n, N, C(1.0, 0.0), Einv, N, V, n, C(0.0, 0.0), U, n, &gs);
+    // kp W = w^2 W + [Ky U; -Kx U]
+    for (int e = tid; e < N * n; e += nt) {
+        const int i = e / n;
+        Ao[e] = cfma(ky_of(b, c, i), U[e], cscale(W[e], w2));
+        Ao[(size_t)N * n + e] = cfms(kx_of(b, c, i), U[e], cscale(W[(size_t)N * n + e], w2));
+    }
+    for (int e = tid; e < n * n; e += nt) Wo[e] = W[e];
+    for (int i = tid; i < n; i += nt) Lq[b.s_n * sl + i] = at(b.q1, b.s_n, cell)[i];
+    if (tid == 0) Lh[sl] = c.h;
+}
+
+// kp block (2 x 2 per order) and kz of a homogeneous half-space (rcwa2d.cpp:254-273)
+__device__ __forceinline__ void half_space(const StackBucket& sb, const CellDev& c, cplx nreg, int i, cplx& ka,
+                                           cplx& kb, cplx& kc, cplx& kd, cplx& kz) {
+    const int p = i / (2 * sb.My + 1) - sb.Mx, q = i % (2 * sb.My + 1) - sb.My;
+    const cplx kx = csub(c.kx0, C(2.0 * PI * (double)p / c.px, 0.0));
+    const cplx ky = csub(c.ky0, C(2.0 * PI * (double)q / c.py, 0.0));
+    const cplx er = cmul(nreg, nreg);
+    kp_uniform(cinv(er), c.omega, kx, ky, ka, kb, kc, kd);
+    kz = kz_uniform(er, c.omega, kx, ky);
+}
+
+// One CTA per stack. dynamic smem: lu_stage_bytes(n)
+__global__ void __launch_bounds__(kRT) rcwa_stack_smat(StackBucket sb) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    cplx* stg = reinterpret_cast<cplx*>(smem);
+    __shared__ GemmSmem gs;
+    __shared__ RedScratch rs;
+    const int st = blockIdx.x;
+    const CellDev c = sb.cells[st];
+    const StackDev sd = sb.stacks[st];
+    const int N = sb.N, n = sb.n;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const size_t nn = sb.s_nn;
+    cplx* S12 = sb.S12 + nn * st;
+    cplx* S22 = sb.S22 + nn * st;
+    cplx* Q = sb.Q + nn * st;
+    cplx* P = sb.P + nn * st;
+    cplx* X = sb.X + nn * st;
+    cplx* Y = sb.Y + nn * st;
+    cplx* Z1 = sb.Z1 + nn * st;
+    cplx* vec = sb.vec + 10 * sb.s_n * st;
+    cplx* u = vec + 4 * sb.s_n;  // S11 a0, [n x 2]
+    cplx* w = vec + 6 * sb.s_n;  // T12 u, [n x 2]
+    int* piv = sb.piv + sb.s_n * st;
+    const int i0 = sb.Mx * (2 * sb.My + 1) + sb.My;
+    int status = 0;
+    // S11 a0 = a0 (columns X: Ex0 = 1, Y: Ey0 = 1), S21 a0 = 0, S12 = 0, S22 = I
+    for (int e = tid; e < 2 * n; e += nt) {
+        const int i = e / 2, r = e % 2;
+        u[e] = (r == 0) ? C(i == N + i0 ? 1.0 : 0.0, 0.0) : C(i == i0 ? -1.0 : 0.0, 0.0);
+        vec[(size_t)r * sb.s_n + i] = C(0.0, 0.0);
+        vec[(2 + (size_t)r) * sb.s_n + i] = C(0.0, 0.0);
+    }
+    for (int e = tid; e < n * n; e += nt) {
+        S12[e] = C(0.0, 0.0);
+        S22[e] = C(e / n == e % n ? 1.0 : 0.0, 0.0);
+    }
+    __syncthreads();
+    const int NL = sd.nl + 2;  // regions: incident, layers, substrate
+    for (int ia = 0; ia + 1 < NL; ++ia) {
+        const int ib = ia + 1;
+        const bool a_inc = ia == 0, b_sub = ib == NL - 1;
+        const int sa = sd.slot0 + ia - 1, sbb = sd.slot0 + ib - 1;
+        const cplx* qa = a_inc ? nullptr : sb.Lq + sb.s_n * sa;
+        const cplx* qb = b_sub ? nullptr : sb.Lq + sb.s_n * sbb;
+        const double ha = a_inc ? 0.0 : sb.Lh[sa], hb = b_sub ? 0.0 : sb.Lh[sbb];
+        // Q = phi_a^-1 phi_b ; P = A_a^-1 A_b  (A = kp phi; half-spaces: phi = I, A = kp)
+        for (int e = tid; e < n * n; e += nt) {
+            const int i = e / n, j = e % n;
+            cplx qv, pv;
+            if (b_sub) {
+                qv = C(i == j ? 1.0 : 0.0, 0.0);
+                const int m = i % N;
+                cplx ka, kb, kc, kd, kz;
+                half_space(sb, c, c.n_sub, m, ka, kb, kc, kd, kz);
+                // kp of the substrate: [[ka, kb], [kc, kd]] on rows / columns (m, N + m)
+                pv = C(0.0, 0.0);
+                if (j == m) pv = i < N ? ka : kc;
+                else if (j == N + m) pv = i < N ? kb : kd;
+            } else {
+                qv = sb.LW[nn * sbb + e];
+                pv = sb.LA[nn * sbb + e];
+            }
+            Q[e] = qv;
+            P[e] = pv;
+        }
+        __syncthreads();
+        if (a_inc) {
+            // phi_a = I: Q is phi_b already; P <- kp_inc^-1 P by 2 x 2 blocks per order
+            for (int e = tid; e < N * n; e += nt) {
+                const int m = e / n, j = e % n;
+                cplx ka, kb, kc, kd, kz;
+                half_space(sb, c, c.n_inc, m, ka, kb, kc, kd, kz);
+                const cplx idet = cinv(csub(cmul(ka, kd), cmul(kb, kc)));
+                const cplx x0 = P[(size_t)m * n + j], x1 = P[(size_t)(N + m) * n + j];
+                P[(size_t)m * n + j] = cmul(idet, csub(cmul(kd, x0), cmul(kb, x1)));
+                P[(size_t)(N + m) * n + j] = cmul(idet, csub(cmul(ka, x1), cmul(kc, x0)));
+            }
+        } else {
+            // the layer store's W and A of region a are not needed after this interface
+            cplx* Wa = sb.LW + nn * sa;
+            cplx* Aa = sb.LA + nn * sa;
+            int inf = blk_lu_blocked(n, Wa, n, piv, &rs, stg, &gs);
+            blk_lu_solve_blocked(n, Wa, n, piv, n, Q, n, stg, &gs);
+            if (inf) status = inf;
+            inf = blk_lu_blocked(n, Aa, n, piv, &rs, stg, &gs);
+            blk_lu_solve_blocked(n, Aa, n, piv, n, P, n, stg, &gs);
+            if (inf) status = inf;
+        }
+        __syncthreads();
+        // P <- diag(q_a) P diag(1/q_b); T11 = (Q + P)/2 -> Q, T12 = (Q - P)/2 -> P
+        for (int e = tid; e < n * n; e += nt) {
+            const int i = e / n, j = e % n;
+            cplx qai, qbj;
+            if (a_inc) {
+                cplx ka, kb, kc, kd;
+                half_space(sb, c, c.n_inc, i % N, ka, kb, kc, kd, qai);
+            } else {
+                qai = qa[i];
+            }
+            if (b_sub) {
+                cplx ka, kb, kc, kd;
+                half_space(sb, c, c.n_sub, j % N, ka, kb, kc, kd, qbj);
+            } else {
+                qbj = qb[j];
+            }
+            const cplx pv = cdiv(cmul(qai, P[e]), qbj), qv = Q[e];
+            Q[e] = cscale(cadd(qv, pv), 0.5);
+            P[e] = cscale(csub(qv, pv), 0.5);
+        }
+        // X = T11 - d1 S12 T12 ; Y = d1 S12 T11 - T12   (d1 = exp(i q_a h_a) on the rows)
+        blk_gemm(n, n, n, C(1.0, 0.0), S12, n, P, n, C(0.0, 0.0), X, n, &gs);
+        blk_gemm(n, n, n, C(1.0, 0.0), S12, n, Q, n, C(0.0, 0.0), Y, n, &gs);
+        for (int e = tid; e < n * n; e += nt) {
+            const int i = e / n;
+            const cplx d1 = a_inc ? C(1.0, 0.0) : cexpi(cscale(qa[i], ha));
+            X[e] = cfms(d1, X[e], Q[e]);
+            Y[e] = csub(cmul(d1, Y[e]), P[e]);
+        }
+        for (int e = tid; e < 2 * n; e += nt) {
+            const int i = e / 2;
+            const cplx d1 = a_inc ? C(1.0, 0.0) : cexpi(cscale(qa[i], ha));
+            u[e] = cmul(d1, u[e]);
+        }
+        const int inf = blk_lu_blocked(n, X, n, piv, &rs, stg, &gs);
+        if (inf) status = inf;
+        blk_lu_solve_blocked(n, X, n, piv, n, Y, n, stg, &gs);  // Y = X^-1 (d1 S12 T11 - T12)
+        blk_lu_solve_blocked(n, X, n, piv, 2, u, 2, stg, &gs);  // u = S11' a0 = X^-1 d1 S11 a0
+        // S12' = Y diag(d2)
+        for (int e = tid; e < n * n; e += nt) {
+            const int j = e % n;
+            const cplx d2 = b_sub ? C(1.0, 0.0) : cexpi(cscale(qb[j], hb));
+            S12[e] = cmul(Y[e], d2);
+        }
+        // S21' a0 = S21 a0 + S22 T12 u'
+        for (int e = tid; e < 2 * n; e += nt) stg[e] = u[e];
+        __syncthreads();
+        blk_matvec2(n, n, P, n, stg, w, 2, 1, false);  // w = T12 u'
+        __syncthreads();
+        for (int e = tid; e < 2 * n; e += nt) stg[e] = w[e];
+        __syncthreads();
+        blk_matvec2(n, n, S22, n, stg, vec + 2 * sb.s_n, 1, sb.s_n, true);
+        // S22' = S22 (T12 S12' + T11 diag(d2))
+        blk_gemm(n, n, n, C(1.0, 0.0), P, n, S12, n, C(0.0, 0.0), Z1, n, &gs);
+        for (int e = tid; e < n * n; e += nt) {
+            const int j = e % n;
+            const cplx d2 = b_sub ? C(1.0, 0.0) : cexpi(cscale(qb[j], hb));
+            Z1[e] = cfma(Q[e], d2, Z1[e]);
+        }
+        blk_gemm(n, n, n, C(1.0, 0.0), S22, n, Z1, n, C(0.0, 0.0), X, n, &gs);  // X is free after the solves
+        for (int e = tid; e < n * n; e += nt) S22[e] = X[e];
+        __syncthreads();
+    }
+    // exterior amplitudes for the epilogue: aN = S11 a0 (2 columns)
+    for (int e = tid; e < 2 * n; e += nt) {
+        const int i = e / 2, r = e % 2;
+        vec[(size_t)r * sb.s_n + i] = u[e];
+    }
+    if (tid == 0 && status != 0) sb.info[st] = -status;
+}
+
 // ---- flux and order-0 field (rcwa2d.cpp:416-463) ---------------------------------------------
 __global__ void __launch_bounds__(kRT) rcwa_epilogue(Bucket b) {
     __shared__ RedScratch rs;
@@ -826,7 +1057,8 @@ int set_smem_limits(const SmemNeeds& s) {
 
 // Launch the stage sequence of one bucket on `st`. ev (ST_COUNT + 1 events) is
 // optional: stage boundaries are recorded into it.
-void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEvent_t* ev) {
+// eig_only: stop after the eigenvectors (the layers of a multi-layer stack).
+void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEvent_t* ev, bool eig_only = false) {
     const int nc = b.ncell, n = b.n;
     const int* T = cfg.threads;
     if (ev) cudaEventRecord(ev[0], st);
@@ -859,6 +1091,10 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
     if (ev) cudaEventRecord(ev[4], st);
     rcwa_vec<<<nc, T[ST_VEC], 0, st>>>(b);
     if (ev) cudaEventRecord(ev[5], st);
+    if (eig_only) {
+        count_launch(4);
+        return;
+    }
     const size_t sm_stage = lu_stage_bytes(n);
     rcwa_smat1<<<nc, T[ST_SMAT1], sm_stage, st>>>(b);
     if (ev) cudaEventRecord(ev[6], st);
@@ -1202,6 +1438,248 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
     return CELERIS_OK;
 }
 
+// ---- multi-layer stacks ----------------------------------------------------------------------
+// Device buffers owned by one call (the stack path keeps its own allocations, so
+// it does not disturb the single-layer batch's workspace or cached graph).
+struct DevBuf {
+    std::vector<void*> ptrs;
+    ~DevBuf() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+    template <typename T>
+    int get(T** out, size_t count) {
+        void* p = nullptr;
+        CEL_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+        ptrs.push_back(p);
+        *out = static_cast<T*>(p);
+        return CELERIS_OK;
+    }
+};
+
+// stacks[s] = (first layer index, layer count) into `layers`; exc holds 4 doubles
+// (Ex0 re, im, Ey0 re, im) per stack; results nexc per stack.
+int run_stacks(const celeris_rcwa_cell* layers, const std::vector<std::pair<int, int>>& stacks,
+               const double* exc, celeris_rcwa_result* out, int* info_out, int nexc) {
+    CEL_TRY(celeris_rt::require_device());
+    int dev = 0, smem_optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaStream_t st = nullptr;
+    CEL_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } sg{st};
+    // stacks grouped by (Mx, My): one layer store and one recursion launch per group
+    std::map<std::pair<int, int>, std::vector<int>> groups;
+    for (int s = 0; s < (int)stacks.size(); ++s) {
+        const celeris_rcwa_cell& f = layers[stacks[s].first];
+        groups[{f.Mx, f.My}].push_back(s);
+    }
+    size_t free_b = 0, total_b = 0;
+    CEL_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t budget = free_b / 2;
+    for (auto& g : groups) {
+        const int Mx = g.first.first, My = g.first.second;
+        const int N = (2 * Mx + 1) * (2 * My + 1), n = 2 * N;
+        const size_t s_nn = (size_t)n * n, s_n = (size_t)n, s_NN = (size_t)N * N;
+        // stacks in chunks whose layer store, eigen buffers and recursion buffers fit the budget
+        const size_t per_layer = (7 * s_nn + 3 * s_NN + 4 * s_n) * sizeof(cplx) + 4096;
+        const size_t per_stack = (7 * s_nn + 11 * s_n) * sizeof(cplx) + 4096;
+        size_t c0 = 0;
+        while (c0 < g.second.size()) {
+            std::vector<int> ids;
+            size_t bytes = 0;
+            while (c0 < g.second.size()) {
+                const size_t need = per_stack + per_layer * stacks[g.second[c0]].second;
+                if (!ids.empty() && bytes + need > budget) break;
+                ids.push_back(g.second[c0++]);
+                bytes += need;
+            }
+            const int ns = (int)ids.size();
+            DevBuf mem;
+            // layer store slots, in stack order
+            std::vector<HostCell> sub;
+            std::vector<int> first_slot(ns);
+            for (int k = 0; k < ns; ++k) {
+                first_slot[k] = (int)sub.size();
+                const auto& sp = stacks[ids[k]];
+                for (int l = 0; l < sp.second; ++l)
+                    sub.push_back(make_cell(layers[sp.first + l], (int)sub.size(), 1.0, 0.0, 0.0, 0.0, 2));
+            }
+            const int nslot = (int)sub.size();
+            cplx *LW, *LA, *Lq;
+            double* Lh;
+            CEL_TRY(mem.get(&LW, s_nn * nslot));
+            CEL_TRY(mem.get(&LA, s_nn * nslot));
+            CEL_TRY(mem.get(&Lq, s_n * nslot));
+            CEL_TRY(mem.get(&Lh, (size_t)nslot));
+            std::vector<int> sub_info(nslot, 0);
+            // eigen-solutions of every layer, one bucket per raster class
+            std::map<int, std::vector<int>> by_ng;
+            for (int i = 0; i < nslot; ++i) by_ng[sub[i].ng].push_back(i);
+            for (auto& kv : by_ng) {
+                const int ng = kv.first;
+                const std::vector<int>& si = kv.second;
+                const int nc = (int)si.size();
+                if (ng > 0 && laurent_smem(Mx, My, ng) + 1024 > (size_t)smem_optin)
+                    return set_error(CELERIS_ERR_TOO_LARGE, "raster %d with M=(%d,%d) exceeds shared memory", ng,
+                                     Mx, My);
+                DevBuf bm;
+                Bucket b;
+                std::memset(&b, 0, sizeof(b));
+                b.Mx = Mx;
+                b.My = My;
+                b.N = N;
+                b.n = n;
+                b.ng = ng;
+                b.ncell = nc;
+                b.s_nn = s_nn;
+                b.s_ns = (size_t)n * (n + 2);
+                b.s_NN = s_NN;
+                b.s_n = s_n;
+                CellDev* dcells;
+                CEL_TRY(bm.get(&dcells, (size_t)nc));
+                b.cells = dcells;
+                cplx** mats[] = {&b.H, &b.Z, &b.X, &b.W, &b.A};
+                for (cplx** m : mats) CEL_TRY(bm.get(m, s_nn * nc));
+                CEL_TRY(bm.get(&b.Einv, s_NN * nc));
+                CEL_TRY(bm.get(&b.Exx, s_NN * nc));
+                CEL_TRY(bm.get(&b.Eyy, s_NN * nc));
+                CEL_TRY(bm.get(&b.q1, s_n * nc));
+                CEL_TRY(bm.get(&b.piv, s_n * nc));
+                CEL_TRY(bm.get(&b.info, (size_t)nc));
+                if (ng > 0) {
+                    cplx *phx, *phy;
+                    CEL_TRY(bm.get(&phx, (size_t)(4 * Mx + 1) * ng));
+                    CEL_TRY(bm.get(&phy, (size_t)(4 * My + 1) * ng));
+                    b.phx = phx;
+                    b.phy = phy;
+                }
+                std::vector<CellDev> hd(nc);
+                std::vector<int> hslot(nc);
+                for (int i = 0; i < nc; ++i) {
+                    hd[i] = sub[si[i]].d;
+                    hslot[i] = si[i];
+                }
+                int* dslot;
+                CEL_TRY(bm.get(&dslot, (size_t)nc));
+                CEL_CUDA(cudaMemcpyAsync(dcells, hd.data(), sizeof(CellDev) * nc, cudaMemcpyHostToDevice, st));
+                CEL_CUDA(cudaMemcpyAsync(dslot, hslot.data(), sizeof(int) * nc, cudaMemcpyHostToDevice, st));
+                SmemNeeds needs;
+                needs.add(Mx, My, ng, n);
+                CEL_TRY(set_smem_limits(needs));
+                launch_bucket(b, uniform_cfg(256), st, nullptr, true);
+                rcwa_layer_out<<<nc, kRT, 0, st>>>(b, LW, LA, Lq, Lh, dslot);
+                count_launch(1);
+                CEL_CUDA(cudaGetLastError());
+                std::vector<int> hinfo(nc);
+                CEL_CUDA(cudaMemcpyAsync(hinfo.data(), b.info, sizeof(int) * nc, cudaMemcpyDeviceToHost, st));
+                CEL_CUDA(cudaStreamSynchronize(st));
+                for (int i = 0; i < nc; ++i) sub_info[si[i]] = hinfo[i];
+            }
+            // S-matrix recursion and outputs, one CTA per stack
+            StackBucket sb;
+            std::memset(&sb, 0, sizeof(sb));
+            sb.Mx = Mx;
+            sb.My = My;
+            sb.N = N;
+            sb.n = n;
+            sb.nstack = ns;
+            sb.LW = LW;
+            sb.LA = LA;
+            sb.Lq = Lq;
+            sb.Lh = Lh;
+            sb.s_nn = s_nn;
+            sb.s_n = s_n;
+            cplx** smats[] = {&sb.S12, &sb.S22, &sb.Q, &sb.P, &sb.X, &sb.Y, &sb.Z1};
+            for (cplx** m : smats) CEL_TRY(mem.get(m, s_nn * ns));
+            CEL_TRY(mem.get(&sb.vec, 10 * s_n * ns));
+            CEL_TRY(mem.get(&sb.piv, s_n * ns));
+            CEL_TRY(mem.get(&sb.info, (size_t)ns));
+            CellDev* scells;
+            StackDev* sdev;
+            celeris_rcwa_result* dres;
+            CEL_TRY(mem.get(&scells, (size_t)ns));
+            CEL_TRY(mem.get(&sdev, (size_t)ns));
+            CEL_TRY(mem.get(&dres, (size_t)ns * nexc));
+            std::vector<CellDev> hc(ns);
+            std::vector<StackDev> hs(ns);
+            std::vector<int> hinfo(ns, 0);
+            for (int k = 0; k < ns; ++k) {
+                const auto& sp = stacks[ids[k]];
+                const double* e = exc + 4 * (size_t)ids[k];
+                hc[k] = make_cell(layers[sp.first], ids[k], e[0], e[1], e[2], e[3], nexc).d;
+                hs[k].nl = sp.second;
+                hs[k].slot0 = first_slot[k];
+                for (int l = 0; l < sp.second; ++l)
+                    if (sub_info[first_slot[k] + l] != 0 && hinfo[k] == 0) hinfo[k] = sub_info[first_slot[k] + l];
+            }
+            CEL_CUDA(cudaMemcpyAsync(scells, hc.data(), sizeof(CellDev) * ns, cudaMemcpyHostToDevice, st));
+            CEL_CUDA(cudaMemcpyAsync(sdev, hs.data(), sizeof(StackDev) * ns, cudaMemcpyHostToDevice, st));
+            CEL_CUDA(cudaMemcpyAsync(sb.info, hinfo.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, st));
+            sb.cells = scells;
+            sb.stacks = sdev;
+            const size_t sm_stage = lu_stage_bytes(n);
+            CEL_CUDA(cudaFuncSetAttribute(rcwa_stack_smat, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_stage));
+            rcwa_stack_smat<<<ns, kRT, sm_stage, st>>>(sb);
+            Bucket eb;
+            std::memset(&eb, 0, sizeof(eb));
+            eb.Mx = Mx;
+            eb.My = My;
+            eb.N = N;
+            eb.n = n;
+            eb.ncell = ns;
+            eb.cells = scells;
+            eb.vec = sb.vec;
+            eb.info = sb.info;
+            eb.res = dres;
+            eb.s_n = s_n;
+            eb.s_nn = s_nn;
+            rcwa_epilogue<<<ns, kRT, 0, st>>>(eb);
+            count_launch(2);
+            CEL_CUDA(cudaGetLastError());
+            std::vector<celeris_rcwa_result> hres((size_t)ns * nexc);
+            CEL_CUDA(cudaMemcpyAsync(hres.data(), dres, sizeof(celeris_rcwa_result) * ns * nexc,
+                                     cudaMemcpyDeviceToHost, st));
+            CEL_CUDA(cudaMemcpyAsync(hinfo.data(), sb.info, sizeof(int) * ns, cudaMemcpyDeviceToHost, st));
+            CEL_CUDA(cudaStreamSynchronize(st));
+            for (int k = 0; k < ns; ++k) {
+                for (int e = 0; e < nexc; ++e) out[(size_t)ids[k] * nexc + e] = hres[(size_t)k * nexc + e];
+                if (info_out) info_out[ids[k]] = hinfo[k];
+            }
+            if (!info_out)
+                for (int k = 0; k < ns; ++k) {
+                    if (hinfo[k] > 0)
+                        return set_error(CELERIS_ERR_EIG_NOCONV, "eigensolve did not converge (a layer of stack %d)",
+                                         ids[k]);
+                    if (hinfo[k] < 0)
+                        return set_error(CELERIS_ERR_SINGULAR, "singular interface system (stack %d)", ids[k]);
+                }
+        }
+    }
+    return CELERIS_OK;
+}
+
+// Layers of one stack must share everything but the pattern, materials and thickness.
+int validate_stack(const celeris_rcwa_cell* l, int nl) {
+    if (nl < 1) return set_error(CELERIS_ERR_INVALID_ARG, "a stack needs at least one layer");
+    for (int i = 0; i < nl; ++i) CEL_TRY(validate(l[i]));
+    const celeris_rcwa_cell& f = l[0];
+    for (int i = 1; i < nl; ++i) {
+        const celeris_rcwa_cell& c = l[i];
+        if (c.Mx != f.Mx || c.My != f.My || c.period_x_um != f.period_x_um || c.period_y_um != f.period_y_um ||
+            c.wavelength_um != f.wavelength_um || c.theta_rad != f.theta_rad || c.phi_rad != f.phi_rad ||
+            c.n_inc[0] != f.n_inc[0] || c.n_inc[1] != f.n_inc[1] || c.n_sub[0] != f.n_sub[0] ||
+            c.n_sub[1] != f.n_sub[1])
+            return set_error(CELERIS_ERR_INVALID_ARG,
+                             "layer %d of a stack differs from layer 0 in orders, periods, wavelength, angles or "
+                             "half-spaces",
+                             i);
+    }
+    return CELERIS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1228,6 +1706,31 @@ int celeris_rcwa_tuning_report(char* buf, int len) {
     }
     std::snprintf(buf, (size_t)len, "%s", s.c_str());
     return CELERIS_OK;
+}
+
+int celeris_solve_rcwa_2d_stack(const celeris_rcwa_cell* layers, int nlayers, const double* Ex0, const double* Ey0,
+                                celeris_rcwa_result* out) {
+    if (!layers || !Ex0 || !Ey0 || !out) return set_error(CELERIS_ERR_INVALID_ARG, "NULL argument");
+    CEL_TRY(validate_stack(layers, nlayers));
+    const double exc[4] = {Ex0[0], Ex0[1], Ey0[0], Ey0[1]};
+    return run_stacks(layers, {{0, nlayers}}, exc, out, nullptr, 1);
+}
+
+int celeris_rcwa_stack_batch(const celeris_rcwa_cell* layers, const int* layer_start, int nstack,
+                             celeris_rcwa_result* out, int* info) {
+    if (nstack < 0) return set_error(CELERIS_ERR_INVALID_ARG, "nstack < 0");
+    if (nstack == 0) return CELERIS_OK;
+    if (!layers || !layer_start || !out) return set_error(CELERIS_ERR_INVALID_ARG, "NULL argument");
+    std::vector<std::pair<int, int>> stacks;
+    std::vector<double> exc(4 * (size_t)nstack, 0.0);
+    for (int s = 0; s < nstack; ++s) {
+        const int a = layer_start[s], nl = layer_start[s + 1] - layer_start[s];
+        if (a < 0 || nl < 1) return set_error(CELERIS_ERR_INVALID_ARG, "stack %d: bad layer range", s);
+        CEL_TRY(validate_stack(layers + a, nl));
+        stacks.push_back({a, nl});
+        exc[4 * (size_t)s] = 1.0;  // slot 0 = X polarization (Ex0 = 1), slot 1 = Y
+    }
+    return run_stacks(layers, stacks, exc.data(), out, info, 2);
 }
 
 int celeris_rcwa_batch(const celeris_rcwa_cell* cells, int ncell, celeris_rcwa_result* out, int* info) {

@@ -3,7 +3,8 @@
 // (materials, aperture assembly, library lookup, lens design, focal metrics),
 // written to the same specifications:
 //   materials        material.cpp:13-81, database.cpp:12-46
-//   solve_rcwa_2d    rcwa2d.cpp:209-222 argument checks, then celeris_solve_rcwa_2d
+//   solve_rcwa_2d    rcwa2d.cpp:209-222 argument checks, then celeris_solve_rcwa_2d (one
+//                    layer) or celeris_solve_rcwa_2d_stack (several layers)
 //   library sweep    metalens.cpp:122-163 (one batched GPU launch sequence)
 //   lookup / design  metalens.cpp:14-69, 112-120, 230-272
 //   height sweep     metalens.cpp:165-228
@@ -233,30 +234,41 @@ Rcwa2DResult solve_rcwa_2d(const Material& incident, const Rcwa2DStack& stack, c
                            int Mx, int My) {
     if (Mx < 0 || My < 0) throw std::invalid_argument("M must be >= 0");
     if (stack.layers.empty()) throw std::invalid_argument("solve_rcwa_2d: stack has no layers");
-    if (stack.layers.size() != 1)
-        throw std::invalid_argument("solve_rcwa_2d: this build solves one patterned layer per cell");
-    const celeris_rcwa_cell c = to_cell(incident, stack.layers[0], substrate, stack.period_x_um,
-                                        stack.period_y_um, wavelength_um, theta_rad, phi_rad, Mx, My, 0, false);
+    std::vector<celeris_rcwa_cell> cc;
+    cc.reserve(stack.layers.size());
+    for (const RectCell2D& L : stack.layers)
+        cc.push_back(to_cell(incident, L, substrate, stack.period_x_um, stack.period_y_um, wavelength_um, theta_rad,
+                             phi_rad, Mx, My, 0, false));
     const double ex[2] = {Ex0.real(), Ex0.imag()}, ey[2] = {Ey0.real(), Ey0.imag()};
     celeris_rcwa_result r{};
-    check(celeris_solve_rcwa_2d(&c, ex, ey, &r), "solve_rcwa_2d");
+    if (cc.size() == 1)
+        check(celeris_solve_rcwa_2d(&cc[0], ex, ey, &r), "solve_rcwa_2d");
+    else
+        check(celeris_solve_rcwa_2d_stack(cc.data(), static_cast<int>(cc.size()), ex, ey, &r), "solve_rcwa_2d");
     return from_result(r);
 }
 
 std::vector<std::array<Rcwa2DResult, 2>> solve_rcwa_2d_batch(const std::vector<CellSpec>& cells) {
     std::vector<celeris_rcwa_cell> cc;
-    cc.reserve(cells.size());
+    std::vector<int> start(1, 0);
+    bool multi = false;
     for (const CellSpec& s : cells) {
-        if (s.stack.layers.size() != 1)
-            throw std::invalid_argument("solve_rcwa_2d_batch: one patterned layer per cell");
-        cc.push_back(to_cell(s.incident, s.stack.layers[0], s.substrate, s.stack.period_x_um, s.stack.period_y_um,
-                             s.wavelength_um, 0.0, 0.0, s.M, s.M, s.grid, s.force_laurent));
+        if (s.stack.layers.empty()) throw std::invalid_argument("solve_rcwa_2d_batch: stack has no layers");
+        multi = multi || s.stack.layers.size() > 1;
+        for (const RectCell2D& L : s.stack.layers)
+            cc.push_back(to_cell(s.incident, L, s.substrate, s.stack.period_x_um, s.stack.period_y_um,
+                                 s.wavelength_um, 0.0, 0.0, s.M, s.M, s.grid, s.force_laurent));
+        start.push_back(static_cast<int>(cc.size()));
     }
-    std::vector<celeris_rcwa_result> r(2 * cc.size());
-    std::vector<int> info(cc.size());
-    check(celeris_rcwa_batch(cc.data(), static_cast<int>(cc.size()), r.data(), info.data()), "rcwa_batch");
-    std::vector<std::array<Rcwa2DResult, 2>> out(cc.size());
-    for (size_t i = 0; i < cc.size(); ++i) out[i] = {from_result(r[2 * i]), from_result(r[2 * i + 1])};
+    const int ns = static_cast<int>(cells.size());
+    std::vector<celeris_rcwa_result> r(2 * cells.size());
+    std::vector<int> info(cells.size());
+    if (multi)
+        check(celeris_rcwa_stack_batch(cc.data(), start.data(), ns, r.data(), info.data()), "rcwa_stack_batch");
+    else
+        check(celeris_rcwa_batch(cc.data(), ns, r.data(), info.data()), "rcwa_batch");
+    std::vector<std::array<Rcwa2DResult, 2>> out(cells.size());
+    for (size_t i = 0; i < cells.size(); ++i) out[i] = {from_result(r[2 * i]), from_result(r[2 * i + 1])};
     return out;
 }
 

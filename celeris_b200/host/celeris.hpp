@@ -79,13 +79,14 @@ struct Rcwa2DResult {
     cdouble tx0, ty0;
 };
 
-// One patterned layer between the incident and substrate half-spaces (the
-// metalens unit cell); stacks of more layers raise std::invalid_argument.
+// Patterned layers between the incident and substrate half-spaces; layers[0]
+// is next to the incident side (rcwa2d.cpp:361-364).
 Rcwa2DResult solve_rcwa_2d(const Material& incident, const Rcwa2DStack& stack, const Material& substrate,
                            double wavelength_um, double theta_rad, double phi_rad, cdouble Ex0, cdouble Ey0,
                            int Mx, int My);
 
-// New: both polarizations of many uneven cells in one batched launch sequence.
+// New: both polarizations of many uneven cells in one batched launch sequence
+// (multi-layer stacks go through the stack batch).
 struct CellSpec {
     Rcwa2DStack stack;
     Material incident;

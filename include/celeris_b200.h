@@ -215,6 +215,26 @@ int celeris_solve_rcwa_2d(const celeris_rcwa_cell* cell, const double* Ex0,
 int celeris_rcwa_batch(const celeris_rcwa_cell* cells, int ncell,
                        celeris_rcwa_result* out, int* info);
 
+/* Drop-in for celeris::solve_rcwa_2d on a multi-layer stack (rcwa2d.cpp:209-488;
+ * the S-matrix recursion of rcwa2d.cpp:376-401 over nlayers + 1 interfaces).
+ * layers[0] is next to the incident half-space, layers[nlayers-1] next to the
+ * substrate. Orders, periods, wavelength, angles and both half-space indices
+ * must agree across the layers (the reference's Rcwa2DStack holds them once);
+ * each layer carries its own pattern, materials and thickness. Synchronous,
+ * host buffers. */
+int celeris_solve_rcwa_2d_stack(const celeris_rcwa_cell* layers, int nlayers,
+                                const double* Ex0, const double* Ey0,
+                                celeris_rcwa_result* out);
+
+/* New: batched multi-layer stacks. Stack s is layers[layer_start[s] ..
+ * layer_start[s+1]) (layer_start holds nstack + 1 offsets). Like
+ * celeris_rcwa_batch, each stack is solved once for both excitations:
+ * out[2s] = X (Ex0=1), out[2s+1] = Y (Ey0=1). info (nstack ints, may be NULL)
+ * receives 0, the eigensolve failure code of a layer (> 0), or minus the
+ * singular pivot of an interface system (< 0) per stack. */
+int celeris_rcwa_stack_batch(const celeris_rcwa_cell* layers, const int* layer_start,
+                             int nstack, celeris_rcwa_result* out, int* info);
+
 /* New: the autotuner's table (one line per bucket shape Mx, My, raster: the
  * threads per CTA it chose for each RCWA stage), NUL-terminated into buf. The
  * batch runs all buckets as one CUDA graph (one stream per bucket), captured on

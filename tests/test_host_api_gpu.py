@@ -43,6 +43,24 @@ def test_solve_rcwa_2d_reference_signature_and_errors():
         cel.solve_rcwa_2d(air, cel.Rcwa2DStack(0.35, 0.35, []), fs, 0.532, 0.0, 0.0, 1.0, 0.0, 3, 3)
 
 
+def test_solve_rcwa_2d_multilayer_stack():
+    """Two patterned layers (a TiO2 pillar on a silica grating) through the
+    reference's signature, against the oracle's multi-layer recursion."""
+    tio2 = cel.Material.constant(2.45 + 0j, "TiO2")
+    sio2 = cel.Material.constant(1.46 + 0j, "SiO2")
+    air = cel.materials.air()
+    sub = cel.Material.constant(1.46 + 0j, "sub")
+    layers = [cel.RectCell2D(tio2, air, 0.5, 0.4, 0.45), cel.RectCell2D(sio2, air, 0.7, 0.7, 0.2)]
+    stack = cel.Rcwa2DStack(0.35, 0.35, layers)
+    r = cel.solve_rcwa_2d(air, stack, sub, 0.532, 0.0, 0.0, 1.0, 0.0, 3, 3)
+    want = RO.solve(1.0, [dict(eps_pillar=2.45 ** 2, eps_bg=1.0, fill_x=0.5, fill_y=0.4, thickness=0.45),
+                          dict(eps_pillar=1.46 ** 2, eps_bg=1.0, fill_x=0.7, fill_y=0.7, thickness=0.2)],
+                    1.46, 0.35, 0.35, 0.532, 0.0, 0.0, 1.0, 0.0, 3, 3)
+    assert abs(r.tx0 - want["tx0"]) <= 1e-10 * abs(want["tx0"])
+    assert abs(r.R - want["R"]) <= 1e-10 and abs(r.T - want["T"]) <= 1e-10
+    assert abs(r.sum_de - 1.0) <= 1e-10
+
+
 def test_selftest9_metalens_pipeline():
     tio2 = cel.Material.constant(2.40 + 0j, "TiO2~")
     air = cel.materials.air()

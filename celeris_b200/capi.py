@@ -53,6 +53,7 @@ EXPORTED = [
     "celeris_probe_peaks", "celeris_set_kernel_timing", "celeris_last_kernel_ms",
     "celeris_rs_field_noalloc", "celeris_probe_sincos", "celeris_rcwa_tuning_report",
     "celeris_probe_dmma", "celeris_solve_rcwa_2d_stack", "celeris_rcwa_stack_batch",
+    "celeris_solve_rcwa_2d_orders",
 ]
 
 
@@ -82,6 +83,14 @@ class RcwaResult(ctypes.Structure):
         ("R", ctypes.c_double), ("T", ctypes.c_double), ("sum_de", ctypes.c_double),
         ("de_t0", ctypes.c_double), ("de_r0", ctypes.c_double),
         ("tx0", ctypes.c_double * 2), ("ty0", ctypes.c_double * 2),
+    ]
+
+
+class RcwaOrder(ctypes.Structure):
+    """celeris_rcwa_order (include/celeris_b200.h)."""
+    _fields_ = [
+        ("p", ctypes.c_int), ("q", ctypes.c_int), ("de_t", ctypes.c_double), ("de_r", ctypes.c_double),
+        ("prop_t", ctypes.c_int), ("prop_r", ctypes.c_int),
     ]
 
 
@@ -126,6 +135,8 @@ def load(path: str = LIB_PATH):
         "celeris_rcwa_tuning_report": (_I, [ctypes.c_char_p, _I]),
         "celeris_solve_rcwa_2d_stack": (_I, [ctypes.POINTER(RcwaCell), _I, _P, _P, ctypes.POINTER(RcwaResult)]),
         "celeris_rcwa_stack_batch": (_I, [ctypes.POINTER(RcwaCell), _PI, _I, ctypes.POINTER(RcwaResult), _PI]),
+        "celeris_solve_rcwa_2d_orders": (_I, [ctypes.POINTER(RcwaCell), _I, _P, _P, ctypes.POINTER(RcwaResult),
+                                              ctypes.POINTER(RcwaOrder), _I]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -291,3 +302,17 @@ def rcwa_stack_batch(stacks) -> tuple[list[dict], np.ndarray]:
     check(load().celeris_rcwa_stack_batch(arr, start.ctypes.data_as(_PI), len(stacks), out,
                                           info.ctypes.data_as(_PI)))
     return [result_dict(out[i]) for i in range(2 * len(stacks))], info[:len(stacks)]
+
+
+def solve_rcwa_2d_orders(layers, Ex0=1.0 + 0j, Ey0=0.0 + 0j) -> tuple[dict, list[dict]]:
+    """One stack (one layer or several) with the per-order efficiencies."""
+    n = len(layers)
+    arr = (RcwaCell * n)(*layers)
+    N = (2 * layers[0].Mx + 1) * (2 * layers[0].My + 1)
+    ex = np.array([complex(Ex0).real, complex(Ex0).imag])
+    ey = np.array([complex(Ey0).real, complex(Ey0).imag])
+    out = RcwaResult()
+    orders = (RcwaOrder * N)()
+    check(load().celeris_solve_rcwa_2d_orders(arr, n, _dp(ex), _dp(ey), ctypes.byref(out), orders, N))
+    return result_dict(out), [dict(p=o.p, q=o.q, de_t=o.de_t, de_r=o.de_r, prop_t=bool(o.prop_t),
+                                   prop_r=bool(o.prop_r)) for o in orders]

@@ -24,6 +24,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <complex>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -75,6 +76,7 @@ struct Bucket {
     const cplx* phx;  // [(4Mx+1) x ng] centred DFT phase table (x)
     const cplx* phy;  // [(4My+1) x ng]
     long long* dbg;   // optional per-cell counters, kDbgSlots each (CELERIS_RCWA_STAGE_CLOCKS=1), else NULL
+    double* ord;      // optional per-order efficiencies: per cell and excitation [N][2] = (de_t, de_r), else NULL
 };
 
 __device__ __forceinline__ cplx* at(cplx* base, size_t stride, int c) { return base + stride * c; }
@@ -853,6 +855,11 @@ __global__ void __launch_bounds__(kRT) rcwa_epilogue(Bucket b) {
             const double fw = cmulc(Sa0, aNs).x + cmulc(Sa1, aNp).x;
             sR += -bw * norm;
             sT += fw * norm;
+            if (b.ord) {  // rcwa2d.cpp:479-480
+                double* o = b.ord + 2 * ((size_t)(cell * c.nexc + ex) * N + i);
+                o[0] = fw * norm;
+                o[1] = -bw * norm;
+            }
             if (i == i0) {
                 sums[0] = -bw * norm;   // de_r0
                 sums[1] = fw * norm;    // de_t0
@@ -1458,8 +1465,9 @@ struct DevBuf {
 
 // stacks[s] = (first layer index, layer count) into `layers`; exc holds 4 doubles
 // (Ex0 re, im, Ey0 re, im) per stack; results nexc per stack.
+// ord_out (may be NULL): per stack and excitation N x (de_t, de_r).
 int run_stacks(const celeris_rcwa_cell* layers, const std::vector<std::pair<int, int>>& stacks,
-               const double* exc, celeris_rcwa_result* out, int* info_out, int nexc) {
+               const double* exc, celeris_rcwa_result* out, int* info_out, int nexc, double* ord_out = nullptr) {
     CEL_TRY(celeris_rt::require_device());
     int dev = 0, smem_optin = 0;
     cudaGetDevice(&dev);
@@ -1636,6 +1644,7 @@ int run_stacks(const celeris_rcwa_cell* layers, const std::vector<std::pair<int,
             eb.res = dres;
             eb.s_n = s_n;
             eb.s_nn = s_nn;
+            if (ord_out) CEL_TRY(mem.get(&eb.ord, (size_t)ns * nexc * N * 2));
             rcwa_epilogue<<<ns, kRT, 0, st>>>(eb);
             count_launch(2);
             CEL_CUDA(cudaGetLastError());
@@ -1643,7 +1652,17 @@ int run_stacks(const celeris_rcwa_cell* layers, const std::vector<std::pair<int,
             CEL_CUDA(cudaMemcpyAsync(hres.data(), dres, sizeof(celeris_rcwa_result) * ns * nexc,
                                      cudaMemcpyDeviceToHost, st));
             CEL_CUDA(cudaMemcpyAsync(hinfo.data(), sb.info, sizeof(int) * ns, cudaMemcpyDeviceToHost, st));
+            std::vector<double> hord;
+            if (ord_out) {
+                hord.resize((size_t)ns * nexc * N * 2);
+                CEL_CUDA(cudaMemcpyAsync(hord.data(), eb.ord, sizeof(double) * hord.size(), cudaMemcpyDeviceToHost,
+                                         st));
+            }
             CEL_CUDA(cudaStreamSynchronize(st));
+            if (ord_out)
+                for (int k = 0; k < ns; ++k)
+                    std::memcpy(ord_out + (size_t)ids[k] * nexc * N * 2, hord.data() + (size_t)k * nexc * N * 2,
+                                sizeof(double) * nexc * N * 2);
             for (int k = 0; k < ns; ++k) {
                 for (int e = 0; e < nexc; ++e) out[(size_t)ids[k] * nexc + e] = hres[(size_t)k * nexc + e];
                 if (info_out) info_out[ids[k]] = hinfo[k];
@@ -1714,6 +1733,41 @@ int celeris_solve_rcwa_2d_stack(const celeris_rcwa_cell* layers, int nlayers, co
     CEL_TRY(validate_stack(layers, nlayers));
     const double exc[4] = {Ex0[0], Ex0[1], Ey0[0], Ey0[1]};
     return run_stacks(layers, {{0, nlayers}}, exc, out, nullptr, 1);
+}
+
+int celeris_solve_rcwa_2d_orders(const celeris_rcwa_cell* layers, int nlayers, const double* Ex0, const double* Ey0,
+                                 celeris_rcwa_result* out, celeris_rcwa_order* orders, int max_orders) {
+    if (!layers || !Ex0 || !Ey0 || !out || !orders) return set_error(CELERIS_ERR_INVALID_ARG, "NULL argument");
+    CEL_TRY(validate_stack(layers, nlayers));
+    const celeris_rcwa_cell& f = layers[0];
+    const int N = (2 * f.Mx + 1) * (2 * f.My + 1);
+    if (max_orders < N) return set_error(CELERIS_ERR_INVALID_ARG, "orders holds %d records, %d needed", max_orders, N);
+    const double exc[4] = {Ex0[0], Ex0[1], Ey0[0], Ey0[1]};
+    std::vector<double> ord((size_t)N * 2);
+    CEL_TRY(run_stacks(layers, {{0, nlayers}}, exc, out, nullptr, 1, ord.data()));
+    // order labels and the propagation test of rcwa2d.cpp:469-484 (same arithmetic)
+    typedef std::complex<double> cd;
+    const double k0 = 2.0 * PI / f.wavelength_um;
+    const cd n_inc(f.n_inc[0], f.n_inc[1]);
+    const cd kx0 = n_inc * std::sin(f.theta_rad) * std::cos(f.phi_rad) * k0;
+    const cd ky0 = n_inc * std::sin(f.theta_rad) * std::sin(f.phi_rad) * k0;
+    const double k0sub = (f.n_sub[0] * k0) * (f.n_sub[0] * k0);
+    const double k0inc = (f.n_inc[0] * k0) * (f.n_inc[0] * k0);
+    for (int p = -f.Mx; p <= f.Mx; ++p)
+        for (int q = -f.My; q <= f.My; ++q) {
+            const int i = (p + f.Mx) * (2 * f.My + 1) + (q + f.My);
+            const cd kx = kx0 - 2.0 * PI * (double)p / f.period_x_um;
+            const cd ky = ky0 - 2.0 * PI * (double)q / f.period_y_um;
+            const double kt2 = (kx * kx + ky * ky).real();
+            celeris_rcwa_order& o = orders[i];
+            o.p = p;
+            o.q = q;
+            o.de_t = ord[2 * (size_t)i];
+            o.de_r = ord[2 * (size_t)i + 1];
+            o.prop_t = k0sub - kt2 > 0.0;
+            o.prop_r = k0inc - kt2 > 0.0;
+        }
+    return CELERIS_OK;
 }
 
 int celeris_rcwa_stack_batch(const celeris_rcwa_cell* layers, const int* layer_start, int nstack,

@@ -97,6 +97,37 @@ PYBIND11_MODULE(_celeris, m) {
              cdouble ex, cdouble ey, int Mx, int My) { return solve_rcwa_2d(inc, st, sub, wl, th, ph, ex, ey, Mx, My); },
           py::arg("incident"), py::arg("stack"), py::arg("substrate"), py::arg("wavelength_um"),
           py::arg("theta_rad"), py::arg("phi_rad"), py::arg("Ex0"), py::arg("Ey0"), py::arg("Mx"), py::arg("My"));
+    py::class_<OrderEfficiency>(m, "OrderEfficiency")
+        .def_readonly("p", &OrderEfficiency::p)
+        .def_readonly("q", &OrderEfficiency::q)
+        .def_readonly("de_t", &OrderEfficiency::de_t)
+        .def_readonly("de_r", &OrderEfficiency::de_r)
+        .def_readonly("prop_t", &OrderEfficiency::prop_t)
+        .def_readonly("prop_r", &OrderEfficiency::prop_r);
+    m.def("solve_rcwa_2d_orders",
+          [](const Material& inc, const Rcwa2DStack& st, const Material& sub, double wl, double th, double ph,
+             cdouble ex, cdouble ey, int Mx, int My) {
+              std::vector<OrderEfficiency> o;
+              Rcwa2DResult r = solve_rcwa_2d(inc, st, sub, wl, th, ph, ex, ey, Mx, My, &o);
+              return py::make_tuple(r, o);
+          },
+          py::arg("incident"), py::arg("stack"), py::arg("substrate"), py::arg("wavelength_um"),
+          py::arg("theta_rad"), py::arg("phi_rad"), py::arg("Ex0"), py::arg("Ey0"), py::arg("Mx"), py::arg("My"));
+    py::class_<EfficiencyBudget>(m, "EfficiencyBudget")
+        .def_readonly("reflection", &EfficiencyBudget::reflection)
+        .def_readonly("transmission", &EfficiencyBudget::transmission)
+        .def_readonly("absorption", &EfficiencyBudget::absorption)
+        .def_readonly("t_zero", &EfficiencyBudget::t_zero)
+        .def_readonly("r_zero", &EfficiencyBudget::r_zero)
+        .def_readonly("t_stray", &EfficiencyBudget::t_stray)
+        .def_readonly("r_stray", &EfficiencyBudget::r_stray)
+        .def_readonly("n_prop_t", &EfficiencyBudget::n_prop_t)
+        .def_readonly("n_prop_r", &EfficiencyBudget::n_prop_r)
+        .def_readonly("orders", &EfficiencyBudget::orders);
+    m.def("analyze_efficiency", &analyze_efficiency, py::arg("incident"), py::arg("pillar"), py::arg("background"),
+          py::arg("substrate"), py::arg("period_x_um"), py::arg("period_y_um"), py::arg("fill_x"), py::arg("fill_y"),
+          py::arg("thickness_um"), py::arg("wavelength_um"), py::arg("Ex0"), py::arg("Ey0"), py::arg("M"),
+          py::arg("shape") = MetaShape::Rectangle, py::arg("shape_param") = 0.5);
 
     py::class_<UnitCellLibrary>(m, "UnitCellLibrary")
         .def(py::init<>())

@@ -231,7 +231,7 @@ const Material& silicon_nitride() {  // Luke et al. 2015
 // ---- RCWA ------------------------------------------------------------------------------
 Rcwa2DResult solve_rcwa_2d(const Material& incident, const Rcwa2DStack& stack, const Material& substrate,
                            double wavelength_um, double theta_rad, double phi_rad, cdouble Ex0, cdouble Ey0,
-                           int Mx, int My) {
+                           int Mx, int My, std::vector<OrderEfficiency>* orders_out) {
     if (Mx < 0 || My < 0) throw std::invalid_argument("M must be >= 0");
     if (stack.layers.empty()) throw std::invalid_argument("solve_rcwa_2d: stack has no layers");
     std::vector<celeris_rcwa_cell> cc;
@@ -241,11 +241,48 @@ Rcwa2DResult solve_rcwa_2d(const Material& incident, const Rcwa2DStack& stack, c
                              phi_rad, Mx, My, 0, false));
     const double ex[2] = {Ex0.real(), Ex0.imag()}, ey[2] = {Ey0.real(), Ey0.imag()};
     celeris_rcwa_result r{};
-    if (cc.size() == 1)
+    if (orders_out) {
+        const int N = (2 * Mx + 1) * (2 * My + 1);
+        std::vector<celeris_rcwa_order> o(N);
+        check(celeris_solve_rcwa_2d_orders(cc.data(), static_cast<int>(cc.size()), ex, ey, &r, o.data(), N),
+              "solve_rcwa_2d");
+        orders_out->clear();
+        orders_out->reserve(N);
+        for (const celeris_rcwa_order& x : o)
+            orders_out->push_back(OrderEfficiency{x.p, x.q, x.de_t, x.de_r, x.prop_t != 0, x.prop_r != 0});
+    } else if (cc.size() == 1)
         check(celeris_solve_rcwa_2d(&cc[0], ex, ey, &r), "solve_rcwa_2d");
     else
         check(celeris_solve_rcwa_2d_stack(cc.data(), static_cast<int>(cc.size()), ex, ey, &r), "solve_rcwa_2d");
     return from_result(r);
+}
+
+// analysis/efficiency.cpp:7-46: one solve with orders, then the budget.
+EfficiencyBudget analyze_efficiency(const Material& incident, const Material& pillar, const Material& background,
+                                    const Material& substrate, double period_x_um, double period_y_um, double fill_x,
+                                    double fill_y, double thickness_um, double wavelength_um, cdouble Ex0,
+                                    cdouble Ey0, int M, MetaShape shape, double shape_param) {
+    RectCell2D cell{pillar, background, fill_x, fill_y, thickness_um, shape, shape_param};
+    Rcwa2DStack stack{period_x_um, period_y_um, {cell}};
+    std::vector<OrderEfficiency> orders;
+    const Rcwa2DResult r =
+        solve_rcwa_2d(incident, stack, substrate, wavelength_um, 0.0, 0.0, Ex0, Ey0, M, M, &orders);
+    EfficiencyBudget b{};
+    b.reflection = r.R;
+    b.transmission = r.T;
+    b.absorption = std::max(0.0, 1.0 - r.R - r.T);
+    b.t_zero = r.de_t0;
+    b.r_zero = r.de_r0;
+    b.t_stray = std::max(0.0, r.T - r.de_t0);
+    b.r_stray = std::max(0.0, r.R - r.de_r0);
+    for (const OrderEfficiency& o : orders) {
+        b.n_prop_t += o.prop_t ? 1 : 0;
+        b.n_prop_r += o.prop_r ? 1 : 0;
+    }
+    std::sort(orders.begin(), orders.end(),
+              [](const OrderEfficiency& a, const OrderEfficiency& c) { return a.de_t > c.de_t; });
+    b.orders = std::move(orders);
+    return b;
 }
 
 std::vector<std::array<Rcwa2DResult, 2>> solve_rcwa_2d_batch(const std::vector<CellSpec>& cells) {

@@ -79,11 +79,33 @@ struct Rcwa2DResult {
     cdouble tx0, ty0;
 };
 
+struct OrderEfficiency {
+    int p, q;
+    double de_t;
+    double de_r;
+    bool prop_t;
+    bool prop_r;
+};
+
 // Patterned layers between the incident and substrate half-spaces; layers[0]
-// is next to the incident side (rcwa2d.cpp:361-364).
+// is next to the incident side (rcwa2d.cpp:361-364). orders_out (optional)
+// receives every order's efficiencies (rcwa2d.cpp:464-485).
 Rcwa2DResult solve_rcwa_2d(const Material& incident, const Rcwa2DStack& stack, const Material& substrate,
                            double wavelength_um, double theta_rad, double phi_rad, cdouble Ex0, cdouble Ey0,
-                           int Mx, int My);
+                           int Mx, int My, std::vector<OrderEfficiency>* orders_out = nullptr);
+
+// Energy budget of one meta-atom (analysis/efficiency.hpp:18-44).
+struct EfficiencyBudget {
+    double reflection, transmission, absorption;
+    double t_zero, r_zero, t_stray, r_stray;
+    int n_prop_t, n_prop_r;
+    std::vector<OrderEfficiency> orders;  // sorted by transmitted power, descending
+};
+EfficiencyBudget analyze_efficiency(const Material& incident, const Material& pillar, const Material& background,
+                                    const Material& substrate, double period_x_um, double period_y_um, double fill_x,
+                                    double fill_y, double thickness_um, double wavelength_um, cdouble Ex0,
+                                    cdouble Ey0, int M, MetaShape shape = MetaShape::Rectangle,
+                                    double shape_param = 0.5);
 
 // New: both polarizations of many uneven cells in one batched launch sequence
 // (multi-layer stacks go through the stack batch).

@@ -226,6 +226,22 @@ int celeris_solve_rcwa_2d_stack(const celeris_rcwa_cell* layers, int nlayers,
                                 const double* Ex0, const double* Ey0,
                                 celeris_rcwa_result* out);
 
+/* Per-order efficiency (OrderEfficiency, rcwa2d.hpp:101-107). */
+typedef struct celeris_rcwa_order {
+    int p, q;          /* diffraction order */
+    double de_t, de_r; /* transmitted / reflected efficiency of the order */
+    int prop_t, prop_r; /* 1 if the order propagates in the substrate / incident medium */
+} celeris_rcwa_order;
+
+/* Drop-in for celeris::solve_rcwa_2d with its orders_out argument
+ * (rcwa2d.cpp:464-485): as celeris_solve_rcwa_2d_stack (one layer or several),
+ * and orders[i] for every order i = (p + Mx)(2 My + 1) + (q + My), in the
+ * reference's loop order. orders holds max_orders >= (2Mx+1)(2My+1) records. */
+int celeris_solve_rcwa_2d_orders(const celeris_rcwa_cell* layers, int nlayers,
+                                 const double* Ex0, const double* Ey0,
+                                 celeris_rcwa_result* out, celeris_rcwa_order* orders,
+                                 int max_orders);
+
 /* New: batched multi-layer stacks. Stack s is layers[layer_start[s] ..
  * layer_start[s+1]) (layer_start holds nstack + 1 offsets). Like
  * celeris_rcwa_batch, each stack is solved once for both excitations:

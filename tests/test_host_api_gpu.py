@@ -61,6 +61,25 @@ def test_solve_rcwa_2d_multilayer_stack():
     assert abs(r.sum_de - 1.0) <= 1e-10
 
 
+def test_analyze_efficiency_budget():
+    """analyze_efficiency (analysis/efficiency.cpp:7-46) on a lossy, diffracting
+    meta-atom: the budget's sums and counts against the oracle's orders."""
+    pil = cel.Material.constant(2.0 + 0.05j, "lossy")
+    air = cel.materials.air()
+    sub = cel.Material.constant(1.46 + 0j, "sub")
+    b = cel.analyze_efficiency(air, pil, air, sub, 0.8, 0.8, 0.5, 0.5, 0.6, 0.633, 1.0, 0.0, 3)
+    want = RO.solve(1.0, [dict(eps_pillar=(2.0 + 0.05j) ** 2, eps_bg=1.0, fill_x=0.5, fill_y=0.5, thickness=0.6)],
+                    1.46, 0.8, 0.8, 0.633, 0.0, 0.0, 1.0, 0.0, 3, 3, orders_out=True)
+    assert abs(b.reflection - want["R"]) <= 1e-10 and abs(b.transmission - want["T"]) <= 1e-10
+    assert abs(b.absorption - max(0.0, 1 - want["R"] - want["T"])) <= 1e-10 and b.absorption > 1e-3
+    assert abs(b.t_stray - max(0.0, want["T"] - want["de_t0"])) <= 1e-10
+    assert b.n_prop_t == sum(o["prop_t"] for o in want["orders"])
+    assert b.n_prop_r == sum(o["prop_r"] for o in want["orders"])
+    de_t = [o.de_t for o in b.orders]
+    assert de_t == sorted(de_t, reverse=True)
+    assert abs(de_t[0] - max(o["de_t"] for o in want["orders"])) <= 1e-10
+
+
 def test_selftest9_metalens_pipeline():
     tio2 = cel.Material.constant(2.40 + 0j, "TiO2~")
     air = cel.materials.air()

@@ -132,3 +132,35 @@ def test_stack_M5_blocked():
     assert info[0] == 0
     check(res[0], ref(stack, 1.0, 0.0))
     check(res[1], ref(stack, 0.0, 1.0))
+
+
+@pytest.mark.parametrize("name", ["two_rect_M3", "oblique_two_M32"])
+def test_orders_out_matches_oracle(name):
+    """Per-order efficiencies (solve_rcwa_2d's orders_out, rcwa2d.cpp:464-485):
+    labels and propagation flags exact, efficiencies within 1e-10."""
+    stack = STACKS[name]
+    c = stack[0]
+    got, orders = capi.solve_rcwa_2d_orders(cells(stack), 1.0, 0.0)
+    px = c.get("period_x_um", c.get("period_um"))
+    py = c.get("period_y_um", c.get("period_um"))
+    want = RO.solve(c["n_inc"], [oracle_layer(x) for x in stack], c["n_sub"], px, py, c["wavelength_um"],
+                    c.get("theta_rad", 0.0), c.get("phi_rad", 0.0), 1.0, 0.0, c["Mx"], c.get("My", c["Mx"]),
+                    orders_out=True)
+    check(got, want, lossless=False)
+    assert len(orders) == len(want["orders"])
+    for g, w in zip(orders, want["orders"]):
+        assert (g["p"], g["q"], g["prop_t"], g["prop_r"]) == (w["p"], w["q"], w["prop_t"], w["prop_r"])
+        assert abs(g["de_t"] - w["de_t"]) <= TOL and abs(g["de_r"] - w["de_r"]) <= TOL
+    assert abs(sum(o["de_t"] for o in orders) - got["T"]) <= TOL
+
+
+def test_orders_one_layer_diffracting():
+    """A period above the wavelength in the substrate (p = 0.9 um at 0.633 um):
+    several orders propagate and carry power."""
+    c = layer(period_um=0.9, fill_x=0.4, thickness_um=0.5)
+    got, orders = capi.solve_rcwa_2d_orders(cells([c]), 0.0, 1.0)
+    want = RO.solve(1.0, [oracle_layer(c)], 1.46, 0.9, 0.9, 0.633, 0.0, 0.0, 0.0, 1.0, 3, 3, orders_out=True)
+    check(got, want)
+    assert sum(o["prop_t"] for o in orders) > 1
+    for g, w in zip(orders, want["orders"]):
+        assert g["prop_t"] == w["prop_t"] and abs(g["de_t"] - w["de_t"]) <= TOL

@@ -299,6 +299,166 @@ PYBIND11_MODULE(_celeris, m) {
           py::arg("wavelength_um"), py::arg("diameter_um"), py::arg("max_angle_deg"), py::arg("n_half"),
           py::arg("psf_n"));
 
+    // ---- library builders on the batched RCWA, designs and on-axis checks
+    m.def("build_unit_cell_library_stack", &build_unit_cell_library_stack, py::arg("stack"), py::arg("active_layer"),
+          py::arg("incident"), py::arg("substrate"), py::arg("wavelength_um"), py::arg("fill_min"),
+          py::arg("fill_max"), py::arg("n_samples"), py::arg("M"));
+    py::class_<MetaAtomSpec>(m, "MetaAtomSpec")
+        .def(py::init([](MetaShape shape, double fx, double fy, double h, double sp) {
+                 return MetaAtomSpec{shape, fx, fy, h, sp};
+             }),
+             py::arg("shape") = MetaShape::Rectangle, py::arg("fill_x") = 0.5, py::arg("fill_y") = 0.5,
+             py::arg("thickness_um") = 0.6, py::arg("shape_param") = 0.5)
+        .def_readwrite("shape", &MetaAtomSpec::shape)
+        .def_readwrite("fill_x", &MetaAtomSpec::fill_x)
+        .def_readwrite("fill_y", &MetaAtomSpec::fill_y)
+        .def_readwrite("thickness_um", &MetaAtomSpec::thickness_um)
+        .def_readwrite("shape_param", &MetaAtomSpec::shape_param);
+    py::class_<DispersiveAtom>(m, "DispersiveAtom")
+        .def(py::init<>())
+        .def_readwrite("fill", &DispersiveAtom::fill)
+        .def_readwrite("thickness_um", &DispersiveAtom::thickness_um)
+        .def_readwrite("shape", &DispersiveAtom::shape)
+        .def_readwrite("fill_x", &DispersiveAtom::fill_x)
+        .def_readwrite("fill_y", &DispersiveAtom::fill_y)
+        .def_readwrite("shape_param", &DispersiveAtom::shape_param)
+        .def_readwrite("phase0_rad", &DispersiveAtom::phase0_rad)
+        .def_readwrite("group_delay_fs", &DispersiveAtom::group_delay_fs)
+        .def_readwrite("mean_amplitude", &DispersiveAtom::mean_amplitude)
+        .def_readwrite("phase_rad", &DispersiveAtom::phase_rad)
+        .def_readwrite("amplitude", &DispersiveAtom::amplitude);
+    py::class_<DispersiveLibrary>(m, "DispersiveLibrary")
+        .def(py::init<>())
+        .def_readwrite("wavelengths_um", &DispersiveLibrary::wavelengths_um)
+        .def_readwrite("center_wavelength_um", &DispersiveLibrary::center_wavelength_um)
+        .def_readwrite("center_index", &DispersiveLibrary::center_index)
+        .def_readwrite("period_um", &DispersiveLibrary::period_um)
+        .def_readwrite("n_fill", &DispersiveLibrary::n_fill)
+        .def_readwrite("n_height", &DispersiveLibrary::n_height)
+        .def_readwrite("atoms", &DispersiveLibrary::atoms)
+        .def_readwrite("gd_min_fs", &DispersiveLibrary::gd_min_fs)
+        .def_readwrite("gd_max_fs", &DispersiveLibrary::gd_max_fs);
+    m.def("build_dispersive_library_from_specs", &build_dispersive_library_from_specs, py::arg("pillar"),
+          py::arg("background"), py::arg("incident"), py::arg("substrate"), py::arg("period_um"),
+          py::arg("band_wavelengths_um"), py::arg("center_wavelength_um"), py::arg("specs"), py::arg("M"));
+    m.def("build_dispersive_library", &build_dispersive_library, py::arg("pillar"), py::arg("background"),
+          py::arg("incident"), py::arg("substrate"), py::arg("period_um"), py::arg("band_wavelengths_um"),
+          py::arg("center_wavelength_um"), py::arg("fill_min"), py::arg("fill_max"), py::arg("n_fills"),
+          py::arg("thick_lo"), py::arg("thick_hi"), py::arg("n_heights"), py::arg("M"));
+    m.def("build_single_etch_library", &build_single_etch_library, py::arg("pillar"), py::arg("background"),
+          py::arg("incident"), py::arg("substrate"), py::arg("period_um"), py::arg("band_wavelengths_um"),
+          py::arg("center_wavelength_um"), py::arg("fill_min"), py::arg("fill_max"), py::arg("n_fills"),
+          py::arg("thickness_um"), py::arg("M"));
+    py::class_<AchromaticDesign>(m, "AchromaticDesign")
+        .def(py::init<>())
+        .def_readwrite("n_cells", &AchromaticDesign::n_cells)
+        .def_readwrite("period_um", &AchromaticDesign::period_um)
+        .def_readwrite("atom_index", &AchromaticDesign::atom_index)
+        .def_readwrite("fill_map", &AchromaticDesign::fill_map)
+        .def_readwrite("thickness_map", &AchromaticDesign::thickness_map)
+        .def_readwrite("center_wavelength_um", &AchromaticDesign::center_wavelength_um)
+        .def_readwrite("focal_length_um", &AchromaticDesign::focal_length_um)
+        .def_readwrite("diameter_um", &AchromaticDesign::diameter_um)
+        .def_readwrite("rms_phase_error_deg", &AchromaticDesign::rms_phase_error_deg)
+        .def_readwrite("rms_group_delay_error_fs", &AchromaticDesign::rms_group_delay_error_fs)
+        .def_readwrite("mean_amplitude", &AchromaticDesign::mean_amplitude)
+        .def_readwrite("required_gd_span_fs", &AchromaticDesign::required_gd_span_fs)
+        .def_readwrite("available_gd_span_fs", &AchromaticDesign::available_gd_span_fs)
+        .def_readwrite("gd_coverage", &AchromaticDesign::gd_coverage)
+        .def_readwrite("single_height", &AchromaticDesign::single_height)
+        .def_readwrite("min_height_um", &AchromaticDesign::min_height_um)
+        .def_readwrite("max_height_um", &AchromaticDesign::max_height_um);
+    m.def("design_achromatic_metalens", &design_achromatic_metalens, py::arg("lib"), py::arg("focal_length_um"),
+          py::arg("diameter_um"), py::arg("gd_weight") = 1.0, py::arg("amplitude_weight") = 0.25);
+    py::class_<AchromaticFocalPoint>(m, "AchromaticFocalPoint")
+        .def_readonly("wavelength_um", &AchromaticFocalPoint::wavelength_um)
+        .def_readonly("focal_length_um", &AchromaticFocalPoint::focal_length_um)
+        .def_readonly("rel_peak", &AchromaticFocalPoint::rel_peak);
+    m.def("verify_achromatic_focus", &verify_achromatic_focus, py::arg("lib"), py::arg("design"));
+    m.def("to_metalens_design", &to_metalens_design, py::arg("design"));
+    py::class_<DispersivePbAtom>(m, "DispersivePbAtom")
+        .def(py::init<>())
+        .def_readwrite("fill_x", &DispersivePbAtom::fill_x)
+        .def_readwrite("fill_y", &DispersivePbAtom::fill_y)
+        .def_readwrite("thickness_um", &DispersivePbAtom::thickness_um)
+        .def_readwrite("phase0_rad", &DispersivePbAtom::phase0_rad)
+        .def_readwrite("group_delay_fs", &DispersivePbAtom::group_delay_fs)
+        .def_readwrite("mean_amplitude", &DispersivePbAtom::mean_amplitude)
+        .def_readwrite("mean_conversion", &DispersivePbAtom::mean_conversion)
+        .def_readwrite("retardance_center_deg", &DispersivePbAtom::retardance_center_deg)
+        .def_readwrite("cross", &DispersivePbAtom::cross);
+    py::class_<DispersivePbLibrary>(m, "DispersivePbLibrary")
+        .def(py::init<>())
+        .def_readwrite("wavelengths_um", &DispersivePbLibrary::wavelengths_um)
+        .def_readwrite("center_wavelength_um", &DispersivePbLibrary::center_wavelength_um)
+        .def_readwrite("center_index", &DispersivePbLibrary::center_index)
+        .def_readwrite("period_um", &DispersivePbLibrary::period_um)
+        .def_readwrite("thickness_um", &DispersivePbLibrary::thickness_um)
+        .def_readwrite("n_fill", &DispersivePbLibrary::n_fill)
+        .def_readwrite("atoms", &DispersivePbLibrary::atoms)
+        .def_readwrite("gd_min_fs", &DispersivePbLibrary::gd_min_fs)
+        .def_readwrite("gd_max_fs", &DispersivePbLibrary::gd_max_fs);
+    m.def("build_dispersive_pb_library", &build_dispersive_pb_library, py::arg("pillar"), py::arg("background"),
+          py::arg("incident"), py::arg("substrate"), py::arg("period_um"), py::arg("band_wavelengths_um"),
+          py::arg("center_wavelength_um"), py::arg("fill_min"), py::arg("fill_max"), py::arg("n_fills"),
+          py::arg("thickness_um"), py::arg("M"), py::arg("min_amplitude") = 0.30);
+    py::class_<PbAchromaticDesign>(m, "PbAchromaticDesign")
+        .def(py::init<>())
+        .def_readwrite("n_cells", &PbAchromaticDesign::n_cells)
+        .def_readwrite("period_um", &PbAchromaticDesign::period_um)
+        .def_readwrite("thickness_um", &PbAchromaticDesign::thickness_um)
+        .def_readwrite("handedness", &PbAchromaticDesign::handedness)
+        .def_readwrite("atom_index", &PbAchromaticDesign::atom_index)
+        .def_readwrite("rotation_rad", &PbAchromaticDesign::rotation_rad)
+        .def_readwrite("fill_x_map", &PbAchromaticDesign::fill_x_map)
+        .def_readwrite("fill_y_map", &PbAchromaticDesign::fill_y_map)
+        .def_readwrite("center_wavelength_um", &PbAchromaticDesign::center_wavelength_um)
+        .def_readwrite("focal_length_um", &PbAchromaticDesign::focal_length_um)
+        .def_readwrite("diameter_um", &PbAchromaticDesign::diameter_um)
+        .def_readwrite("rms_phase_error_deg", &PbAchromaticDesign::rms_phase_error_deg)
+        .def_readwrite("rms_group_delay_error_fs", &PbAchromaticDesign::rms_group_delay_error_fs)
+        .def_readwrite("mean_amplitude", &PbAchromaticDesign::mean_amplitude)
+        .def_readwrite("mean_conversion", &PbAchromaticDesign::mean_conversion)
+        .def_readwrite("required_gd_span_fs", &PbAchromaticDesign::required_gd_span_fs)
+        .def_readwrite("available_gd_span_fs", &PbAchromaticDesign::available_gd_span_fs)
+        .def_readwrite("gd_coverage", &PbAchromaticDesign::gd_coverage);
+    m.def("design_pb_achromatic_metalens", &design_pb_achromatic_metalens, py::arg("lib"),
+          py::arg("focal_length_um"), py::arg("diameter_um"), py::arg("handedness") = 1, py::arg("gd_weight") = 1.0,
+          py::arg("amplitude_weight") = 0.25);
+    m.def("verify_pb_achromatic_focus", &verify_pb_achromatic_focus, py::arg("lib"), py::arg("design"));
+    py::class_<PolarCell>(m, "PolarCell")
+        .def(py::init<>())
+        .def_readwrite("fill_x", &PolarCell::fill_x)
+        .def_readwrite("fill_y", &PolarCell::fill_y)
+        .def_readwrite("phase_x", &PolarCell::phase_x)
+        .def_readwrite("phase_y", &PolarCell::phase_y)
+        .def_readwrite("amp_x", &PolarCell::amp_x)
+        .def_readwrite("amp_y", &PolarCell::amp_y);
+    py::class_<PolarizationLibrary>(m, "PolarizationLibrary")
+        .def(py::init<>())
+        .def_readwrite("period_um", &PolarizationLibrary::period_um)
+        .def_readwrite("wavelength_um", &PolarizationLibrary::wavelength_um)
+        .def_readwrite("thickness_um", &PolarizationLibrary::thickness_um)
+        .def_readwrite("cells", &PolarizationLibrary::cells)
+        .def("lookup", &PolarizationLibrary::lookup, py::arg("target_x"), py::arg("target_y"),
+             py::arg("amplitude_weight") = 0.0);
+    m.def("build_polarization_library", &build_polarization_library, py::arg("pillar"), py::arg("background"),
+          py::arg("incident"), py::arg("substrate"), py::arg("period_um"), py::arg("wavelength_um"),
+          py::arg("thickness_um"), py::arg("fill_min"), py::arg("fill_max"), py::arg("n_samples"), py::arg("M"));
+    py::class_<PolarMetalensDesign>(m, "PolarMetalensDesign")
+        .def_readonly("n_cells", &PolarMetalensDesign::n_cells)
+        .def_readonly("period_um", &PolarMetalensDesign::period_um)
+        .def_readonly("fill_x", &PolarMetalensDesign::fill_x)
+        .def_readonly("fill_y", &PolarMetalensDesign::fill_y)
+        .def_readonly("t_x", &PolarMetalensDesign::t_x)
+        .def_readonly("t_y", &PolarMetalensDesign::t_y)
+        .def_readonly("rms_phase_error_x_deg", &PolarMetalensDesign::rms_phase_error_x_deg)
+        .def_readonly("rms_phase_error_y_deg", &PolarMetalensDesign::rms_phase_error_y_deg)
+        .def_readonly("mean_amp_x", &PolarMetalensDesign::mean_amp_x)
+        .def_readonly("mean_amp_y", &PolarMetalensDesign::mean_amp_y);
+    m.def("design_polarization_metalens", &design_polarization_metalens, py::arg("lib"), py::arg("focal_x_um"),
+          py::arg("focal_y_um"), py::arg("diameter_um"), py::arg("amplitude_weight") = 0.25);
+
     m.def("cuda_available", &cuda::available);
     m.def("cuda_device_name", &cuda::device_name);
 }

@@ -20,9 +20,10 @@
 #include <stdexcept>
 
 #include "celeris_b200.h"
+#include "detail.hpp"
 
 namespace celeris {
-namespace {
+namespace detail {
 
 void check(int status, const char* what) {
     if (status == CELERIS_OK) return;
@@ -75,30 +76,6 @@ Rcwa2DResult from_result(const celeris_rcwa_result& r) {
                         cdouble(r.ty0[0], r.ty0[1])};
 }
 
-struct Cell {
-    double x, y;
-    cdouble t;
-};
-
-std::vector<Cell> aperture_cells(const MetalensDesign& lens, const UnitCellLibrary& lib, double diameter_um,
-                                 double k_tilt_sin = 0.0) {
-    // focal.cpp:156-164 (circular aperture mask, nearest-fill transmission)
-    const double p = lens.period_um;
-    const double center = (lens.n_cells - 1) / 2.0;
-    const double R_ap = diameter_um / 2.0;
-    std::vector<Cell> cells;
-    for (int iy = 0; iy < lens.n_cells; ++iy)
-        for (int ix = 0; ix < lens.n_cells; ++ix) {
-            const double x = (ix - center) * p, y = (iy - center) * p;
-            if (std::sqrt(x * x + y * y) > R_ap) continue;
-            const double fill = lens.fill_map[static_cast<size_t>(iy) * lens.n_cells + ix];
-            cdouble t = lib.transmission_for_fill(fill);
-            if (k_tilt_sin != 0.0) t *= std::polar(1.0, k_tilt_sin * x);
-            cells.push_back({x, y, t});
-        }
-    return cells;
-}
-
 // |E|^2 of the plain FP64 form on the n x n grid (the GPU kernel).
 std::vector<double> psf_gpu(const std::vector<Cell>& cells, double cx, double cy, double z, double k, int n,
                             double W) {
@@ -134,6 +111,30 @@ std::vector<double> zx_gpu(const std::vector<Cell>& cells, double xmin, double x
     return out;
 }
 
+}  // namespace detail
+
+namespace {
+using namespace detail;
+
+std::vector<Cell> aperture_cells(const MetalensDesign& lens, const UnitCellLibrary& lib, double diameter_um,
+                                 double k_tilt_sin = 0.0) {
+    // focal.cpp:156-164 (circular aperture mask, nearest-fill transmission)
+    const double p = lens.period_um;
+    const double center = (lens.n_cells - 1) / 2.0;
+    const double R_ap = diameter_um / 2.0;
+    std::vector<Cell> cells;
+    for (int iy = 0; iy < lens.n_cells; ++iy)
+        for (int ix = 0; ix < lens.n_cells; ++ix) {
+            const double x = (ix - center) * p, y = (iy - center) * p;
+            if (std::sqrt(x * x + y * y) > R_ap) continue;
+            const double fill = lens.fill_map[static_cast<size_t>(iy) * lens.n_cells + ix];
+            cdouble t = lib.transmission_for_fill(fill);
+            if (k_tilt_sin != 0.0) t *= std::polar(1.0, k_tilt_sin * x);
+            cells.push_back({x, y, t});
+        }
+    return cells;
+}
+
 // Peak |E|^2 and the x of its pixel on an NG x NG grid centred at (xc, 0): the
 // search of field.cpp:48-75 / 106-134 (first maximum in row-major order, strict >).
 std::pair<double, double> peak_on_grid(const std::vector<Cell>& cells, double xc, double W, double z, double k) {
@@ -154,6 +155,7 @@ std::pair<double, double> peak_on_grid(const std::vector<Cell>& cells, double xc
 }
 
 }  // namespace
+using namespace detail;
 
 // ---- materials ---------------------------------------------------------------------
 Material::Material(std::function<cdouble(double)> dispersion, std::string name)

@@ -182,6 +182,168 @@ MetalensDesign design_metalens(const UnitCellLibrary& lib, const PhaseProfile& p
 MetalensDesign design_metalens(const UnitCellLibrary& lib, double focal_length_um, double diameter_um,
                                double amplitude_weight = 0.25);
 
+// ---- library builders on the batched RCWA and their on-axis checks ------------------------
+// design/metalens.cpp:71-110: one layer of a multi-layer stack swept in fill.
+UnitCellLibrary build_unit_cell_library_stack(Rcwa2DStack stack, int active_layer, const Material& incident,
+                                              const Material& substrate, double wavelength_um, double fill_min,
+                                              double fill_max, int n_samples, int M);
+
+// design/achromatic.hpp:33-161
+struct DispersiveAtom {
+    double fill = 0;
+    double thickness_um = 0;
+    MetaShape shape = MetaShape::Rectangle;
+    double fill_x = 0, fill_y = 0;
+    double shape_param = 0.5;
+    double phase0_rad = 0;       // phase at the centre wavelength
+    double group_delay_fs = 0;   // least-squares d(phase)/d(omega) over the band
+    double mean_amplitude = 0;
+    std::vector<double> phase_rad;
+    std::vector<double> amplitude;
+};
+struct MetaAtomSpec {
+    MetaShape shape = MetaShape::Rectangle;
+    double fill_x = 0.5;
+    double fill_y = 0.5;
+    double thickness_um = 0.6;
+    double shape_param = 0.5;
+};
+struct DispersiveLibrary {
+    std::vector<double> wavelengths_um;
+    double center_wavelength_um = 0;
+    int center_index = 0;
+    double period_um = 0;
+    int n_fill = 0, n_height = 0;
+    std::vector<DispersiveAtom> atoms;
+    double gd_min_fs = 0, gd_max_fs = 0;
+};
+DispersiveLibrary build_dispersive_library_from_specs(const Material& pillar, const Material& background,
+                                                      const Material& incident, const Material& substrate,
+                                                      double period_um, const std::vector<double>& band_wavelengths_um,
+                                                      double center_wavelength_um,
+                                                      const std::vector<MetaAtomSpec>& specs, int M);
+DispersiveLibrary build_dispersive_library(const Material& pillar, const Material& background,
+                                           const Material& incident, const Material& substrate, double period_um,
+                                           const std::vector<double>& band_wavelengths_um,
+                                           double center_wavelength_um, double fill_min, double fill_max,
+                                           int n_fills, double thick_lo, double thick_hi, int n_heights, int M);
+DispersiveLibrary build_single_etch_library(const Material& pillar, const Material& background,
+                                            const Material& incident, const Material& substrate, double period_um,
+                                            const std::vector<double>& band_wavelengths_um,
+                                            double center_wavelength_um, double fill_min, double fill_max,
+                                            int n_fills, double thickness_um, int M);
+struct AchromaticDesign {
+    int n_cells = 0;
+    double period_um = 0;
+    std::vector<int> atom_index;
+    std::vector<double> fill_map;
+    std::vector<double> thickness_map;
+    double center_wavelength_um = 0;
+    double focal_length_um = 0;
+    double diameter_um = 0;
+    double rms_phase_error_deg = 0;
+    double rms_group_delay_error_fs = 0;
+    double mean_amplitude = 0;
+    double required_gd_span_fs = 0;
+    double available_gd_span_fs = 0;
+    double gd_coverage = 0;
+    bool single_height = true;
+    double min_height_um = 0, max_height_um = 0;
+};
+AchromaticDesign design_achromatic_metalens(const DispersiveLibrary& lib, double focal_length_um,
+                                            double diameter_um, double gd_weight = 1.0,
+                                            double amplitude_weight = 0.25);
+struct AchromaticFocalPoint {
+    double wavelength_um;
+    double focal_length_um;
+    double rel_peak;
+};
+// On-axis focus search per band sample: 200-point z scans on the GPU far field.
+std::vector<AchromaticFocalPoint> verify_achromatic_focus(const DispersiveLibrary& lib,
+                                                          const AchromaticDesign& design);
+MetalensDesign to_metalens_design(const AchromaticDesign& d);
+
+// design/pb_achromatic.hpp:40-121
+struct DispersivePbAtom {
+    double fill_x = 0, fill_y = 0;
+    double thickness_um = 0;
+    double phase0_rad = 0;
+    double group_delay_fs = 0;
+    double mean_amplitude = 0;
+    double mean_conversion = 0;
+    double retardance_center_deg = 0;
+    std::vector<cdouble> cross;  // (t_x - t_y) / 2 per band sample
+};
+struct DispersivePbLibrary {
+    std::vector<double> wavelengths_um;
+    double center_wavelength_um = 0;
+    int center_index = 0;
+    double period_um = 0;
+    double thickness_um = 0;
+    int n_fill = 0;
+    std::vector<DispersivePbAtom> atoms;
+    double gd_min_fs = 0, gd_max_fs = 0;
+};
+DispersivePbLibrary build_dispersive_pb_library(const Material& pillar, const Material& background,
+                                                const Material& incident, const Material& substrate,
+                                                double period_um, const std::vector<double>& band_wavelengths_um,
+                                                double center_wavelength_um, double fill_min, double fill_max,
+                                                int n_fills, double thickness_um, int M, double min_amplitude = 0.30);
+struct PbAchromaticDesign {
+    int n_cells = 0;
+    double period_um = 0;
+    double thickness_um = 0;
+    int handedness = +1;
+    std::vector<int> atom_index;
+    std::vector<double> rotation_rad;
+    std::vector<double> fill_x_map;
+    std::vector<double> fill_y_map;
+    double center_wavelength_um = 0;
+    double focal_length_um = 0;
+    double diameter_um = 0;
+    double rms_phase_error_deg = 0;
+    double rms_group_delay_error_fs = 0;
+    double mean_amplitude = 0;
+    double mean_conversion = 0;
+    double required_gd_span_fs = 0;
+    double available_gd_span_fs = 0;
+    double gd_coverage = 0;
+};
+PbAchromaticDesign design_pb_achromatic_metalens(const DispersivePbLibrary& lib, double focal_length_um,
+                                                 double diameter_um, int handedness = +1, double gd_weight = 1.0,
+                                                 double amplitude_weight = 0.25);
+std::vector<AchromaticFocalPoint> verify_pb_achromatic_focus(const DispersivePbLibrary& lib,
+                                                             const PbAchromaticDesign& design);
+
+// design/polar_metalens.hpp:17-60
+struct PolarCell {
+    double fill_x, fill_y;
+    double phase_x, phase_y;
+    double amp_x, amp_y;
+};
+struct PolarizationLibrary {
+    double period_um = 0, wavelength_um = 0, thickness_um = 0;
+    std::vector<PolarCell> cells;
+    int lookup(double target_x, double target_y, double amplitude_weight = 0.0) const;
+};
+PolarizationLibrary build_polarization_library(const Material& pillar, const Material& background,
+                                               const Material& incident, const Material& substrate,
+                                               double period_um, double wavelength_um, double thickness_um,
+                                               double fill_min, double fill_max, int n_samples, int M);
+struct PolarMetalensDesign {
+    int n_cells = 0;
+    double period_um = 0;
+    std::vector<double> fill_x;
+    std::vector<double> fill_y;
+    std::vector<cdouble> t_x;
+    std::vector<cdouble> t_y;
+    double rms_phase_error_x_deg = 0, rms_phase_error_y_deg = 0;
+    double mean_amp_x = 0, mean_amp_y = 0;
+};
+PolarMetalensDesign design_polarization_metalens(const PolarizationLibrary& lib, double focal_x_um,
+                                                 double focal_y_um, double diameter_um,
+                                                 double amplitude_weight = 0.25);
+
 // ---- reference inverse-design gradient (optimize.hpp) --------------------------------
 struct PillarTarget {
     double wavelength_um, target_phase_rad, amplitude_weight;

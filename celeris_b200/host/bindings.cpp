@@ -3,6 +3,7 @@
 // host mirror in celeris.hpp. Maps are returned as numpy arrays like the
 // reference (PsfMap.intensity, MetalensDesign.fill_map).
 #include <pybind11/complex.h>
+#include <pybind11/functional.h>
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
@@ -274,6 +275,16 @@ PYBIND11_MODULE(_celeris, m) {
     m.def("analyze_through_focus", &analyze_through_focus, py::arg("lens"), py::arg("lib"),
           py::arg("focal_length_um"), py::arg("wavelength_um"), py::arg("diameter_um"));
 
+    py::class_<ChromaticPoint>(m, "ChromaticPoint")
+        .def_readonly("wavelength_um", &ChromaticPoint::wavelength_um)
+        .def_readonly("focal_length_um", &ChromaticPoint::focal_length_um)
+        .def_readonly("rel_peak", &ChromaticPoint::rel_peak);
+    m.def("analyze_chromatic", &analyze_chromatic, py::arg("lens"), py::arg("lib"), py::arg("design_focal"),
+          py::arg("design_wavelength"), py::arg("diameter"), py::arg("lambda_min"), py::arg("lambda_max"),
+          py::arg("n"));
+    m.def("analyze_chromatic_dispersive", &analyze_chromatic_dispersive, py::arg("lens"), py::arg("build_lib_at"),
+          py::arg("design_focal"), py::arg("design_wavelength"), py::arg("diameter"), py::arg("lambda_min"),
+          py::arg("lambda_max"), py::arg("n"));
     py::class_<FieldPoint>(m, "FieldPoint")
         .def_readonly("angle_deg", &FieldPoint::angle_deg)
         .def_readonly("rel_strehl", &FieldPoint::rel_strehl)

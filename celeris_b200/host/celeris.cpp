@@ -714,6 +714,67 @@ FieldPsf compute_psf_field(const MetalensDesign& lens, const UnitCellLibrary& li
 }
 
 // ---- through-focus (throughfocus.cpp:15-135) -------------------------------------------------
+// ---- chromatic focal shift (chromatic.cpp) -------------------------------------------------
+namespace {
+// First maximum of a 120-point on-axis scan over [0.55, 1.6] x f0 lambda0 / lambda
+// (chromatic.cpp:46-56), on the GPU far field.
+ChromaticPoint chromatic_point(const std::vector<Cell>& cells, double design_focal, double design_wavelength,
+                               double lam, double design_peak) {
+    constexpr int NZ = 120;
+    const double k = 2.0 * pi / lam;
+    const double expected = design_focal * design_wavelength / lam;
+    const double zlo = 0.55 * expected, zhi = 1.6 * expected;
+    double best_z = expected, best_I = -1.0;
+    if (!cells.empty()) {
+        const std::vector<double> I = zx_gpu(cells, 0.0, 0.0, 2, zlo, zhi, NZ, k);
+        for (int j = 0; j < NZ; ++j) {
+            const double v = I[static_cast<size_t>(j) * 2];
+            if (v > best_I) {
+                best_I = v;
+                best_z = zlo + (zhi - zlo) * j / (NZ - 1);
+            }
+        }
+    } else {
+        best_I = 0.0;
+    }
+    return {lam, best_z, design_peak > 0 ? best_I / design_peak : 0.0};
+}
+double on_axis_peak(const std::vector<Cell>& cells, double z, double k) {
+    return cells.empty() ? 0.0 : zx_gpu(cells, 0.0, 0.0, 2, z, z, 2, k)[0];
+}
+}  // namespace
+
+std::vector<ChromaticPoint> analyze_chromatic(const MetalensDesign& lens, const UnitCellLibrary& lib,
+                                              double design_focal, double design_wavelength, double diameter,
+                                              double lambda_min, double lambda_max, int n) {
+    const std::vector<Cell> cells = aperture_cells(lens, lib, diameter);
+    const double peak0 = on_axis_peak(cells, design_focal, 2.0 * pi / design_wavelength);
+    std::vector<ChromaticPoint> out;
+    for (int i = 0; i < n; ++i) {
+        const double lam = lambda_min + (lambda_max - lambda_min) * i / (n - 1);
+        out.push_back(chromatic_point(cells, design_focal, design_wavelength, lam, peak0));
+    }
+    return out;
+}
+
+std::vector<ChromaticPoint> analyze_chromatic_dispersive(const MetalensDesign& lens,
+                                                         const std::function<UnitCellLibrary(double)>& build_lib_at,
+                                                         double design_focal, double design_wavelength,
+                                                         double diameter, double lambda_min, double lambda_max,
+                                                         int n) {
+    // the aperture is fixed by the design; each wavelength's library sets the transmissions
+    const double peak0 =
+        on_axis_peak(aperture_cells(lens, build_lib_at(design_wavelength), diameter), design_focal,
+                     2.0 * pi / design_wavelength);
+    std::vector<ChromaticPoint> out;
+    for (int i = 0; i < n; ++i) {
+        const double lam = lambda_min + (lambda_max - lambda_min) * i / (n - 1);
+        const std::vector<Cell> cells = aperture_cells(lens, build_lib_at(lam), diameter);
+        out.push_back(chromatic_point(cells, design_focal, design_wavelength, lam, peak0));
+    }
+    return out;
+}
+
 ThroughFocus analyze_through_focus(const MetalensDesign& lens, const UnitCellLibrary& lib, double focal_length_um,
                                    double wavelength_um, double diameter_um) {
     const double R = diameter_um / 2.0;

@@ -381,6 +381,22 @@ FieldPsf compute_psf_field(const MetalensDesign& lens, const UnitCellLibrary& li
                            double half_window_um, double on_axis_peak = 0.0);
 
 // ---- through-focus and off-axis analyses (callers of the far field) ----------------------
+// chromatic.hpp:10-34: on-axis focus search (120 z samples around f0 lambda0 / lambda)
+// per wavelength; the dispersive form rebuilds the library at every wavelength.
+struct ChromaticPoint {
+    double wavelength_um;
+    double focal_length_um;
+    double rel_peak;
+};
+std::vector<ChromaticPoint> analyze_chromatic(const MetalensDesign& lens, const UnitCellLibrary& lib,
+                                              double design_focal, double design_wavelength, double diameter,
+                                              double lambda_min, double lambda_max, int n);
+std::vector<ChromaticPoint> analyze_chromatic_dispersive(const MetalensDesign& lens,
+                                                         const std::function<UnitCellLibrary(double)>& build_lib_at,
+                                                         double design_focal, double design_wavelength,
+                                                         double diameter, double lambda_min, double lambda_max,
+                                                         int n);
+
 // throughfocus.hpp:13-35: on-axis z scan (161 points) + x-z caustic (201 x 201 on the GPU).
 struct ThroughFocus {
     std::vector<float> z_um;

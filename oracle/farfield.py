@@ -170,3 +170,12 @@ def ref_field_grid(lens_args, f, wl, D, max_angle, n_half, psf_n):
     r.ref_field_grid(*args, _D(f), _D(wl), _D(D), _D(max_angle), ctypes.c_int(n_half), ctypes.c_int(psf_n),
                      _dp(out))
     return out
+
+
+def ref_chromatic(lens_args, f, wl, D, lam_min, lam_max, n):
+    """celeris::analyze_chromatic (chromatic.cpp, CPU): rows (lambda, focal z, rel_peak)."""
+    r = _ref_or_raise()
+    args, keep = _lens_args(*lens_args)
+    out = np.zeros((n, 3))
+    r.ref_chromatic(*args, _D(f), _D(wl), _D(D), _D(lam_min), _D(lam_max), ctypes.c_int(n), _dp(out))
+    return out

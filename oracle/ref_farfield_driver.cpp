@@ -12,6 +12,7 @@
 #include <thread>
 #include <vector>
 
+#include "celeris/analysis/chromatic.hpp"
 #include "celeris/analysis/field.hpp"
 #include "celeris/analysis/focal.hpp"
 #include "celeris/analysis/throughfocus.hpp"
@@ -118,4 +119,20 @@ REF_API int ref_field_grid(int n_cells, double period_um, const double* fill_map
         for (int q = 0; q < 7; ++q) out[7 * i + q] = v[q];
     }
     return static_cast<int>(g.points.size());
+}
+
+// celeris::analyze_chromatic (chromatic.cpp, CPU): per wavelength (lambda, z of the
+// on-axis peak, peak relative to the design point); returns the count.
+REF_API int ref_chromatic(int n_cells, double period_um, const double* fill_map, int nlib, const double* lfill,
+                          const double* lphase, const double* lamp, double lib_wl, double f, double wl, double D,
+                          double lam_min, double lam_max, int n, double* out) {
+    const auto lens = make_lens(n_cells, period_um, fill_map);
+    const auto lib = make_lib(period_um, lib_wl, 0.0, nlib, lfill, lphase, lamp);
+    const auto pts = celeris::analyze_chromatic(lens, lib, f, wl, D, lam_min, lam_max, n);
+    for (size_t i = 0; i < pts.size(); ++i) {
+        out[3 * i] = pts[i].wavelength_um;
+        out[3 * i + 1] = pts[i].focal_length_um;
+        out[3 * i + 2] = pts[i].rel_peak;
+    }
+    return static_cast<int>(pts.size());
 }

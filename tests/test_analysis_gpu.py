@@ -92,3 +92,63 @@ def test_field_grid_matches_reference():
         assert got[:2] == list(w[:2])
         assert got[2] == pytest.approx(w[2], rel=1e-9)
         assert got[3:] == pytest.approx(list(w[3:]), abs=1e-9)
+
+
+def test_chromatic_matches_reference():
+    """analyze_chromatic (chromatic.cpp): 120-point on-axis scans per wavelength."""
+    cel, lib, lens, args = lens_and_lib()
+    got = cel.analyze_chromatic(lens, lib, F_UM, WL, D_UM, 0.5, 0.7, 5)
+    want = F.ref_chromatic(args, F_UM, WL, D_UM, 0.5, 0.7, 5)
+    for g, w in zip(got, want):
+        assert g.wavelength_um == w[0]
+        assert g.focal_length_um == pytest.approx(w[1], abs=1e-9)
+        assert g.rel_peak == pytest.approx(w[2], rel=1e-9)
+
+
+def test_chromatic_dispersive_with_per_wavelength_libraries():
+    """analyze_chromatic_dispersive: with the same library at every wavelength it
+    is analyze_chromatic of the reference; with a wavelength-dependent library
+    (phases scaled by lambda0 / lambda) each scan is checked against the
+    oracle's on-axis sum and the reference's first-maximum rule."""
+    cel, lib, lens, args = lens_and_lib()
+    got = cel.analyze_chromatic_dispersive(lens, lambda lam: lib, F_UM, WL, D_UM, 0.5, 0.7, 4)
+    want = F.ref_chromatic(args, F_UM, WL, D_UM, 0.5, 0.7, 4)
+    for g, w in zip(got, want):
+        assert g.focal_length_um == pytest.approx(w[1], abs=1e-9)
+        assert g.rel_peak == pytest.approx(w[2], rel=1e-9)
+
+    def lib_at(lam):
+        out = cel.UnitCellLibrary()
+        out.period_um, out.wavelength_um, out.thickness_um = lib.period_um, lam, lib.thickness_um
+        out.fill = list(lib.fill)
+        out.phase = [float(np.angle(np.exp(1j * p * WL / lam))) for p in lib.phase]
+        out.amplitude = list(lib.amplitude)
+        return out
+
+    got = cel.analyze_chromatic_dispersive(lens, lib_at, F_UM, WL, D_UM, 0.55, 0.7, 3)
+    n, p = lens.n_cells, lens.period_um
+    c = (n - 1) / 2.0
+    fm = np.asarray(lens.fill_map).reshape(n, n)
+
+    def cells(l):
+        px, py, t = [], [], []
+        for iy in range(n):
+            for ix in range(n):
+                x, y = (ix - c) * p, (iy - c) * p
+                if math.sqrt(x * x + y * y) > D_UM / 2:
+                    continue
+                px.append(x)
+                py.append(y)
+                t.append(l.transmission_for_fill(fm[iy, ix]))
+        return np.array(px), np.array(py), np.array(t)
+
+    px, py, t = cells(lib_at(WL))
+    k0 = 2 * math.pi / WL
+    peak0 = F.rs_zx(px, py, t, 0.0, 0.0, 2, F_UM, F_UM, 2, k0)[0, 0]
+    for g, lam in zip(got, [0.55, 0.625, 0.7]):
+        px, py, t = cells(lib_at(lam))
+        exp = F_UM * WL / lam
+        I = F.rs_zx(px, py, t, 0.0, 0.0, 2, 0.55 * exp, 1.6 * exp, 120, 2 * math.pi / lam)[:, 0]
+        j = int(np.argmax(I))  # first maximum, as the reference's strict > scan
+        assert g.focal_length_um == pytest.approx(0.55 * exp + (1.6 * exp - 0.55 * exp) * j / 119, abs=1e-9)
+        assert g.rel_peak == pytest.approx(I[j] / peak0, rel=1e-9)

@@ -51,7 +51,7 @@ constexpr int kTile64 = 256;  // pillars (or pixels) per stage, 32 B records -> 
 constexpr int kTile32 = 512;  // pillars per stage, 16 B records -> 8 KB
 constexpr int kStages = 4;
 constexpr int kPPT64 = 2;     // pixels per thread, plain form
-constexpr int kPPT32 = 12;    // pixels per thread, precision form (per-pillar record load and dy shared by 12 terms)
+constexpr int kPPT32 = 6;     // pixels per thread, precision form: 3 packed pixel pairs share each pillar record
 constexpr int kAdjPPT = 2;    // pillars per thread, adjoint
 
 enum { GEOM_PSF = 0, GEOM_ZX = 1 };
@@ -243,6 +243,35 @@ __device__ __forceinline__ float cos_approx(float x) {
     asm("cos.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
+// Packed FP32 pairs (add / mul / fma .rn.f32x2, sm_100): one instruction does the
+// same IEEE-rounded operation on two pixels, halving the issue slots of the
+// term arithmetic. A pair lives in a 64-bit register, low half = first pixel.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pk2(float a, float b) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ f32x2 dup2(float a) { return pk2(a, a); }
+__device__ __forceinline__ void upk2(f32x2 r, float& a, float& b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
 // Knuth TwoSum: s + c += x with the rounding error of s + x kept in c.
 __device__ __forceinline__ void two_sum_acc(float& s, float& c, float x) {
     const float t = s + x;
@@ -252,7 +281,7 @@ __device__ __forceinline__ void two_sum_acc(float& s, float& c, float x) {
     s = t;
 }
 
-__global__ void __launch_bounds__(kThreads) rs_f32c_kernel(const float4* __restrict__ rec,
+__global__ void __launch_bounds__(kThreads, 3) rs_f32c_kernel(const float4* __restrict__ rec,
                                                            int npil, int chunk_len, Geom g,
                                                            float il_hi, float il_lo,
                                                            double2* __restrict__ partial) {
@@ -276,9 +305,15 @@ __global__ void __launch_bounds__(kThreads) rs_f32c_kernel(const float4* __restr
         z = (float)fz;
     }
     const float z2 = z * z;
-    const float z2x = 2.0f * z;
     const float kMagic = 12582912.0f;  // 1.5 * 2^23: x + M - M rounds x to an integer
-    const float kTwoPi = 6.28318530717958647692f;
+    // pixel pairs and the constants of the packed term arithmetic
+    constexpr int kPairs = kPPT32 / 2;
+    f32x2 fx2[kPairs];
+#pragma unroll
+    for (int h = 0; h < kPairs; ++h) fx2[h] = pk2(fxr[2 * h], fxr[2 * h + 1]);
+    const f32x2 NEG1 = dup2(-1.0f), NZ = dup2(-z), Z2X = dup2(2.0f * z), NHALF = dup2(-0.5f);
+    const f32x2 ILHI = dup2(il_hi), ILLO = dup2(il_lo), MAGIC = dup2(kMagic);
+    const f32x2 TWOPI = dup2(6.28318530717958647692f);
 
     TilePipe<float4, kTile32> pipe;
     const int lo = blockIdx.y * chunk_len;
@@ -293,37 +328,49 @@ __global__ void __launch_bounds__(kThreads) rs_f32c_kernel(const float4* __restr
         if (got) {
             const float4* tile = buf[t % kStages];
             const int cnt = pipe.count(t);
-            float er[kPPT32], ei[kPPT32];
+            f32x2 er[kPairs], ei[kPairs];
 #pragma unroll
-            for (int q = 0; q < kPPT32; ++q) er[q] = ei[q] = 0.f;
+            for (int h = 0; h < kPairs; ++h) er[h] = ei[h] = 0ull;
 #pragma unroll 2
             for (int p = 0; p < cnt; ++p) {
                 const float4 r = tile[p];  // {x, y, |t|, arg t / 2pi}
                 const float dy = fyr - r.y;
-                const float dy2 = dy * dy;
+                const f32x2 RX = dup2(r.x), RW = dup2(r.w), RZ = dup2(r.z);
+                const f32x2 U0 = dup2(fmaf(dy, dy, z2));  // dy^2 + z^2 (seed only)
+                const f32x2 ND2 = dup2(-(dy * dy));        // -dy^2
 #pragma unroll
-                for (int q = 0; q < kPPT32; ++q) {
-                    const float dx = fxr[q] - r.x;
-                    const float s = fmaf(dx, dx, dy2);     // rho^2
-                    const float u = s + z2;                // R^2 (rounded; seed only)
-                    const float ri = rsqrt_approx(u);      // ~1/R
-                    const float d0 = u * ri - z;           // ~R - z
+                for (int h = 0; h < kPairs; ++h) {
+                    const f32x2 dx = fma2(RX, NEG1, fx2[h]);   // fx - x
+                    const f32x2 ndx = fma2(fx2[h], NEG1, RX);  // x - fx
+                    const f32x2 u = fma2(dx, dx, U0);          // R^2 (seed only)
+                    const f32x2 ns = fma2(dx, ndx, ND2);       // -rho^2, one rounding
+                    float ua, ub;
+                    upk2(u, ua, ub);
+                    const f32x2 ri = pk2(rsqrt_approx(ua), rsqrt_approx(ub));  // ~1/R
+                    const f32x2 d0 = fma2(u, ri, NZ);          // ~R - z
                     // Newton on f(d) = d^2 + 2 z d - rho^2 (exact root R - z)
-                    const float gg = fmaf(d0, d0, fmaf(z2x, d0, -s));
-                    const float d = fmaf(gg * ri, -0.5f, d0);
+                    const f32x2 gg = fma2(d0, d0, fma2(Z2X, d0, ns));
+                    const f32x2 d = fma2(mul2(gg, ri), NHALF, d0);
                     // phase in turns: (R - z)/lambda + arg(t)/2pi; k z is added in FP64
-                    const float th = fmaf(d, il_hi, fmaf(d, il_lo, r.w));
-                    const float rn = (th + kMagic) - kMagic;
-                    const float ang = (th - rn) * kTwoPi;  // in [-pi, pi]
-                    const float a = r.z * ri;              // |t| / R
-                    er[q] = fmaf(a, cos_approx(ang), er[q]);
-                    ei[q] = fmaf(a, sin_approx(ang), ei[q]);
+                    const f32x2 th = fma2(d, ILHI, fma2(d, ILLO, RW));
+                    const f32x2 w = fma2(add2(th, MAGIC), NEG1, MAGIC);  // -(th rounded to an integer)
+                    const f32x2 ang = mul2(add2(th, w), TWOPI);          // in [-pi, pi]
+                    const f32x2 a = mul2(RZ, ri);                         // |t| / R
+                    float aa, ab;
+                    upk2(ang, aa, ab);
+                    er[h] = fma2(a, pk2(cos_approx(aa), cos_approx(ab)), er[h]);
+                    ei[h] = fma2(a, pk2(sin_approx(aa), sin_approx(ab)), ei[h]);
                 }
             }
 #pragma unroll
-            for (int q = 0; q < kPPT32; ++q) {
-                two_sum_acc(sr[q], cr[q], er[q]);
-                two_sum_acc(si[q], ci[q], ei[q]);
+            for (int h = 0; h < kPairs; ++h) {
+                float e0, e1, f0, f1;
+                upk2(er[h], e0, e1);
+                upk2(ei[h], f0, f1);
+                two_sum_acc(sr[2 * h], cr[2 * h], e0);
+                two_sum_acc(sr[2 * h + 1], cr[2 * h + 1], e1);
+                two_sum_acc(si[2 * h], ci[2 * h], f0);
+                two_sum_acc(si[2 * h + 1], ci[2 * h + 1], f1);
             }
         }
         if (!pipe.release(t, got)) return;
@@ -625,8 +672,8 @@ int ff_run(int form, const double* d_px, const double* d_py, const double* d_pt,
         const double il = k / (2.0 * 3.14159265358979323846);  // 1/lambda in turns per micron
         const float hi = (float)il;
         const float lo = (float)(il - (double)hi);
-        rs_f32c_kernel<<<grid, kThreads, 0, st>>>(static_cast<const float4*>(rec), npil, chunk_len,
-                                                  g, hi, lo, partial);
+        rs_f32c_kernel<<<grid, kThreads, 0, st>>>(static_cast<const float4*>(rec), npil, chunk_len, g, hi, lo,
+                                                  partial);
     } else {
         rs_f64_kernel<<<grid, kThreads, 0, st>>>(static_cast<const double4*>(rec), npil,
                                                  chunk_len, g, k, partial);

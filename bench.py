@@ -101,6 +101,41 @@ def shard_center(rank, n, half_window_um):
     return rank * n * step
 
 
+def shard_cells(cells, world):
+    """Partition RCWA cells over `world` ranks by flop weight (n^3, n = 2 (2Mx+1)(2My+1)):
+    greedy longest-first onto the least-loaded rank. Returns one index list per
+    rank; every cell lands on exactly one rank (independent cells, no exchange
+    beyond the result gather)."""
+    w = [(2 * (2 * c["Mx"] + 1) * (2 * c.get("My", c["Mx"]) + 1)) ** 3 for c in cells]
+    parts, loads = [[] for _ in range(world)], [0] * world
+    for i in sorted(range(len(cells)), key=lambda i: (-w[i], i)):
+        r = min(range(world), key=lambda k: (loads[k], k))
+        parts[r].append(i)
+        loads[r] += w[i]
+    return [sorted(p) for p in parts]
+
+
+def measure_rcwa_sharded(world, rank):
+    """4096 uneven cells split over the ranks by flop weight (strong scaling):
+    each rank solves its share in one batched call; max-over-ranks wall time of
+    the warm call (the batch is synchronous, the host clock brackets the device
+    work) gives the whole-job cells/s."""
+    from celeris_b200 import capi
+    from celeris_b200.workloads import rcwa_uneven_4096
+
+    cells = rcwa_uneven_4096()
+    mine = shard_cells(cells, world)[rank]
+    cc = [capi.rcwa_cell(**cells[i]) for i in mine]
+    capi.rcwa_batch(cc)  # tuning + graph capture
+    barrier(world)
+    t0 = time.perf_counter()
+    res, info = capi.rcwa_batch(cc)
+    dt = max_over_ranks(world, time.perf_counter() - t0)
+    bad = max_over_ranks(world, float(np.sum(info != 0)))
+    return {"value": len(cells) / dt, "unit": "cells/s", "s": dt, "ranks": world, "scaling": "strong",
+            "sharding": "cells by n^3 weight, greedy longest-first", "failed_cells": int(bad)}
+
+
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
@@ -487,6 +522,11 @@ def run_gpu(args):
         "gpu_launches": int(launches),
         "clocks": clk,
     }
+    if world > 1 and not args.quick:
+        try:
+            out["rcwa_sharded"] = measure_rcwa_sharded(world, rank)
+        except Exception as exc:
+            out["rcwa_sharded"] = {"unavailable": str(exc)[:200]}
     if rank != 0:
         return
     # ---- error of the chosen form against the FP64 form (full grid) ----------

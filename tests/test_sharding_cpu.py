@@ -67,3 +67,52 @@ def test_row_block_shards_tile_the_window_and_max_reduces():
     for rank, cy, tile, _ in tiles:
         ref = E[rank * n:(rank + 1) * n]
         assert np.max(np.abs(tile - ref)) <= 1e-11 * np.max(np.abs(E))
+
+
+def test_rcwa_cells_shard_by_flop_weight():
+    """The RCWA batch splits over ranks by n^3 weight: every cell exactly once,
+    loads within one largest cell of each other."""
+    import bench
+    from celeris_b200.workloads import rcwa_uneven_4096
+
+    cells = rcwa_uneven_4096()
+    for world in (1, 2, 3, 8):
+        parts = bench.shard_cells(cells, world)
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(cells)))
+        w = [(2 * (2 * c["Mx"] + 1) * (2 * c.get("My", c["Mx"]) + 1)) ** 3 for c in cells]
+        loads = [sum(w[i] for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(w)
+
+
+def _rcwa_worker(rank, world, port, out):
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        import bench
+        from celeris_b200.workloads import rcwa_uneven_4096
+
+        parts = bench.shard_cells(rcwa_uneven_4096(), world)
+        got = [None] * world
+        dist.all_gather_object(got, (rank, parts[rank], bench.max_over_ranks(world, 1.0 + rank)))
+        if rank == 0:
+            out.put(got)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(240)
+def test_rcwa_shards_agree_across_ranks():
+    """Each gloo rank computes the same partition independently (no exchange
+    needed to agree) and the timing reduction returns the slowest rank."""
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.SimpleQueue()
+    mp.start_processes(_rcwa_worker, args=(world, _free_port(), q), nprocs=world, join=True, start_method="spawn")
+    got = q.get()
+    parts = [g[1] for g in sorted(got)]
+    assert sorted(parts[0] + parts[1]) == list(range(4096))
+    assert not set(parts[0]) & set(parts[1])
+    assert all(g[2] == float(world) for g in got)

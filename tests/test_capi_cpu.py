@@ -56,3 +56,36 @@ def test_invalid_arguments_are_rejected_before_device_work():
     st = lib.celeris_propagate_zx(None, None, None, 0, 0.0, 1.0, 1, 0.0, 1.0, 5, 1.0, None)
     assert st == capi.ERR_INVALID_ARG
     assert b"nx" in lib.celeris_last_error()
+
+
+def test_stack_arguments_are_rejected_before_device_work():
+    """Multi-layer stack entry points: layers that disagree on what the
+    reference's Rcwa2DStack holds once (orders, periods, wavelength, angles,
+    half-spaces), empty stacks, bad offsets and short order buffers are
+    argument errors, reported without touching a device."""
+    base = dict(period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46, eps_pillar=4.0, eps_bg=1.0,
+                fill_x=0.5, thickness_um=0.3, Mx=2)
+    a = capi.rcwa_cell(**base)
+    for change in (dict(period_um=0.5), dict(wavelength_um=0.6), dict(Mx=3), dict(n_sub=1.5),
+                   dict(theta_rad=0.1)):
+        b = capi.rcwa_cell(**{**base, **change})
+        with pytest.raises(capi.CelerisError) as e:
+            capi.solve_rcwa_2d_stack([a, b])
+        assert e.value.status == capi.ERR_INVALID_ARG
+        with pytest.raises(capi.CelerisError) as e:
+            capi.rcwa_stack_batch([[a], [a, b]])
+        assert e.value.status == capi.ERR_INVALID_ARG
+    with pytest.raises(capi.CelerisError) as e:
+        capi.rcwa_stack_batch([[a], []])
+    assert e.value.status == capi.ERR_INVALID_ARG
+    lib = capi.load()
+    import ctypes
+
+    arr = (capi.RcwaCell * 1)(a)
+    out = capi.RcwaResult()
+    orders = (capi.RcwaOrder * 4)()
+    ex = (ctypes.c_double * 2)(1.0, 0.0)
+    ey = (ctypes.c_double * 2)(0.0, 0.0)
+    st = lib.celeris_solve_rcwa_2d_orders(arr, 1, ex, ey, ctypes.byref(out), orders, 4)  # 25 orders needed
+    assert st == capi.ERR_INVALID_ARG and b"orders" in lib.celeris_last_error()
+    assert lib.celeris_solve_rcwa_2d_stack(arr, 0, ex, ey, ctypes.byref(out)) == capi.ERR_INVALID_ARG

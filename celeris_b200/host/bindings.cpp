@@ -470,6 +470,73 @@ PYBIND11_MODULE(_celeris, m) {
     m.def("design_polarization_metalens", &design_polarization_metalens, py::arg("lib"), py::arg("focal_x_um"),
           py::arg("focal_y_um"), py::arg("diameter_um"), py::arg("amplitude_weight") = 0.25);
 
+    py::class_<JonesMatrix>(m, "JonesMatrix")
+        .def_readonly("xx", &JonesMatrix::xx)
+        .def_readonly("xy", &JonesMatrix::xy)
+        .def_readonly("yx", &JonesMatrix::yx)
+        .def_readonly("yy", &JonesMatrix::yy);
+    m.def("solve_jones", &solve_jones, py::arg("incident"), py::arg("stack"), py::arg("substrate"),
+          py::arg("wavelength_um"), py::arg("M"));
+    py::class_<HwpAtom>(m, "HwpAtom")
+        .def(py::init<>())
+        .def_readwrite("fill_x", &HwpAtom::fill_x)
+        .def_readwrite("fill_y", &HwpAtom::fill_y)
+        .def_readwrite("thickness_um", &HwpAtom::thickness_um)
+        .def_readwrite("t_x", &HwpAtom::t_x)
+        .def_readwrite("t_y", &HwpAtom::t_y)
+        .def_readwrite("retardance_deg", &HwpAtom::retardance_deg)
+        .def_readwrite("conversion_efficiency", &HwpAtom::conversion_efficiency);
+    m.def("find_hwp_atom", &find_hwp_atom, py::arg("pillar"), py::arg("background"), py::arg("incident"),
+          py::arg("substrate"), py::arg("period_um"), py::arg("wavelength_um"), py::arg("thickness_um"),
+          py::arg("fill_min"), py::arg("fill_max"), py::arg("n_samples"), py::arg("M"));
+    py::class_<PbVerifyPoint>(m, "PbVerifyPoint")
+        .def_readonly("rotation_deg", &PbVerifyPoint::rotation_deg)
+        .def_readonly("cross_phase_deg", &PbVerifyPoint::cross_phase_deg)
+        .def_readonly("conversion_eff", &PbVerifyPoint::conversion_eff)
+        .def_readonly("copol_leakage", &PbVerifyPoint::copol_leakage);
+    m.def("verify_pb_phase", &verify_pb_phase, py::arg("pillar"), py::arg("background"), py::arg("incident"),
+          py::arg("substrate"), py::arg("period_um"), py::arg("wavelength_um"), py::arg("atom"),
+          py::arg("rotations_rad"), py::arg("M"));
+    py::class_<PbMetalensDesign>(m, "PbMetalensDesign")
+        .def_readonly("n_cells", &PbMetalensDesign::n_cells)
+        .def_readonly("period_um", &PbMetalensDesign::period_um)
+        .def_readonly("atom", &PbMetalensDesign::atom)
+        .def_readonly("rotation_rad", &PbMetalensDesign::rotation_rad)
+        .def_readonly("t_cross", &PbMetalensDesign::t_cross)
+        .def_readonly("rms_phase_error_deg", &PbMetalensDesign::rms_phase_error_deg)
+        .def_readonly("conversion_efficiency", &PbMetalensDesign::conversion_efficiency);
+    m.def("design_pb_metalens",
+          py::overload_cast<const HwpAtom&, double, double, const PhaseProfile&, double, int>(&design_pb_metalens),
+          py::arg("atom"), py::arg("period_um"), py::arg("wavelength_um"), py::arg("profile"), py::arg("diameter_um"),
+          py::arg("handedness") = 1);
+    m.def("design_pb_metalens",
+          py::overload_cast<const HwpAtom&, double, double, double, double, int>(&design_pb_metalens),
+          py::arg("atom"), py::arg("period_um"), py::arg("wavelength_um"), py::arg("focal_length_um"),
+          py::arg("diameter_um"), py::arg("handedness") = 1);
+    py::class_<BirefringencePoint>(m, "BirefringencePoint")
+        .def_readonly("fill_x", &BirefringencePoint::fill_x)
+        .def_readonly("fill_y", &BirefringencePoint::fill_y)
+        .def_readonly("phase_x_deg", &BirefringencePoint::phase_x_deg)
+        .def_readonly("phase_y_deg", &BirefringencePoint::phase_y_deg)
+        .def_readonly("retardance_deg", &BirefringencePoint::retardance_deg)
+        .def_readonly("tx", &BirefringencePoint::tx)
+        .def_readonly("ty", &BirefringencePoint::ty);
+    m.def("analyze_birefringence", &analyze_birefringence, py::arg("pillar"), py::arg("background"),
+          py::arg("incident"), py::arg("substrate"), py::arg("period_um"), py::arg("wavelength_um"),
+          py::arg("thickness_um"), py::arg("fill_y"), py::arg("fill_min"), py::arg("fill_max"), py::arg("n_samples"),
+          py::arg("M"));
+    py::class_<SystemOptResult>(m, "SystemOptResult")
+        .def_readonly("period_um", &SystemOptResult::period_um)
+        .def_readonly("thickness_um", &SystemOptResult::thickness_um)
+        .def_readonly("strehl", &SystemOptResult::strehl)
+        .def_readonly("mean_amplitude", &SystemOptResult::mean_amplitude)
+        .def_readonly("merit", &SystemOptResult::merit);
+    m.def("optimize_system", &optimize_system, py::arg("pillar"), py::arg("background"), py::arg("incident"),
+          py::arg("substrate"), py::arg("focal_um"), py::arg("diameter_um"), py::arg("wavelength_um"),
+          py::arg("period_lo"), py::arg("period_hi"), py::arg("thick_lo"), py::arg("thick_hi"), py::arg("grid"),
+          py::arg("M"), py::arg("fill_samples"), py::arg("efficiency_weight"),
+          py::arg("progress") = std::function<void(float)>());
+
     m.def("cuda_available", &cuda::available);
     m.def("cuda_device_name", &cuda::device_name);
 }

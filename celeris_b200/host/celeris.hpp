@@ -344,6 +344,74 @@ PolarMetalensDesign design_polarization_metalens(const PolarizationLibrary& lib,
                                                  double focal_y_um, double diameter_um,
                                                  double amplitude_weight = 0.25);
 
+// design/pb_metalens.hpp:13-70: Jones matrix of a cell, the half-wave-plate atom
+// search, the rotated-atom check and the geometric-phase (PB) metalens.
+struct JonesMatrix {
+    cdouble xx, xy, yx, yy;
+};
+JonesMatrix solve_jones(const Material& incident, const Rcwa2DStack& stack, const Material& substrate,
+                        double wavelength_um, int M);
+struct HwpAtom {
+    double fill_x = 0, fill_y = 0;
+    double thickness_um = 0;
+    cdouble t_x = 0, t_y = 0;
+    double retardance_deg = 0;
+    double conversion_efficiency = 0;
+};
+HwpAtom find_hwp_atom(const Material& pillar, const Material& background, const Material& incident,
+                      const Material& substrate, double period_um, double wavelength_um, double thickness_um,
+                      double fill_min, double fill_max, int n_samples, int M);
+struct PbVerifyPoint {
+    double rotation_deg;
+    double cross_phase_deg;
+    double conversion_eff;
+    double copol_leakage;
+};
+std::vector<PbVerifyPoint> verify_pb_phase(const Material& pillar, const Material& background,
+                                           const Material& incident, const Material& substrate, double period_um,
+                                           double wavelength_um, const HwpAtom& atom,
+                                           const std::vector<double>& rotations_rad, int M);
+struct PbMetalensDesign {
+    int n_cells = 0;
+    double period_um = 0;
+    HwpAtom atom;
+    std::vector<double> rotation_rad;
+    std::vector<cdouble> t_cross;
+    double rms_phase_error_deg = 0;
+    double conversion_efficiency = 0;
+};
+PbMetalensDesign design_pb_metalens(const HwpAtom& atom, double period_um, double wavelength_um,
+                                    const PhaseProfile& profile, double diameter_um, int handedness = +1);
+PbMetalensDesign design_pb_metalens(const HwpAtom& atom, double period_um, double wavelength_um,
+                                    double focal_length_um, double diameter_um, int handedness = +1);
+
+// analysis/polarization.hpp:14-36: x / y phase and retardance of a fill_x sweep.
+struct BirefringencePoint {
+    double fill_x, fill_y;
+    double phase_x_deg, phase_y_deg, retardance_deg;
+    double tx, ty;
+};
+std::vector<BirefringencePoint> analyze_birefringence(const Material& pillar, const Material& background,
+                                                      const Material& incident, const Material& substrate,
+                                                      double period_um, double wavelength_um, double thickness_um,
+                                                      double fill_y, double fill_min, double fill_max,
+                                                      int n_samples, int M);
+
+// design/system_opt.hpp:12-31: period x thickness grid search on Strehl and
+// efficiency; every grid point's library comes from ONE batched RCWA call.
+struct SystemOptResult {
+    double period_um;
+    double thickness_um;
+    double strehl;
+    double mean_amplitude;
+    double merit;
+};
+SystemOptResult optimize_system(const Material& pillar, const Material& background, const Material& incident,
+                                const Material& substrate, double focal_um, double diameter_um,
+                                double wavelength_um, double period_lo, double period_hi, double thick_lo,
+                                double thick_hi, int grid, int M, int fill_samples, double efficiency_weight,
+                                const std::function<void(float)>& progress);
+
 // ---- reference inverse-design gradient (optimize.hpp) --------------------------------
 struct PillarTarget {
     double wavelength_um, target_phase_rad, amplitude_weight;

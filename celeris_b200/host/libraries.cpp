@@ -11,6 +11,10 @@
 //   dispersive PB library           design/pb_achromatic.cpp:47-154
 //   design / verify (PB)            design/pb_achromatic.cpp:156-300
 //   polarization library / design   design/polar_metalens.cpp:23-121
+//   Jones / HWP atom / PB check      design/pb_metalens.cpp:36-104 (rotated atoms in one batch)
+//   PB metalens design              design/pb_metalens.cpp:106-151
+//   birefringence sweep             analysis/polarization.cpp:23-60
+//   system optimisation             design/system_opt.cpp:9-43 (all grid libraries in one batch)
 //
 // The selection costs, grids and reductions follow the reference's formulas so
 // that the libraries and designs are the reference's for the same solver output.
@@ -639,6 +643,201 @@ PolarMetalensDesign design_polarization_metalens(const PolarizationLibrary& lib,
         d.mean_amp_y = ay / cnt;
     }
     return d;
+}
+
+// ---- Jones matrices and the Pancharatnam-Berry metalens (pb_metalens.cpp) -----------------
+namespace {
+double wrap_angle(double a) {
+    while (a > pi) a -= 2.0 * pi;
+    while (a <= -pi) a += 2.0 * pi;
+    return a;
+}
+// (co, cross) circular amplitudes of J applied to right-circular input
+// (pb_metalens.cpp:19-33): e_R = (x - i y)/sqrt2, e_L = (x + i y)/sqrt2.
+void circular_parts(const JonesMatrix& J, cdouble& co, cdouble& cross) {
+    const cdouble I(0.0, 1.0);
+    const double r = 1.0 / std::sqrt(2.0);
+    const cdouble ex = (J.xx - I * J.xy) * r, ey = (J.yx - I * J.yy) * r;
+    co = (ex + I * ey) * r;
+    cross = (ex - I * ey) * r;
+}
+// Columns of the Jones matrix: X (Ex0 = 1) and Y (Ey0 = 1) results of one solve.
+JonesMatrix jones_of(const celeris_rcwa_result& rx, const celeris_rcwa_result& ry) {
+    return {tx_of(rx), tx_of(ry), ty_of(rx), ty_of(ry)};
+}
+}  // namespace
+
+JonesMatrix solve_jones(const Material& incident, const Rcwa2DStack& stack, const Material& substrate,
+                        double wavelength_um, int M) {
+    if (stack.layers.empty()) throw std::invalid_argument("solve_jones: stack has no layers");
+    std::vector<celeris_rcwa_cell> cc;
+    for (const RectCell2D& L : stack.layers)
+        cc.push_back(to_cell(incident, L, substrate, stack.period_x_um, stack.period_y_um, wavelength_um, 0.0, 0.0,
+                             M, M, 0, false));
+    std::vector<celeris_rcwa_result> r(2);
+    if (cc.size() == 1) {
+        check(celeris_rcwa_batch(cc.data(), 1, r.data(), nullptr), "solve_jones");
+    } else {
+        const int start[2] = {0, static_cast<int>(cc.size())};
+        check(celeris_rcwa_stack_batch(cc.data(), start, 1, r.data(), nullptr), "solve_jones");
+    }
+    return jones_of(r[0], r[1]);
+}
+
+HwpAtom find_hwp_atom(const Material& pillar, const Material& background, const Material& incident,
+                      const Material& substrate, double period_um, double wavelength_um, double thickness_um,
+                      double fill_min, double fill_max, int n_samples, int M) {
+    const PolarizationLibrary lib = build_polarization_library(pillar, background, incident, substrate, period_um,
+                                                               wavelength_um, thickness_um, fill_min, fill_max,
+                                                               n_samples, M);
+    HwpAtom best;
+    double best_eff = -1.0;
+    for (const PolarCell& c : lib.cells) {
+        const cdouble tx = std::polar(c.amp_x, c.phase_x), ty = std::polar(c.amp_y, c.phase_y);
+        const double eff = std::norm(tx - ty) / 4.0;  // spin-flip conversion |t_x - t_y|^2 / 4
+        if (eff > best_eff) {
+            best_eff = eff;
+            best.fill_x = c.fill_x;
+            best.fill_y = c.fill_y;
+            best.thickness_um = thickness_um;
+            best.t_x = tx;
+            best.t_y = ty;
+            best.retardance_deg = wrap_angle(c.phase_x - c.phase_y) * 180.0 / pi;
+            best.conversion_efficiency = eff;
+        }
+    }
+    return best;
+}
+
+std::vector<PbVerifyPoint> verify_pb_phase(const Material& pillar, const Material& background,
+                                           const Material& incident, const Material& substrate, double period_um,
+                                           double wavelength_um, const HwpAtom& atom,
+                                           const std::vector<double>& rotations_rad, int M) {
+    std::vector<celeris_rcwa_cell> cc;
+    for (double rot : rotations_rad) {
+        RectCell2D L{pillar, background, atom.fill_x, atom.fill_y, atom.thickness_um, MetaShape::Rectangle, 0.5,
+                     rot};
+        cc.push_back(to_cell(incident, L, substrate, period_um, period_um, wavelength_um, 0.0, 0.0, M, M, 0, false));
+    }
+    const std::vector<celeris_rcwa_result> r = solve_batch(cc, "verify_pb_phase");
+    std::vector<PbVerifyPoint> out(rotations_rad.size());
+    for (size_t i = 0; i < rotations_rad.size(); ++i) {
+        cdouble co, cross;
+        circular_parts(jones_of(r[2 * i], r[2 * i + 1]), co, cross);
+        out[i] = {rotations_rad[i] * 180.0 / pi, std::arg(cross) * 180.0 / pi, std::norm(cross), std::norm(co)};
+    }
+    return out;
+}
+
+PbMetalensDesign design_pb_metalens(const HwpAtom& atom, double period_um, double wavelength_um,
+                                    const PhaseProfile& profile, double diameter_um, int handedness) {
+    const int n = std::max(1, static_cast<int>(std::round(diameter_um / period_um)));
+    const double c = (n - 1) / 2.0;
+    PbMetalensDesign d;
+    d.n_cells = n;
+    d.period_um = period_um;
+    d.atom = atom;
+    const size_t nn = static_cast<size_t>(n) * n;
+    d.rotation_rad.resize(nn);
+    d.t_cross.resize(nn);
+    // geometric phase on the cross output: -2 handedness theta; the atom's own
+    // spin-flip amplitude is a global piston
+    const cdouble a0 = (atom.t_x - atom.t_y) / 2.0;
+    const double piston = std::arg(a0);
+    double e2 = 0.0;
+    int cnt = 0;
+    for (int iy = 0; iy < n; ++iy)
+        for (int ix = 0; ix < n; ++ix) {
+            const double x = (ix - c) * period_um, y = (iy - c) * period_um;
+            const double phi = phase_profile_value(profile, x, y, wavelength_um);
+            const size_t off = static_cast<size_t>(iy) * n + ix;
+            d.rotation_rad[off] = -handedness * phi / 2.0;
+            d.t_cross[off] = a0 * std::polar(1.0, phi);
+            const double err = wrap_angle(std::arg(d.t_cross[off]) - phi - piston);
+            e2 += err * err;
+            ++cnt;
+        }
+    if (cnt) d.rms_phase_error_deg = std::sqrt(e2 / cnt) * 180.0 / pi;
+    d.conversion_efficiency = std::norm(a0);
+    return d;
+}
+
+PbMetalensDesign design_pb_metalens(const HwpAtom& atom, double period_um, double wavelength_um,
+                                    double focal_length_um, double diameter_um, int handedness) {
+    PhaseProfile p;
+    p.kind = PhaseProfileKind::Focusing;
+    p.focal_length_um = focal_length_um;
+    return design_pb_metalens(atom, period_um, wavelength_um, p, diameter_um, handedness);
+}
+
+// ---- birefringence sweep (analysis/polarization.cpp) ------------------------------------------
+std::vector<BirefringencePoint> analyze_birefringence(const Material& pillar, const Material& background,
+                                                      const Material& incident, const Material& substrate,
+                                                      double period_um, double wavelength_um, double thickness_um,
+                                                      double fill_y, double fill_min, double fill_max,
+                                                      int n_samples, int M) {
+    const int ns = std::max(0, n_samples);
+    std::vector<celeris_rcwa_cell> cc(ns);
+    std::vector<double> fx(ns);
+    for (int i = 0; i < ns; ++i) {
+        fx[i] = fill_min + (fill_max - fill_min) * i / (n_samples - 1);
+        RectCell2D L{pillar, background, fx[i], fill_y, thickness_um};
+        cc[i] = to_cell(incident, L, substrate, period_um, period_um, wavelength_um, 0.0, 0.0, M, M, 0, false);
+    }
+    const std::vector<celeris_rcwa_result> r = solve_batch(cc, "analyze_birefringence");
+    auto deg = [](double a) { return wrap_angle(a) * 180.0 / pi; };
+    std::vector<BirefringencePoint> out(ns);
+    for (int i = 0; i < ns; ++i) {
+        const cdouble tx = tx_of(r[2 * i]), ty = ty_of(r[2 * i + 1]);  // co-pol of X and of Y input
+        out[i] = {fx[i], fill_y, deg(std::arg(tx)), deg(std::arg(ty)), deg(std::arg(tx) - std::arg(ty)),
+                  std::abs(tx), std::abs(ty)};
+    }
+    return out;
+}
+
+// ---- period x thickness system optimisation (design/system_opt.cpp) ---------------------------
+SystemOptResult optimize_system(const Material& pillar, const Material& background, const Material& incident,
+                                const Material& substrate, double focal_um, double diameter_um,
+                                double wavelength_um, double period_lo, double period_hi, double thick_lo,
+                                double thick_hi, int grid, int M, int fill_samples, double efficiency_weight,
+                                const std::function<void(float)>& progress) {
+    grid = std::max(2, grid);
+    const int nf = std::max(0, fill_samples);
+    // every grid point's library sweep (fill 0.08 .. 0.92) in one batched call
+    std::vector<celeris_rcwa_cell> cc;
+    cc.reserve(static_cast<size_t>(grid) * grid * nf);
+    auto period_at = [&](int ip) { return period_lo + (period_hi - period_lo) * ip / (grid - 1); };
+    auto thick_at = [&](int it) { return thick_lo + (thick_hi - thick_lo) * it / (grid - 1); };
+    for (int ip = 0; ip < grid; ++ip)
+        for (int it = 0; it < grid; ++it)
+            for (int i = 0; i < nf; ++i) {
+                const double f = 0.08 + (0.92 - 0.08) * i / (nf - 1);
+                RectCell2D L{pillar, background, f, f, thick_at(it), MetaShape::Rectangle, 0.5};
+                cc.push_back(to_cell(incident, L, substrate, period_at(ip), period_at(ip), wavelength_um, 0.0, 0.0,
+                                     M, M, 0, false));
+            }
+    const std::vector<celeris_rcwa_result> r = solve_batch(cc, "optimize_system");
+    SystemOptResult best{period_lo, thick_lo, 0, 0, -1};
+    int done = 0, k = 0;
+    for (int ip = 0; ip < grid; ++ip)
+        for (int it = 0; it < grid; ++it) {
+            UnitCellLibrary lib;
+            lib.period_um = period_at(ip);
+            lib.wavelength_um = wavelength_um;
+            lib.thickness_um = thick_at(it);
+            for (int i = 0; i < nf; ++i, ++k) {
+                const cdouble t = tx_of(r[2 * static_cast<size_t>(k)]);
+                lib.fill.push_back(0.08 + (0.92 - 0.08) * i / (nf - 1));
+                lib.phase.push_back(std::arg(t));
+                lib.amplitude.push_back(std::abs(t));
+            }
+            const MetalensDesign lens = design_metalens(lib, focal_um, diameter_um);
+            const FocalAnalysis foc = analyze_focus(lens, lib, focal_um, wavelength_um, diameter_um);
+            const double merit = foc.strehl + efficiency_weight * lens.mean_amplitude;
+            if (merit > best.merit) best = {lib.period_um, lib.thickness_um, foc.strehl, lens.mean_amplitude, merit};
+            if (progress) progress(static_cast<float>(++done) / (grid * grid));
+        }
+    return best;
 }
 
 }  // namespace celeris

@@ -2,8 +2,9 @@
 
 ctypes access to oracle/_ref/libref_library.so: the REFERENCE's own library
 builders, designs and on-axis focus checks (src/celeris/design/achromatic.cpp,
-pb_achromatic.cpp, polar_metalens.cpp, metalens.cpp:71-110) compiled from the
-reference tree by oracle/Makefile. The reference's cell solve (rcwa2d.cpp) needs
+pb_achromatic.cpp, polar_metalens.cpp, pb_metalens.cpp, system_opt.cpp,
+metalens.cpp:71-110, analysis/polarization.cpp) compiled from the reference tree
+by oracle/Makefile. The reference's cell solve (rcwa2d.cpp) needs
 Eigen, which is absent; the shim forwards every solve_rcwa_2d call to the numpy
 restatement `oracle.rcwa.solve` through a callback registered here. So the
 outputs are the reference's builder code over the oracle's cell solves.
@@ -206,3 +207,67 @@ def polarization_design(period, wavelength, cells, fx_um, fy_um, d_um, amp_weigh
     lib.ref_polarization_design(f(period), f(wavelength), pC, len(cells), f(fx_um), f(fy_um), f(d_um),
                                 f(amp_weight), fills.ctypes.data_as(_P), metrics.ctypes.data_as(_P))
     return fills.reshape(n * n, 2), metrics
+
+
+def solve_jones(indices, period, fill_x, fill_y, thickness, rotation, wavelength, M):
+    lib = load()
+    mats, pm = _d(_mats(*indices))
+    out = np.zeros(8)
+    f = ctypes.c_double
+    lib.ref_solve_jones(pm, f(period), f(fill_x), f(fill_y), f(thickness), f(rotation), f(wavelength), M,
+                        out.ctypes.data_as(_P))
+    return out[0::2] + 1j * out[1::2]  # xx, xy, yx, yy
+
+
+def find_hwp_atom(indices, period, wavelength, thickness, fill_min, fill_max, n_samples, M):
+    lib = load()
+    mats, pm = _d(_mats(*indices))
+    out = np.zeros(9)
+    f = ctypes.c_double
+    lib.ref_find_hwp_atom(pm, f(period), f(wavelength), f(thickness), f(fill_min), f(fill_max), n_samples, M,
+                          out.ctypes.data_as(_P))
+    return dict(fill_x=out[0], fill_y=out[1], thickness=out[2], t_x=complex(out[3], out[4]),
+                t_y=complex(out[5], out[6]), retardance=out[7], efficiency=out[8])
+
+
+def verify_pb_phase(indices, period, wavelength, fill_x, fill_y, thickness, rotations, M):
+    lib = load()
+    mats, pm = _d(_mats(*indices))
+    r, pr = _d(rotations)
+    out = np.zeros(4 * len(rotations))
+    f = ctypes.c_double
+    lib.ref_verify_pb_phase(pm, f(period), f(wavelength), f(fill_x), f(fill_y), f(thickness), pr, len(rotations), M,
+                            out.ctypes.data_as(_P))
+    return out.reshape(-1, 4)
+
+
+def design_pb_metalens(t_x, t_y, period, wavelength, f_um, d_um, handedness):
+    lib = load()
+    tx, ptx = _d([complex(t_x).real, complex(t_x).imag])
+    ty, pty = _d([complex(t_y).real, complex(t_y).imag])
+    n = max(1, int(round(d_um / period)))
+    rot, tc, met = np.zeros(n * n), np.zeros(2 * n * n), np.zeros(2)
+    f = ctypes.c_double
+    lib.ref_design_pb_metalens(ptx, pty, f(period), f(wavelength), f(f_um), f(d_um), handedness,
+                               rot.ctypes.data_as(_P), tc.ctypes.data_as(_P), met.ctypes.data_as(_P))
+    return rot, tc[0::2] + 1j * tc[1::2], met
+
+
+def analyze_birefringence(indices, period, wavelength, thickness, fill_y, fill_min, fill_max, n_samples, M):
+    lib = load()
+    mats, pm = _d(_mats(*indices))
+    out = np.zeros(7 * n_samples)
+    f = ctypes.c_double
+    lib.ref_analyze_birefringence(pm, f(period), f(wavelength), f(thickness), f(fill_y), f(fill_min), f(fill_max),
+                                  n_samples, M, out.ctypes.data_as(_P))
+    return out.reshape(-1, 7)
+
+
+def optimize_system(indices, f_um, d_um, wavelength, p_lo, p_hi, t_lo, t_hi, grid, M, fill_samples, eff_weight):
+    lib = load()
+    mats, pm = _d(_mats(*indices))
+    out = np.zeros(5)
+    f = ctypes.c_double
+    lib.ref_optimize_system(pm, f(f_um), f(d_um), f(wavelength), f(p_lo), f(p_hi), f(t_lo), f(t_hi), grid, M,
+                            fill_samples, f(eff_weight), out.ctypes.data_as(_P))
+    return out

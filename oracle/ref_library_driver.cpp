@@ -2,7 +2,8 @@
 //
 // A C-ABI shim over the REFERENCE's own library builders, designs and on-axis
 // focus checks (src/celeris/design/achromatic.cpp, pb_achromatic.cpp,
-// polar_metalens.cpp, metalens.cpp), compiled from the sources where they lie by
+// polar_metalens.cpp, pb_metalens.cpp, system_opt.cpp, metalens.cpp,
+// analysis/polarization.cpp, focal.cpp), compiled from the sources where they lie by
 // oracle/Makefile into oracle/_ref/libref_library.so. The reference's RCWA
 // (rcwa2d.cpp) needs Eigen, which is absent, so this file supplies
 // celeris::solve_rcwa_2d itself: it forwards every solve to a callback that the
@@ -17,6 +18,9 @@
 #include "celeris/design/achromatic.hpp"
 #include "celeris/design/metalens.hpp"
 #include "celeris/design/pb_achromatic.hpp"
+#include "celeris/design/pb_metalens.hpp"
+#include "celeris/design/system_opt.hpp"
+#include "celeris/analysis/polarization.hpp"
 #include "celeris/design/polar_metalens.hpp"
 #include "celeris/rcwa/rcwa2d.hpp"
 
@@ -290,4 +294,94 @@ REF_API int ref_polarization_design(double period_um, double wavelength_um, cons
     const double m[4] = {d.rms_phase_error_x_deg, d.rms_phase_error_y_deg, d.mean_amp_x, d.mean_amp_y};
     for (int k = 0; k < 4; ++k) out_metrics[k] = m[k];
     return d.n_cells;
+}
+
+// Rectangle cell with constant indices: mats = pillar, background, incident, substrate (re, im each).
+// solve_jones: out = xx, xy, yx, yy (re, im each).
+REF_API int ref_solve_jones(const double* mats, double period_um, double fill_x, double fill_y, double thickness_um,
+                            double rotation_rad, double wavelength_um, int M, double* out) {
+    celeris::RectCell2D cell{mat(mats), mat(mats + 2), fill_x, fill_y, thickness_um, celeris::MetaShape::Rectangle,
+                             0.5, rotation_rad};
+    const celeris::Rcwa2DStack st{period_um, period_um, {cell}};
+    const auto J = celeris::solve_jones(mat(mats + 4), st, mat(mats + 6), wavelength_um, M);
+    const cd v[4] = {J.xx, J.xy, J.yx, J.yy};
+    for (int i = 0; i < 4; ++i) {
+        out[2 * i] = v[i].real();
+        out[2 * i + 1] = v[i].imag();
+    }
+    return 0;
+}
+
+// find_hwp_atom: out = fill_x, fill_y, thickness, t_x (2), t_y (2), retardance, efficiency.
+REF_API int ref_find_hwp_atom(const double* mats, double period_um, double wavelength_um, double thickness_um,
+                              double fill_min, double fill_max, int n_samples, int M, double* out) {
+    const auto a = celeris::find_hwp_atom(mat(mats), mat(mats + 2), mat(mats + 4), mat(mats + 6), period_um,
+                                          wavelength_um, thickness_um, fill_min, fill_max, n_samples, M);
+    const double v[9] = {a.fill_x, a.fill_y, a.thickness_um, a.t_x.real(), a.t_x.imag(), a.t_y.real(),
+                         a.t_y.imag(), a.retardance_deg, a.conversion_efficiency};
+    for (int i = 0; i < 9; ++i) out[i] = v[i];
+    return 0;
+}
+
+// verify_pb_phase for an atom (fill_x, fill_y, thickness): 4 doubles per rotation.
+REF_API int ref_verify_pb_phase(const double* mats, double period_um, double wavelength_um, double fill_x,
+                                double fill_y, double thickness_um, const double* rot, int nrot, int M, double* out) {
+    celeris::HwpAtom a;
+    a.fill_x = fill_x;
+    a.fill_y = fill_y;
+    a.thickness_um = thickness_um;
+    const auto pts = celeris::verify_pb_phase(mat(mats), mat(mats + 2), mat(mats + 4), mat(mats + 6), period_um,
+                                              wavelength_um, a, std::vector<double>(rot, rot + nrot), M);
+    for (int i = 0; i < nrot; ++i) {
+        const double v[4] = {pts[i].rotation_deg, pts[i].cross_phase_deg, pts[i].conversion_eff,
+                             pts[i].copol_leakage};
+        for (int k = 0; k < 4; ++k) out[4 * i + k] = v[k];
+    }
+    return 0;
+}
+
+// design_pb_metalens (focusing) for an atom given by t_x, t_y: out_rot n^2, out_t n^2 (re, im),
+// out_metrics = rms phase error, conversion efficiency; returns n.
+REF_API int ref_design_pb_metalens(const double* tx, const double* ty, double period_um, double wavelength_um,
+                                   double f_um, double d_um, int handedness, double* out_rot, double* out_t,
+                                   double* out_metrics) {
+    celeris::HwpAtom a;
+    a.t_x = cd(tx[0], tx[1]);
+    a.t_y = cd(ty[0], ty[1]);
+    const auto d = celeris::design_pb_metalens(a, period_um, wavelength_um, f_um, d_um, handedness);
+    for (size_t i = 0; i < d.rotation_rad.size(); ++i) {
+        out_rot[i] = d.rotation_rad[i];
+        out_t[2 * i] = d.t_cross[i].real();
+        out_t[2 * i + 1] = d.t_cross[i].imag();
+    }
+    out_metrics[0] = d.rms_phase_error_deg;
+    out_metrics[1] = d.conversion_efficiency;
+    return d.n_cells;
+}
+
+// analyze_birefringence: 7 doubles per sample.
+REF_API int ref_analyze_birefringence(const double* mats, double period_um, double wavelength_um,
+                                      double thickness_um, double fill_y, double fill_min, double fill_max,
+                                      int n_samples, int M, double* out) {
+    const auto pts = celeris::analyze_birefringence(mat(mats), mat(mats + 2), mat(mats + 4), mat(mats + 6),
+                                                    period_um, wavelength_um, thickness_um, fill_y, fill_min,
+                                                    fill_max, n_samples, M);
+    for (size_t i = 0; i < pts.size(); ++i) {
+        const auto& p = pts[i];
+        const double v[7] = {p.fill_x, p.fill_y, p.phase_x_deg, p.phase_y_deg, p.retardance_deg, p.tx, p.ty};
+        for (int k = 0; k < 7; ++k) out[7 * i + k] = v[k];
+    }
+    return static_cast<int>(pts.size());
+}
+
+// optimize_system: out = period, thickness, strehl, mean amplitude, merit.
+REF_API int ref_optimize_system(const double* mats, double f_um, double d_um, double wavelength_um, double p_lo,
+                                double p_hi, double t_lo, double t_hi, int grid, int M, int fill_samples,
+                                double eff_weight, double* out) {
+    const auto r = celeris::optimize_system(mat(mats), mat(mats + 2), mat(mats + 4), mat(mats + 6), f_um, d_um,
+                                            wavelength_um, p_lo, p_hi, t_lo, t_hi, grid, M, fill_samples, eff_weight,
+                                            nullptr);
+    const double v[5] = {r.period_um, r.thickness_um, r.strehl, r.mean_amplitude, r.merit};
+    for (int k = 0; k < 5; ++k) out[k] = v[k];
+    return 0;
 }

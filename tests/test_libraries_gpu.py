@@ -194,3 +194,65 @@ def test_pb_achromatic_design_and_focus_scan():
         for g, w in zip(focus, wf):
             assert g.focal_length_um == pytest.approx(w[1], abs=1e-9)
             assert g.rel_peak == pytest.approx(w[2], rel=1e-9)
+
+
+def test_jones_hwp_atom_and_rotated_pb_check():
+    """solve_jones, find_hwp_atom and verify_pb_phase (pb_metalens.cpp:36-104):
+    the rotated atoms run the Laurent path with rotation, all in one batch."""
+    import celeris_b200 as cel
+
+    pil, bg, inc, sub = mats(cel)
+    st = cel.Rcwa2DStack(0.4, 0.4, [cel.RectCell2D(pil, bg, 0.7, 0.3, 0.6)])
+    J = cel.solve_jones(inc, st, sub, 0.633, 3)
+    Jw = OL.solve_jones((N_PIL, N_BG, N_INC, N_SUB), 0.4, 0.7, 0.3, 0.6, 0.0, 0.633, 3)
+    got = np.array([J.xx, J.xy, J.yx, J.yy])
+    assert np.max(np.abs(got - Jw)) <= 1e-10 * np.max(np.abs(Jw))
+    a = cel.find_hwp_atom(pil, bg, inc, sub, 0.4, 0.633, 0.6, 0.2, 0.8, 4, 3)
+    aw = OL.find_hwp_atom((N_PIL, N_BG, N_INC, N_SUB), 0.4, 0.633, 0.6, 0.2, 0.8, 4, 3)
+    assert (a.fill_x, a.fill_y) == (aw["fill_x"], aw["fill_y"])
+    assert abs(a.t_x - aw["t_x"]) <= 1e-9 and abs(a.t_y - aw["t_y"]) <= 1e-9
+    assert a.conversion_efficiency == pytest.approx(aw["efficiency"], abs=1e-9)
+    assert a.retardance_deg == pytest.approx(aw["retardance"], abs=1e-7)
+    rots = [0.0, 0.3, 0.7, 1.2]
+    v = cel.verify_pb_phase(pil, bg, inc, sub, 0.4, 0.633, a, rots, 2)
+    vw = OL.verify_pb_phase((N_PIL, N_BG, N_INC, N_SUB), 0.4, 0.633, a.fill_x, a.fill_y, 0.6, rots, 2)
+    for g, w in zip(v, vw):
+        assert g.rotation_deg == w[0]
+        assert abs((g.cross_phase_deg - w[1] + 180) % 360 - 180) <= 1e-6
+        assert g.conversion_eff == pytest.approx(w[2], abs=1e-9)
+        assert g.copol_leakage == pytest.approx(w[3], abs=1e-9)
+    # geometric-phase lens from the atom (host only)
+    d = cel.design_pb_metalens(a, 0.4, 0.633, 20.0, 8.0, -1)
+    rot, tc, met = OL.design_pb_metalens(a.t_x, a.t_y, 0.4, 0.633, 20.0, 8.0, -1)
+    assert np.max(np.abs(np.asarray(d.rotation_rad) - rot)) <= 1e-12
+    assert np.max(np.abs(np.asarray(d.t_cross) - tc)) <= 1e-12
+    assert d.conversion_efficiency == pytest.approx(met[1], rel=1e-12)
+    assert d.rms_phase_error_deg == pytest.approx(met[0], abs=1e-9)
+
+
+def test_birefringence_sweep():
+    import celeris_b200 as cel
+
+    got = cel.analyze_birefringence(*mats(cel), 0.4, 0.633, 0.6, 0.35, 0.2, 0.8, 5, 3)
+    want = OL.analyze_birefringence((N_PIL, N_BG, N_INC, N_SUB), 0.4, 0.633, 0.6, 0.35, 0.2, 0.8, 5, 3)
+    for g, w in zip(got, want):
+        assert (g.fill_x, g.fill_y) == (w[0], w[1])
+        for a, b in ((g.phase_x_deg, w[2]), (g.phase_y_deg, w[3]), (g.retardance_deg, w[4])):
+            assert abs((a - b + 180) % 360 - 180) <= 1e-6
+        assert g.tx == pytest.approx(w[5], abs=1e-9) and g.ty == pytest.approx(w[6], abs=1e-9)
+
+
+def test_optimize_system_grid():
+    """optimize_system (system_opt.cpp): a 2 x 2 period x thickness grid, every
+    library from one batched call, then design + focal analysis per point."""
+    import celeris_b200 as cel
+
+    calls = []
+    got = cel.optimize_system(*mats(cel), 30.0, 10.0, 0.633, 0.35, 0.45, 0.5, 0.7, 2, 2, 12, 0.3,
+                              lambda x: calls.append(x))
+    want = OL.optimize_system((N_PIL, N_BG, N_INC, N_SUB), 30.0, 10.0, 0.633, 0.35, 0.45, 0.5, 0.7, 2, 2, 12, 0.3)
+    assert (got.period_um, got.thickness_um) == (want[0], want[1])
+    assert got.strehl == pytest.approx(want[2], rel=1e-6)
+    assert got.mean_amplitude == pytest.approx(want[3], abs=1e-9)
+    assert got.merit == pytest.approx(want[4], rel=1e-6)
+    assert calls == pytest.approx([0.25, 0.5, 0.75, 1.0])

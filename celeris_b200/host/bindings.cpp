@@ -275,6 +275,14 @@ PYBIND11_MODULE(_celeris, m) {
     m.def("analyze_through_focus", &analyze_through_focus, py::arg("lens"), py::arg("lib"),
           py::arg("focal_length_um"), py::arg("wavelength_um"), py::arg("diameter_um"));
 
+    py::class_<ToleranceResult>(m, "ToleranceResult")
+        .def_readonly("sigma_nm", &ToleranceResult::sigma_nm)
+        .def_readonly("mean_strehl", &ToleranceResult::mean_strehl)
+        .def_readonly("std_strehl", &ToleranceResult::std_strehl)
+        .def_readonly("worst_strehl", &ToleranceResult::worst_strehl);
+    m.def("analyze_tolerance", &analyze_tolerance, py::arg("lens"), py::arg("lib"), py::arg("focal_length_um"),
+          py::arg("wavelength_um"), py::arg("diameter_um"), py::arg("sigmas_nm"), py::arg("trials"),
+          py::arg("seed"));
     py::class_<ChromaticPoint>(m, "ChromaticPoint")
         .def_readonly("wavelength_um", &ChromaticPoint::wavelength_um)
         .def_readonly("focal_length_um", &ChromaticPoint::focal_length_um)

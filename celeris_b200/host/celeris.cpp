@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <fstream>
+#include <random>
 #include <sstream>
 #include <stdexcept>
 
@@ -714,6 +715,32 @@ FieldPsf compute_psf_field(const MetalensDesign& lens, const UnitCellLibrary& li
 }
 
 // ---- through-focus (throughfocus.cpp:15-135) -------------------------------------------------
+// ---- fabrication tolerance (tolerance.cpp) --------------------------------------------------
+std::vector<ToleranceResult> analyze_tolerance(const MetalensDesign& lens, const UnitCellLibrary& lib,
+                                               double focal_length_um, double wavelength_um, double diameter_um,
+                                               const std::vector<double>& sigmas_nm, int trials, unsigned seed) {
+    std::vector<ToleranceResult> out;
+    for (double sigma_nm : sigmas_nm) {
+        const double sigma_fill = (sigma_nm / 1000.0) / lens.period_um;  // CD error -> fill fraction
+        const int n = std::max(1, trials);
+        double sum = 0.0, sum2 = 0.0, worst = 1e300;
+        for (int t = 0; t < n; ++t) {
+            // per-trial stream as tolerance.cpp:26-31
+            std::mt19937 rng(seed + static_cast<unsigned>(t) * 7919u + static_cast<unsigned>(sigma_nm * 13.0));
+            std::normal_distribution<double> g(0.0, sigma_fill);
+            MetalensDesign perturbed = lens;
+            for (double& f : perturbed.fill_map) f = std::clamp(f + g(rng), 0.05, 0.95);
+            const double s = analyze_focus(perturbed, lib, focal_length_um, wavelength_um, diameter_um).strehl;
+            sum += s;
+            sum2 += s * s;
+            worst = std::min(worst, s);
+        }
+        const double mean = sum / n;
+        out.push_back({sigma_nm, mean, std::sqrt(std::max(0.0, sum2 / n - mean * mean)), worst});
+    }
+    return out;
+}
+
 // ---- chromatic focal shift (chromatic.cpp) -------------------------------------------------
 namespace {
 // First maximum of a 120-point on-axis scan over [0.55, 1.6] x f0 lambda0 / lambda

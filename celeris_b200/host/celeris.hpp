@@ -448,6 +448,17 @@ FieldPsf compute_psf_field(const MetalensDesign& lens, const UnitCellLibrary& li
                            double wavelength_um, double diameter_um, double angle_deg, int n,
                            double half_window_um, double on_axis_peak = 0.0);
 
+// ---- fabrication tolerance (tolerance.hpp:12-27) ------------------------------------------
+// Monte-Carlo Strehl under Gaussian pillar-size errors: the reference's seeds,
+// generator (std::mt19937) and std::normal_distribution, each trial one GPU
+// focal analysis.
+struct ToleranceResult {
+    double sigma_nm, mean_strehl, std_strehl, worst_strehl;
+};
+std::vector<ToleranceResult> analyze_tolerance(const MetalensDesign& lens, const UnitCellLibrary& lib,
+                                               double focal_length_um, double wavelength_um, double diameter_um,
+                                               const std::vector<double>& sigmas_nm, int trials, unsigned seed);
+
 // ---- through-focus and off-axis analyses (callers of the far field) ----------------------
 // chromatic.hpp:10-34: on-axis focus search (120 z samples around f0 lambda0 / lambda)
 // per wavelength; the dispersive form rebuilds the library at every wavelength.

@@ -179,3 +179,14 @@ def ref_chromatic(lens_args, f, wl, D, lam_min, lam_max, n):
     out = np.zeros((n, 3))
     r.ref_chromatic(*args, _D(f), _D(wl), _D(D), _D(lam_min), _D(lam_max), ctypes.c_int(n), _dp(out))
     return out
+
+
+def ref_tolerance(lens_args, f, wl, D, sigmas, trials, seed):
+    """celeris::analyze_tolerance (tolerance.cpp, CPU): rows (sigma, mean, std, worst Strehl)."""
+    r = _ref_or_raise()
+    args, keep = _lens_args(*lens_args)
+    sg = _f64(sigmas)
+    out = np.zeros((len(sigmas), 4))
+    r.ref_tolerance(*args, _D(f), _D(wl), _D(D), _dp(sg), ctypes.c_int(len(sigmas)), ctypes.c_int(trials),
+                    ctypes.c_uint(seed), _dp(out))
+    return out

@@ -14,6 +14,7 @@
 
 #include "celeris/analysis/chromatic.hpp"
 #include "celeris/analysis/field.hpp"
+#include "celeris/analysis/tolerance.hpp"
 #include "celeris/analysis/focal.hpp"
 #include "celeris/analysis/throughfocus.hpp"
 
@@ -135,4 +136,21 @@ REF_API int ref_chromatic(int n_cells, double period_um, const double* fill_map,
         out[3 * i + 2] = pts[i].rel_peak;
     }
     return static_cast<int>(pts.size());
+}
+
+// celeris::analyze_tolerance (tolerance.cpp, CPU): rows (sigma, mean, std, worst Strehl).
+REF_API int ref_tolerance(int n_cells, double period_um, const double* fill_map, int nlib, const double* lfill,
+                          const double* lphase, const double* lamp, double lib_wl, double f, double wl, double D,
+                          const double* sigmas, int nsig, int trials, unsigned seed, double* out) {
+    const auto lens = make_lens(n_cells, period_um, fill_map);
+    const auto lib = make_lib(period_um, lib_wl, 0.0, nlib, lfill, lphase, lamp);
+    const auto r = celeris::analyze_tolerance(lens, lib, f, wl, D, std::vector<double>(sigmas, sigmas + nsig),
+                                              trials, seed);
+    for (size_t i = 0; i < r.size(); ++i) {
+        out[4 * i] = r[i].sigma_nm;
+        out[4 * i + 1] = r[i].mean_strehl;
+        out[4 * i + 2] = r[i].std_strehl;
+        out[4 * i + 3] = r[i].worst_strehl;
+    }
+    return static_cast<int>(r.size());
 }

@@ -152,3 +152,15 @@ def test_chromatic_dispersive_with_per_wavelength_libraries():
         j = int(np.argmax(I))  # first maximum, as the reference's strict > scan
         assert g.focal_length_um == pytest.approx(0.55 * exp + (1.6 * exp - 0.55 * exp) * j / 119, abs=1e-9)
         assert g.rel_peak == pytest.approx(I[j] / peak0, rel=1e-9)
+
+
+def test_tolerance_monte_carlo_matches_reference():
+    """analyze_tolerance (tolerance.cpp): same seeds, generator and normal
+    distribution, each trial a focal analysis on the GPU."""
+    cel, lib, lens, args = lens_and_lib()
+    got = cel.analyze_tolerance(lens, lib, F_UM, WL, D_UM, [5.0, 25.0], 3, 7)
+    want = F.ref_tolerance(args, F_UM, WL, D_UM, [5.0, 25.0], 3, 7)
+    for g, w in zip(got, want):
+        assert g.sigma_nm == w[0]
+        assert [g.mean_strehl, g.worst_strehl] == pytest.approx([w[1], w[3]], rel=1e-6)
+        assert g.std_strehl == pytest.approx(w[2], rel=1e-4, abs=1e-7)

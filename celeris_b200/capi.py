@@ -53,7 +53,7 @@ EXPORTED = [
     "celeris_probe_peaks", "celeris_set_kernel_timing", "celeris_last_kernel_ms",
     "celeris_rs_field_noalloc", "celeris_probe_sincos", "celeris_rcwa_tuning_report",
     "celeris_probe_dmma", "celeris_solve_rcwa_2d_stack", "celeris_rcwa_stack_batch",
-    "celeris_solve_rcwa_2d_orders",
+    "celeris_solve_rcwa_2d_orders", "celeris_eig_general", "celeris_eig_general_batch",
 ]
 
 
@@ -135,6 +135,8 @@ def load(path: str = LIB_PATH):
         "celeris_rcwa_tuning_report": (_I, [ctypes.c_char_p, _I]),
         "celeris_solve_rcwa_2d_stack": (_I, [ctypes.POINTER(RcwaCell), _I, _P, _P, ctypes.POINTER(RcwaResult)]),
         "celeris_rcwa_stack_batch": (_I, [ctypes.POINTER(RcwaCell), _PI, _I, ctypes.POINTER(RcwaResult), _PI]),
+        "celeris_eig_general": (_I, [_P, _I, _P, _P]),
+        "celeris_eig_general_batch": (_I, [_P, _I, _I, _P, _P, _PI]),
         "celeris_solve_rcwa_2d_orders": (_I, [ctypes.POINTER(RcwaCell), _I, _P, _P, ctypes.POINTER(RcwaResult),
                                               ctypes.POINTER(RcwaOrder), _I]),
     }
@@ -316,3 +318,20 @@ def solve_rcwa_2d_orders(layers, Ex0=1.0 + 0j, Ey0=0.0 + 0j) -> tuple[dict, list
     check(load().celeris_solve_rcwa_2d_orders(arr, n, _dp(ex), _dp(ey), ctypes.byref(out), orders, N))
     return result_dict(out), [dict(p=o.p, q=o.q, de_t=o.de_t, de_r=o.de_r, prop_t=bool(o.prop_t),
                                    prop_r=bool(o.prop_r)) for o in orders]
+
+
+def eig_general(A):
+    """Eigenpairs of one complex matrix or a stack [count, n, n]: (evals, evecs, info),
+    evecs[..., :, i] the unit-norm eigenvector of evals[..., i]."""
+    A = np.asarray(A, dtype=np.complex128)
+    single = A.ndim == 2
+    A3 = A[None] if single else A
+    count, n = A3.shape[0], A3.shape[1]
+    colmajor = np.ascontiguousarray(np.transpose(A3, (0, 2, 1)))  # Fortran order per matrix
+    vals = np.zeros((count, n), dtype=np.complex128)
+    vecs = np.zeros((count, n, n), dtype=np.complex128)  # column-major per matrix: [count, col, row]
+    info = np.zeros(count, dtype=np.int32)
+    check(load().celeris_eig_general_batch(_dp(colmajor.view(np.float64)), n, count, _dp(vals.view(np.float64)),
+                                           _dp(vecs.view(np.float64)), info.ctypes.data_as(_PI)))
+    vecs = np.transpose(vecs, (0, 2, 1))
+    return (vals[0], vecs[0], info[0]) if single else (vals, vecs, info)

@@ -811,6 +811,52 @@ __global__ void __launch_bounds__(kRT) rcwa_stack_smat(StackBucket sb) {
     if (tid == 0 && status != 0) sb.info[st] = -status;
 }
 
+// ---- standalone eigensolve (eig.hpp:25) ------------------------------------------------------
+// The RCWA eigen-stages on caller matrices: eig_load transposes a column-major
+// (Eigen / LAPACK) matrix into the row-major H of its cell; eig_store writes the
+// eigenvalues (diagonal of the Schur form) and the eigenvectors W = Z X in
+// column-major order, each scaled to unit 2-norm with its largest-magnitude
+// component real and positive (zgeev's normalisation).
+__global__ void __launch_bounds__(kRT) eig_load(const cplx* __restrict__ A, Bucket b) {
+    const int cell = blockIdx.x, n = b.n;
+    const cplx* src = A + b.s_nn * cell;
+    cplx* H = at(b.H, b.s_nn, cell);
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int i = e / n, j = e % n;
+        H[e] = src[(size_t)j * n + i];
+    }
+}
+
+__global__ void __launch_bounds__(kRT) eig_store(Bucket b, cplx* __restrict__ evals, cplx* __restrict__ evecs) {
+    __shared__ RedScratch rs;
+    const int cell = blockIdx.x, n = b.n;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const cplx* H = at(b.H, b.s_nn, cell);
+    const cplx* W = at(b.W, b.s_nn, cell);
+    cplx* out = evecs + b.s_nn * cell;
+    for (int i = tid; i < n; i += nt) evals[(size_t)cell * n + i] = H[(size_t)i * n + i];
+    for (int j = 0; j < n; ++j) {
+        double s2 = 0.0, big = -1.0;
+        int arg = 0;
+        for (int i = tid; i < n; i += nt) {
+            const double m2 = cnorm2(W[(size_t)i * n + j]);
+            s2 += m2;
+            if (m2 > big) {
+                big = m2;
+                arg = i;
+            }
+        }
+        const double tot = blk_sum(s2, &rs);
+        const int imax = blk_argmax(big, arg, &rs);
+        const cplx wm = W[(size_t)imax * n + j];
+        const double am = cabs(wm);
+        // conj(phase of the largest component) / norm
+        const cplx sc = am > 0.0 && tot > 0.0 ? cscale(cconj(wm), 1.0 / (am * sqrt(tot))) : C(1.0, 0.0);
+        for (int i = tid; i < n; i += nt) out[(size_t)j * n + i] = cmul(W[(size_t)i * n + j], sc);
+        __syncthreads();
+    }
+}
+
 // ---- flux and order-0 field (rcwa2d.cpp:416-463) ---------------------------------------------
 __global__ void __launch_bounds__(kRT) rcwa_epilogue(Bucket b) {
     __shared__ RedScratch rs;
@@ -1699,6 +1745,71 @@ int validate_stack(const celeris_rcwa_cell* l, int nl) {
     return CELERIS_OK;
 }
 
+// ---- standalone eigensolve: batches of n x n matrices through the eigen-stages ------------
+int run_eig(const double* A, int n, int count, double* evals, double* evecs, int* info_out) {
+    CEL_TRY(celeris_rt::require_device());
+    const size_t s_nn = (size_t)n * n, s_n = (size_t)n;
+    cudaStream_t st = nullptr;
+    CEL_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } sg{st};
+    if (n <= kSmemEigMaxN)
+        CEL_CUDA(cudaFuncSetAttribute(rcwa_hess<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)((s_nn + 2 * s_n) * sizeof(cplx))));
+    else
+        CEL_CUDA(cudaFuncSetAttribute(rcwa_hess<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)hess_stage_bytes(n)));
+    CEL_CUDA(cudaFuncSetAttribute(rcwa_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSchurSmemOneCta));
+    size_t free_b = 0, total_b = 0;
+    CEL_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t per = (7 * s_nn + 2 * s_n) * sizeof(cplx) + 4096;
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)count, (free_b / 2) / per));
+    for (int c0 = 0; c0 < count; c0 += chunk) {
+        const int nc = std::min(chunk, count - c0);
+        DevBuf mem;
+        Bucket b;
+        std::memset(&b, 0, sizeof(b));
+        b.n = n;
+        b.N = n / 2;
+        b.ncell = nc;
+        b.s_nn = s_nn;
+        b.s_n = s_n;
+        cplx *dA, *dval, *dvec;
+        CEL_TRY(mem.get(&dA, s_nn * nc));
+        cplx** mats[] = {&b.H, &b.Z, &b.X, &b.W, &b.A};
+        for (cplx** m : mats) CEL_TRY(mem.get(m, s_nn * nc));
+        CEL_TRY(mem.get(&b.q1, s_n * nc));
+        CEL_TRY(mem.get(&b.info, (size_t)nc));
+        CEL_TRY(mem.get(&dval, s_n * nc));
+        dvec = b.A;  // free after the eigenvectors
+        CEL_CUDA(cudaMemcpyAsync(dA, A + 2 * s_nn * c0, sizeof(cplx) * s_nn * nc, cudaMemcpyHostToDevice, st));
+        CEL_CUDA(cudaMemsetAsync(b.info, 0, sizeof(int) * nc, st));
+        eig_load<<<nc, kRT, 0, st>>>(dA, b);
+        if (n <= kSmemEigMaxN)
+            rcwa_hess<true><<<nc, kRT, (s_nn + 2 * s_n) * sizeof(cplx), st>>>(b);
+        else
+            rcwa_hess<false><<<nc, kRT, hess_stage_bytes(n), st>>>(b);
+        rcwa_schur<<<nc, kSchurThreads, schur_smem(nc), st>>>(b);
+        rcwa_vec<<<nc, kRT, 0, st>>>(b);
+        eig_store<<<nc, kRT, 0, st>>>(b, dval, dvec);
+        count_launch(6);
+        CEL_CUDA(cudaGetLastError());
+        std::vector<int> hinfo(nc);
+        CEL_CUDA(cudaMemcpyAsync(evals + 2 * s_n * c0, dval, sizeof(cplx) * s_n * nc, cudaMemcpyDeviceToHost, st));
+        CEL_CUDA(cudaMemcpyAsync(evecs + 2 * s_nn * c0, dvec, sizeof(cplx) * s_nn * nc, cudaMemcpyDeviceToHost, st));
+        CEL_CUDA(cudaMemcpyAsync(hinfo.data(), b.info, sizeof(int) * nc, cudaMemcpyDeviceToHost, st));
+        CEL_CUDA(cudaStreamSynchronize(st));
+        for (int i = 0; i < nc; ++i) {
+            if (info_out) info_out[c0 + i] = hinfo[i];
+            else if (hinfo[i] != 0)
+                return set_error(CELERIS_ERR_EIG_NOCONV, "QR did not converge (info %d)", hinfo[i]);
+        }
+    }
+    return CELERIS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1733,6 +1844,28 @@ int celeris_solve_rcwa_2d_stack(const celeris_rcwa_cell* layers, int nlayers, co
     CEL_TRY(validate_stack(layers, nlayers));
     const double exc[4] = {Ex0[0], Ex0[1], Ey0[0], Ey0[1]};
     return run_stacks(layers, {{0, nlayers}}, exc, out, nullptr, 1);
+}
+
+int celeris_eig_general_batch(const double* A, int n, int count, double* evals, double* evecs, int* info) {
+    if (n < 1 || count < 0) return set_error(CELERIS_ERR_INVALID_ARG, "n must be >= 1 and count >= 0");
+    if (n > kMaxN) return set_error(CELERIS_ERR_TOO_LARGE, "n = %d > %d", n, kMaxN);
+    if (count == 0) return CELERIS_OK;
+    if (!A || !evals || !evecs) return set_error(CELERIS_ERR_INVALID_ARG, "NULL argument");
+    if (n == 1) {  // nothing to reduce
+        for (int c = 0; c < count; ++c) {
+            evals[2 * c] = A[2 * c];
+            evals[2 * c + 1] = A[2 * c + 1];
+            evecs[2 * c] = 1.0;
+            evecs[2 * c + 1] = 0.0;
+            if (info) info[c] = 0;
+        }
+        return CELERIS_OK;
+    }
+    return run_eig(A, n, count, evals, evecs, info);
+}
+
+int celeris_eig_general(const double* A, int n, double* evals, double* evecs) {
+    return celeris_eig_general_batch(A, n, 1, evals, evecs, nullptr);
 }
 
 int celeris_solve_rcwa_2d_orders(const celeris_rcwa_cell* layers, int nlayers, const double* Ex0, const double* Ey0,

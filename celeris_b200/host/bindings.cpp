@@ -98,6 +98,20 @@ PYBIND11_MODULE(_celeris, m) {
              cdouble ex, cdouble ey, int Mx, int My) { return solve_rcwa_2d(inc, st, sub, wl, th, ph, ex, ey, Mx, My); },
           py::arg("incident"), py::arg("stack"), py::arg("substrate"), py::arg("wavelength_um"),
           py::arg("theta_rad"), py::arg("phi_rad"), py::arg("Ex0"), py::arg("Ey0"), py::arg("Mx"), py::arg("My"));
+    m.def(
+        "eig_general",
+        [](py::array_t<std::complex<double>, py::array::f_style | py::array::forcecast> A) {
+            if (A.ndim() != 2 || A.shape(0) != A.shape(1)) throw std::invalid_argument("eig_general: square matrix");
+            const int n = static_cast<int>(A.shape(0));
+            std::vector<cdouble> a(A.data(), A.data() + static_cast<size_t>(n) * n), vals, vecs;
+            eig_general(a, n, vals, vecs);
+            py::array_t<std::complex<double>> ev(n);
+            std::copy(vals.begin(), vals.end(), ev.mutable_data());
+            py::array_t<std::complex<double>, py::array::f_style> V({n, n});
+            std::copy(vecs.begin(), vecs.end(), V.mutable_data());
+            return py::make_tuple(ev, V);
+        },
+        py::arg("A"));
     py::class_<OrderEfficiency>(m, "OrderEfficiency")
         .def_readonly("p", &OrderEfficiency::p)
         .def_readonly("q", &OrderEfficiency::q)

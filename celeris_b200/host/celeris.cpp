@@ -260,6 +260,16 @@ Rcwa2DResult solve_rcwa_2d(const Material& incident, const Rcwa2DStack& stack, c
     return from_result(r);
 }
 
+void eig_general(const std::vector<cdouble>& A, int n, std::vector<cdouble>& evals, std::vector<cdouble>& evecs) {
+    if (n < 1 || A.size() != static_cast<size_t>(n) * n)
+        throw std::invalid_argument("eig_general: A must hold n * n entries, n >= 1");
+    evals.assign(n, cdouble(0.0, 0.0));
+    evecs.assign(static_cast<size_t>(n) * n, cdouble(0.0, 0.0));
+    check(celeris_eig_general(reinterpret_cast<const double*>(A.data()), n, reinterpret_cast<double*>(evals.data()),
+                              reinterpret_cast<double*>(evecs.data())),
+          "eig_general");
+}
+
 // analysis/efficiency.cpp:7-46: one solve with orders, then the budget.
 EfficiencyBudget analyze_efficiency(const Material& incident, const Material& pillar, const Material& background,
                                     const Material& substrate, double period_x_um, double period_y_um, double fill_x,

@@ -87,6 +87,10 @@ struct OrderEfficiency {
     bool prop_r;
 };
 
+// eig.hpp:25 with plain containers: A (n x n, column-major) -> eigenvalues and
+// unit-norm right eigenvectors (column-major), on the GPU eigen-stages.
+void eig_general(const std::vector<cdouble>& A, int n, std::vector<cdouble>& evals, std::vector<cdouble>& evecs);
+
 // Patterned layers between the incident and substrate half-spaces; layers[0]
 // is next to the incident side (rcwa2d.cpp:361-364). orders_out (optional)
 // receives every order's efficiencies (rcwa2d.cpp:464-485).

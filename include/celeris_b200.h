@@ -226,6 +226,22 @@ int celeris_solve_rcwa_2d_stack(const celeris_rcwa_cell* layers, int nlayers,
                                 const double* Ex0, const double* Ey0,
                                 celeris_rcwa_result* out);
 
+/* Drop-in for celeris::eig_general (eig.hpp:25; eig.cpp:52-92): right
+ * eigenpairs of a general complex n x n matrix, A * v_i = lambda_i * v_i. A and
+ * evecs are column-major complex (Eigen::MatrixXcd / LAPACK layout, n*n
+ * interleaved (re, im) pairs), evals n complex. Each eigenvector has unit
+ * 2-norm and its largest-magnitude component real and positive (zgeev's
+ * normalisation); the order of the eigenvalues is the QR's. The device path is
+ * the RCWA eigen-stages (Hessenberg, multishift QR with early deflation,
+ * back substitution). n <= 1024. Synchronous, host buffers. */
+int celeris_eig_general(const double* A, int n, double* evals, double* evecs);
+
+/* New: `count` matrices of order n at once (one CTA per matrix), stored one
+ * after another; info (count ints, may be NULL) receives 0 or the QR failure
+ * code per matrix (without info a failure is CELERIS_ERR_EIG_NOCONV). */
+int celeris_eig_general_batch(const double* A, int n, int count, double* evals,
+                              double* evecs, int* info);
+
 /* Per-order efficiency (OrderEfficiency, rcwa2d.hpp:101-107). */
 typedef struct celeris_rcwa_order {
     int p, q;          /* diffraction order */

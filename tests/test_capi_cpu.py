@@ -89,3 +89,15 @@ def test_stack_arguments_are_rejected_before_device_work():
     st = lib.celeris_solve_rcwa_2d_orders(arr, 1, ex, ey, ctypes.byref(out), orders, 4)  # 25 orders needed
     assert st == capi.ERR_INVALID_ARG and b"orders" in lib.celeris_last_error()
     assert lib.celeris_solve_rcwa_2d_stack(arr, 0, ex, ey, ctypes.byref(out)) == capi.ERR_INVALID_ARG
+
+
+def test_eig_arguments_are_rejected_before_device_work():
+    import numpy as np
+
+    lib = capi.load()
+    buf = np.zeros(8)
+    assert lib.celeris_eig_general_batch(capi._dp(buf), 0, 1, capi._dp(buf), capi._dp(buf), None) == \
+        capi.ERR_INVALID_ARG
+    assert lib.celeris_eig_general_batch(capi._dp(buf), 2000, 1, capi._dp(buf), capi._dp(buf), None) == \
+        capi.ERR_TOO_LARGE
+    assert lib.celeris_eig_general(None, 4, capi._dp(buf), capi._dp(buf)) == capi.ERR_INVALID_ARG

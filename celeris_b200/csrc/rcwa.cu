@@ -1069,8 +1069,8 @@ size_t per_cell_bytes(int n, int nexc) {
            celeris_rt::align256(sizeof(CellDev)) + 14 * 256;
 }
 
-// Dynamic shared-memory limits are per kernel function, so they are set once
-// per wave to the largest need over its buckets (outside any capture).
+// The largest dynamic shared memory each stage kernel needs over a wave's
+// buckets; raised once per wave, outside any capture.
 struct SmemNeeds {
     size_t laurent = 0, rect = 0, hess_s = 0, hess_g = 0, smat = 0;
     bool aed = false;
@@ -1088,22 +1088,38 @@ struct SmemNeeds {
     }
 };
 
+// Dynamic shared-memory limits are per kernel function and process-wide, so
+// they only ever grow: a call that needs less never lowers the limit another
+// thread's launch relies on (a larger limit does not change a launch that asks
+// for less).
+int raise_dyn_smem(const void* fn, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> cur;
+    int dev = 0;
+    CEL_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& c = cur[{dev, fn}];
+    if (bytes <= c) return CELERIS_OK;
+    CEL_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    c = bytes;
+    return CELERIS_OK;
+}
+
 int set_smem_limits(const SmemNeeds& s) {
     if (s.laurent)
-        CEL_CUDA(cudaFuncSetAttribute(rcwa_fourier_laurent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.laurent));
+        CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_fourier_laurent), s.laurent));
     if (s.rect)
-        CEL_CUDA(cudaFuncSetAttribute(rcwa_fourier_rect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.rect));
+        CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_fourier_rect), s.rect));
     if (s.aed)
-        CEL_CUDA(cudaFuncSetAttribute(rcwa_schur, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)kSchurSmemOneCta));
+        CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_schur), kSchurSmemOneCta));
     if (s.hess_g)
-        CEL_CUDA(cudaFuncSetAttribute(rcwa_hess<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.hess_g));
+        CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_hess<false>), s.hess_g));
     if (s.hess_s) {
-        CEL_CUDA(cudaFuncSetAttribute(rcwa_hess<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.hess_s));
+        CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_hess<true>), s.hess_s));
     }
     if (s.smat) {
-        CEL_CUDA(cudaFuncSetAttribute(rcwa_smat1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smat));
-        CEL_CUDA(cudaFuncSetAttribute(rcwa_smat2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smat));
+        CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_smat1), s.smat));
+        CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_smat2), s.smat));
     }
     return CELERIS_OK;
 }
@@ -1675,7 +1691,7 @@ int run_stacks(const celeris_rcwa_cell* layers, const std::vector<std::pair<int,
             sb.cells = scells;
             sb.stacks = sdev;
             const size_t sm_stage = lu_stage_bytes(n);
-            CEL_CUDA(cudaFuncSetAttribute(rcwa_stack_smat, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_stage));
+            CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_stack_smat), sm_stage));
             rcwa_stack_smat<<<ns, kRT, sm_stage, st>>>(sb);
             Bucket eb;
             std::memset(&eb, 0, sizeof(eb));
@@ -1756,12 +1772,10 @@ int run_eig(const double* A, int n, int count, double* evals, double* evecs, int
         ~StreamGuard() { cudaStreamDestroy(s); }
     } sg{st};
     if (n <= kSmemEigMaxN)
-        CEL_CUDA(cudaFuncSetAttribute(rcwa_hess<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)((s_nn + 2 * s_n) * sizeof(cplx))));
+        CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_hess<true>), (s_nn + 2 * s_n) * sizeof(cplx)));
     else
-        CEL_CUDA(cudaFuncSetAttribute(rcwa_hess<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)hess_stage_bytes(n)));
-    CEL_CUDA(cudaFuncSetAttribute(rcwa_schur, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSchurSmemOneCta));
+        CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_hess<false>), hess_stage_bytes(n)));
+    CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_schur), kSchurSmemOneCta));
     size_t free_b = 0, total_b = 0;
     CEL_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t per = (7 * s_nn + 2 * s_n) * sizeof(cplx) + 4096;

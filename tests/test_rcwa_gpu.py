@@ -130,3 +130,30 @@ def test_invalid_arguments():
     with pytest.raises(capi.CelerisError) as e:
         capi.solve_rcwa_2d(c)
     assert e.value.status == capi.ERR_INVALID_ARG
+
+
+def test_concurrent_calls_from_two_threads():
+    """The reference runs solves concurrently on std::async workers
+    (metalens.cpp:153-161); here two host threads batch different harmonic
+    counts at once (each with its own stream, graph and workspace) and must get
+    the results of the same calls made one after the other."""
+    import threading
+
+    groups = [[dict(period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46, eps_pillar=4.0, eps_bg=1.0,
+                    fill_x=0.3 + 0.05 * i, thickness_um=0.6, Mx=M) for i in range(6)] for M in (2, 5)]
+    cells = [[capi.rcwa_cell(**c) for c in g] for g in groups]
+    seq = [capi.rcwa_batch(c)[0] for c in cells]
+    out = [None, None]
+
+    def run(k):
+        for _ in range(3):
+            out[k] = capi.rcwa_batch(cells[k])[0]
+
+    th = [threading.Thread(target=run, args=(k,)) for k in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    for k in range(2):
+        for a, b in zip(out[k], seq[k]):
+            assert a == b

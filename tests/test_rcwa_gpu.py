@@ -71,6 +71,15 @@ MIXED = [
          n_sub=1.46, eps_pillar=4.0, eps_bg=1.0, fill_x=0.5, fill_y=0.6, thickness_um=0.5, Mx=3, My=1),
     dict(name="zero_order_only_M0", period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46, eps_pillar=4.0,
          eps_bg=1.0, fill_x=0.5, thickness_um=0.6, Mx=0),
+    # metallic pillar (negative permittivity, absorbing): evanescent-heavy modes
+    dict(name="metal_pillar_M3", period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46,
+         eps_pillar=complex(-20.0, 1.5), eps_bg=1.0, fill_x=0.4, thickness_um=0.05, Mx=3, lossy=True),
+    # near-grazing incidence
+    dict(name="grazing_theta75_M3", period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46, eps_pillar=4.0,
+         eps_bg=1.0, fill_x=0.5, thickness_um=0.4, Mx=3, theta_rad=math.radians(75.0), phi_rad=0.2),
+    # period above the wavelength: several propagating orders in both half-spaces
+    dict(name="diffractive_p900_M3", period_um=0.9, wavelength_um=0.633, n_inc=1.0, n_sub=1.46, eps_pillar=4.0,
+         eps_bg=1.0, fill_x=0.35, thickness_um=0.5, Mx=3),
 ]
 LOSSY = dict(name="lossy_M3", period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46, eps_pillar=(2.0 + 0.05j) ** 2,
              eps_bg=1.0, fill_x=0.5, thickness_um=0.6, Mx=3)
@@ -83,7 +92,7 @@ def test_mixed_cells_batch(cell):
     # The reference maps the order-0 excitation with its normal-incidence
     # convention (rcwa2d.cpp:404-411), so R + T = 1 holds for lossless cells at
     # normal incidence only; off-normal cells are compared with the oracle only.
-    lossless = cell is not LOSSY and cell.get("theta_rad", 0.0) == 0.0
+    lossless = cell is not LOSSY and not cell.get("lossy") and cell.get("theta_rad", 0.0) == 0.0
     check(res[0], ref(cell, 1.0, 0.0), lossless)
     check(res[1], ref(cell, 0.0, 1.0), lossless)
 

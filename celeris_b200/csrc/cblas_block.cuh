@@ -964,7 +964,7 @@ __device__ __forceinline__ cplx wilkinson(cplx a, cplx b, cplx c, cplx d) {
     return cabs1(csub(e1, d)) <= cabs1(csub(e2, d)) ? e1 : e2;
 }
 
-constexpr int kMaxN = 1024;  // largest matrix order (deflation flags are per row)
+constexpr int kMaxN = 2048;  // largest matrix order (deflation flags are per row; 2N <= 1922 for M <= 15)
 
 // ---- eigenvectors of the triangular Schur factor ----------------------------------------
 // X (n x n, row-major) <- right eigenvectors of upper-triangular T: column k

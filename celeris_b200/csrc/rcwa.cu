@@ -953,7 +953,7 @@ int validate(const celeris_rcwa_cell& c) {
         return set_error(CELERIS_ERR_INVALID_ARG, "wavelength and periods must be > 0");
     if (c.shape < 0 || c.shape > 3) return set_error(CELERIS_ERR_INVALID_ARG, "unknown shape %d", c.shape);
     const int n = 2 * (2 * c.Mx + 1) * (2 * c.My + 1);
-    if (n > 1024) return set_error(CELERIS_ERR_TOO_LARGE, "2N = %d > 1024", n);
+    if (n > kMaxN) return set_error(CELERIS_ERR_TOO_LARGE, "2N = %d > %d", n, kMaxN);
     if (c.grid > 1024) return set_error(CELERIS_ERR_TOO_LARGE, "grid %d > 1024", c.grid);
     return CELERIS_OK;
 }

@@ -233,7 +233,7 @@ int celeris_solve_rcwa_2d_stack(const celeris_rcwa_cell* layers, int nlayers,
  * 2-norm and its largest-magnitude component real and positive (zgeev's
  * normalisation); the order of the eigenvalues is the QR's. The device path is
  * the RCWA eigen-stages (Hessenberg, multishift QR with early deflation,
- * back substitution). n <= 1024. Synchronous, host buffers. */
+ * back substitution). n <= 2048. Synchronous, host buffers. */
 int celeris_eig_general(const double* A, int n, double* evals, double* evecs);
 
 /* New: `count` matrices of order n at once (one CTA per matrix), stored one

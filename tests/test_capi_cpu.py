@@ -98,6 +98,6 @@ def test_eig_arguments_are_rejected_before_device_work():
     buf = np.zeros(8)
     assert lib.celeris_eig_general_batch(capi._dp(buf), 0, 1, capi._dp(buf), capi._dp(buf), None) == \
         capi.ERR_INVALID_ARG
-    assert lib.celeris_eig_general_batch(capi._dp(buf), 2000, 1, capi._dp(buf), capi._dp(buf), None) == \
+    assert lib.celeris_eig_general_batch(capi._dp(buf), 5000, 1, capi._dp(buf), capi._dp(buf), None) == \
         capi.ERR_TOO_LARGE
     assert lib.celeris_eig_general(None, 4, capi._dp(buf), capi._dp(buf)) == capi.ERR_INVALID_ARG

@@ -166,3 +166,40 @@ def test_concurrent_calls_from_two_threads():
     for k in range(2):
         for a, b in zip(out[k], seq[k]):
             assert a == b
+
+
+FS532 = RO.sellmeier_index(RO.FUSED_SILICA, 0.532)
+
+
+def test_selftest8_known_answers_and_high_orders():
+    """The reference's own RCWA known answers (cli/selftest.cpp case [8]) through
+    the GPU path: [8a] grating vs grcwa at M = 10 (2N = 882), [8b] energy of the
+    square TiO2 pillar for M = 6..12 (2N up to 1250), [8c] the asymmetric pillar
+    vs grcwa at M = 12, [8d] Laurent-rule shapes at M = 8; the M = 12 pillar also
+    against the oracle at 1e-10."""
+    g = dict(period_um=0.3, wavelength_um=0.5, n_inc=1.0, n_sub=1.0, eps_pillar=2.25, eps_bg=1.0, fill_x=0.5,
+             fill_y=1.0, thickness_um=0.5, Mx=10)
+    res, info = capi.rcwa_batch([capi.rcwa_cell(**g)])
+    assert info[0] == 0
+    tm, te = res[0], res[1]  # X = E along x (TM), Y = E along y (TE)
+    assert abs(te["de_t0"] - 0.93334) < 2e-3 and abs(tm["de_t0"] - 0.96050) < 5e-3
+    sq = [dict(period_um=0.35, wavelength_um=0.532, n_inc=1.0, n_sub=FS532, eps_pillar=2.45 ** 2, eps_bg=1.0,
+               fill_x=0.5, thickness_um=0.6, Mx=m) for m in (6, 8, 10, 12)]
+    res, info = capi.rcwa_batch([capi.rcwa_cell(**c) for c in sq])
+    assert np.all(info == 0)
+    assert max(abs(res[2 * k]["sum_de"] - 1.0) for k in range(4)) < 1e-4
+    rect = dict(period_um=0.35, wavelength_um=0.532, n_inc=1.0, n_sub=FS532, eps_pillar=2.45 ** 2, eps_bg=1.0,
+                fill_x=0.6, fill_y=0.3, thickness_um=0.6, Mx=12)
+    res, info = capi.rcwa_batch([capi.rcwa_cell(**rect)])
+    assert info[0] == 0
+    assert abs(res[0]["de_t0"] - 0.954) < 0.03 and abs(res[1]["de_t0"] - 0.972) < 0.03
+    assert abs(res[0]["sum_de"] - 1.0) < 1e-4
+    check(res[0], ref(rect, 1.0, 0.0))
+    check(res[1], ref(rect, 0.0, 1.0))
+    shapes = [dict(period_um=0.35, wavelength_um=0.532, n_inc=1.0, n_sub=FS532, eps_pillar=2.45 ** 2, eps_bg=1.0,
+                   fill_x=f, thickness_um=0.6, Mx=8, shape=sh, shape_param=p)
+              for sh, f, p in ((capi.SHAPE_ELLIPSE, 0.7, 0.5), (capi.SHAPE_CROSS, 0.8, 0.4),
+                               (capi.SHAPE_RING, 0.9, 0.5))]
+    res, info = capi.rcwa_batch([capi.rcwa_cell(**c) for c in shapes])
+    assert np.all(info == 0)
+    assert max(abs(res[2 * k]["sum_de"] - 1.0) for k in range(3)) < 2e-3

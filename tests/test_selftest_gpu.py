@@ -2,7 +2,9 @@
 run through the host mirror on the GPU: [12] form birefringence grows with
 pillar asymmetry, [16] the Khorasaninejad 2016 nanofin is a near-ideal
 half-wave plate with exact geometric phase, [20] efficiency budgets of a
-lossless and an absorbing atom. Materials are constant-index stand-ins where the
+lossless and an absorbing atom, [15] / [15b] / [15c] / [18] achromatic designs
+(group-delay objective flattens the focal drift / lowers the group-delay RMS,
+geometric phase exact, one etch). Materials are constant-index stand-ins where the
 reference reads tabulated files (TiO2 2.45, SiO2 1.46, gold 0.54 + 2.2i at 532 nm).
 """
 import math
@@ -64,3 +66,55 @@ def test_selftest20_efficiency_budget():
     assert abs(bt.t_zero - bt.transmission) < 1e-4 and bt.n_prop_t == 1
     bg = cel.analyze_efficiency(air, au, air, sio2, 0.35, 0.35, 0.5, 0.5, 0.10, 0.532, 1.0, 0.0, 6)
     assert abs(bg.transmission + bg.reflection + bg.absorption - 1.0) < 1e-3 and bg.absorption > 0.2
+
+
+BAND = [0.532 * 0.9, 0.532, 0.532 * 1.1]
+
+
+def test_selftest15_achromatic_fill_height():
+    """[15]: the group-delay objective flattens the chromatic focal drift while
+    the base phase stays diffraction-limited."""
+    tio2 = cel.Material.constant(2.40 + 0j, "TiO2~")
+    air = cel.materials.air()
+    dl = cel.build_dispersive_library(tio2, air, air, cel.materials.fused_silica(), 0.35, BAND, 0.532, 0.08, 0.92,
+                                      10, 0.40, 1.40, 6, 5)
+    sd = cel.design_achromatic_metalens(dl, 20.0, 6.0, 0.0)
+    ad = cel.design_achromatic_metalens(dl, 20.0, 6.0, 1.0)
+
+    def drift(c):
+        z = [p.focal_length_um for p in c]
+        return max(z) - min(z)
+
+    assert drift(cel.verify_achromatic_focus(dl, ad)) < drift(cel.verify_achromatic_focus(dl, sd))
+    assert ad.rms_phase_error_deg < 25.0
+
+
+def test_selftest15b_single_etch():
+    tio2 = cel.Material.constant(2.40 + 0j, "TiO2~")
+    air = cel.materials.air()
+    dl = cel.build_single_etch_library(tio2, air, air, cel.materials.fused_silica(), 0.35, BAND, 0.532, 0.08, 0.92,
+                                       5, 0.80, 5)
+    sd = cel.design_achromatic_metalens(dl, 20.0, 6.0, 0.0)
+    ad = cel.design_achromatic_metalens(dl, 20.0, 6.0, 1.0)
+    assert sd.single_height and ad.single_height
+    assert ad.rms_group_delay_error_fs < sd.rms_group_delay_error_fs and ad.rms_phase_error_deg < 25.0
+
+
+@pytest.mark.parametrize("case", ["15c", "18"])
+def test_selftest15c_18_achromatic_pb(case):
+    """[15c] / [18]: geometric base phase exact for both designs, group-delay RMS
+    reduced by the group-delay objective, one etch depth."""
+    tio2 = cel.Material.constant(2.40 + 0j, "TiO2~")
+    air = cel.materials.air()
+    if case == "15c":
+        lib = cel.build_dispersive_pb_library(tio2, air, air, cel.materials.bk7(), 0.35, BAND, 0.532, 0.10, 0.90, 6,
+                                              1.10, 5)
+        f, D = 20.0, 6.0
+    else:
+        lib = cel.build_dispersive_pb_library(tio2, air, air, cel.materials.fused_silica(), 0.400,
+                                              [0.470, 0.570, 0.670], 0.570, 0.10, 0.90, 6, 0.600, 5)
+        f, D = 8.0, 5.0
+    sd = cel.design_pb_achromatic_metalens(lib, f, D, 1, 0.0)
+    ad = cel.design_pb_achromatic_metalens(lib, f, D, 1, 1.0)
+    assert sd.rms_phase_error_deg < 1e-6 and ad.rms_phase_error_deg < 1e-6
+    assert ad.rms_group_delay_error_fs < sd.rms_group_delay_error_fs

@@ -559,6 +559,17 @@ PYBIND11_MODULE(_celeris, m) {
           py::arg("M"), py::arg("fill_samples"), py::arg("efficiency_weight"),
           py::arg("progress") = std::function<void(float)>());
 
+    m.def(
+        "cuda_geev_batched",
+        [](py::array_t<std::complex<double>, py::array::c_style | py::array::forcecast> As) {
+            // As: [batch, n, n] with each matrix column-major (the reference's layout)
+            if (As.ndim() != 3 || As.shape(1) != As.shape(2)) throw std::invalid_argument("[batch, n, n] expected");
+            const int batch = static_cast<int>(As.shape(0)), n = static_cast<int>(As.shape(1));
+            py::array_t<std::complex<double>> w({batch, n}), vr({batch, n, n});
+            const bool ok = cuda::geev_batched(As.data(), n, batch, w.mutable_data(), vr.mutable_data());
+            return py::make_tuple(ok, w, vr);
+        },
+        py::arg("As"));
     m.def("cuda_available", &cuda::available);
     m.def("cuda_device_name", &cuda::device_name);
 }

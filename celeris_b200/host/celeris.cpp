@@ -994,6 +994,15 @@ bool propagate_zx(const double* px, const double* py, const std::complex<double>
     return celeris_propagate_zx(px, py, reinterpret_cast<const double*>(pt), npil, xmin, xmax, nx, zmin, zmax, nz,
                                 k, out) == CELERIS_OK;
 }
+bool geev(const std::complex<double>* A, int n, std::complex<double>* w, std::complex<double>* vr) {
+    return celeris_eig_general(reinterpret_cast<const double*>(A), n, reinterpret_cast<double*>(w),
+                               reinterpret_cast<double*>(vr)) == CELERIS_OK;
+}
+bool geev_batched(const std::complex<double>* As, int n, int batch, std::complex<double>* ws,
+                  std::complex<double>* vrs, int /*streams*/) {
+    return celeris_eig_general_batch(reinterpret_cast<const double*>(As), n, batch, reinterpret_cast<double*>(ws),
+                                     reinterpret_cast<double*>(vrs), nullptr) == CELERIS_OK;
+}
 }  // namespace cuda
 
 }  // namespace celeris

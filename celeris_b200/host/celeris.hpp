@@ -528,6 +528,12 @@ bool propagate_psf(const double* px, const double* py, const std::complex<double
                    double cy, double z, double k, int n, double half_window, double* out);
 bool propagate_zx(const double* px, const double* py, const std::complex<double>* pt, int npil, double xmin,
                   double xmax, int nx, double zmin, double zmax, int nz, double k, double* out);
+// cuda/eigensolve.hpp:14-31: general complex eigendecomposition (column-major);
+// `streams` is accepted for the signature and unused (the batch is one launch
+// sequence, one CTA per matrix).
+bool geev(const std::complex<double>* A, int n, std::complex<double>* w, std::complex<double>* vr);
+bool geev_batched(const std::complex<double>* As, int n, int batch, std::complex<double>* ws,
+                  std::complex<double>* vrs, int streams = 4);
 }  // namespace cuda
 
 }  // namespace celeris

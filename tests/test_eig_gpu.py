@@ -86,3 +86,20 @@ def test_host_mirror_signature():
     vals, V = cel.eig_general(A)
     v2, V2, _ = capi.eig_general(A)
     assert np.array_equal(np.asarray(vals), v2) and np.array_equal(np.asarray(V), V2)
+
+
+def test_reference_geev_batched_signature():
+    """celeris::cuda::geev_batched (cuda/eigensolve.hpp:26-31): matrices column-major
+    one after another, eigenvalues and right eigenvectors out; the reference's
+    [10] check (eigenvalues of a 578 x 578 random matrix against the CPU solver)."""
+    import celeris_b200 as cel
+
+    rng = np.random.default_rng(42)
+    A = rng.uniform(-1, 1, (578, 578)) + 1j * rng.uniform(-1, 1, (578, 578))
+    As = np.stack([A.T, rand_matrix(578, 1).T])  # C-order of the transpose = column-major of A
+    ok, w, vr = cel.cuda_geev_batched(As)
+    assert ok
+    ev = np.linalg.eigvals(A)
+    assert np.max(np.abs(np.sort_complex(w[0]) - np.sort_complex(ev))) <= 1e-10 * np.linalg.norm(A, 2)
+    V = vr[0].T  # back to row-major columns = eigenvectors
+    assert np.linalg.norm(A @ V - V * w[0]) <= 1e-12 * np.linalg.norm(A, 2) * 578 ** 0.5

@@ -651,8 +651,9 @@ __device__ __forceinline__ void half_space(const StackBucket& sb, const CellDev&
     kz = kz_uniform(er, c.omega, kx, ky);
 }
 
-// One CTA per stack. dynamic smem: lu_stage_bytes(n)
-__global__ void __launch_bounds__(kRT) rcwa_stack_smat(StackBucket sb) {
+// One CTA per stack, two per SM (measured faster than one at 255 registers despite
+// the spills at 128). dynamic smem: lu_stage_bytes(n)
+__global__ void __launch_bounds__(kRT, 2) rcwa_stack_smat(StackBucket sb) {
     extern __shared__ __align__(16) unsigned char smem[];
     cplx* stg = reinterpret_cast<cplx*>(smem);
     __shared__ GemmSmem gs;
@@ -1525,6 +1526,23 @@ struct DevBuf {
     }
 };
 
+// Sub-allocation from one reserved region (the stack path's per-stream
+// workspace arena): no cudaMalloc / cudaFree per call.
+struct Bump {
+    char* p = nullptr;
+    size_t left = 0;
+    template <typename T>
+    int get(T** out, size_t count) {
+        const size_t b = celeris_rt::align256(std::max<size_t>(count, 1) * sizeof(T));
+        if (b > left) return set_error(CELERIS_ERR_OOM, "stack workspace: carve of %zu bytes over its plan", b);
+        *out = reinterpret_cast<T*>(p);
+        p += b;
+        left -= b;
+        return CELERIS_OK;
+    }
+};
+size_t a256(size_t b) { return celeris_rt::align256(std::max<size_t>(b, 1)); }
+
 // stacks[s] = (first layer index, layer count) into `layers`; exc holds 4 doubles
 // (Ex0 re, im, Ey0 re, im) per stack; results nexc per stack.
 // ord_out (may be NULL): per stack and excitation N x (de_t, de_r).
@@ -1534,12 +1552,15 @@ int run_stacks(const celeris_rcwa_cell* layers, const std::vector<std::pair<int,
     int dev = 0, smem_optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cudaStream_t st = nullptr;
-    CEL_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    struct StreamGuard {
-        cudaStream_t s;
-        ~StreamGuard() { cudaStreamDestroy(s); }
-    } sg{st};
+    // one stream (and so one workspace arena) per calling thread for the stack path
+    static thread_local cudaStream_t t_stack_st = nullptr;
+    static thread_local int t_stack_dev = -1;
+    if (!t_stack_st || t_stack_dev != dev) {
+        CEL_CUDA(cudaStreamCreateWithFlags(&t_stack_st, cudaStreamNonBlocking));
+        t_stack_dev = dev;
+    }
+    cudaStream_t st = t_stack_st;
+    Workspace& ws = Workspace::for_stream(st);
     // stacks grouped by (Mx, My): one layer store and one recursion launch per group
     std::map<std::pair<int, int>, std::vector<int>> groups;
     for (int s = 0; s < (int)stacks.size(); ++s) {
@@ -1567,7 +1588,6 @@ int run_stacks(const celeris_rcwa_cell* layers, const std::vector<std::pair<int,
                 bytes += need;
             }
             const int ns = (int)ids.size();
-            DevBuf mem;
             // layer store slots, in stack order
             std::vector<HostCell> sub;
             std::vector<int> first_slot(ns);
@@ -1578,6 +1598,26 @@ int run_stacks(const celeris_rcwa_cell* layers, const std::vector<std::pair<int,
                     sub.push_back(make_cell(layers[sp.first + l], (int)sub.size(), 1.0, 0.0, 0.0, 0.0, 2));
             }
             const int nslot = (int)sub.size();
+            std::map<int, std::vector<int>> by_ng;
+            for (int i = 0; i < nslot; ++i) by_ng[sub[i].ng].push_back(i);
+            // region plan: layer store + recursion, then one raster class's bucket at a time
+            const size_t c16 = sizeof(cplx);
+            size_t fixed = 2 * a256(s_nn * nslot * c16) + a256(s_n * nslot * c16) + a256(nslot * sizeof(double)) +
+                           7 * a256(s_nn * ns * c16) + a256(10 * s_n * ns * c16) + a256(s_n * ns * sizeof(int)) +
+                           a256(ns * sizeof(int)) + a256(ns * sizeof(CellDev)) + a256(ns * sizeof(StackDev)) +
+                           a256(ns * nexc * sizeof(celeris_rcwa_result));
+            if (ord_out) fixed += a256((size_t)ns * nexc * N * 2 * sizeof(double));
+            size_t class_max = 0;
+            for (auto& kv : by_ng) {
+                const size_t nc = kv.second.size(), ng = (size_t)std::max(kv.first, 0);
+                size_t b = a256(nc * sizeof(CellDev)) + 5 * a256(s_nn * nc * c16) + 3 * a256(s_NN * nc * c16) +
+                           a256(s_n * nc * c16) + a256(s_n * nc * sizeof(int)) + 2 * a256(nc * sizeof(int));
+                if (ng > 0) b += a256((4 * Mx + 1) * ng * c16) + a256((4 * My + 1) * ng * c16);
+                class_max = std::max(class_max, b);
+            }
+            CEL_TRY(ws.reserve(st, fixed + class_max));
+            char* region = static_cast<char*>(ws.take(fixed + class_max));
+            Bump mem{region, fixed};
             cplx *LW, *LA, *Lq;
             double* Lh;
             CEL_TRY(mem.get(&LW, s_nn * nslot));
@@ -1586,8 +1626,6 @@ int run_stacks(const celeris_rcwa_cell* layers, const std::vector<std::pair<int,
             CEL_TRY(mem.get(&Lh, (size_t)nslot));
             std::vector<int> sub_info(nslot, 0);
             // eigen-solutions of every layer, one bucket per raster class
-            std::map<int, std::vector<int>> by_ng;
-            for (int i = 0; i < nslot; ++i) by_ng[sub[i].ng].push_back(i);
             for (auto& kv : by_ng) {
                 const int ng = kv.first;
                 const std::vector<int>& si = kv.second;
@@ -1595,7 +1633,7 @@ int run_stacks(const celeris_rcwa_cell* layers, const std::vector<std::pair<int,
                 if (ng > 0 && laurent_smem(Mx, My, ng) + 1024 > (size_t)smem_optin)
                     return set_error(CELERIS_ERR_TOO_LARGE, "raster %d with M=(%d,%d) exceeds shared memory", ng,
                                      Mx, My);
-                DevBuf bm;
+                Bump bm{region + fixed, class_max};  // reused by each class in turn (the stream is synchronised)
                 Bucket b;
                 std::memset(&b, 0, sizeof(b));
                 b.Mx = Mx;

@@ -1509,23 +1509,6 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
 }
 
 // ---- multi-layer stacks ----------------------------------------------------------------------
-// Device buffers owned by one call (the stack path keeps its own allocations, so
-// it does not disturb the single-layer batch's workspace or cached graph).
-struct DevBuf {
-    std::vector<void*> ptrs;
-    ~DevBuf() {
-        for (void* p : ptrs) cudaFree(p);
-    }
-    template <typename T>
-    int get(T** out, size_t count) {
-        void* p = nullptr;
-        CEL_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
-        ptrs.push_back(p);
-        *out = static_cast<T*>(p);
-        return CELERIS_OK;
-    }
-};
-
 // Sub-allocation from one reserved region (the stack path's per-stream
 // workspace arena): no cudaMalloc / cudaFree per call.
 struct Bump {
@@ -1803,12 +1786,16 @@ int validate_stack(const celeris_rcwa_cell* l, int nl) {
 int run_eig(const double* A, int n, int count, double* evals, double* evecs, int* info_out) {
     CEL_TRY(celeris_rt::require_device());
     const size_t s_nn = (size_t)n * n, s_n = (size_t)n;
-    cudaStream_t st = nullptr;
-    CEL_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    struct StreamGuard {
-        cudaStream_t s;
-        ~StreamGuard() { cudaStreamDestroy(s); }
-    } sg{st};
+    int dev = 0;
+    CEL_CUDA(cudaGetDevice(&dev));
+    static thread_local cudaStream_t t_eig_st = nullptr;  // one stream and arena per calling thread
+    static thread_local int t_eig_dev = -1;
+    if (!t_eig_st || t_eig_dev != dev) {
+        CEL_CUDA(cudaStreamCreateWithFlags(&t_eig_st, cudaStreamNonBlocking));
+        t_eig_dev = dev;
+    }
+    cudaStream_t st = t_eig_st;
+    Workspace& ws = Workspace::for_stream(st);
     if (n <= kSmemEigMaxN)
         CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_hess<true>), (s_nn + 2 * s_n) * sizeof(cplx)));
     else
@@ -1820,7 +1807,10 @@ int run_eig(const double* A, int n, int count, double* evals, double* evecs, int
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)count, (free_b / 2) / per));
     for (int c0 = 0; c0 < count; c0 += chunk) {
         const int nc = std::min(chunk, count - c0);
-        DevBuf mem;
+        const size_t c16 = sizeof(cplx);
+        const size_t plan = 6 * a256(s_nn * nc * c16) + 2 * a256(s_n * nc * c16) + a256(nc * sizeof(int));
+        CEL_TRY(ws.reserve(st, plan));
+        Bump mem{static_cast<char*>(ws.take(plan)), plan};
         Bucket b;
         std::memset(&b, 0, sizeof(b));
         b.n = n;

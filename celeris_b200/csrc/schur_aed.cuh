@@ -72,6 +72,24 @@ __device__ __forceinline__ void wrot_cols(cplx* B, int ld, int k, double c, cplx
     }
 }
 
+// The same rotations by a group of `nl` lanes (lane index l in the group).
+__device__ __forceinline__ void grot_rows(cplx* B, int ld, int r, double c, cplx s, int c0, int c1, int l, int nl) {
+    const cplx ms = cneg(cconj(s));
+    for (int col = c0 + l; col < c1; col += nl) {
+        const cplx x = B[r * ld + col], y = B[(r + 1) * ld + col];
+        B[r * ld + col] = cfma(s, y, cscale(x, c));
+        B[(r + 1) * ld + col] = cfma(ms, x, cscale(y, c));
+    }
+}
+__device__ __forceinline__ void grot_cols(cplx* B, int ld, int k, double c, cplx s, int r0, int r1, int l, int nl) {
+    const cplx cs = cconj(s), ns = cneg(s);
+    for (int row = r0 + l; row < r1; row += nl) {
+        const cplx x = B[row * ld + k], y = B[row * ld + k + 1];
+        B[row * ld + k] = cfma(cs, y, cscale(x, c));
+        B[row * ld + k + 1] = cfma(ns, x, cscale(y, c));
+    }
+}
+
 // Single-shift QR of the m x m upper Hessenberg matrix B (shared, ld) to upper
 // triangular form, U <- U Q (rows [0, mu)). One warp. Returns 0, or the
 // (1-based) row where the iteration cap ran out.
@@ -511,37 +529,45 @@ __device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, i
         }
         const long long t0 = clock64();
         load_window(H, ldh, ws, w, sh);
+        // Each warp carries bulges b and b + nwarp, one per half-warp, so their
+        // rotations run side by side (bulges 2 rows apart touch disjoint rows in
+        // phase 1 and disjoint columns in phase 2).
+        const int hl = lane & 15;
         for (int t = 0; t < S; ++t) {
-            // phase 1: row rotations (one warp per bulge)
-            for (int b = warp; b < nsh; b += nwarp) {
-                int p;
-                bool intro = false;
-                if (first) {
-                    if (t < 2 * b) continue;
-                    intro = t == 2 * b;
-                    p = intro ? lo : lo + t - 2 * b;
-                } else {
-                    const int p0 = sh->pos[b];
-                    if (p0 < 0) continue;
-                    p = p0 + t;
-                    if (p > hi - 1) continue;
+            // phase 1: row rotations
+            for (int b0 = warp; b0 < nsh; b0 += 2 * nwarp) {
+                const int b = b0 + (lane >> 4) * nwarp;
+                int p = 0;
+                bool intro = false, act = b < nsh;
+                if (act) {
+                    if (first) {
+                        act = t >= 2 * b;
+                        intro = t == 2 * b;
+                        p = intro ? lo : lo + t - 2 * b;
+                    } else {
+                        const int p0 = sh->pos[b];
+                        p = p0 + t;
+                        act = p0 >= 0 && p <= hi - 1;
+                    }
                 }
                 const int k = p - ws;
-                cplx a, bb;
-                if (intro) {
-                    a = csub(B[k * ldb + k], sh->shift[b]);
-                    bb = B[(k + 1) * ldb + k];
-                } else {
-                    a = B[k * ldb + k - 1];
-                    bb = B[(k + 1) * ldb + k - 1];
+                double c = 1.0;
+                cplx s = C(0.0, 0.0);
+                if (act) {
+                    cplx a, bb;
+                    if (intro) {
+                        a = csub(B[k * ldb + k], sh->shift[b]);
+                        bb = B[(k + 1) * ldb + k];
+                    } else {
+                        a = B[k * ldb + k - 1];
+                        bb = B[(k + 1) * ldb + k - 1];
+                    }
+                    givens(a, bb, c, s);
                 }
-                double c;
-                cplx s;
-                givens(a, bb, c, s);
                 __syncwarp();
-                wrot_rows(B, ldb, k, c, s, intro ? k : k - 1, w, lane);
+                if (act) grot_rows(B, ldb, k, c, s, intro ? k : k - 1, w, hl, 16);
                 __syncwarp();
-                if (lane == 0) {
+                if (act && hl == 0) {
                     if (!intro) B[(k + 1) * ldb + k - 1] = C(0.0, 0.0);
                     sh->rc[b] = c;
                     sh->rs[b] = s;
@@ -549,22 +575,27 @@ __device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, i
             }
             __syncthreads();
             // phase 2: column rotations
-            for (int b = warp; b < nsh; b += nwarp) {
-                int p;
-                if (first) {
-                    if (t < 2 * b) continue;
-                    p = t == 2 * b ? lo : lo + t - 2 * b;
-                } else {
-                    const int p0 = sh->pos[b];
-                    if (p0 < 0) continue;
-                    p = p0 + t;
-                    if (p > hi - 1) continue;
+            for (int b0 = warp; b0 < nsh; b0 += 2 * nwarp) {
+                const int b = b0 + (lane >> 4) * nwarp;
+                int p = 0;
+                bool act = b < nsh;
+                if (act) {
+                    if (first) {
+                        act = t >= 2 * b;
+                        p = t == 2 * b ? lo : lo + t - 2 * b;
+                    } else {
+                        const int p0 = sh->pos[b];
+                        p = p0 + t;
+                        act = p0 >= 0 && p <= hi - 1;
+                    }
                 }
-                const int k = p - ws;
-                const double c = sh->rc[b];
-                const cplx s = sh->rs[b];
-                wrot_cols(B, ldb, k, c, s, 0, min(p + 2, hi) - ws + 1, lane);
-                wrot_cols(U, ldu, k, c, s, 0, w, lane);
+                if (act) {
+                    const int k = p - ws;
+                    const double c = sh->rc[b];
+                    const cplx s = sh->rs[b];
+                    grot_cols(B, ldb, k, c, s, 0, min(p + 2, hi) - ws + 1, hl, 16);
+                    grot_cols(U, ldu, k, c, s, 0, w, hl, 16);
+                }
             }
             __syncthreads();
         }

@@ -377,7 +377,7 @@ def measure_rcwa(peaks, quick=False, with_cpu=True, sampler=None):
     lc = [capi.rcwa_cell(**c) for c in lib]
     capi.rcwa_batch(lc)
     t = []
-    for _ in range(5):
+    for _ in range(11):  # ~12 ms host-synchronous calls: the median of 11 rides out host-side jitter
         t0 = time.perf_counter()
         capi.rcwa_batch(lc)
         t.append(time.perf_counter() - t0)

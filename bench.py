@@ -422,7 +422,7 @@ def measure_rcwa(peaks, quick=False, with_cpu=True, sampler=None):
     return out
 
 
-def measure_inverse_design(steps=20, warmup=3):
+def measure_inverse_design(steps=20, warmup=3, form=None):
     """Inverse-design step of the differentiation form: loss = -(encircled energy
     within 1 um) / (total) on the 70,688-pillar x 161^2 metalens, fills -> t by
     natural cubic splines over the 64-width RCWA library, gradient by the adjoint
@@ -448,9 +448,11 @@ def measure_inverse_design(steps=20, warmup=3):
     w = torch.tensor(w0, device=dev, requires_grad=True)
     opt = torch.optim.Adam([w], lr=1e-3)
 
+    form = capi.FORM_PLAIN_F64 if form is None else form
+
     def step():
         opt.zero_grad()
-        L = T.encircled_energy_loss(T.rs_field(spline(w), px, py, grid), grid, 1.0)
+        L = T.encircled_energy_loss(T.rs_field(spline(w), px, py, grid, form), grid, 1.0)
         L.backward()
         opt.step()
         return L
@@ -466,7 +468,9 @@ def measure_inverse_design(steps=20, warmup=3):
     torch.cuda.synchronize()
     ms = a.elapsed_time(b) / steps
     terms = ap.npil * g.n * g.n
-    return {"workload": "metalens_70k_161sq adjoint + Adam", "ms_per_step": ms, "steps": steps,
+    return {"workload": "metalens_70k_161sq adjoint + Adam",
+            "form": "f32c (precision forward + adjoint)" if form == capi.FORM_F32C else "plain FP64",
+            "ms_per_step": ms, "steps": steps,
             "terms_per_s_fwd_plus_adjoint": 2 * terms / (ms * 1e-3),
             "loss_first": float(L0.detach()), "loss_last": float(L.detach())}
 
@@ -599,6 +603,7 @@ def run_gpu(args):
     if not args.quick:
         try:
             out["inverse_design"] = measure_inverse_design()
+            out["inverse_design_f32c"] = measure_inverse_design(form=capi.FORM_F32C)
         except Exception as exc:
             out["inverse_design"] = {"unavailable": str(exc)[:200]}
     rclk = ClockSampler(local)

@@ -53,6 +53,7 @@ constexpr int kStages = 4;
 constexpr int kPPT64 = 2;     // pixels per thread, plain form
 constexpr int kPPT32 = 6;     // pixels per thread, precision form: 3 packed pixel pairs share each pillar record
 constexpr int kAdjPPT = 2;    // pillars per thread, adjoint
+constexpr int kAdjPPT32 = 6;  // pillars per thread, precision-form adjoint (3 packed pairs)
 
 enum { GEOM_PSF = 0, GEOM_ZX = 1 };
 
@@ -116,6 +117,18 @@ __global__ void ff_pack_pix(Geom g, const double2* __restrict__ v, double4* __re
     pixel_pos(g, i, j, fx, fy, fz);
     double2 vv = v[p];
     rec[p] = make_double4(fx, fy, vv.x, vv.y);
+}
+
+// precision-form adjoint: float4 {fx - ox, fy - oy, Re v, Im v} per pixel
+__global__ void ff_pack_pix_f32(Geom g, const double2* __restrict__ v, float4* __restrict__ rec) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    int npix = g.nx * g.ny;
+    if (p >= npix) return;
+    int j = p / g.nx, i = p - j * g.nx;
+    double fx, fy, fz;
+    pixel_pos(g, i, j, fx, fy, fz);
+    double2 vv = v[p];
+    rec[p] = make_float4((float)(fx - g.ox), (float)(fy - g.oy), (float)vv.x, (float)vv.y);
 }
 
 // ---- tile pipeline (shared by all main kernels) ----------------------------
@@ -382,6 +395,109 @@ __global__ void __launch_bounds__(kThreads, 3) rs_f32c_kernel(const float4* __re
                 partial[(size_t)blockIdx.y * npix + (size_t)j * g.nx + i0 + q] =
                     make_double2((double)sr[q] + (double)cr[q], (double)si[q] + (double)ci[q]);
     }
+}
+
+// ---- precision-form adjoint: out_j = e^{-ikz} sum_p (1/R) e^{-2 pi i (R - z)/lambda} v_p
+// The forward kernel's arithmetic with the roles swapped: each thread owns
+// kAdjPPT32 pillars (packed pairs), pixel records stream through the tiles; the
+// product with v is conj(g) v = (1/R) [(c vr + s vi) + i (c vi - s vr)].
+__global__ void __launch_bounds__(kThreads, 3) rs_adj_f32c_kernel(const float4* __restrict__ pix, int npix,
+                                                                  int chunk_len, const double* __restrict__ px,
+                                                                  const double* __restrict__ py, int npil, Geom g,
+                                                                  float z, float il_hi, float il_lo,
+                                                                  double2* __restrict__ partial) {
+    __shared__ __align__(128) float4 buf[kStages][kTile32];
+    __shared__ __align__(8) uint64_t full[kStages];
+    constexpr int kPairs = kAdjPPT32 / 2;
+    const int j0 = (blockIdx.x * kThreads + threadIdx.x) * kAdjPPT32;
+    f32x2 xj[kPairs], yj[kPairs];
+#pragma unroll
+    for (int h = 0; h < kPairs; ++h) {
+        const int a = min(j0 + 2 * h, npil - 1), b = min(j0 + 2 * h + 1, npil - 1);
+        xj[h] = pk2((float)(px[a] - g.ox), (float)(px[b] - g.ox));
+        yj[h] = pk2((float)(py[a] - g.oy), (float)(py[b] - g.oy));
+    }
+    const f32x2 NEG1 = dup2(-1.0f), NZ = dup2(-z), Z2X = dup2(2.0f * z), NHALF = dup2(-0.5f);
+    const f32x2 Z2 = dup2(z * z), ILHI = dup2(il_hi), ILLO = dup2(il_lo), MAGIC = dup2(12582912.0f);
+    const f32x2 TWOPI = dup2(6.28318530717958647692f);
+
+    TilePipe<float4, kTile32> pipe;
+    const int lo = blockIdx.y * chunk_len;
+    pipe.init(buf, full, pix, lo, min(npix, lo + chunk_len));
+
+    float sr[kAdjPPT32], cr[kAdjPPT32], si[kAdjPPT32], ci[kAdjPPT32];
+#pragma unroll
+    for (int q = 0; q < kAdjPPT32; ++q) sr[q] = cr[q] = si[q] = ci[q] = 0.f;
+
+    for (int t = 0; t < pipe.ntiles; ++t) {
+        const bool got = pipe.wait(t);
+        if (got) {
+            const float4* tile = buf[t % kStages];
+            const int cnt = pipe.count(t);
+            f32x2 er[kPairs], ei[kPairs];
+#pragma unroll
+            for (int h = 0; h < kPairs; ++h) er[h] = ei[h] = 0ull;
+#pragma unroll 2
+            for (int p = 0; p < cnt; ++p) {
+                const float4 r = tile[p];  // {fx, fy, Re v, Im v}
+                const f32x2 FX = dup2(r.x), FY = dup2(r.y), VR = dup2(r.z), VI = dup2(r.w), NVR = dup2(-r.z);
+#pragma unroll
+                for (int h = 0; h < kPairs; ++h) {
+                    const f32x2 dx = fma2(xj[h], NEG1, FX), ndx = fma2(FX, NEG1, xj[h]);
+                    const f32x2 dy = fma2(yj[h], NEG1, FY), ndy = fma2(FY, NEG1, yj[h]);
+                    const f32x2 u = fma2(dx, dx, fma2(dy, dy, Z2));         // R^2 (seed only)
+                    const f32x2 ns = fma2(dx, ndx, mul2(dy, ndy));          // -rho^2
+                    float ua, ub;
+                    upk2(u, ua, ub);
+                    const f32x2 ri = pk2(rsqrt_approx(ua), rsqrt_approx(ub));  // ~1/R
+                    const f32x2 d0 = fma2(u, ri, NZ);
+                    const f32x2 gg = fma2(d0, d0, fma2(Z2X, d0, ns));
+                    const f32x2 d = fma2(mul2(gg, ri), NHALF, d0);           // R - z
+                    const f32x2 th = fma2(d, ILHI, mul2(d, ILLO));           // (R - z)/lambda, turns
+                    const f32x2 w = fma2(add2(th, MAGIC), NEG1, MAGIC);
+                    const f32x2 ang = mul2(add2(th, w), TWOPI);
+                    float aa, ab;
+                    upk2(ang, aa, ab);
+                    const f32x2 pr = mul2(ri, pk2(cos_approx(aa), cos_approx(ab)));
+                    const f32x2 pi = mul2(ri, pk2(sin_approx(aa), sin_approx(ab)));
+                    er[h] = fma2(pi, VI, fma2(pr, VR, er[h]));
+                    ei[h] = fma2(pi, NVR, fma2(pr, VI, ei[h]));
+                }
+            }
+#pragma unroll
+            for (int h = 0; h < kPairs; ++h) {
+                float e0, e1, f0, f1;
+                upk2(er[h], e0, e1);
+                upk2(ei[h], f0, f1);
+                two_sum_acc(sr[2 * h], cr[2 * h], e0);
+                two_sum_acc(sr[2 * h + 1], cr[2 * h + 1], e1);
+                two_sum_acc(si[2 * h], ci[2 * h], f0);
+                two_sum_acc(si[2 * h + 1], ci[2 * h + 1], f1);
+            }
+        }
+        if (!pipe.release(t, got)) return;
+    }
+#pragma unroll
+    for (int q = 0; q < kAdjPPT32; ++q)
+        if (j0 + q < npil)
+            partial[(size_t)blockIdx.y * npil + j0 + q] =
+                make_double2((double)sr[q] + (double)cr[q], (double)si[q] + (double)ci[q]);
+}
+
+// chunk sums of the precision-form adjoint, then the factor e^{-ikz} in FP64
+__global__ void adj_f32c_reduce(const double2* __restrict__ partial, int nchunk, int n, double kz,
+                                double2* __restrict__ out) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double r = 0.0, i = 0.0;
+    for (int c = 0; c < nchunk; ++c) {
+        const double2 v = partial[(size_t)c * n + j];
+        r += v.x;
+        i += v.y;
+    }
+    double sn, cs;
+    sincos(kz, &sn, &cs);
+    out[j] = make_double2(r * cs + i * sn, i * cs - r * sn);
 }
 
 // ---- chunk reduction + epilogue ---------------------------------------------
@@ -687,11 +803,36 @@ int ff_run(int form, const double* d_px, const double* d_py, const double* d_pt,
 }
 
 int ff_adjoint(const double* d_px, const double* d_py, int npil, const Geom& g, double k,
-               const double* d_v, double* d_out, cudaStream_t st) {
+               const double* d_v, double* d_out, cudaStream_t st, int form = CELERIS_FORM_PLAIN_F64) {
     const long npix = (long)g.nx * g.ny;
     if (npil <= 0) return CELERIS_OK;
     if (npix <= 0) {
         CEL_CUDA(cudaMemsetAsync(d_out, 0, (size_t)npil * 2 * sizeof(double), st));
+        return CELERIS_OK;
+    }
+    if (form == CELERIS_FORM_F32C) {
+        const int ctas = (int)(((long)npil + kThreads * kAdjPPT32 - 1) / (kThreads * kAdjPPT32));
+        int nchunk = 1, chunk_len = (int)npix;
+        plan_chunks(ctas, (int)npix, kTile32, 3, &nchunk, &chunk_len);
+        Workspace& ws = Workspace::for_stream(st);
+        const size_t rec_bytes = (size_t)npix * sizeof(float4);
+        const size_t part_bytes = (size_t)nchunk * npil * sizeof(double2);
+        CEL_TRY(ws.reserve(st, celeris_rt::align256(rec_bytes) + celeris_rt::align256(part_bytes)));
+        float4* rec = static_cast<float4*>(ws.take(rec_bytes));
+        double2* partial = static_cast<double2*>(ws.take(part_bytes));
+        ff_pack_pix_f32<<<(int)((npix + 255) / 256), 256, 0, st>>>(g, reinterpret_cast<const double2*>(d_v), rec);
+        const double il = k / (2.0 * 3.14159265358979323846);
+        const float hi = (float)il, lo = (float)(il - (double)hi);
+        const float zf = (float)g.z;
+        dim3 grid(ctas, nchunk);
+        timer_begin(st);
+        rs_adj_f32c_kernel<<<grid, kThreads, 0, st>>>(rec, (int)npix, chunk_len, d_px, d_py, npil, g, zf, hi, lo,
+                                                      partial);
+        timer_end(st);
+        adj_f32c_reduce<<<(npil + 255) / 256, 256, 0, st>>>(partial, nchunk, npil, k * (double)zf,
+                                                           reinterpret_cast<double2*>(d_out));
+        count_launch(3);
+        CEL_CUDA(cudaGetLastError());
         return CELERIS_OK;
     }
     const int ctas = (int)(((long)npil + kThreads * kAdjPPT - 1) / (kThreads * kAdjPPT));
@@ -990,14 +1131,13 @@ int celeris_rs_field_dev(int form, const double* d_px, const double* d_py, const
 int celeris_rs_adjoint_dev(int form, const double* d_px, const double* d_py, int npil, double cx,
                            double cy, double z, double k, int n, double half_window,
                            const double* d_v, double* d_out, void* stream) {
-    if (form != CELERIS_FORM_PLAIN_F64)
-        return set_error(CELERIS_ERR_INVALID_ARG, "adjoint: only the plain FP64 form is provided");
+    if (!valid_form(form)) return set_error(CELERIS_ERR_INVALID_ARG, "unknown form %d", form);
     if (n < 0 || npil < 0) return set_error(CELERIS_ERR_INVALID_ARG, "negative size");
     if (npil > 0 && (!d_px || !d_py || !d_out)) return set_error(CELERIS_ERR_INVALID_ARG, "NULL arrays");
     if ((long)n * n > 0 && !d_v) return set_error(CELERIS_ERR_INVALID_ARG, "d_v is NULL");
     CEL_TRY(celeris_rt::require_device());
     return ff_adjoint(d_px, d_py, npil, psf_geom(cx, cy, z, n, half_window), k, d_v, d_out,
-                      static_cast<cudaStream_t>(stream));
+                      static_cast<cudaStream_t>(stream), form);
 }
 
 int celeris_rs_check_dev(const double* d_px, const double* d_py, const double* d_pt, int npil,

@@ -65,11 +65,13 @@ def rs_field_dev(px, py, t, grid: FarFieldGrid, form=capi.FORM_PLAIN_F64, want_i
     return (E, inten) if want_intensity else E
 
 
-def rs_adjoint_dev(px, py, v, grid: FarFieldGrid):
+def rs_adjoint_dev(px, py, v, grid: FarFieldGrid, form=capi.FORM_PLAIN_F64):
+    """out_j = sum_p conj(g_pj) v_p in the plain FP64 or the precision (packed FP32,
+    compensated sums, e^{-ikz} in FP64) form."""
     lib = capi.load()
     out = torch.empty(px.numel(), dtype=torch.complex128, device=v.device)
     v = v.contiguous()
-    capi.check(lib.celeris_rs_adjoint_dev(capi.FORM_PLAIN_F64, _ptr(px), _ptr(py), int(px.numel()), grid.cx,
+    capi.check(lib.celeris_rs_adjoint_dev(form, _ptr(px), _ptr(py), int(px.numel()), grid.cx,
                                           grid.cy, grid.z, grid.k, grid.n, grid.W, _ptr(v), _ptr(out),
                                           _stream()))
     return out
@@ -81,13 +83,15 @@ class RSField(torch.autograd.Function):
         t = t.contiguous()
         ctx.save_for_backward(px, py)
         ctx.grid = grid
+        ctx.form = form
         return rs_field_dev(px, py, t, grid, form)
 
     @staticmethod
     def backward(ctx, grad_E):
+        # the adjoint runs in the forward's form
         px, py = ctx.saved_tensors
         g = grad_E.to(torch.complex128).contiguous()
-        return rs_adjoint_dev(px, py, g, ctx.grid), None, None, None, None
+        return rs_adjoint_dev(px, py, g, ctx.grid, ctx.form), None, None, None, None
 
 
 def rs_field(t, px, py, grid: FarFieldGrid, form=capi.FORM_PLAIN_F64):

@@ -149,6 +149,9 @@ int celeris_rs_field_noalloc(int form, const double* d_px, const double* d_py,
  *   d_out[j] = sum_p conj(g_pj) * d_v[p],   g_pj = exp(i k R_pj) / R_pj.
  * d_v: n*n complex, d_out: npil complex. This is the vector-Jacobian product of
  * celeris_rs_field_dev w.r.t. the pillar transmissions t (PyTorch convention).
+ * form: CELERIS_FORM_PLAIN_F64, or CELERIS_FORM_F32C (the precision form's
+ * arithmetic with pillars as outputs: packed FP32 terms, compensated sums,
+ * e^{-ikz} applied in FP64).
  * The reference has no adjoint (its only gradient is central finite differences
  * of RCWA, src/celeris/design/optimize.cpp:60-71). */
 int celeris_rs_adjoint_dev(int form, const double* d_px, const double* d_py,

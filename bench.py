@@ -271,6 +271,17 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------- GPU arm
+def measured_hbm_gbs():
+    """HBM copy bandwidth measured on this pool's B200s (MEASURED_PEAKS.json), else
+    the pool's earlier measurement."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json)"
+    except Exception:
+        return 6650.0, "fallback (6.65 TB/s, an earlier measurement on this pool)"
+
+
 def profiles_traffic(kernel):
     """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", f"{kernel}.md")
@@ -554,6 +565,12 @@ def run_gpu(args):
         "measured_peaks": peaks, "kernel_ms_per_launch": k_ms,
         "algorithmic_bytes_per_launch": ap.npil * 16 + g.npix * 16,
     }
+    # the HBM roof against the driver-measured copy bandwidth, for reference: far
+    # below the binding SFU roof (the kernel reads each pillar tile once per CTA)
+    hbm, src = measured_hbm_gbs()
+    alg_gbs = (ap.npil * 16 + g.npix * 16) / (k_ms * 1e-3) / 1e9
+    out["roofline"]["hbm"] = {"bound": "hbm", "achieved": alg_gbs, "peak": hbm, "unit": "GB/s",
+                              "frac": alg_gbs / hbm, "traffic": out["roofline"]["traffic"], "peak_source": src}
     # ---- plain FP64 form, same workload ----------------------------------------
     f64 = lambda: T.rs_field_dev(px, py, t, grid, capi.FORM_PLAIN_F64)  # noqa: E731
     f64()

@@ -674,10 +674,25 @@ int sm_count() {
 void plan_chunks(int ctas_other, int nrec, int tile, int resident_per_sm, int* nchunk,
                  int* chunk_len) {
     const int ntiles = std::max(1, (nrec + tile - 1) / tile);
-    const long target = (long)sm_count() * resident_per_sm * 8;
+    const long slots = (long)sm_count() * resident_per_sm;  // CTAs resident at once
+    const long target = slots * 8;
     long want = (target + ctas_other - 1) / std::max(1, ctas_other);
     want = std::max(1L, std::min<long>(want, ntiles));
-    const int tiles_per = (int)((ntiles + want - 1) / want);
+    // Among want .. 2 want chunks pick the count whose grid fills its last wave
+    // of resident CTAs best (CTAs of one launch take about equally long).
+    long best_c = want;
+    double best_fill = -1.0;
+    for (long c = want; c <= std::min<long>(2 * want, ntiles); ++c) {
+        const int tiles_per = (int)((ntiles + c - 1) / c);
+        const long chunks = (ntiles + tiles_per - 1) / tiles_per;
+        const double waves = (double)(ctas_other * chunks) / (double)slots;
+        const double fill = waves / std::ceil(waves);
+        if (fill > best_fill + 1e-9) {
+            best_fill = fill;
+            best_c = c;
+        }
+    }
+    const int tiles_per = (int)((ntiles + best_c - 1) / best_c);
     *chunk_len = tiles_per * tile;
     *nchunk = (nrec + *chunk_len - 1) / *chunk_len;
     if (*nchunk < 1) *nchunk = 1;

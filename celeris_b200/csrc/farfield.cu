@@ -872,12 +872,14 @@ int ff_adjoint(const double* d_px, const double* d_py, int npil, const Geom& g, 
     return CELERIS_OK;
 }
 
-int ff_check(const double* d_px, const double* d_py, const double* d_pt, int npil, const Geom& g,
-             double k, const double* d_field, const int* d_idx, int ns, double* err_out,
-             cudaStream_t st) {
+// Enqueue the sampled FP64 check on st: when st reaches the end, h_bits[0] and
+// h_bits[1] hold the bits of max |E - E_FP64| over the samples and of
+// max |E| over the field (h_bits: host memory; pinned keeps the copy
+// asynchronous).
+int ff_check_enqueue(const double* d_px, const double* d_py, const double* d_pt, int npil, const Geom& g,
+                     double k, const double* d_field, const int* d_idx, int ns, unsigned long long* h_bits,
+                     cudaStream_t st) {
     const long npix = (long)g.nx * g.ny;
-    *err_out = 0.0;
-    if (npil <= 0 || npix <= 0 || ns <= 0) return CELERIS_OK;
     Workspace& ws = Workspace::for_stream(st);
     const size_t rec_bytes = (size_t)npil * sizeof(double4);
     CEL_TRY(ws.reserve(st, celeris_rt::align256(rec_bytes) + 256));
@@ -892,27 +894,84 @@ int ff_check(const double* d_px, const double* d_py, const double* d_pt, int npi
                                                    (int)npix, bits + 1);
     count_launch(3);
     CEL_CUDA(cudaGetLastError());
-    unsigned long long h[2];
-    CEL_CUDA(cudaMemcpyAsync(h, bits, sizeof(h), cudaMemcpyDeviceToHost, st));
-    CEL_CUDA(cudaStreamSynchronize(st));
+    CEL_CUDA(cudaMemcpyAsync(h_bits, bits, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    return CELERIS_OK;
+}
+
+// The stated error from the two words of ff_check_enqueue: max error / max |E|.
+double check_ratio(const unsigned long long* h) {
     double e, m;
     std::memcpy(&e, &h[0], sizeof(double));
     std::memcpy(&m, &h[1], sizeof(double));
-    *err_out = m > 0.0 ? e / m : e;
+    return m > 0.0 ? e / m : e;
+}
+
+int ff_check(const double* d_px, const double* d_py, const double* d_pt, int npil, const Geom& g,
+             double k, const double* d_field, const int* d_idx, int ns, double* err_out,
+             cudaStream_t st) {
+    *err_out = 0.0;
+    if (npil <= 0 || (long)g.nx * g.ny <= 0 || ns <= 0) return CELERIS_OK;
+    unsigned long long h[2] = {0, 0};
+    CEL_TRY(ff_check_enqueue(d_px, d_py, d_pt, npil, g, k, d_field, d_idx, ns, h, st));
+    CEL_CUDA(cudaStreamSynchronize(st));
+    *err_out = check_ratio(h);
     return check_status_and_reset();
 }
 
-// One non-blocking stream per host thread for the synchronous host-buffer calls.
-cudaStream_t thread_stream() {
-    thread_local cudaStream_t s = nullptr;
+// Non-blocking streams per host thread for the synchronous host-buffer calls:
+// which = 0 carries the call, which = 1 the stated-error check beside it.
+cudaStream_t thread_stream(int which = 0) {
+    thread_local cudaStream_t s[2] = {nullptr, nullptr};
+    thread_local int dev[2] = {-1, -1};
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (!s[which] || dev[which] != cur) {
+        cudaStreamCreateWithFlags(&s[which], cudaStreamNonBlocking);
+        dev[which] = cur;
+    }
+    return s[which];
+}
+
+// Per-thread events without timing, created on first use.
+cudaEvent_t thread_event(size_t i) {
+    thread_local std::vector<cudaEvent_t> ev;
     thread_local int dev = -1;
     int cur = 0;
     cudaGetDevice(&cur);
-    if (!s || dev != cur) {
-        cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (dev != cur) {
+        ev.clear();  // events of another device stay with it
         dev = cur;
     }
-    return s;
+    while (ev.size() <= i) {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+        ev.push_back(e);
+    }
+    return ev[i];
+}
+
+// Host <-> device copies through pinned staging go in pieces of this size, so
+// the host copy of one piece overlaps the transfer of the next.
+constexpr size_t kPiece = (size_t)4 << 20;
+
+// D2H of `bytes` from src into the caller's dst through pinned `stage`
+// (per-thread events 1, 2, ...).
+int download(void* dst, char* stage, const void* src, size_t bytes, cudaStream_t st) {
+    if (!dst || bytes == 0) return CELERIS_OK;
+    const size_t np = (bytes + kPiece - 1) / kPiece;
+    for (size_t i = 0; i < np; ++i) {
+        const size_t o = i * kPiece, b = std::min(kPiece, bytes - o);
+        cudaEvent_t e = thread_event(1 + i);
+        if (!e) return set_error(CELERIS_ERR_CUDA, "cudaEventCreate failed");
+        CEL_CUDA(cudaMemcpyAsync(stage + o, static_cast<const char*>(src) + o, b, cudaMemcpyDeviceToHost, st));
+        CEL_CUDA(cudaEventRecord(e, st));
+    }
+    for (size_t i = 0; i < np; ++i) {
+        const size_t o = i * kPiece, b = std::min(kPiece, bytes - o);
+        CEL_CUDA(cudaEventSynchronize(thread_event(1 + i)));
+        std::memcpy(static_cast<char*>(dst) + o, stage + o, b);
+    }
+    return CELERIS_OK;
 }
 
 // Sample of pixel indices for the stated error: a strided lattice plus the
@@ -950,7 +1009,8 @@ int ff_host(int form, const double* px, const double* py, const double* pt, int 
     const size_t idx_bytes = sidx.size() * sizeof(int);
     const size_t pin_bytes = celeris_rt::align256(in_bytes) + celeris_rt::align256(fld_bytes) +
                              celeris_rt::align256(int_bytes) + celeris_rt::align256(idx_bytes);
-    char* pin = static_cast<char*>(celeris_rt::pinned_staging(pin_bytes));
+    // pinned: the device I/O layout, then the two words of the error check
+    char* pin = static_cast<char*>(celeris_rt::pinned_staging(pin_bytes + 256));
     if (!pin) return set_error(CELERIS_ERR_OOM, "pinned staging of %zu bytes failed", pin_bytes);
 
     // Device I/O buffers live in their own persistent arena (separate from the
@@ -976,12 +1036,20 @@ int ff_host(int form, const double* px, const double* py, const double* pt, int 
                                               celeris_rt::align256(fld_bytes));
     int* d_idx = reinterpret_cast<int*>(d + celeris_rt::align256(in_bytes) +
                                         celeris_rt::align256(fld_bytes) + celeris_rt::align256(int_bytes));
-    double* h_px = reinterpret_cast<double*>(pin);
     if (npil > 0) {
-        std::memcpy(h_px, px, npil * sizeof(double));
-        std::memcpy(h_px + npil, py, npil * sizeof(double));
-        std::memcpy(h_px + 2 * npil, pt, npil * 2 * sizeof(double));
-        CEL_CUDA(cudaMemcpyAsync(d_px, h_px, in_bytes, cudaMemcpyHostToDevice, st));
+        // px | py | pt, each piece sent while the next one is staged
+        const char* src[3] = {reinterpret_cast<const char*>(px), reinterpret_cast<const char*>(py),
+                              reinterpret_cast<const char*>(pt)};
+        const size_t len[3] = {npil * sizeof(double), npil * sizeof(double), npil * 2 * sizeof(double)};
+        size_t off = 0;
+        for (int a = 0; a < 3; ++a) {
+            for (size_t o = 0; o < len[a]; o += kPiece) {
+                const size_t b = std::min(kPiece, len[a] - o);
+                std::memcpy(pin + off + o, src[a] + o, b);
+                CEL_CUDA(cudaMemcpyAsync(d + off + o, pin + off + o, b, cudaMemcpyHostToDevice, st));
+            }
+            off += len[a];
+        }
     }
     if (want_err) {
         int* h_idx = reinterpret_cast<int*>(pin + celeris_rt::align256(in_bytes) +
@@ -992,18 +1060,28 @@ int ff_host(int form, const double* px, const double* py, const double* pt, int 
     const bool need_field = field_out || want_err;
     CEL_TRY(ff_run(form, d_px, d_py, d_pt, npil, g, k, need_field ? d_fld : nullptr,
                    int_out ? d_int : nullptr, st));
-    double* h_fld = reinterpret_cast<double*>(pin + celeris_rt::align256(in_bytes));
-    double* h_int = reinterpret_cast<double*>(pin + celeris_rt::align256(in_bytes) + celeris_rt::align256(fld_bytes));
-    if (field_out) CEL_CUDA(cudaMemcpyAsync(h_fld, d_fld, fld_bytes, cudaMemcpyDeviceToHost, st));
-    if (int_out) CEL_CUDA(cudaMemcpyAsync(h_int, d_int, int_bytes, cudaMemcpyDeviceToHost, st));
+    char* h_fld = pin + celeris_rt::align256(in_bytes);
+    char* h_int = h_fld + celeris_rt::align256(fld_bytes);
+    unsigned long long* h_bits = reinterpret_cast<unsigned long long*>(pin + pin_bytes);
+    // the stated-error check runs on the second stream while the field downloads
+    cudaStream_t st2 = want_err ? thread_stream(1) : nullptr;
     if (want_err) {
-        CEL_TRY(ff_check(d_px, d_py, d_pt, npil, g, k, d_fld, d_idx, (int)sidx.size(), err_out, st));
+        h_bits[0] = h_bits[1] = 0;
+        cudaEvent_t done = thread_event(0);
+        if (!done) return set_error(CELERIS_ERR_CUDA, "cudaEventCreate failed");
+        CEL_CUDA(cudaEventRecord(done, st));
+        CEL_CUDA(cudaStreamWaitEvent(st2, done, 0));
+        CEL_TRY(ff_check_enqueue(d_px, d_py, d_pt, npil, g, k, d_fld, d_idx, (int)sidx.size(), h_bits, st2));
     }
-    CEL_CUDA(cudaStreamSynchronize(st));
-    CEL_TRY(check_status_and_reset());
-    if (field_out) std::memcpy(field_out, h_fld, fld_bytes);
-    if (int_out) std::memcpy(int_out, h_int, int_bytes);
-    return CELERIS_OK;
+    const int rd = download(field_out, h_fld, d_fld, field_out ? fld_bytes : 0, st);
+    const int ri = rd == CELERIS_OK ? download(int_out, h_int, d_int, int_out ? int_bytes : 0, st) : rd;
+    cudaError_t e1 = cudaStreamSynchronize(st);
+    cudaError_t e2 = want_err ? cudaStreamSynchronize(st2) : cudaSuccess;
+    CEL_TRY(ri);
+    CEL_CUDA(e1);
+    CEL_CUDA(e2);
+    if (want_err) *err_out = check_ratio(h_bits);
+    return check_status_and_reset();
 }
 
 bool valid_form(int form) { return form == CELERIS_FORM_PLAIN_F64 || form == CELERIS_FORM_F32C; }

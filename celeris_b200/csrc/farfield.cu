@@ -745,6 +745,11 @@ std::atomic<int> g_time_kernels{0};
 struct KernelTimer {
     cudaEvent_t a = nullptr, b = nullptr;
     bool pending = false;
+    ~KernelTimer() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+        cudaGetLastError();
+    }
 };
 thread_local KernelTimer t_timer;
 
@@ -920,35 +925,61 @@ int ff_check(const double* d_px, const double* d_py, const double* d_pt, int npi
 
 // Non-blocking streams per host thread for the synchronous host-buffer calls:
 // which = 0 carries the call, which = 1 the stated-error check beside it.
-cudaStream_t thread_stream(int which = 0) {
-    thread_local cudaStream_t s[2] = {nullptr, nullptr};
-    thread_local int dev[2] = {-1, -1};
-    int cur = 0;
-    cudaGetDevice(&cur);
-    if (!s[which] || dev[which] != cur) {
-        cudaStreamCreateWithFlags(&s[which], cudaStreamNonBlocking);
-        dev[which] = cur;
-    }
-    return s[which];
-}
+thread_local celeris_rt::ThreadStream t_streams[2];
 
-// Per-thread events without timing, created on first use.
+int thread_stream(cudaStream_t* out, int which = 0) { return t_streams[which].get(out); }
+
+// Per-thread events without timing, created on first use, destroyed with the
+// thread (and when the thread moves to another device).
+struct ThreadEvents {
+    std::vector<cudaEvent_t> ev;
+    int dev = -1;
+    void clear() {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+        ev.clear();
+        cudaGetLastError();
+    }
+    ~ThreadEvents() { clear(); }
+};
+thread_local ThreadEvents t_events;
+
 cudaEvent_t thread_event(size_t i) {
-    thread_local std::vector<cudaEvent_t> ev;
-    thread_local int dev = -1;
     int cur = 0;
     cudaGetDevice(&cur);
-    if (dev != cur) {
-        ev.clear();  // events of another device stay with it
-        dev = cur;
+    if (t_events.dev != cur) {
+        t_events.clear();
+        t_events.dev = cur;
     }
-    while (ev.size() <= i) {
+    while (t_events.ev.size() <= i) {
         cudaEvent_t e = nullptr;
         if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
-        ev.push_back(e);
+        t_events.ev.push_back(e);
     }
-    return ev[i];
+    return t_events.ev[i];
 }
+
+// Device I/O buffers of the host-buffer calls, one per thread (separate from
+// the scratch arena the kernels use on the same stream); freed with the thread.
+struct ThreadIo {
+    void* p = nullptr;
+    size_t cap = 0;
+    int dev = -1;
+    void release() {
+        if (p) {
+            int cur = 0;
+            cudaGetDevice(&cur);
+            cudaSetDevice(dev);
+            cudaFree(p);
+            cudaSetDevice(cur);
+            cudaGetLastError();
+        }
+        p = nullptr;
+        cap = 0;
+        dev = -1;
+    }
+    ~ThreadIo() { release(); }
+};
+thread_local ThreadIo t_io;
 
 // Host <-> device copies through pinned staging go in pieces of this size, so
 // the host copy of one piece overlaps the transfer of the next.
@@ -998,7 +1029,8 @@ int ff_host(int form, const double* px, const double* py, const double* pt, int 
     if (npix <= 0) return CELERIS_OK;
     if (npil < 0) return set_error(CELERIS_ERR_INVALID_ARG, "npil < 0");
     if (npil > 0 && (!px || !py || !pt)) return set_error(CELERIS_ERR_INVALID_ARG, "NULL pillar arrays");
-    cudaStream_t st = thread_stream();
+    cudaStream_t st = nullptr;
+    CEL_TRY(thread_stream(&st));
     const bool want_err = (form == CELERIS_FORM_F32C) && err_out && npil > 0;
     std::vector<int> sidx;
     if (want_err) sidx = sample_pixels(g.nx, g.ny, 256);
@@ -1013,21 +1045,16 @@ int ff_host(int form, const double* px, const double* py, const double* pt, int 
     char* pin = static_cast<char*>(celeris_rt::pinned_staging(pin_bytes + 256));
     if (!pin) return set_error(CELERIS_ERR_OOM, "pinned staging of %zu bytes failed", pin_bytes);
 
-    // Device I/O buffers live in their own persistent arena (separate from the
-    // scratch arena the kernels use on the same stream).
-    static thread_local void* d_io = nullptr;
-    static thread_local size_t d_io_cap = 0;
-    if (d_io_cap < pin_bytes) {
-        if (d_io) {
-            cudaStreamSynchronize(st);
-            cudaFree(d_io);
-        }
-        d_io = nullptr;
-        d_io_cap = 0;
-        CEL_CUDA(cudaMalloc(&d_io, pin_bytes));
-        d_io_cap = pin_bytes;
+    int dev = 0;
+    CEL_CUDA(cudaGetDevice(&dev));
+    if (t_io.cap < pin_bytes || t_io.dev != dev) {
+        CEL_CUDA(cudaStreamSynchronize(st));
+        t_io.release();
+        CEL_CUDA(cudaMalloc(&t_io.p, pin_bytes));
+        t_io.cap = pin_bytes;
+        t_io.dev = dev;
     }
-    char* d = static_cast<char*>(d_io);
+    char* d = static_cast<char*>(t_io.p);
     double* d_px = reinterpret_cast<double*>(d);
     double* d_py = d_px + npil;
     double* d_pt = d_py + npil;
@@ -1064,8 +1091,9 @@ int ff_host(int form, const double* px, const double* py, const double* pt, int 
     char* h_int = h_fld + celeris_rt::align256(fld_bytes);
     unsigned long long* h_bits = reinterpret_cast<unsigned long long*>(pin + pin_bytes);
     // the stated-error check runs on the second stream while the field downloads
-    cudaStream_t st2 = want_err ? thread_stream(1) : nullptr;
+    cudaStream_t st2 = nullptr;
     if (want_err) {
+        CEL_TRY(thread_stream(&st2, 1));
         h_bits[0] = h_bits[1] = 0;
         cudaEvent_t done = thread_event(0);
         if (!done) return set_error(CELERIS_ERR_CUDA, "cudaEventCreate failed");

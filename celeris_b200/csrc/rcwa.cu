@@ -1206,7 +1206,11 @@ int autotune(const BucketPlan& p, cudaStream_t st, StageCfg* out) {
 }
 
 // Per-thread execution context: streams, pinned staging and the cached graph.
+// The device objects follow the thread's current device (rebuilt when it
+// changes) and are released, with the main stream's workspace arena, when the
+// thread exits.
 struct BatchCtx {
+    int dev = -1;
     cudaStream_t main = nullptr;
     std::vector<cudaStream_t> side;
     std::vector<cudaEvent_t> fork, join;
@@ -1215,12 +1219,50 @@ struct BatchCtx {
     cudaGraphExec_t exec = nullptr;
     std::string sig;
     uint64_t nkern = 0;  // kernels per graph launch
+
+    void drop_device_objects() {
+        if (!main) return;
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(dev);
+        cudaStreamSynchronize(main);
+        for (cudaStream_t s : side) cudaStreamSynchronize(s);
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        sig.clear();
+        Workspace::release_stream(main);
+        for (cudaStream_t s : side) {
+            Workspace::release_stream(s);
+            cudaStreamDestroy(s);
+        }
+        for (cudaEvent_t e : fork) cudaEventDestroy(e);
+        for (cudaEvent_t e : join) cudaEventDestroy(e);
+        cudaStreamDestroy(main);
+        side.clear();
+        fork.clear();
+        join.clear();
+        main = nullptr;
+        dev = -1;
+        cudaSetDevice(cur);
+        cudaGetLastError();  // a failure here (e.g. the runtime shutting down) is nobody's call's error
+    }
+    ~BatchCtx() {
+        drop_device_objects();
+        if (pinned) cudaFreeHost(pinned);
+        cudaGetLastError();
+    }
 };
 thread_local BatchCtx t_ctx;
 
 int ensure_streams(int nb) {
     BatchCtx& c = t_ctx;
-    if (!c.main) CEL_CUDA(cudaStreamCreateWithFlags(&c.main, cudaStreamNonBlocking));
+    int cur = 0;
+    CEL_CUDA(cudaGetDevice(&cur));
+    if (c.main && c.dev != cur) c.drop_device_objects();
+    if (!c.main) {
+        CEL_CUDA(cudaStreamCreateWithFlags(&c.main, cudaStreamNonBlocking));
+        c.dev = cur;
+    }
     while ((int)c.side.size() < nb) {
         cudaStream_t s;
         cudaEvent_t f, j;
@@ -1536,13 +1578,9 @@ int run_stacks(const celeris_rcwa_cell* layers, const std::vector<std::pair<int,
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     // one stream (and so one workspace arena) per calling thread for the stack path
-    static thread_local cudaStream_t t_stack_st = nullptr;
-    static thread_local int t_stack_dev = -1;
-    if (!t_stack_st || t_stack_dev != dev) {
-        CEL_CUDA(cudaStreamCreateWithFlags(&t_stack_st, cudaStreamNonBlocking));
-        t_stack_dev = dev;
-    }
-    cudaStream_t st = t_stack_st;
+    static thread_local celeris_rt::ThreadStream t_stack_st;
+    cudaStream_t st = nullptr;
+    CEL_TRY(t_stack_st.get(&st));
     Workspace& ws = Workspace::for_stream(st);
     // stacks grouped by (Mx, My): one layer store and one recursion launch per group
     std::map<std::pair<int, int>, std::vector<int>> groups;
@@ -1788,13 +1826,9 @@ int run_eig(const double* A, int n, int count, double* evals, double* evecs, int
     const size_t s_nn = (size_t)n * n, s_n = (size_t)n;
     int dev = 0;
     CEL_CUDA(cudaGetDevice(&dev));
-    static thread_local cudaStream_t t_eig_st = nullptr;  // one stream and arena per calling thread
-    static thread_local int t_eig_dev = -1;
-    if (!t_eig_st || t_eig_dev != dev) {
-        CEL_CUDA(cudaStreamCreateWithFlags(&t_eig_st, cudaStreamNonBlocking));
-        t_eig_dev = dev;
-    }
-    cudaStream_t st = t_eig_st;
+    static thread_local celeris_rt::ThreadStream t_eig_st;  // one stream and arena per calling thread
+    cudaStream_t st = nullptr;
+    CEL_TRY(t_eig_st.get(&st));
     Workspace& ws = Workspace::for_stream(st);
     if (n <= kSmemEigMaxN)
         CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_hess<true>), (s_nn + 2 * s_n) * sizeof(cplx)));

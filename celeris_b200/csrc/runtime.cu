@@ -112,6 +112,52 @@ Workspace& Workspace::for_stream(cudaStream_t stream) {
     return *it->second;
 }
 
+void Workspace::release_stream(cudaStream_t stream) {
+    std::lock_guard<std::mutex> lk(g_ws_mu);
+    auto& m = ws_map();
+    for (auto it = m.begin(); it != m.end();) {
+        if (it->first.second != stream) {
+            ++it;
+            continue;
+        }
+        if (it->second->base_) {
+            int cur = 0;
+            cudaGetDevice(&cur);
+            cudaSetDevice(it->first.first);
+            cudaFree(it->second->base_);
+            cudaSetDevice(cur);
+        }
+        delete it->second;
+        it = m.erase(it);
+    }
+}
+
+int ThreadStream::get(cudaStream_t* out) {
+    int cur = 0;
+    CEL_CUDA(cudaGetDevice(&cur));
+    if (!s_ || dev_ != cur) {
+        drop();
+        CEL_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
+        dev_ = cur;
+    }
+    *out = s_;
+    return CELERIS_OK;
+}
+
+void ThreadStream::drop() {
+    if (!s_) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(dev_);
+    cudaStreamSynchronize(s_);
+    Workspace::release_stream(s_);
+    cudaStreamDestroy(s_);
+    cudaSetDevice(cur);
+    cudaGetLastError();  // a failure here (e.g. the runtime shutting down) is nobody's call's error
+    s_ = nullptr;
+    dev_ = -1;
+}
+
 void Workspace::release_all() {
     std::lock_guard<std::mutex> lk(g_ws_mu);
     for (auto& kv : ws_map()) {

@@ -54,6 +54,9 @@ public:
 
     static Workspace& for_stream(cudaStream_t stream);
     static void release_all();
+    // Free the arenas that belong to `stream` (on any device); the stream must
+    // be idle.
+    static void release_stream(cudaStream_t stream);
 
 private:
     void* base_ = nullptr;
@@ -62,6 +65,21 @@ private:
 };
 
 inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// A non-blocking stream owned by the calling thread (declare it thread_local):
+// created on first use for the current device and replaced when the device
+// changes. When it is replaced, and when the thread exits, the stream is
+// synchronized, its workspace arenas are freed and it is destroyed.
+class ThreadStream {
+public:
+    int get(cudaStream_t* out);
+    ~ThreadStream() { drop(); }
+
+private:
+    void drop();
+    cudaStream_t s_ = nullptr;
+    int dev_ = -1;
+};
 
 // Pinned host staging for the synchronous host-buffer entry points (one per
 // calling thread; grows).

@@ -773,6 +773,106 @@ __device__ void blk_hessenberg(int n, cplx* H, int ldh, cplx* Z, int ldz, cplx* 
     }
 }
 
+// The same reduction without Z: reflector k (v_k of length m = n-k-1, beta_k;
+// beta_k = 0 where column k needed none) is recorded in row k of `refl`
+// (n x n, global): v_k in [0, m), beta_k in the real part of entry n-1.
+// blk_form_q builds Q from these afterwards. For a shared-memory H this keeps
+// every per-column pass in shared memory (the forward accumulation of Z is a
+// matrix-vector product and a rank-1 update of an n x n global matrix per
+// column).
+__device__ void blk_hessenberg_refl(int n, cplx* H, int ldh, cplx* refl, cplx* v, cplx* w, RedScratch* rs) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int warp = tid >> 5, lane = tid & 31, nwarp = nt >> 5;
+    for (int k = 0; k + 2 < n; ++k) {
+        const int m = n - k - 1;
+        cplx* rk = refl + (size_t)k * n;
+        double s = 0.0;
+        for (int i = tid; i < m; i += nt) s += cnorm2(H[(size_t)(k + 1 + i) * ldh + k]);
+        const double xnorm2 = blk_sum(s, rs);
+        const cplx x0 = H[(size_t)(k + 1) * ldh + k];
+        const double tail = xnorm2 - cnorm2(x0);
+        if (tail <= 0.0) {  // already zero below the subdiagonal
+            if (tid == 0) rk[n - 1] = C(0.0, 0.0);
+            __syncthreads();
+            continue;
+        }
+        const double xn = sqrt(xnorm2);
+        const double ax0 = cabs(x0);
+        const cplx ph = ax0 > 0.0 ? cscale(x0, 1.0 / ax0) : C(1.0, 0.0);
+        const cplx alpha = cscale(ph, -xn);
+        const cplx v0 = csub(x0, alpha);
+        const double beta = 2.0 / (tail + cnorm2(v0));
+        for (int i = tid; i < m; i += nt) {
+            const cplx vi = (i == 0) ? v0 : H[(size_t)(k + 1 + i) * ldh + k];
+            v[i] = vi;
+            rk[i] = vi;
+        }
+        if (tid == 0) rk[n - 1] = C(beta, 0.0);
+        __syncthreads();
+        for (int j = k + 1 + tid; j < n; j += nt) {
+            const cplx* col = H + (size_t)(k + 1) * ldh + j;
+            cplx acc[4] = {C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0)};
+            int i = 0;
+            for (; i + 8 <= m; i += 8) {
+                cplx h[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) h[u] = col[(size_t)(i + u) * ldh];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) acc[u & 3] = cfma(cconj(v[i + u]), h[u], acc[u & 3]);
+            }
+            for (; i < m; ++i) acc[0] = cfma(cconj(v[i]), col[(size_t)i * ldh], acc[0]);
+            w[j] = cscale(cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3])), beta);
+        }
+        __syncthreads();
+        blk_rank1<false>(m, n - k - 1, H + (size_t)(k + 1) * ldh + k + 1, ldh, v, w + k + 1);
+        for (int i = tid; i < m; i += nt) H[(size_t)(k + 1 + i) * ldh + k] = (i == 0) ? alpha : C(0.0, 0.0);
+        __syncthreads();
+        blk_matvec_rows(n, m, H + k + 1, ldh, v, w, beta, warp, lane, nwarp);
+        __syncthreads();
+        blk_rank1<true>(n, m, H + k + 1, ldh, w, v);
+        __syncthreads();
+    }
+}
+
+// Q = P_0 P_1 ... P_{n-3} from the reflectors of blk_hessenberg_refl, formed
+// backward in Z (n x n, shared): Z = I, then Z <- P_k Z for k = n-3 .. 0.
+// Before step k, Z is the identity outside its trailing block from k+2, so P_k
+// changes only Z[k+1:, k+1:] (LAPACK's xUNGHR order). v, w: scratch of length n.
+__device__ void blk_form_q(int n, cplx* Z, int ldz, const cplx* refl, cplx* v, cplx* w) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e = tid; e < n * n; e += nt) {
+        const int i = e / n, j = e % n;
+        Z[(size_t)i * ldz + j] = C(i == j ? 1.0 : 0.0, 0.0);
+    }
+    __syncthreads();
+    for (int k = n - 3; k >= 0; --k) {
+        const int m = n - k - 1;
+        const cplx* rk = refl + (size_t)k * n;
+        const double beta = rk[n - 1].x;
+        if (beta == 0.0) continue;  // the same value in every thread
+        for (int i = tid; i < m; i += nt) v[i] = rk[i];
+        __syncthreads();
+        // w[j] = beta * sum_i conj(v[i]) Z[k+1+i][k+1+j]
+        for (int j = tid; j < m; j += nt) {
+            const cplx* col = Z + (size_t)(k + 1) * ldz + k + 1 + j;
+            cplx acc[4] = {C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0)};
+            int i = 0;
+            for (; i + 8 <= m; i += 8) {
+                cplx h[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) h[u] = col[(size_t)(i + u) * ldz];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) acc[u & 3] = cfma(cconj(v[i + u]), h[u], acc[u & 3]);
+            }
+            for (; i < m; ++i) acc[0] = cfma(cconj(v[i]), col[(size_t)i * ldz], acc[0]);
+            w[j] = cscale(cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3])), beta);
+        }
+        __syncthreads();
+        blk_rank1<false>(m, m, Z + (size_t)(k + 1) * ldz + k + 1, ldz, v, w);
+        __syncthreads();
+    }
+}
+
 // Blocked Householder reduction (panels of LNB columns, compact WY form).
 // Reflector P_j = I - b_j v_j v_j^H (b_j real, P_j Hermitian) as in
 // blk_hessenberg; a panel's product is Q = I - V T V^H with T upper triangular.

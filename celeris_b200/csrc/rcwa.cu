@@ -355,13 +355,22 @@ __global__ void __launch_bounds__(kRT) rcwa_hess(Bucket b) {
     const int tid = threadIdx.x, nt = blockDim.x;
     cplx* Hg = at(b.H, b.s_nn, cell);
     if constexpr (SMEM) {
+        // reduce H in shared memory recording the reflectors in X (free until
+        // the eigenvectors), write H back, then form Z = Q in the same shared
+        // buffer
         cplx* H = reinterpret_cast<cplx*>(smem);
         cplx* v = H + (size_t)n * n;
+        cplx* refl = at(b.X, b.s_nn, cell);
         for (int e = tid; e < n * n; e += nt) H[e] = Hg[e];
         __syncthreads();
-        blk_hessenberg(n, H, n, at(b.Z, b.s_nn, cell), n, v, v + n, &rs);
+        blk_hessenberg_refl(n, H, n, refl, v, v + n, &rs);
         __syncthreads();
         for (int e = tid; e < n * n; e += nt) Hg[e] = H[e];
+        __syncthreads();
+        blk_form_q(n, H, n, refl, v, v + n);
+        __syncthreads();
+        cplx* Zg = at(b.Z, b.s_nn, cell);
+        for (int e = tid; e < n * n; e += nt) Zg[e] = H[e];
     } else {
         __shared__ GemmSmem gs;
         blk_hessenberg_blocked(n, Hg, n, at(b.Z, b.s_nn, cell), n, at(b.X, b.s_nn, cell),

@@ -14,8 +14,10 @@
 //                   of LNB columns with GEMM trailing updates, same pivots
 //   blk_lu_solve    X = A^{-1} B from the LU factors, any number of RHS
 //                   (blk_lu_solve_blocked: block rows with GEMM updates)
-//   blk_hessenberg  Householder reduction to upper Hessenberg, Z accumulated
-//                   (blk_hessenberg_blocked: compact-WY panels, GEMM updates)
+//   blk_hessenberg_refl  Householder reduction to upper Hessenberg (shared H),
+//                   reflectors recorded; blk_form_q forms Q from them
+//                   (blk_hessenberg_blocked: compact-WY panels, GEMM updates, Z
+//                   accumulated)
 //   givens, wilkinson  rotation and shift helpers of the Schur form (schur_aed.cuh)
 //   blk_trevc       right eigenvectors of triangular T by back substitution
 #pragma once
@@ -711,69 +713,10 @@ __device__ void blk_lu_solve_blocked(int n, const cplx* LU, int lda, const int* 
 }
 
 // ---- Hessenberg reduction ------------------------------------------------------------
-// H (n x n) <- Q^H H Q upper Hessenberg; Z <- Q (Z is initialised here).
-// v, w: scratch vectors of length n (shared or global).
-__device__ void blk_hessenberg(int n, cplx* H, int ldh, cplx* Z, int ldz, cplx* v, cplx* w, RedScratch* rs) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int warp = tid >> 5, lane = tid & 31, nwarp = nt >> 5;
-    for (int e = tid; e < n * n; e += nt) {
-        const int i = e / n, j = e % n;
-        Z[(size_t)i * ldz + j] = C(i == j ? 1.0 : 0.0, 0.0);
-    }
-    __syncthreads();
-    for (int k = 0; k + 2 < n; ++k) {
-        const int m = n - k - 1;  // length of x = H[k+1:, k]
-        double s = 0.0;
-        for (int i = tid; i < m; i += nt) s += cnorm2(H[(size_t)(k + 1 + i) * ldh + k]);
-        const double xnorm2 = blk_sum(s, rs);
-        const cplx x0 = H[(size_t)(k + 1) * ldh + k];
-        const double tail = xnorm2 - cnorm2(x0);
-        if (tail <= 0.0) {  // already zero below the subdiagonal
-            __syncthreads();
-            continue;
-        }
-        const double xn = sqrt(xnorm2);
-        const double ax0 = cabs(x0);
-        const cplx ph = ax0 > 0.0 ? cscale(x0, 1.0 / ax0) : C(1.0, 0.0);
-        const cplx alpha = cscale(ph, -xn);          // -e^{i arg x0} ||x||
-        const cplx v0 = csub(x0, alpha);
-        const double vnorm2 = tail + cnorm2(v0);
-        const double beta = 2.0 / vnorm2;            // H <- (I - beta v v^H) H (...)
-        for (int i = tid; i < m; i += nt) v[i] = (i == 0) ? v0 : H[(size_t)(k + 1 + i) * ldh + k];
-        __syncthreads();
-        // left: rows k+1.., columns k+1..n-1 (column k becomes alpha e1)
-        for (int j = k + 1 + tid; j < n; j += nt) {
-            const cplx* col = H + (size_t)(k + 1) * ldh + j;
-            cplx acc[4] = {C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0)};
-            int i = 0;
-            for (; i + 8 <= m; i += 8) {  // 8 loads in flight
-                cplx h[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) h[u] = col[(size_t)(i + u) * ldh];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) acc[u & 3] = cfma(cconj(v[i + u]), h[u], acc[u & 3]);
-            }
-            for (; i < m; ++i) acc[0] = cfma(cconj(v[i]), col[(size_t)i * ldh], acc[0]);
-            w[j] = cscale(cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3])), beta);
-        }
-        __syncthreads();
-        blk_rank1<false>(m, n - k - 1, H + (size_t)(k + 1) * ldh + k + 1, ldh, v, w + k + 1);
-        for (int i = tid; i < m; i += nt) H[(size_t)(k + 1 + i) * ldh + k] = (i == 0) ? alpha : C(0.0, 0.0);
-        __syncthreads();
-        // right: all rows, columns k+1..n-1: H <- H (I - beta v v^H)
-        blk_matvec_rows(n, m, H + k + 1, ldh, v, w, beta, warp, lane, nwarp);
-        __syncthreads();
-        blk_rank1<true>(n, m, H + k + 1, ldh, w, v);
-        __syncthreads();
-        // Z <- Z (I - beta v v^H)
-        blk_matvec_rows(n, m, Z + k + 1, ldz, v, w, beta, warp, lane, nwarp);
-        __syncthreads();
-        blk_rank1<true>(n, m, Z + k + 1, ldz, w, v);
-        __syncthreads();
-    }
-}
-
-// The same reduction without Z: reflector k (v_k of length m = n-k-1, beta_k;
+// H (n x n) <- Q^H H Q upper Hessenberg by Householder reflectors
+// P_k = I - beta v v^H (beta real, P_k Hermitian and unitary), applied from
+// both sides one column at a time.
+// Reflector k (v_k of length m = n-k-1, beta_k;
 // beta_k = 0 where column k needed none) is recorded in row k of `refl`
 // (n x n, global): v_k in [0, m), beta_k in the real part of entry n-1.
 // blk_form_q builds Q from these afterwards. For a shared-memory H this keeps
@@ -875,7 +818,7 @@ __device__ void blk_form_q(int n, cplx* Z, int ldz, const cplx* refl, cplx* v, c
 
 // Blocked Householder reduction (panels of LNB columns, compact WY form).
 // Reflector P_j = I - b_j v_j v_j^H (b_j real, P_j Hermitian) as in
-// blk_hessenberg; a panel's product is Q = I - V T V^H with T upper triangular.
+// blk_hessenberg_refl; a panel's product is Q = I - V T V^H with T upper triangular.
 // For each panel column the right update by the earlier reflectors uses
 // Y = A V T (A at the panel start), the left update applies Q_prev^H to that
 // column only, and Y gains A v_j by one matrix-vector product over the columns

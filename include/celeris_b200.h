@@ -63,7 +63,10 @@ const char* celeris_last_error(void);
 int celeris_abi_version(void);
 /* New: number of kernels this library launched since load (all threads). */
 uint64_t celeris_launch_count(void);
-/* New: release the per-device workspace arenas and pinned staging buffers. */
+/* New: free every device workspace arena (all devices, all threads' streams);
+ * the next call allocates again. Call it with no call of this library in
+ * flight on any thread. A thread's streams, events, pinned staging and device
+ * I/O buffer are released when that thread exits. */
 int celeris_release_workspace(void);
 
 /* New: measured op rates of the current device (MUFU sin.approx results/s,

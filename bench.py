@@ -101,26 +101,13 @@ def shard_center(rank, n, half_window_um):
     return rank * n * step
 
 
-def shard_cells(cells, world):
-    """Partition RCWA cells over `world` ranks by flop weight (n^3, n = 2 (2Mx+1)(2My+1)):
-    greedy longest-first onto the least-loaded rank. Returns one index list per
-    rank; every cell lands on exactly one rank (independent cells, no exchange
-    beyond the result gather)."""
-    w = [(2 * (2 * c["Mx"] + 1) * (2 * c.get("My", c["Mx"]) + 1)) ** 3 for c in cells]
-    parts, loads = [[] for _ in range(world)], [0] * world
-    for i in sorted(range(len(cells)), key=lambda i: (-w[i], i)):
-        r = min(range(world), key=lambda k: (loads[k], k))
-        parts[r].append(i)
-        loads[r] += w[i]
-    return [sorted(p) for p in parts]
-
-
 def measure_rcwa_sharded(world, rank):
     """4096 uneven cells split over the ranks by flop weight (strong scaling):
     each rank solves its share in one batched call; max-over-ranks wall time of
     the warm call (the batch is synchronous, the host clock brackets the device
     work) gives the whole-job cells/s."""
     from celeris_b200 import capi
+    from celeris_b200.multigpu import shard_cells
     from celeris_b200.workloads import rcwa_uneven_4096
 
     cells = rcwa_uneven_4096()
@@ -372,6 +359,28 @@ def rcwa_cpu_baseline(cells, budget_s=15.0):
                       f"scaled to the whole batch"}
 
 
+def rcwa_library_cpu_baseline(cells):
+    """The oracle port over the whole 64-cell library sweep, X and Y solved
+    separately as the reference does (polarization.cpp:35-39), one cell per
+    process over all host cores, one BLAS thread each."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    os.environ.setdefault("MKL_NUM_THREADS", "1")
+    workers = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    with cf.ProcessPoolExecutor(max_workers=min(workers, len(cells)), mp_context=ctx) as ex:
+        list(ex.map(_oracle_cell_time, cells[:min(workers, len(cells))]))  # start the workers, import numpy
+        t0 = time.perf_counter()
+        list(ex.map(_oracle_cell_time, cells))
+        wall = time.perf_counter() - t0
+    return {"value": len(cells) / wall, "unit": "cells/s", "cores": workers, "kind": "port",
+            "sample": f"all {len(cells)} cells of the sweep, X and Y each solved by the numpy/LAPACK restatement of "
+                      f"solve_rcwa_2d, {workers} processes x 1 BLAS thread, {wall:.2f} s wall"}
+
+
 def measure_rcwa(peaks, quick=False, with_cpu=True, sampler=None):
     """RCWA cells/s. `sampler` (a ClockSampler) is started after the 64-cell
     sweep: its ~12 ms host-synchronous calls slow down measurably while
@@ -402,6 +411,11 @@ def measure_rcwa(peaks, quick=False, with_cpu=True, sampler=None):
                             "batched_over_per_cell": per_cell / (dt / 64),
                             "roofline": {"bound": "fp64", "achieved": fl / dt, "peak": p_fp64, "unit": "FLOP/s",
                                          "frac": fl / dt / p_fp64}}
+    if with_cpu:
+        try:
+            out["library_64_M3"]["cpu_baseline"] = rcwa_library_cpu_baseline(lib)
+        except Exception as exc:
+            out["library_64_M3"]["cpu_baseline"] = {"unavailable": str(exc)[:200]}
     if sampler is not None:
         sampler.start()
     if not quick:
@@ -484,6 +498,53 @@ def measure_inverse_design(steps=20, warmup=3, form=None):
             "ms_per_step": ms, "steps": steps,
             "terms_per_s_fwd_plus_adjoint": 2 * terms / (ms * 1e-3),
             "loss_first": float(L0.detach()), "loss_last": float(L.detach())}
+
+
+def measure_reference_gpu_kernel(ap, g, E64h, f32c_err, dev):
+    """The reference's FP32 psf_kernel (src/celeris/cuda/propagate.cu:36-84),
+    compiled unmodified for sm_100a into oracle/_ref, on this GPU: kernel-only
+    terms/s and the error of its |E|^2 against the FP64 form, on the
+    785,456-pillar x 1024^2 metalens and on the 70,688-pillar x 161^2 metalens,
+    beside the same figures of the precision form; plus its public host-buffer
+    call propagate_psf on the 70k metalens (per-call allocation and copies)."""
+    import torch
+
+    from celeris_b200 import capi
+    from celeris_b200 import torch_ops as T
+    from celeris_b200.workloads import metalens_70k
+    from oracle import ref_cuda as RC
+
+    if not RC.available():
+        return {"unavailable": "oracle/_ref/libref_psf_cuda.so not built"}
+    res = {"kernel": "psf_kernel (reference, FP32 throughout: sqrtf, sincosf(k R), 1/R)"}
+    I64 = np.abs(E64h) ** 2
+    RC.psf_kernel(ap.px, ap.py, ap.t, 0.0, 0.0, g.z_um, ap.k, 64, g.half_window_um, reps=1)  # warm-up
+    I_ref, ms = RC.psf_kernel(ap.px, ap.py, ap.t, 0.0, 0.0, g.z_um, ap.k, g.n, g.half_window_um, reps=1)
+    res["metalens_785k_1024sq"] = {
+        "terms_per_s": ap.npil * g.npix / (ms * 1e-3), "kernel_ms": ms,
+        "intensity_error_vs_fp64": float(np.max(np.abs(I_ref - I64)) / I64.max()),
+        "field_error_vs_fp64_of_f32c": f32c_err}
+    a0, g0 = metalens_70k()
+    grid0 = T.FarFieldGrid(g0.n, g0.half_window_um, g0.z_um, a0.wavelength_um)
+    px0, py0, t0_ = (torch.tensor(v, device=dev) for v in (a0.px, a0.py, a0.t))
+    E64_0 = T.rs_field_dev(px0, py0, t0_, grid0, capi.FORM_PLAIN_F64).cpu().numpy()
+    E32_0 = T.rs_field_dev(px0, py0, t0_, grid0, capi.FORM_F32C).cpu().numpy()
+    I64_0 = np.abs(E64_0) ** 2
+    RC.psf_kernel(a0.px, a0.py, a0.t, 0.0, 0.0, g0.z_um, a0.k, g0.n, g0.half_window_um, reps=2)
+    I_ref0, ms0 = RC.psf_kernel(a0.px, a0.py, a0.t, 0.0, 0.0, g0.z_um, a0.k, g0.n, g0.half_window_um, reps=10)
+    RC.propagate_psf(a0.px, a0.py, a0.t, 0.0, 0.0, g0.z_um, a0.k, g0.n, g0.half_window_um)
+    t_api = []
+    for _ in range(5):
+        t1 = time.perf_counter()
+        RC.propagate_psf(a0.px, a0.py, a0.t, 0.0, 0.0, g0.z_um, a0.k, g0.n, g0.half_window_um)
+        t_api.append(time.perf_counter() - t1)
+    res["metalens_70k_161sq"] = {
+        "terms_per_s": a0.npil * g0.npix / (ms0 * 1e-3), "kernel_ms": ms0,
+        "api_call_terms_per_s": a0.npil * g0.npix / float(np.median(t_api)),
+        "intensity_error_vs_fp64": float(np.max(np.abs(I_ref0 - I64_0)) / I64_0.max()),
+        "intensity_error_vs_fp64_of_f32c": float(np.max(np.abs(np.abs(E32_0) ** 2 - I64_0)) / I64_0.max()),
+        "field_error_vs_fp64_of_f32c": float(np.max(np.abs(E32_0 - E64_0)) / np.max(np.abs(E64_0)))}
+    return res
 
 
 def run_gpu(args):
@@ -601,21 +662,30 @@ def run_gpu(args):
     # ---- e2e: the C-ABI host-buffer call ----------------------------------------
     E_host = None
     for _ in range(2):
-        E_host, _, _ = capi.rs_field(ap.px, ap.py, ap.t, 0.0, cy, g.z_um, ap.k, g.n, g.half_window_um,
-                                     form=capi.FORM_F32C, want_intensity=False, want_err=True)
+        E_host, _, _, _ = capi.rs_field_bounded(ap.px, ap.py, ap.t, 0.0, cy, g.z_um, ap.k, g.n, g.half_window_um)
     e2e_t = []
-    stated = None
+    stated = bound = None
     for _ in range(args.steps):
         flush()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        E_host, _, stated = capi.rs_field(ap.px, ap.py, ap.t, 0.0, cy, g.z_um, ap.k, g.n, g.half_window_um,
-                                          form=capi.FORM_F32C, want_intensity=False, want_err=True)
+        E_host, _, stated, bound = capi.rs_field_bounded(ap.px, ap.py, ap.t, 0.0, cy, g.z_um, ap.k, g.n,
+                                                         g.half_window_um)
         e2e_t.append(time.perf_counter() - t0)
+    # the true full-grid error of the returned field against the FP64 form
+    E64h = E64.cpu().numpy()
+    true_err = float(np.max(np.abs(E_host - E64h)) / np.max(np.abs(E_host)))
     out["e2e"] = {"value": terms / float(np.mean(e2e_t)), "unit": UNIT,
                   "h2d_bytes_per_step": int(ap.npil * 32), "d2h_bytes_per_step": int(g.npix * 16),
-                  "api": "celeris_rs_field (C ABI, host buffers, F32C form, stated error on)",
-                  "stated_error": stated, "ms_per_step": 1e3 * float(np.mean(e2e_t))}
+                  "api": "celeris_rs_field_bounded (C ABI, host buffers, F32C form, sampled error and bound stated)",
+                  "stated_error": stated, "stated_bound": bound, "error_vs_fp64_full_grid": true_err,
+                  "ms_per_step": 1e3 * float(np.mean(e2e_t))}
+    # ---- the reference's own FP32 CUDA kernel (psf_kernel), unmodified ----------------
+    if not args.quick:
+        try:
+            out["reference_gpu_kernel"] = measure_reference_gpu_kernel(ap, g, E64h, float(err), dev)
+        except Exception as exc:
+            out["reference_gpu_kernel"] = {"unavailable": str(exc)[:200]}
     # ---- RCWA cells/s ------------------------------------------------------------
     if not args.quick:
         try:

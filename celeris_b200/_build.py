@@ -85,8 +85,16 @@ def build_host(verbose=False):
     return out
 
 
+# The reference checkout the oracle recipe compiles its checker libraries from
+# (CELERIS_REFERENCE overrides; the GPU hosts have none and use the prebuilt files).
+REFERENCE = os.environ.get("CELERIS_REFERENCE", "/root/reference")
+
+
 def build_oracle(verbose=False):
-    _run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], verbose)
+    cmd = ["make", "-s", "-C", os.path.join(ROOT, "oracle")]
+    if os.path.isdir(os.path.join(REFERENCE, "src", "celeris")):
+        cmd.append("REF=" + REFERENCE)
+    _run(cmd, verbose)
 
 
 def build_all(verbose=False):

@@ -51,9 +51,12 @@ EXPORTED = [
     "celeris_propagate_zx", "celeris_rs_field", "celeris_rs_field_dev", "celeris_rs_adjoint_dev",
     "celeris_rs_check_dev", "celeris_sync_status", "celeris_solve_rcwa_2d", "celeris_rcwa_batch",
     "celeris_probe_peaks", "celeris_set_kernel_timing", "celeris_last_kernel_ms",
-    "celeris_rs_field_noalloc", "celeris_probe_sincos", "celeris_rcwa_tuning_report",
+    "celeris_rs_field_noalloc", "celeris_rcwa_tuning_report",
     "celeris_probe_dmma", "celeris_solve_rcwa_2d_stack", "celeris_rcwa_stack_batch",
     "celeris_solve_rcwa_2d_orders", "celeris_eig_general", "celeris_eig_general_batch",
+    "celeris_probe_mufu_accuracy", "celeris_rs_field_bounded", "celeris_rs_error_bound_dev",
+    "celeris_rs_field_rows_dev", "celeris_rs_adjoint_rows_dev", "celeris_device_wait_selftest",
+    "celeris_debug_fail_alloc", "celeris_debug_qr_iteration_cap",
 ]
 
 
@@ -127,7 +130,14 @@ def load(path: str = LIB_PATH):
         "celeris_sync_status": (_I, [_V]),
         "celeris_probe_peaks": (_I, [_P, _P, _P]),
         "celeris_probe_dmma": (_I, [_P]),
-        "celeris_probe_sincos": (_I, [_D, _I, _P]),
+        "celeris_probe_mufu_accuracy": (_I, [_P, _P]),
+        "celeris_rs_field_bounded": (_I, [_I, _P, _P, _P, _I, _D, _D, _D, _D, _I, _D, _P, _P, _P, _P]),
+        "celeris_rs_error_bound_dev": (_I, [_V, _V, _V, _I, _D, _D, _D, _D, _I, _D, _V, _P, _V]),
+        "celeris_rs_field_rows_dev": (_I, [_I, _V, _V, _V, _I, _D, _D, _D, _D, _I, _D, _I, _I, _V, _V, _V]),
+        "celeris_rs_adjoint_rows_dev": (_I, [_I, _V, _V, _I, _D, _D, _D, _D, _I, _D, _I, _I, _V, _V, _V]),
+        "celeris_device_wait_selftest": (_I, [ctypes.c_uint]),
+        "celeris_debug_fail_alloc": (_I, [_I]),
+        "celeris_debug_qr_iteration_cap": (_I, [_I]),
         "celeris_set_kernel_timing": (_I, [_I]),
         "celeris_last_kernel_ms": (_I, [_P]),
         "celeris_solve_rcwa_2d": (_I, [ctypes.POINTER(RcwaCell), _P, _P, ctypes.POINTER(RcwaResult)]),
@@ -227,6 +237,29 @@ def rs_field(px, py, pt, cx, cy, z, k, n, half_window, form=FORM_PLAIN_F64, want
                                   _dp(inten) if inten is not None else None,
                                   _dp(err) if want_err else None))
     return fld, inten, float(err[0])
+
+
+def rs_field_bounded(px, py, pt, cx, cy, z, k, n, half_window, form=FORM_F32C, want_field=True,
+                     want_intensity=False):
+    """celeris_rs_field_bounded: (field | None, intensity | None, sampled error, error bound)."""
+    px, py, pt = _f64(px), _f64(py), _c128(pt)
+    fld = np.empty((n, n), dtype=np.complex128) if want_field else None
+    inten = np.empty((n, n), dtype=np.float64) if want_intensity else None
+    err = np.zeros(1, dtype=np.float64)
+    bound = np.zeros(1, dtype=np.float64)
+    check(load().celeris_rs_field_bounded(form, _dp(px), _dp(py), _dp(pt.view(np.float64)), len(px), cx, cy, z,
+                                          k, n, half_window, _dp(fld.view(np.float64)) if fld is not None else None,
+                                          _dp(inten) if inten is not None else None, _dp(err), _dp(bound)))
+    return fld, inten, float(err[0]), float(bound[0])
+
+
+def probe_mufu_accuracy() -> dict:
+    """Measured (exhaustive) and assumed accuracy of sin/cos/rsqrt.approx."""
+    m = np.zeros(3)
+    a = np.zeros(3)
+    check(load().celeris_probe_mufu_accuracy(_dp(m), _dp(a)))
+    return {"measured": {"sin_abs": m[0], "cos_abs": m[1], "rsqrt_rel": m[2]},
+            "model": {"sin_abs": a[0], "cos_abs": a[1], "rsqrt_rel": a[2]}}
 
 
 def rcwa_cell(**kw) -> RcwaCell:

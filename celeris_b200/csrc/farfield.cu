@@ -44,7 +44,16 @@ using celeris_rt::set_error;
 using celeris_rt::Workspace;
 using namespace celeris_dev;
 
-__device__ int g_ff_status;  // CELERIS_ERR_DEVICE_TIMEOUT after a wait ran out
+// Device-side failure flags of the far-field kernels, read and cleared by the
+// host after a synchronous call (or by celeris_sync_status).
+constexpr int kFlagTimeout = 1;    // a bounded device wait ran out
+constexpr int kFlagNonFinite = 2;  // a pillar coordinate / transmission or an adjoint input was NaN or Inf
+// One status word per stream (hashed into kStatusSlots slots, the legacy
+// default stream in slot 0), so a flag raised by an asynchronous call on one
+// stream is reported by the call or celeris_sync_status on that stream, not by
+// an unrelated call on another.
+constexpr int kStatusSlots = 1024;
+__device__ int g_ff_status[kStatusSlots];
 
 constexpr int kThreads = 256;
 constexpr int kTile64 = 256;  // pillars (or pixels) per stage, 32 B records -> 8 KB
@@ -67,13 +76,15 @@ struct Geom {
     double b0, b1;  // PSF: cy - W, step      ZX: zmin, zmax
     double z;       // PSF: z
     double ox, oy;  // origin subtracted from pillars and pixels in the f32 form
+    int row0;       // PSF: first row of a row block (pixel row j is grid row row0 + j)
+    int slot;       // status word of the launching stream (g_ff_status)
 };
 
 __device__ __forceinline__ void pixel_pos(const Geom& g, int i, int j, double& fx,
                                           double& fy, double& fz) {
     if (g.mode == GEOM_PSF) {
         fx = g.a0 + i * g.a1;
-        fy = g.b0 + j * g.b1;
+        fy = g.b0 + (j + g.row0) * g.b1;
         fz = g.z;
     } else {
         fx = g.a0 + (g.a1 - g.a0) * i / (g.nx - 1);
@@ -82,26 +93,34 @@ __device__ __forceinline__ void pixel_pos(const Geom& g, int i, int j, double& f
     }
 }
 
-__device__ __forceinline__ void record_timeout() {
-    atomicExch(&g_ff_status, CELERIS_ERR_DEVICE_TIMEOUT);
+__device__ __forceinline__ void record_timeout(int slot) { atomicOr(&g_ff_status[slot], kFlagTimeout); }
+
+// Non-finite inputs are not screened on the host (that would cost a pass over
+// the caller's arrays and a synchronisation); the packing pass, which reads
+// every input once anyway, flags them and the call reports
+// CELERIS_ERR_INVALID_ARG. Non-finite values propagate to the outputs.
+__device__ __forceinline__ void flag_nonfinite(int slot, double a, double b, double c, double d) {
+    if (!(isfinite(a) && isfinite(b) && isfinite(c) && isfinite(d))) atomicOr(&g_ff_status[slot], kFlagNonFinite);
 }
 
 // ---- packing ----------------------------------------------------------------
 __global__ void ff_pack_f64(const double* __restrict__ px, const double* __restrict__ py,
-                            const double2* __restrict__ pt, int npil,
+                            const double2* __restrict__ pt, int npil, int slot,
                             double4* __restrict__ rec) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= npil) return;
     double2 t = pt[j];
+    flag_nonfinite(slot, px[j], py[j], t.x, t.y);
     rec[j] = make_double4(px[j], py[j], t.x, t.y);
 }
 
 __global__ void ff_pack_f32(const double* __restrict__ px, const double* __restrict__ py,
-                            const double2* __restrict__ pt, int npil, double ox, double oy,
+                            const double2* __restrict__ pt, int npil, double ox, double oy, int slot,
                             float4* __restrict__ rec) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= npil) return;
     double2 t = pt[j];
+    flag_nonfinite(slot, px[j], py[j], t.x, t.y);
     double A = hypot(t.x, t.y);
     double psi = atan2(t.y, t.x) * 0.15915494309189533577;  // turns
     rec[j] = make_float4((float)(px[j] - ox), (float)(py[j] - oy), (float)A, (float)psi);
@@ -116,6 +135,7 @@ __global__ void ff_pack_pix(Geom g, const double2* __restrict__ v, double4* __re
     double fx, fy, fz;
     pixel_pos(g, i, j, fx, fy, fz);
     double2 vv = v[p];
+    flag_nonfinite(g.slot, vv.x, vv.y, 0.0, 0.0);
     rec[p] = make_double4(fx, fy, vv.x, vv.y);
 }
 
@@ -128,6 +148,7 @@ __global__ void ff_pack_pix_f32(Geom g, const double2* __restrict__ v, float4* _
     double fx, fy, fz;
     pixel_pos(g, i, j, fx, fy, fz);
     double2 vv = v[p];
+    flag_nonfinite(g.slot, vv.x, vv.y, 0.0, 0.0);
     rec[p] = make_float4((float)(fx - g.ox), (float)(fy - g.oy), (float)vv.x, (float)vv.y);
 }
 
@@ -140,9 +161,10 @@ struct TilePipe {
     Rec (*buf)[TILE];
     uint64_t* full;
     const Rec* src;
-    int c0, c1, ntiles;
+    int c0, c1, ntiles, slot;
 
-    __device__ void init(Rec (*b)[TILE], uint64_t* f, const Rec* s, int lo, int hi) {
+    __device__ void init(Rec (*b)[TILE], uint64_t* f, const Rec* s, int lo, int hi, int status_slot) {
+        slot = status_slot;
         buf = b;
         full = f;
         src = s;
@@ -169,7 +191,7 @@ struct TilePipe {
     // call after every thread finished reading tile t; returns false on timeout
     __device__ bool release(int t, bool got) {
         if (!__syncthreads_and(got)) {
-            if (threadIdx.x == 0) record_timeout();
+            if (threadIdx.x == 0) record_timeout(slot);
             return false;
         }
         if (threadIdx.x == 0 && t + kStages < ntiles) {
@@ -201,7 +223,7 @@ __global__ void __launch_bounds__(kThreads) rs_f64_kernel(const double4* __restr
 
     TilePipe<double4, kTile64> pipe;
     const int lo = blockIdx.y * chunk_len;
-    pipe.init(buf, full, rec, lo, min(npil, lo + chunk_len));
+    pipe.init(buf, full, rec, lo, min(npil, lo + chunk_len), g.slot);
 
     double er[kPPT64], ei[kPPT64];
 #pragma unroll
@@ -330,7 +352,7 @@ __global__ void __launch_bounds__(kThreads, 3) rs_f32c_kernel(const float4* __re
 
     TilePipe<float4, kTile32> pipe;
     const int lo = blockIdx.y * chunk_len;
-    pipe.init(buf, full, rec, lo, min(npil, lo + chunk_len));
+    pipe.init(buf, full, rec, lo, min(npil, lo + chunk_len), g.slot);
 
     float sr[kPPT32], cr[kPPT32], si[kPPT32], ci[kPPT32];
 #pragma unroll
@@ -423,7 +445,7 @@ __global__ void __launch_bounds__(kThreads, 3) rs_adj_f32c_kernel(const float4* 
 
     TilePipe<float4, kTile32> pipe;
     const int lo = blockIdx.y * chunk_len;
-    pipe.init(buf, full, pix, lo, min(npix, lo + chunk_len));
+    pipe.init(buf, full, pix, lo, min(npix, lo + chunk_len), g.slot);
 
     float sr[kAdjPPT32], cr[kAdjPPT32], si[kAdjPPT32], ci[kAdjPPT32];
 #pragma unroll
@@ -517,9 +539,11 @@ __global__ void rs_reduce_kernel(const double2* __restrict__ partial, int nchunk
         const int j = p / g.nx;
         double fx, fy, fz;
         pixel_pos(g, 0, j, fx, fy, fz);
-        const double zf = (double)(float)fz;  // the z the FP32 terms used
+        // the FP32 terms hold the phase of R - z_f, z_f = (float)z; with the
+        // global phase k z (not k z_f) the field's phase error from rounding z
+        // is k |z - z_f| (1 - z/R), not k |z - z_f|
         double s, c;
-        sincos(k * zf, &s, &c);
+        sincos(k * fz, &s, &c);
         const double r = er * c - ei * s;
         ei = er * s + ei * c;
         er = r;
@@ -533,7 +557,7 @@ __global__ void __launch_bounds__(kThreads) rs_adj_f64_kernel(const double4* __r
                                                               int npix, int chunk_len,
                                                               const double* __restrict__ px,
                                                               const double* __restrict__ py,
-                                                              int npil, double z, double k,
+                                                              int npil, double z, double k, int slot,
                                                               double2* __restrict__ partial) {
     __shared__ __align__(128) double4 buf[kStages][kTile64];
     __shared__ __align__(8) uint64_t full[kStages];
@@ -550,7 +574,7 @@ __global__ void __launch_bounds__(kThreads) rs_adj_f64_kernel(const double4* __r
 
     TilePipe<double4, kTile64> pipe;
     const int lo = blockIdx.y * chunk_len;
-    pipe.init(buf, full, pix, lo, min(npix, lo + chunk_len));
+    pipe.init(buf, full, pix, lo, min(npix, lo + chunk_len), slot);
 
     double gr[kAdjPPT], gi[kAdjPPT];
 #pragma unroll
@@ -598,15 +622,60 @@ __global__ void chunk_sum_kernel(const double2* __restrict__ partial, int nchunk
     out[j] = make_double2(r, i);
 }
 
-// ---- sampled FP64 check -------------------------------------------------------
+// ---- stated error of the precision form ------------------------------------------
+// (1) Sampled: the field recomputed in FP64 at a set of pixels - a strided
+//     lattice, the centre pixel and the 11 x 11 pixels around the peak of |E|
+//     (where errors that add coherently are largest) - against the computed
+//     field there.
+// (2) Bound: an upper bound on max_p |E_p - E64_p| from the error model of the
+//     precision-form arithmetic (ff_bound_kernel).
+constexpr int kPeakHalf = 5;  // the peak neighbourhood is (2 kPeakHalf + 1)^2 pixels
+
+// acc[0]: bits of max_p |E_p| (FP64); acc[1]: (bits of (float)|E_p| << 32) | p,
+// so that atomicMax leaves the index of a peak pixel in the low word.
+__global__ void abs_max_kernel(const double2* __restrict__ field, int npix,
+                               unsigned long long* __restrict__ acc) {
+    double m = 0.0;
+    unsigned long long arg = 0ull;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        const double2 v = field[p];
+        const double a = hypot(v.x, v.y);
+        m = fmax(m, a);
+        const unsigned long long key =
+            ((unsigned long long)__float_as_uint((float)a) << 32) | (unsigned long long)(unsigned)p;
+        arg = key > arg ? key : arg;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+        const unsigned long long other = __shfl_down_sync(0xffffffffu, arg, o);
+        arg = other > arg ? other : arg;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(acc + 0, (unsigned long long)__double_as_longlong(m));
+        atomicMax(acc + 1, arg);
+    }
+}
+
+// One block per sampled pixel: blocks [0, ns) take idx[b]; blocks [ns, ns +
+// (2 kPeakHalf + 1)^2) the neighbourhood of the peak pixel found by
+// abs_max_kernel (clamped to the grid). acc[2] receives the bits of max |E - E64|.
 __global__ void rs_check_kernel(const double4* __restrict__ rec, int npil, Geom g, double k,
                                 const double2* __restrict__ field, const int* __restrict__ idx,
-                                int ns, unsigned long long* __restrict__ maxerr_bits) {
+                                int ns, unsigned long long* __restrict__ acc) {
     __shared__ double red[2][32];
     const int b = blockIdx.x;
-    if (b >= ns) return;
-    const int p = idx[b];
     const int npix = g.nx * g.ny;
+    int p;
+    if (b < ns) {
+        p = idx[b];
+    } else {
+        const int q = b - ns, side = 2 * kPeakHalf + 1;
+        const int peak = (int)(unsigned)(acc[1] & 0xffffffffull);
+        const int pj = peak / g.nx, pi = peak - pj * g.nx;
+        const int i = min(max(pi + q % side - kPeakHalf, 0), g.nx - 1);
+        const int j = min(max(pj + q / side - kPeakHalf, 0), g.ny - 1);
+        p = j * g.nx + i;
+    }
     if (p < 0 || p >= npix) return;
     const int j = p / g.nx, i = p - j * g.nx;
     double fx, fy, fz;
@@ -641,19 +710,89 @@ __global__ void rs_check_kernel(const double4* __restrict__ rec, int npil, Geom 
         }
         const double2 f = field[p];
         const double err = hypot(f.x - sr, f.y - si);
-        atomicMax(maxerr_bits, (unsigned long long)__double_as_longlong(err));
+        atomicMax(acc + 2, (unsigned long long)__double_as_longlong(err));
     }
 }
 
-__global__ void abs_max_kernel(const double2* __restrict__ field, int npix,
-                               unsigned long long* __restrict__ out_bits) {
-    double m = 0.0;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
-        const double2 v = field[p];
-        m = fmax(m, hypot(v.x, v.y));
+// Error model of one precision-form term (rs_f32c_kernel), per pillar j, for
+// every pixel of the window. u = 2^-24 (FP32 round to nearest). With the
+// pillar's offset (xo, yo) from the FP32 origin and the window's half extents
+// (wx, wy), dxm = xo + wx and dym = yo + wy bound |dx|, |dy|, rho^2 <= dxm^2 +
+// dym^2 and delta = R - z <= dmax. Rounding of the FP32 coordinates, of dx,
+// dy and of rho^2 moves rho^2 by at most 6u (dxm^2 + dym^2), hence R - z by
+// that / (2|z|); the Newton step adds u dmax (1 + dmax / 2|z|) and the
+// quadratic remainder of its seed (from rsqrt.approx); the phase in turns
+// th = delta/lambda + psi rounds with u (dmax/lambda + 1/2) plus u for psi and
+// its sum, the reduced angle with u pi; the amplitude |t|/R with 6u.
+//   e_R(j)  = 2 pi (dDelta/lambda + u (dmax/lambda + 1/2) + u) + u pi + 6u
+// The MUFU approximations and the constants are systematic and are summed
+// without cancellation:
+//   e_D(j)  = kRsqrtRelErr + sqrt(2) kSinCosAbsErr + |2 pi_f - 2 pi| / 2
+//             + |z - z_f| / |z| + k |z - z_f| rho_max^2 / (2 z^2)
+// with z_f = (float)z (the z the FP32 terms use; the global phase uses z).
+// Every term has magnitude a_j = |t_j| / R <= |t_j| / |z|. acc (doubles):
+// [0] sum_j a_j e_D(j), [1] sum_j (a_j e_R(j))^2, [2] bits of max_j a_j,
+// [3] sum_j a_j.
+__global__ void ff_bound_kernel(const double* __restrict__ px, const double* __restrict__ py,
+                                const double2* __restrict__ pt, int npil, Geom g, double k,
+                                double* __restrict__ acc) {
+    const double u = 5.9604644775390625e-08;  // 2^-24
+    const double pi = 3.14159265358979323846;
+    const double z = fabs(g.z), zf = fabs((double)(float)g.z), dz = fabs(z - zf);
+    const double lam = 2.0 * pi / k;
+    const double wx = fmax(fabs(g.a0 - g.ox), fabs(g.a0 + (g.nx - 1) * g.a1 - g.ox));
+    const double y_first = g.b0 + g.row0 * g.b1, y_last = g.b0 + (g.row0 + g.ny - 1) * g.b1;
+    const double wy = fmax(fabs(y_first - g.oy), fabs(y_last - g.oy));
+    const double two_pi_f = (double)6.28318530717958647692f;
+    const double eD0 = celeris_dev::kRsqrtRelErr + 1.4142135623730951 * celeris_dev::kSinCosAbsErr +
+                       0.5 * fabs(two_pi_f - 2.0 * pi) + dz / z;
+    double sD = 0.0, sR = 0.0, sA = 0.0, amax = 0.0;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npil; j += gridDim.x * blockDim.x) {
+        const double2 t = pt[j];
+        const double a = hypot(t.x, t.y) / z;
+        const double dxm = fabs(px[j] - g.ox) + wx, dym = fabs(py[j] - g.oy) + wy;
+        const double rho2 = dxm * dxm + dym * dym;
+        const double R = sqrt(rho2 + z * z);
+        const double dmax = rho2 / (R + z);
+        const double seed = R * (celeris_dev::kRsqrtRelErr + 4.0 * u);
+        const double dDelta = 6.0 * u * rho2 / (2.0 * z) + u * dmax * (1.0 + dmax / (2.0 * z)) + seed * seed / z;
+        const double eR = 2.0 * pi * (dDelta / lam + u * (dmax / lam + 0.5) + u) + u * pi + 6.0 * u;
+        const double eD = eD0 + k * dz * rho2 / (2.0 * z * z);
+        sD += a * eD;
+        sR += (a * eR) * (a * eR);
+        sA += a;
+        amax = fmax(amax, a);
     }
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out_bits, (unsigned long long)__double_as_longlong(m));
+    for (int o = 16; o > 0; o >>= 1) {
+        sD += __shfl_down_sync(0xffffffffu, sD, o);
+        sR += __shfl_down_sync(0xffffffffu, sR, o);
+        sA += __shfl_down_sync(0xffffffffu, sA, o);
+        amax = fmax(amax, __shfl_down_sync(0xffffffffu, amax, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(acc + 0, sD);
+        atomicAdd(acc + 1, sR);
+        atomicMax(reinterpret_cast<unsigned long long*>(acc + 2), (unsigned long long)__double_as_longlong(amax));
+        atomicAdd(acc + 3, sA);
+    }
+}
+
+// Failure-path self-test of the bounded device waits: one warp arms an
+// mbarrier that expects two arrivals, arrives once, and waits on it with the
+// same bounded poll loop the tile pipeline uses, limited to `polls`. Nothing
+// else arrives and no copy is issued, so the wait always runs out; the kernel
+// records the timeout in the stream's status word (the path a stalled TMA tile
+// takes) and returns.
+__global__ void ff_wait_selftest_kernel(unsigned polls, int slot) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 2);
+        fence_barrier_init();
+        mbar_arrive(&bar);
+    }
+    __syncwarp();
+    const bool done = mbar_wait(&bar, 0, polls);
+    if (!__all_sync(0xffffffffu, done) && threadIdx.x == 0) record_timeout(slot);
 }
 
 // ---- host-side planning -----------------------------------------------------
@@ -698,14 +837,28 @@ void plan_chunks(int ctas_other, int nrec, int tile, int resident_per_sm, int* n
     if (*nchunk < 1) *nchunk = 1;
 }
 
-int check_status_and_reset() {
+// Status word of a stream: the legacy default stream in slot 0, other streams
+// hashed over the remaining slots.
+int status_slot(cudaStream_t st) {
+    if (!st) return 0;
+    const uint64_t h = (uint64_t)(uintptr_t)st * 0x9E3779B97F4A7C15ull;
+    return 1 + (int)((h >> 33) % (uint64_t)(kStatusSlots - 1));
+}
+
+// Read and clear the status word of `st` (the stream's work must be complete).
+int check_status_and_reset(cudaStream_t stream) {
+    const size_t off = sizeof(int) * (size_t)status_slot(stream);
     int st = 0;
-    cudaError_t e = cudaMemcpyFromSymbol(&st, g_ff_status, sizeof(int));
+    cudaError_t e = cudaMemcpyFromSymbol(&st, g_ff_status, sizeof(int), off);
     if (e != cudaSuccess) return celeris_rt::cuda_error(e, "read far-field status");
     if (st != 0) {
         int zero = 0;
-        cudaMemcpyToSymbol(g_ff_status, &zero, sizeof(int));
-        return set_error(st, "far-field kernel: a bounded device wait ran out");
+        cudaMemcpyToSymbol(g_ff_status, &zero, sizeof(int), off);
+        if (st & kFlagTimeout)
+            return set_error(CELERIS_ERR_DEVICE_TIMEOUT, "far-field kernel: a bounded device wait ran out");
+        return set_error(CELERIS_ERR_INVALID_ARG,
+                         "far-field input holds NaN or Inf (pillar positions / transmissions, or the adjoint's "
+                         "pixel values); the outputs hold non-finite values where it reached them");
     }
     return CELERIS_OK;
 }
@@ -722,6 +875,17 @@ Geom psf_geom(double cx, double cy, double z, int n, double W) {
     g.z = z;
     g.ox = cx;
     g.oy = cy;
+    g.row0 = 0;
+    g.slot = 0;
+    return g;
+}
+
+// Rows [row0, row0 + nrows) of the n x n grid of psf_geom (the same pixel
+// positions and the same FP32 origin), for a focal grid split by rows.
+Geom psf_rows_geom(double cx, double cy, double z, int n, double W, int row0, int nrows) {
+    Geom g = psf_geom(cx, cy, z, n, W);
+    g.ny = nrows;
+    g.row0 = row0;
     return g;
 }
 
@@ -737,6 +901,8 @@ Geom zx_geom(double xmin, double xmax, int nx, double zmin, double zmax, int nz)
     g.z = 0.0;
     g.ox = 0.0;
     g.oy = 0.0;
+    g.row0 = 0;
+    g.slot = 0;
     return g;
 }
 
@@ -769,7 +935,9 @@ void timer_end(cudaStream_t st) {
 
 // Full far-field on device buffers (inputs SoA px, py + interleaved complex pt).
 int ff_run(int form, const double* d_px, const double* d_py, const double* d_pt, int npil,
-           const Geom& g, double k, double* d_field, double* d_int, cudaStream_t st) {
+           const Geom& g0, double k, double* d_field, double* d_int, cudaStream_t st) {
+    Geom g = g0;
+    g.slot = status_slot(st);
     const long npix = (long)g.nx * g.ny;
     if (npix <= 0) return CELERIS_OK;
     if (npix > (1L << 30)) return set_error(CELERIS_ERR_TOO_LARGE, "grid too large (%ld pixels)", npix);
@@ -797,10 +965,10 @@ int ff_run(int form, const double* d_px, const double* d_py, const double* d_pt,
     const int pb = (npil + 255) / 256;
     if (f32) {
         ff_pack_f32<<<pb, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil,
-                                        g.ox, g.oy, static_cast<float4*>(rec));
+                                        g.ox, g.oy, g.slot, static_cast<float4*>(rec));
     } else {
         ff_pack_f64<<<pb, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil,
-                                        static_cast<double4*>(rec));
+                                        g.slot, static_cast<double4*>(rec));
     }
     dim3 grid(ctas_pix, nchunk);
     timer_begin(st);
@@ -822,8 +990,10 @@ int ff_run(int form, const double* d_px, const double* d_py, const double* d_pt,
     return CELERIS_OK;
 }
 
-int ff_adjoint(const double* d_px, const double* d_py, int npil, const Geom& g, double k,
+int ff_adjoint(const double* d_px, const double* d_py, int npil, const Geom& g0, double k,
                const double* d_v, double* d_out, cudaStream_t st, int form = CELERIS_FORM_PLAIN_F64) {
+    Geom g = g0;
+    g.slot = status_slot(st);
     const long npix = (long)g.nx * g.ny;
     if (npil <= 0) return CELERIS_OK;
     if (npix <= 0) {
@@ -849,7 +1019,7 @@ int ff_adjoint(const double* d_px, const double* d_py, int npil, const Geom& g, 
         rs_adj_f32c_kernel<<<grid, kThreads, 0, st>>>(rec, (int)npix, chunk_len, d_px, d_py, npil, g, zf, hi, lo,
                                                       partial);
         timer_end(st);
-        adj_f32c_reduce<<<(npil + 255) / 256, 256, 0, st>>>(partial, nchunk, npil, k * (double)zf,
+        adj_f32c_reduce<<<(npil + 255) / 256, 256, 0, st>>>(partial, nchunk, npil, k * g.z,
                                                            reinterpret_cast<double2*>(d_out));
         count_launch(3);
         CEL_CUDA(cudaGetLastError());
@@ -867,7 +1037,7 @@ int ff_adjoint(const double* d_px, const double* d_py, int npil, const Geom& g, 
     ff_pack_pix<<<(int)((npix + 255) / 256), 256, 0, st>>>(g, reinterpret_cast<const double2*>(d_v), rec);
     dim3 grid(ctas, nchunk);
     timer_begin(st);
-    rs_adj_f64_kernel<<<grid, kThreads, 0, st>>>(rec, (int)npix, chunk_len, d_px, d_py, npil, g.z, k,
+    rs_adj_f64_kernel<<<grid, kThreads, 0, st>>>(rec, (int)npix, chunk_len, d_px, d_py, npil, g.z, k, g.slot,
                                                  partial);
     timer_end(st);
     chunk_sum_kernel<<<(npil + 255) / 256, 256, 0, st>>>(partial, nchunk, npil,
@@ -877,50 +1047,102 @@ int ff_adjoint(const double* d_px, const double* d_py, int npil, const Geom& g, 
     return CELERIS_OK;
 }
 
-// Enqueue the sampled FP64 check on st: when st reaches the end, h_bits[0] and
-// h_bits[1] hold the bits of max |E - E_FP64| over the samples and of
-// max |E| over the field (h_bits: host memory; pinned keeps the copy
-// asynchronous).
-int ff_check_enqueue(const double* d_px, const double* d_py, const double* d_pt, int npil, const Geom& g,
-                     double k, const double* d_field, const int* d_idx, int ns, unsigned long long* h_bits,
-                     cudaStream_t st) {
+// Accumulator words of the stated-error evaluation (device and host copies):
+// [0] bits of max |E|, [1] peak key, [2] bits of max sampled |E - E64|,
+// [3..6] the sums of ff_bound_kernel.
+constexpr int kAccWords = 8;
+
+// Enqueue the stated-error evaluation of the field d_field on st: the sampled
+// FP64 check when ns > 0 (d_idx: ns pixel indices; the peak neighbourhood is
+// added) and the model bound when want_bound. When st reaches the end, h_acc
+// (host memory, kAccWords words; pinned keeps the copy asynchronous) holds the
+// accumulators.
+int ff_check_enqueue(const double* d_px, const double* d_py, const double* d_pt, int npil, const Geom& g0,
+                     double k, const double* d_field, const int* d_idx, int ns, bool want_bound,
+                     unsigned long long* h_acc, cudaStream_t st) {
+    Geom g = g0;
+    g.slot = status_slot(st);
     const long npix = (long)g.nx * g.ny;
     Workspace& ws = Workspace::for_stream(st);
-    const size_t rec_bytes = (size_t)npil * sizeof(double4);
+    const size_t rec_bytes = ns > 0 ? (size_t)npil * sizeof(double4) : 0;
     CEL_TRY(ws.reserve(st, celeris_rt::align256(rec_bytes) + 256));
     double4* rec = static_cast<double4*>(ws.take(rec_bytes));
-    unsigned long long* bits = static_cast<unsigned long long*>(ws.take(2 * sizeof(unsigned long long)));
-    CEL_CUDA(cudaMemsetAsync(bits, 0, 2 * sizeof(unsigned long long), st));
-    ff_pack_f64<<<(npil + 255) / 256, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt),
-                                                    npil, rec);
-    rs_check_kernel<<<ns, 256, 0, st>>>(rec, npil, g, k, reinterpret_cast<const double2*>(d_field),
-                                        d_idx, ns, bits);
-    abs_max_kernel<<<4 * sm_count(), 256, 0, st>>>(reinterpret_cast<const double2*>(d_field),
-                                                   (int)npix, bits + 1);
-    count_launch(3);
+    unsigned long long* acc = static_cast<unsigned long long*>(ws.take(kAccWords * sizeof(unsigned long long)));
+    CEL_CUDA(cudaMemsetAsync(acc, 0, kAccWords * sizeof(unsigned long long), st));
+    abs_max_kernel<<<4 * sm_count(), 256, 0, st>>>(reinterpret_cast<const double2*>(d_field), (int)npix, acc);
+    int launches = 1;
+    if (ns > 0) {
+        ff_pack_f64<<<(npil + 255) / 256, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil,
+                                                        g.slot, rec);
+        const int side = 2 * kPeakHalf + 1;
+        rs_check_kernel<<<ns + side * side, 256, 0, st>>>(rec, npil, g, k, reinterpret_cast<const double2*>(d_field),
+                                                          d_idx, ns, acc);
+        launches += 2;
+    }
+    if (want_bound) {
+        ff_bound_kernel<<<2 * sm_count(), 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil, g,
+                                                        k, reinterpret_cast<double*>(acc + 3));
+        launches += 1;
+    }
+    count_launch(launches);
     CEL_CUDA(cudaGetLastError());
-    CEL_CUDA(cudaMemcpyAsync(h_bits, bits, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CEL_CUDA(cudaMemcpyAsync(h_acc, acc, kAccWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     return CELERIS_OK;
 }
 
-// The stated error from the two words of ff_check_enqueue: max error / max |E|.
+double acc_double(const unsigned long long* h, int i) {
+    double v;
+    std::memcpy(&v, &h[i], sizeof(double));
+    return v;
+}
+
+// The sampled error from the accumulators: max sampled |E - E64| / max |E|.
 double check_ratio(const unsigned long long* h) {
-    double e, m;
-    std::memcpy(&e, &h[0], sizeof(double));
-    std::memcpy(&m, &h[1], sizeof(double));
+    const double e = acc_double(h, 2), m = acc_double(h, 0);
     return m > 0.0 ? e / m : e;
 }
 
-int ff_check(const double* d_px, const double* d_py, const double* d_pt, int npil, const Geom& g,
-             double k, const double* d_field, const int* d_idx, int ns, double* err_out,
-             cudaStream_t st) {
-    *err_out = 0.0;
-    if (npil <= 0 || (long)g.nx * g.ny <= 0 || ns <= 0) return CELERIS_OK;
-    unsigned long long h[2] = {0, 0};
-    CEL_TRY(ff_check_enqueue(d_px, d_py, d_pt, npil, g, k, d_field, d_idx, ns, h, st));
+// The stated bound from the accumulators, relative to max |E|:
+//   B = sum_j a_j e_D(j)                                   (systematic parts)
+//     + sqrt(2) lambda sqrt(sum_j (a_j e_R(j))^2 + T (u a_max C)^2)
+//     + sum_j a_j ((u T)^2 + 64 eps64)
+// The middle line bounds the FP32 rounding errors, modelled as independent and
+// mean zero (the probabilistic rounding-error analysis of Higham and Mary,
+// SIAM J. Sci. Comput. 41 (2019)): per component, a sum of independent terms
+// bounded by c_i exceeds lambda sqrt(sum c_i^2) with probability at most
+// 2 exp(-lambda^2 / 2) (Hoeffding); lambda = 8 makes that 2.5e-14 per pixel and
+// component. It holds the per-term rounding (e_R) and the FP32 accumulation of
+// each tile of kTile32 terms (fma into a running sum: each step errs by at most
+// u |S_k| <= u k a_max, so C = sqrt(sum_{k<=K} k^2), K = kTile32) over at most T
+// = 2 ceil(npil / K) tiles per pixel. The last line covers the compensated
+// (TwoSum) tile folding and the FP64 chunk sums and global phase.
+double bound_ratio(const unsigned long long* h, int npil) {
+    const double u = 5.9604644775390625e-08, eps64 = 1.1102230246251565e-16, lambda = 8.0;
+    const double K = kTile32;
+    const double C = std::sqrt(K * (K + 1.0) * (2.0 * K + 1.0) / 6.0);
+    const double T = 2.0 * std::ceil((double)npil / K);
+    const double sD = acc_double(h, 3), sR = acc_double(h, 4), amax = acc_double(h, 5), sA = acc_double(h, 6);
+    const double rnd = std::sqrt(2.0) * lambda * std::sqrt(sR + T * (u * amax * C) * (u * amax * C));
+    const double B = sD + rnd + sA * ((u * T) * (u * T) + 64.0 * eps64);
+    const double m = acc_double(h, 0);
+    return m > 0.0 ? B / m : B;
+}
+
+// Synchronous stated-error evaluation of a field on the device (sampled error
+// and/or bound), on st.
+int ff_stated(const double* d_px, const double* d_py, const double* d_pt, int npil, const Geom& g, double k,
+              const double* d_field, const int* d_idx, int ns, double* err_out, double* bound_out,
+              cudaStream_t st) {
+    if (err_out) *err_out = 0.0;
+    if (bound_out) *bound_out = 0.0;
+    if (npil <= 0 || (long)g.nx * g.ny <= 0 || (ns <= 0 && !bound_out)) return CELERIS_OK;
+    unsigned long long h[kAccWords] = {0};
+    CEL_TRY(ff_check_enqueue(d_px, d_py, d_pt, npil, g, k, d_field, d_idx, err_out ? ns : 0, bound_out != nullptr,
+                             h, st));
     CEL_CUDA(cudaStreamSynchronize(st));
-    *err_out = check_ratio(h);
-    return check_status_and_reset();
+    if (err_out) *err_out = check_ratio(h);
+    if (bound_out) *bound_out = bound_ratio(h, npil);
+    return check_status_and_reset(st);
 }
 
 // Non-blocking streams per host thread for the synchronous host-buffer calls:
@@ -1022,16 +1244,19 @@ std::vector<int> sample_pixels(int nx, int ny, int want) {
 
 // Host-buffer wrapper: stage inputs through pinned memory, run, copy back.
 int ff_host(int form, const double* px, const double* py, const double* pt, int npil,
-            const Geom& g, double k, double* field_out, double* int_out, double* err_out) {
+            const Geom& g, double k, double* field_out, double* int_out, double* err_out,
+            double* bound_out = nullptr) {
     CEL_TRY(celeris_rt::require_device());
     const long npix = (long)g.nx * g.ny;
     if (err_out) *err_out = 0.0;
+    if (bound_out) *bound_out = 0.0;
     if (npix <= 0) return CELERIS_OK;
     if (npil < 0) return set_error(CELERIS_ERR_INVALID_ARG, "npil < 0");
     if (npil > 0 && (!px || !py || !pt)) return set_error(CELERIS_ERR_INVALID_ARG, "NULL pillar arrays");
     cudaStream_t st = nullptr;
     CEL_TRY(thread_stream(&st));
     const bool want_err = (form == CELERIS_FORM_F32C) && err_out && npil > 0;
+    const bool want_bound = (form == CELERIS_FORM_F32C) && bound_out && npil > 0;
     std::vector<int> sidx;
     if (want_err) sidx = sample_pixels(g.nx, g.ny, 256);
 
@@ -1041,7 +1266,7 @@ int ff_host(int form, const double* px, const double* py, const double* pt, int 
     const size_t idx_bytes = sidx.size() * sizeof(int);
     const size_t pin_bytes = celeris_rt::align256(in_bytes) + celeris_rt::align256(fld_bytes) +
                              celeris_rt::align256(int_bytes) + celeris_rt::align256(idx_bytes);
-    // pinned: the device I/O layout, then the two words of the error check
+    // pinned: the device I/O layout, then the accumulator words of the error check
     char* pin = static_cast<char*>(celeris_rt::pinned_staging(pin_bytes + 256));
     if (!pin) return set_error(CELERIS_ERR_OOM, "pinned staging of %zu bytes failed", pin_bytes);
 
@@ -1050,7 +1275,7 @@ int ff_host(int form, const double* px, const double* py, const double* pt, int 
     if (t_io.cap < pin_bytes || t_io.dev != dev) {
         CEL_CUDA(cudaStreamSynchronize(st));
         t_io.release();
-        CEL_CUDA(cudaMalloc(&t_io.p, pin_bytes));
+        CEL_TRY(celeris_rt::device_alloc(&t_io.p, pin_bytes, "far-field I/O buffer"));
         t_io.cap = pin_bytes;
         t_io.dev = dev;
     }
@@ -1084,43 +1309,50 @@ int ff_host(int form, const double* px, const double* py, const double* pt, int 
         std::memcpy(h_idx, sidx.data(), idx_bytes);
         CEL_CUDA(cudaMemcpyAsync(d_idx, h_idx, idx_bytes, cudaMemcpyHostToDevice, st));
     }
-    const bool need_field = field_out || want_err;
+    const bool need_field = field_out || want_err || want_bound;
     CEL_TRY(ff_run(form, d_px, d_py, d_pt, npil, g, k, need_field ? d_fld : nullptr,
                    int_out ? d_int : nullptr, st));
     char* h_fld = pin + celeris_rt::align256(in_bytes);
     char* h_int = h_fld + celeris_rt::align256(fld_bytes);
-    unsigned long long* h_bits = reinterpret_cast<unsigned long long*>(pin + pin_bytes);
-    // the stated-error check runs on the second stream while the field downloads
+    unsigned long long* h_acc = reinterpret_cast<unsigned long long*>(pin + pin_bytes);
+    // the stated-error evaluation runs on the second stream while the field downloads
     cudaStream_t st2 = nullptr;
-    if (want_err) {
+    const bool stated = want_err || want_bound;
+    if (stated) {
         CEL_TRY(thread_stream(&st2, 1));
-        h_bits[0] = h_bits[1] = 0;
+        for (int i = 0; i < kAccWords; ++i) h_acc[i] = 0;
         cudaEvent_t done = thread_event(0);
         if (!done) return set_error(CELERIS_ERR_CUDA, "cudaEventCreate failed");
         CEL_CUDA(cudaEventRecord(done, st));
         CEL_CUDA(cudaStreamWaitEvent(st2, done, 0));
-        CEL_TRY(ff_check_enqueue(d_px, d_py, d_pt, npil, g, k, d_fld, d_idx, (int)sidx.size(), h_bits, st2));
+        CEL_TRY(ff_check_enqueue(d_px, d_py, d_pt, npil, g, k, d_fld, d_idx, want_err ? (int)sidx.size() : 0,
+                                 want_bound, h_acc, st2));
     }
     const int rd = download(field_out, h_fld, d_fld, field_out ? fld_bytes : 0, st);
     const int ri = rd == CELERIS_OK ? download(int_out, h_int, d_int, int_out ? int_bytes : 0, st) : rd;
     cudaError_t e1 = cudaStreamSynchronize(st);
-    cudaError_t e2 = want_err ? cudaStreamSynchronize(st2) : cudaSuccess;
+    cudaError_t e2 = stated ? cudaStreamSynchronize(st2) : cudaSuccess;
     CEL_TRY(ri);
     CEL_CUDA(e1);
     CEL_CUDA(e2);
-    if (want_err) *err_out = check_ratio(h_bits);
-    return check_status_and_reset();
+    if (want_err) *err_out = check_ratio(h_acc);
+    if (want_bound) *bound_out = bound_ratio(h_acc, npil);
+    const int s1 = check_status_and_reset(st);
+    const int s2 = stated ? check_status_and_reset(st2) : CELERIS_OK;
+    return s1 != CELERIS_OK ? s1 : s2;
 }
 
 bool valid_form(int form) { return form == CELERIS_FORM_PLAIN_F64 || form == CELERIS_FORM_F32C; }
 
 // ---- far-field without allocation ----------------------------------------------
 // Scratch for callers that cannot allocate device memory: the pillar records
-// and the per-chunk partial sums live in this fixed module-scope array, which
-// the CUDA runtime creates once per device when the library is loaded and keeps
-// until the process exits. Host code must not pass the symbol itself to a
-// kernel (on the host it names a shadow variable, not device memory); it passes
-// the device address obtained with cudaGetSymbolAddress below.
+// and the per-chunk partial sums live in this fixed module-scope array. The
+// CUDA runtime creates it on a device when it loads this file's module there -
+// with lazy module loading (the default), at the first use of any far-field
+// kernel or of the array on that device - and keeps it until the process exits.
+// Host code must not pass the symbol itself to a kernel (on the host it names a
+// shadow variable, not device memory); it passes the device address obtained
+// with cudaGetSymbolAddress below.
 constexpr size_t kNoAllocScratchBytes = (size_t)48 << 20;  // 48 MiB per device
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -1145,10 +1377,18 @@ int noalloc_scratch(void** out) {
     return CELERIS_OK;
 }
 
-int ff_run_noalloc(int form, const double* d_px, const double* d_py, const double* d_pt, int npil, const Geom& g,
+int ff_run_noalloc(int form, const double* d_px, const double* d_py, const double* d_pt, int npil, const Geom& g0,
                    double k, double* d_field, double* d_int, cudaStream_t st) {
+    Geom g = g0;
+    g.slot = status_slot(st);
+    // Resolve the scratch first, so that a call with nothing to compute (n = 0
+    // or no pillars) serves as the set-up call: it loads this module on the
+    // device (creating the array) and caches the array's device address.
+    void* base = nullptr;
+    CEL_TRY(noalloc_scratch(&base));
     const long npix = (long)g.nx * g.ny;
     if (npix <= 0) return CELERIS_OK;
+    if (npix > (1L << 30)) return set_error(CELERIS_ERR_TOO_LARGE, "grid too large (%ld pixels)", npix);
     if (npil == 0) {
         if (d_field) CEL_CUDA(cudaMemsetAsync(d_field, 0, npix * 2 * sizeof(double), st));
         if (d_int) CEL_CUDA(cudaMemsetAsync(d_int, 0, npix * sizeof(double), st));
@@ -1174,16 +1414,14 @@ int ff_run_noalloc(int form, const double* d_px, const double* d_py, const doubl
         chunk_len = tiles_per * tile;
         nchunk = (ntiles + tiles_per - 1) / tiles_per;
     }
-    void* base = nullptr;
-    CEL_TRY(noalloc_scratch(&base));
     void* rec = base;
     double2* partial = reinterpret_cast<double2*>(static_cast<char*>(base) + rec_bytes);
     const int pb = (npil + 255) / 256;
     if (f32)
         ff_pack_f32<<<pb, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil, g.ox, g.oy,
-                                        static_cast<float4*>(rec));
+                                        g.slot, static_cast<float4*>(rec));
     else
-        ff_pack_f64<<<pb, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil,
+        ff_pack_f64<<<pb, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil, g.slot,
                                         static_cast<double4*>(rec));
     dim3 grid(ctas_pix, nchunk);
     if (f32) {
@@ -1268,8 +1506,8 @@ int celeris_rs_check_dev(const double* d_px, const double* d_py, const double* d
     if (!err_out) return set_error(CELERIS_ERR_INVALID_ARG, "err_out is NULL");
     if (n < 0 || npil < 0 || ns < 0) return set_error(CELERIS_ERR_INVALID_ARG, "negative size");
     CEL_TRY(celeris_rt::require_device());
-    return ff_check(d_px, d_py, d_pt, npil, psf_geom(cx, cy, z, n, half_window), k, d_field, d_idx,
-                    ns, err_out, static_cast<cudaStream_t>(stream));
+    return ff_stated(d_px, d_py, d_pt, npil, psf_geom(cx, cy, z, n, half_window), k, d_field, d_idx, ns, err_out,
+                     nullptr, static_cast<cudaStream_t>(stream));
 }
 
 int celeris_rs_field_noalloc(int form, const double* d_px, const double* d_py, const double* d_pt, int npil,
@@ -1301,7 +1539,72 @@ int celeris_last_kernel_ms(double* ms) {
 int celeris_sync_status(void* stream) {
     CEL_TRY(celeris_rt::require_device());
     CEL_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
-    return check_status_and_reset();
+    return check_status_and_reset(static_cast<cudaStream_t>(stream));
+}
+
+int celeris_rs_field_bounded(int form, const double* px, const double* py, const double* pt, int npil, double cx,
+                             double cy, double z, double k, int n, double half_window, double* field_out,
+                             double* intensity_out, double* err_out, double* bound_out) {
+    if (!valid_form(form)) return set_error(CELERIS_ERR_INVALID_ARG, "unknown form %d", form);
+    if (n < 0) return set_error(CELERIS_ERR_INVALID_ARG, "n < 0");
+    if (n == 0) {
+        if (err_out) *err_out = 0.0;
+        if (bound_out) *bound_out = 0.0;
+        return CELERIS_OK;
+    }
+    return ff_host(form, px, py, pt, npil, psf_geom(cx, cy, z, n, half_window), k, field_out, intensity_out,
+                   err_out, bound_out);
+}
+
+int celeris_rs_error_bound_dev(const double* d_px, const double* d_py, const double* d_pt, int npil, double cx,
+                               double cy, double z, double k, int n, double half_window, const double* d_field,
+                               double* bound_out, void* stream) {
+    if (!bound_out) return set_error(CELERIS_ERR_INVALID_ARG, "bound_out is NULL");
+    if (n < 0 || npil < 0) return set_error(CELERIS_ERR_INVALID_ARG, "negative size");
+    if (npil > 0 && (!d_px || !d_py || !d_pt)) return set_error(CELERIS_ERR_INVALID_ARG, "NULL pillar arrays");
+    if (n > 0 && !d_field) return set_error(CELERIS_ERR_INVALID_ARG, "d_field is NULL");
+    CEL_TRY(celeris_rt::require_device());
+    return ff_stated(d_px, d_py, d_pt, npil, psf_geom(cx, cy, z, n, half_window), k, d_field, nullptr, 0, nullptr,
+                     bound_out, static_cast<cudaStream_t>(stream));
+}
+
+int celeris_rs_field_rows_dev(int form, const double* d_px, const double* d_py, const double* d_pt, int npil,
+                              double cx, double cy, double z, double k, int n, double half_window, int row0,
+                              int nrows, double* d_field, double* d_intensity, void* stream) {
+    if (!valid_form(form)) return set_error(CELERIS_ERR_INVALID_ARG, "unknown form %d", form);
+    if (n < 0 || npil < 0 || nrows < 0) return set_error(CELERIS_ERR_INVALID_ARG, "negative size");
+    if (row0 < 0 || (long)row0 + nrows > (long)n)
+        return set_error(CELERIS_ERR_INVALID_ARG, "rows [%d, %d) outside the %d-row grid", row0, row0 + nrows, n);
+    if (npil > 0 && (!d_px || !d_py || !d_pt)) return set_error(CELERIS_ERR_INVALID_ARG, "NULL pillar arrays");
+    CEL_TRY(celeris_rt::require_device());
+    return ff_run(form, d_px, d_py, d_pt, npil, psf_rows_geom(cx, cy, z, n, half_window, row0, nrows), k,
+                  d_field, d_intensity, static_cast<cudaStream_t>(stream));
+}
+
+int celeris_rs_adjoint_rows_dev(int form, const double* d_px, const double* d_py, int npil, double cx, double cy,
+                                double z, double k, int n, double half_window, int row0, int nrows,
+                                const double* d_v, double* d_out, void* stream) {
+    if (!valid_form(form)) return set_error(CELERIS_ERR_INVALID_ARG, "unknown form %d", form);
+    if (n < 0 || npil < 0 || nrows < 0) return set_error(CELERIS_ERR_INVALID_ARG, "negative size");
+    if (row0 < 0 || (long)row0 + nrows > (long)n)
+        return set_error(CELERIS_ERR_INVALID_ARG, "rows [%d, %d) outside the %d-row grid", row0, row0 + nrows, n);
+    if (npil > 0 && (!d_px || !d_py || !d_out)) return set_error(CELERIS_ERR_INVALID_ARG, "NULL arrays");
+    if ((long)n * nrows > 0 && !d_v) return set_error(CELERIS_ERR_INVALID_ARG, "d_v is NULL");
+    CEL_TRY(celeris_rt::require_device());
+    return ff_adjoint(d_px, d_py, npil, psf_rows_geom(cx, cy, z, n, half_window, row0, nrows), k, d_v, d_out,
+                      static_cast<cudaStream_t>(stream), form);
+}
+
+int celeris_device_wait_selftest(unsigned polls) {
+    CEL_TRY(celeris_rt::require_device());
+    cudaStream_t st = nullptr;
+    CEL_TRY(thread_stream(&st));
+    const int slot = status_slot(st);
+    ff_wait_selftest_kernel<<<1, 32, 0, st>>>(polls, slot);
+    count_launch(1);
+    CEL_CUDA(cudaGetLastError());
+    CEL_CUDA(cudaStreamSynchronize(st));
+    return check_status_and_reset(st);
 }
 
 }  // extern "C"

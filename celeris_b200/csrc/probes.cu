@@ -1,7 +1,11 @@
-// Throughput probes: measured peaks of the pipes the far-field kernels are
-// bound by (MUFU transcendentals, FP32 FMA, FP64 FMA) on the current device.
-// Used by bench.py for the roofline denominators; not part of any result path.
+// Probes of the current device: measured peaks of the pipes the far-field and
+// RCWA kernels are bound by (MUFU transcendentals, FP32 FMA, FP64 FMA, FP64
+// tensor cores; bench.py's roofline denominators) and the measured accuracy of
+// the MUFU approximations the precision form's stated error bound relies on.
+// Not part of any result path.
 #include <cuda_runtime.h>
+
+#include <cstring>
 
 #include "runtime.cuh"
 
@@ -75,26 +79,50 @@ __global__ void probe_dmma(double a, int iters, double* sink) {
     if (s == 12345.678) sink[0] = s;
 }
 
-// Accuracy of sin.approx / cos.approx against FP64 sin/cos of the same FP32
-// argument, for arguments uniform in [-xmax, xmax]: max |error| and the mean
-// signed error (bias) of each.
-__global__ void probe_sincos_err(float xmax, int npts, double* acc) {
-    double ms = 0.0, mc = 0.0, bs = 0.0, bc = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += gridDim.x * blockDim.x) {
-        const float x = xmax * (2.0f * ((float)i + 0.5f) / (float)npts - 1.0f);
+// Exhaustive accuracy of sin/cos.approx.ftz.f32 over every FP32 x with
+// |x| <= the float with bits `hi_bits`, against FP64 sin/cos of the same x:
+// out[0] = max |sin err|, out[1] = max |cos err| (as order-preserving bits of
+// non-negative doubles, combined by atomicMax).
+__global__ void probe_sincos_exhaustive(uint32_t hi_bits, unsigned long long* out) {
+    const unsigned long long total = 2ull * ((unsigned long long)hi_bits + 1ull);
+    double ms = 0.0, mc = 0.0;
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const uint32_t bits = (uint32_t)(i >> 1) | ((uint32_t)(i & 1ull) << 31);
+        const float x = __uint_as_float(bits);
         float s, c;
         asm("sin.approx.ftz.f32 %0, %1;" : "=f"(s) : "f"(x));
         asm("cos.approx.ftz.f32 %0, %1;" : "=f"(c) : "f"(x));
-        const double es = (double)s - sin((double)x), ec = (double)c - cos((double)x);
-        ms = fmax(ms, fabs(es));
-        mc = fmax(mc, fabs(ec));
-        bs += es;
-        bc += ec;
+        double sr, cr;
+        sincos((double)x, &sr, &cr);
+        ms = fmax(ms, fabs((double)s - sr));
+        mc = fmax(mc, fabs((double)c - cr));
     }
-    atomicMax(reinterpret_cast<unsigned long long*>(acc + 0), (unsigned long long)__double_as_longlong(ms));
-    atomicMax(reinterpret_cast<unsigned long long*>(acc + 1), (unsigned long long)__double_as_longlong(mc));
-    atomicAdd(acc + 2, bs);
-    atomicAdd(acc + 3, bc);
+    for (int o = 16; o > 0; o >>= 1) {
+        ms = fmax(ms, __shfl_down_sync(0xffffffffu, ms, o));
+        mc = fmax(mc, __shfl_down_sync(0xffffffffu, mc, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(out + 0, (unsigned long long)__double_as_longlong(ms));
+        atomicMax(out + 1, (unsigned long long)__double_as_longlong(mc));
+    }
+}
+
+// Exhaustive relative accuracy of rsqrt.approx.ftz.f32 over every FP32 x with
+// bits in [lo_bits, hi_bits), against 1 / sqrt(x) in FP64: out[0] = max
+// |rsqrt.approx(x) * sqrt(x) - 1|.
+__global__ void probe_rsqrt_exhaustive(uint32_t lo_bits, uint32_t hi_bits, unsigned long long* out) {
+    double m = 0.0;
+    const unsigned long long total = (unsigned long long)(hi_bits - lo_bits);
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const float x = __uint_as_float(lo_bits + (uint32_t)i);
+        float r;
+        asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+        m = fmax(m, fabs((double)r * sqrt((double)x) - 1.0));
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
 }
 
 template <typename F>
@@ -117,23 +145,34 @@ int time_probe(F launch, double ops, double* out_per_s) {
 
 }  // namespace
 
-// New: accuracy of the MUFU sine/cosine on [-xmax, xmax] (npts samples):
-// out = {max |sin err|, max |cos err|, mean sin err, mean cos err}.
-extern "C" int celeris_probe_sincos(double xmax, int npts, double* out) {
+// New: measured accuracy of the MUFU approximations used by the precision-form
+// far-field, exhaustively over their input ranges (see celeris_dev::kSinCosAbsErr).
+extern "C" int celeris_probe_mufu_accuracy(double* measured, double* model) {
     CEL_TRY(celeris_rt::require_device());
-    if (!out || npts <= 0) return celeris_rt::set_error(CELERIS_ERR_INVALID_ARG, "bad arguments");
-    double* d = nullptr;
-    CEL_CUDA(cudaMalloc(&d, 4 * sizeof(double)));
-    CEL_CUDA(cudaMemset(d, 0, 4 * sizeof(double)));
-    probe_sincos_err<<<592, 256>>>((float)xmax, npts, d);
-    celeris_rt::count_launch(1);
-    double h[4];
-    CEL_CUDA(cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost));
+    if (!measured || !model) return celeris_rt::set_error(CELERIS_ERR_INVALID_ARG, "null output");
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    unsigned long long* d = nullptr;
+    CEL_CUDA(cudaMalloc(&d, 4 * sizeof(unsigned long long)));
+    CEL_CUDA(cudaMemset(d, 0, 4 * sizeof(unsigned long long)));
+    const float pi_f = 3.14159265358979323846f;  // rounds up to 3.14159274f
+    uint32_t pi_bits;
+    memcpy(&pi_bits, &pi_f, sizeof(pi_bits));
+    probe_sincos_exhaustive<<<sms * 16, 256>>>(pi_bits, d);
+    const float lo_f = 0x1p-10f, hi_f = 0x1p30f;
+    uint32_t lo_bits, hi_bits;
+    memcpy(&lo_bits, &lo_f, sizeof(lo_bits));
+    memcpy(&hi_bits, &hi_f, sizeof(hi_bits));
+    probe_rsqrt_exhaustive<<<sms * 16, 256>>>(lo_bits, hi_bits, d + 2);
+    celeris_rt::count_launch(2);
+    unsigned long long h[4];
+    const cudaError_t e = cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost);
     cudaFree(d);
-    out[0] = h[0];
-    out[1] = h[1];
-    out[2] = h[2] / npts;
-    out[3] = h[3] / npts;
+    CEL_CUDA(e);
+    for (int i = 0; i < 3; ++i) memcpy(&measured[i], &h[i], sizeof(double));
+    model[0] = model[1] = celeris_dev::kSinCosAbsErr;
+    model[2] = celeris_dev::kRsqrtRelErr;
     return CELERIS_OK;
 }
 

@@ -11,8 +11,12 @@
 //                 or 4x4-supersampled raster -> centred DFT -> Laurent Toeplitz)
 //                 and Einv (LU inverse for the Laurent path)
 //   rcwa_build_M  M = ep2 kp - kkT using the diagonal Kx, Ky (two N^3 GEMMs)
-//   rcwa_eig      Householder Hessenberg + single-shift complex QR + triangular
-//                 back substitution; W = Z X; q = branch(sqrt(lambda))
+//   rcwa_hess     Householder reduction to Hessenberg form H = Q^H M Q (in
+//                 shared memory for n <= 112, blocked compact-WY panels above)
+//   rcwa_schur    multishift QR with aggressive early deflation: Schur form
+//                 T = Z^H M Z (schur_aed.cuh)
+//   rcwa_vec      triangular back substitution for the eigenvectors of T;
+//                 W = Z X; q = branch(sqrt(lambda))
 //   rcwa_smat1    A = kp W, T11/T12 of interface 0, S12 and u = T11^{-1} a0
 //   rcwa_smat2    W^{-1}, A^{-1}, T11'/T12' of interface 1, B = T11' - D S12 T12',
 //                 aN = B^{-1} D u, b0 = T12 u + S22 T12' aN
@@ -22,6 +26,8 @@
 // (a0 has two non-zeros), so only 2 columns of the global S11/S21 are formed.
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include <cmath>
 
 #include <algorithm>
 #include <complex>
@@ -292,7 +298,7 @@ __global__ void __launch_bounds__(kRT) rcwa_fourier_laurent(Bucket b) {
     GemmSmem* gs = reinterpret_cast<GemmSmem*>(stg + 2 * N + LNB * LNB);
     int* piv = b.piv + b.s_n * cell;
     const int info = blk_lu_blocked(N, lu, N, piv, &rs, stg, gs);
-    if (info != 0 && tid == 0) b.info[cell] = -info;
+    if (info != 0 && tid == 0 && b.info[cell] == 0) b.info[cell] = -info;  // keep an earlier stage's code
     blk_lu_solve_blocked(N, lu, N, piv, N, Einv, N, stg, gs);  // Einv = epsT^{-1} (rcwa2d.cpp:203)
 }
 
@@ -381,6 +387,10 @@ __global__ void __launch_bounds__(kRT) rcwa_hess(Bucket b) {
 
 // Schur form by multishift QR with aggressive early deflation (schur_aed.cuh).
 // dynamic smem: AedShared.
+// QR iteration cap for failure-path tests (0: the solver's own cap); set by
+// celeris_debug_qr_iteration_cap.
+__device__ int g_qr_iter_cap;
+
 __global__ void __launch_bounds__(kSchurThreads, 2) rcwa_schur(Bucket b) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int cell = blockIdx.x;
@@ -388,7 +398,8 @@ __global__ void __launch_bounds__(kSchurThreads, 2) rcwa_schur(Bucket b) {
     const int tid = threadIdx.x, nt = blockDim.x;
     cplx* H = at(b.H, b.s_nn, cell);
     AedShared* sh = reinterpret_cast<AedShared*>(smem);
-    const int info = blk_schur_aed(n, H, n, at(b.Z, b.s_nn, cell), n, sh, b.dbg ? b.dbg + kDbgSlots * (size_t)cell : nullptr);
+    const int info = blk_schur_aed(n, H, n, at(b.Z, b.s_nn, cell), n, sh,
+                                   b.dbg ? b.dbg + kDbgSlots * (size_t)cell : nullptr, g_qr_iter_cap);
     if (tid == 0) {
         if (info != 0) b.info[cell] = info;
         if (b.dbg) b.dbg[kDbgSlots * (size_t)cell + 6] = sh->nsweep;
@@ -489,7 +500,7 @@ __global__ void __launch_bounds__(kRT) rcwa_smat1(Bucket b) {
     __syncthreads();
     int* piv = b.piv + b.s_n * cell;
     const int info = blk_lu_blocked(n, T11lu, n, piv, &rs, stg, &gs);
-    if (info != 0 && tid == 0) b.info[cell] = -info;
+    if (info != 0 && tid == 0 && b.info[cell] == 0) b.info[cell] = -info;  // keep an earlier stage's code
     blk_lu_solve_blocked(n, T11lu, n, piv, ld, S, ld, stg, &gs);  // [S12 | u_X | u_Y]
 }
 
@@ -536,7 +547,7 @@ __global__ void __launch_bounds__(kRT) rcwa_smat2(Bucket b) {
     }
     int info = blk_lu_blocked(n, A, n, piv, &rs, stg, &gs);
     blk_lu_solve_blocked(n, A, n, piv, n, Q, n, stg, &gs);  // A^-1 K W
-    if (tid == 0 && info) b.info[cell] = -info;
+    if (tid == 0 && info && b.info[cell] == 0) b.info[cell] = -info;
     for (int e = tid; e < n * n; e += nt) Q[e] = cmul(q1[e / n], Q[e]);
     cplx* S = at(b.S12, b.s_ns, cell);
     const int ld = n + 2;
@@ -558,7 +569,7 @@ __global__ void __launch_bounds__(kRT) rcwa_smat2(Bucket b) {
         x[e] = cscale(cmul(cexpi(cscale(q1[i], c.h)), S[(size_t)i * ld + n + r]), 2.0);
     }
     info = blk_lu_blocked(n, Cm, n, piv, &rs, stg, &gs);
-    if (tid == 0 && info) b.info[cell] = -info;
+    if (tid == 0 && info && b.info[cell] == 0) b.info[cell] = -info;
     blk_lu_solve_blocked(n, Cm, n, piv, 2, x, 2, stg, &gs);  // x = y (X, Y)
     cplx* aN = vec;                      // [2][n]
     cplx* b0 = vec + 2 * (size_t)b.s_n;  // [2][n]
@@ -957,6 +968,14 @@ struct HostCell {
 };
 
 int validate(const celeris_rcwa_cell& c) {
+    // every real input must be finite: a NaN or Inf would run through the
+    // eigensolve and come out as a silent non-finite t, R, T
+    const double v[] = {c.period_x_um, c.period_y_um, c.wavelength_um, c.theta_rad, c.phi_rad,
+                        c.n_inc[0], c.n_inc[1], c.n_sub[0], c.n_sub[1], c.eps_pillar[0], c.eps_pillar[1],
+                        c.eps_bg[0], c.eps_bg[1], c.fill_x, c.fill_y, c.thickness_um, c.shape_param,
+                        c.rotation_rad};
+    for (double x : v)
+        if (!std::isfinite(x)) return set_error(CELERIS_ERR_INVALID_ARG, "cell parameter is NaN or Inf");
     if (c.Mx < 0 || c.My < 0) return set_error(CELERIS_ERR_INVALID_ARG, "M must be >= 0");
     if (c.Mx > 15 || c.My > 15) return set_error(CELERIS_ERR_TOO_LARGE, "Mx, My <= 15 supported");
     if (!(c.wavelength_um > 0) || !(c.period_x_um > 0) || !(c.period_y_um > 0))
@@ -1936,6 +1955,14 @@ int celeris_eig_general_batch(const double* A, int n, int count, double* evals, 
     if (n > kMaxN) return set_error(CELERIS_ERR_TOO_LARGE, "n = %d > %d", n, kMaxN);
     if (count == 0) return CELERIS_OK;
     if (!A || !evals || !evecs) return set_error(CELERIS_ERR_INVALID_ARG, "NULL argument");
+    {   // x * 0 is NaN exactly when x is NaN or Inf: one branch-free pass
+        const size_t per = 2 * (size_t)n * n;
+        for (int c = 0; c < count; ++c) {
+            double z = 0.0;
+            for (size_t i = 0; i < per; ++i) z += A[c * per + i] * 0.0;
+            if (z != 0.0) return set_error(CELERIS_ERR_INVALID_ARG, "matrix %d holds NaN or Inf", c);
+        }
+    }
     if (n == 1) {  // nothing to reduce
         for (int c = 0; c < count; ++c) {
             evals[2 * c] = A[2 * c];
@@ -2012,10 +2039,21 @@ int celeris_rcwa_batch(const celeris_rcwa_cell* cells, int ncell, celeris_rcwa_r
     std::vector<HostCell> hc;
     hc.reserve(ncell);
     for (int i = 0; i < ncell; ++i) {
-        CEL_TRY(validate(cells[i]));
+        const int v = validate(cells[i]);
+        if (v != CELERIS_OK) {
+            const std::string msg = celeris_last_error();
+            return set_error(v, "cell %d: %s", i, msg.c_str());
+        }
         hc.push_back(make_cell(cells[i], i, 1.0, 0.0, 0.0, 0.0, 2));
     }
     return run_cells(hc, out, info, 2);
+}
+
+int celeris_debug_qr_iteration_cap(int cap) {
+    if (cap < 0) return set_error(CELERIS_ERR_INVALID_ARG, "cap < 0");
+    CEL_TRY(celeris_rt::require_device());
+    CEL_CUDA(cudaMemcpyToSymbol(g_qr_iter_cap, &cap, sizeof(int)));
+    return CELERIS_OK;
 }
 
 }  // extern "C"

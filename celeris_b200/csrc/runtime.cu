@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -60,6 +61,35 @@ int require_device() {
     return CELERIS_OK;
 }
 
+namespace {
+// Pending injected allocation failures (failure-path tests only).
+std::atomic<int> g_fail_alloc{[] {
+    const char* v = std::getenv("CELERIS_DEBUG_FAIL_ALLOC");
+    return v ? std::atoi(v) : 0;
+}()};
+}  // namespace
+
+// Consumes one pending injected failure; true if there was one.
+bool take_injected_failure() {
+    int pending = g_fail_alloc.load();
+    while (pending > 0)
+        if (g_fail_alloc.compare_exchange_weak(pending, pending - 1)) return true;
+    return false;
+}
+
+int device_alloc(void** p, size_t bytes, const char* what) {
+    *p = nullptr;
+    if (take_injected_failure())
+        return set_error(CELERIS_ERR_OOM, "%s: cudaMalloc(%zu) failed (injected failure)", what, bytes);
+    const cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return set_error(CELERIS_ERR_OOM, "%s: cudaMalloc(%zu) failed: %s", what, bytes, cudaGetErrorString(e));
+    }
+    return CELERIS_OK;
+}
+
 thread_local bool t_counting = true;
 
 void count_launch(uint64_t n) {
@@ -77,18 +107,20 @@ int Workspace::reserve(cudaStream_t stream, size_t bytes) {
         base_ = nullptr;
         cap_ = 0;
     }
+    if (take_injected_failure())
+        return set_error(CELERIS_ERR_OOM, "workspace: cudaMalloc(%zu) failed (injected failure)", bytes);
     size_t want = align256(bytes + bytes / 4);
     cudaError_t e = cudaMalloc(&base_, want);
     if (e != cudaSuccess) {
         base_ = nullptr;
+        cudaGetLastError();
         // retry with the exact size before giving up
         want = align256(bytes);
         e = cudaMalloc(&base_, want);
         if (e != cudaSuccess) {
             base_ = nullptr;
             cudaGetLastError();
-            return set_error(CELERIS_ERR_OOM, "workspace: cudaMalloc(%zu) failed: %s", want,
-                             cudaGetErrorString(e));
+            return set_error(CELERIS_ERR_OOM, "workspace: cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
         }
     }
     cap_ = want;
@@ -225,6 +257,12 @@ uint64_t celeris_launch_count(void) { return celeris_rt::g_launches.load(); }
 
 int celeris_release_workspace(void) {
     celeris_rt::Workspace::release_all();
+    return CELERIS_OK;
+}
+
+int celeris_debug_fail_alloc(int count) {
+    if (count < 0) return celeris_rt::set_error(CELERIS_ERR_INVALID_ARG, "count < 0");
+    celeris_rt::g_fail_alloc.store(count);
     return CELERIS_OK;
 }
 

@@ -32,6 +32,14 @@ int cuda_error(cudaError_t e, const char* where);
 // Returns CELERIS_OK when a CUDA device is present (and selects nothing).
 int require_device();
 
+// cudaMalloc for every device buffer the library owns (workspace arenas, I/O
+// buffers). Fails with CELERIS_ERR_OOM when cudaMalloc fails, and also - for
+// failure-path tests - while an injected-failure count is pending
+// (celeris_debug_fail_alloc, or the environment variable
+// CELERIS_DEBUG_FAIL_ALLOC=<count> read when the library loads): each such call
+// consumes one count and allocates nothing.
+int device_alloc(void** p, size_t bytes, const char* what);
+
 // ---- launch accounting ----------------------------------------------------
 // Kernels launched while the calling thread captures a CUDA graph are not
 // counted (set_launch_counting(false)); a graph launch counts its kernels.
@@ -95,6 +103,19 @@ namespace celeris_dev {
 
 constexpr uint32_t kSpinLimit = 1u << 26;
 
+// Accuracy model of the MUFU approximations in the precision-form far-field
+// terms; the error bound that form states rests on these two figures:
+//   kSinCosAbsErr  max |sin.approx.ftz.f32(x) - sin(x)| (and the same for cos)
+//                  over every FP32 x in [-pi_f, pi_f], pi_f = 3.14159274f (the
+//                  kernel's reduced phase range)
+//   kRsqrtRelErr   max |rsqrt.approx.ftz.f32(x) sqrt(x) - 1| over every normal
+//                  FP32 x in [2^-10, 2^30)
+// celeris_probe_mufu_accuracy measures both exhaustively on the current device
+// against FP64 sin / cos / sqrt, and the GPU tests check the measurement stays
+// within these figures.
+constexpr double kSinCosAbsErr = 6.8e-7;
+constexpr double kRsqrtRelErr = 1.3e-7;
+
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -132,10 +153,10 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 }
 
 // Bounded parity wait. Returns true when the phase with parity `parity`
-// completed, false when the poll budget ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// completed, false when the poll budget (`limit` polls) ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = kSpinLimit) {
     const uint32_t a = smem_addr(bar);
-    for (uint32_t it = 0; it < kSpinLimit; ++it) {
+    for (uint32_t it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -147,6 +168,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         if (done) return true;
     }
     return false;
+}
+
+// Arrive once on `bar` (no transaction bytes).
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_addr(bar))
+                 : "memory");
 }
 
 }  // namespace celeris_dev

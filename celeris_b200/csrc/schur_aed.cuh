@@ -636,7 +636,8 @@ __device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, i
 
 // prof (optional, per cell): clock64 sums of [AED local, AED far, sweep local,
 // sweep far, small blocks, AED QR], [7] chain steps, [8] AED QR rotations.
-__device__ int blk_schur_aed(int n, cplx* H, int ldh, cplx* Z, int ldz, AedShared* sh, long long* prof) {
+__device__ int blk_schur_aed(int n, cplx* H, int ldh, cplx* Z, int ldz, AedShared* sh, long long* prof,
+                             int iter_cap = 0) {
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     const double eps = 2.220446049250313e-16;
     const double smallnum = 2.2250738585072014e-308 * (n / eps);
@@ -649,7 +650,9 @@ __device__ int blk_schur_aed(int n, cplx* H, int ldh, cplx* Z, int ldz, AedShare
         sh->it = 0;
     }
     __syncthreads();
-    const int max_iter = 2 * n + 100;  // AED + sweep iterations (about n / 4 are typical)
+    // AED + sweep iterations (about n / 4 are typical); iter_cap > 0 lowers the
+    // cap (failure-path tests of the non-convergence report)
+    const int max_iter = iter_cap > 0 ? min(iter_cap, 2 * n + 100) : 2 * n + 100;
     for (int iter = 0; iter < max_iter; ++iter) {
         const int hi0 = sh->hi;
         for (int i = 1 + tid; i <= hi0; i += nt) {

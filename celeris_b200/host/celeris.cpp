@@ -634,8 +634,6 @@ FocalAnalysis analyze_focus(const MetalensDesign& lens, const UnitCellLibrary& l
     // ideal lens at the focal centre: |t| = 1, ideal phase (focal.cpp:104); on
     // the GPU as the centre pixel of a 3 x 3 grid with step W' (exactly 0).
     std::vector<Cell> ideal = cells;
-    const double p = lens.period_um;
-    (void)p;
     for (Cell& c : ideal) {
         const double r = std::sqrt(c.x * c.x + c.y * c.y);
         c.t = std::polar(1.0, -k * (std::sqrt(r * r + focal_length_um * focal_length_um) - focal_length_um));

@@ -19,9 +19,12 @@
  *   - Complex arrays are interleaved (re, im) doubles: the memory layout of
  *     std::complex<double>[] and of numpy complex128.
  *   - Host-buffer entry points ("drop-in" forms) are synchronous from the
- *     caller's view, like the reference. *_dev entry points take device
- *     pointers and a cudaStream_t (passed as void*, NULL = legacy default
- *     stream) and are asynchronous with respect to the host.
+ *     caller's view, like the reference, and thread-safe (each calling thread
+ *     gets streams of its own). *_dev entry points take device pointers and a
+ *     cudaStream_t (passed as void*, NULL = legacy default stream) and are
+ *     asynchronous with respect to the host; their scratch comes from a
+ *     workspace arena per (device, stream), so calls on ONE stream from
+ *     several host threads at once must be serialised by the caller.
  *   - Focal grid: pixel (i, j), i = column, j = row, row-major index j*n + i,
  *       fx = cx - W + i * step, fy = cy - W + j * step, step = 2W / (n - 1)
  *     (propagate.cu:51-52, focal.cpp:223-226).
@@ -75,10 +78,14 @@ int celeris_probe_peaks(double* mufu_per_s, double* ffma_per_s, double* dfma_per
 /* New: FP64 FMA/s of the tensor cores (mma.sync m8n8k4 f64) of the current
  * device from a short probe kernel; roofline denominator of the RCWA products. */
 int celeris_probe_dmma(double* fma_per_s);
-/* New: accuracy of the hardware sine/cosine (sin/cos.approx.f32) over
- * [-xmax, xmax]: out[4] = {max |sin err|, max |cos err|, mean sin err,
- * mean cos err} against FP64 sin/cos of the same FP32 arguments. */
-int celeris_probe_sincos(double xmax, int npts, double* out);
+/* New: measured accuracy of the MUFU approximations the precision-form
+ * far-field uses, over EVERY FP32 input of their ranges on the current device:
+ * measured[0] = max |sin.approx(x) - sin(x)| and measured[1] the same for cos,
+ * over all x in [-pi_f, pi_f]; measured[2] = max |rsqrt.approx(x) sqrt(x) - 1|
+ * over all x in [2^-10, 2^30) (references in FP64). model[0..2] receive the
+ * figures the stated error bound of the precision form assumes for the same
+ * three quantities; the bound is valid on a device where measured <= model. */
+int celeris_probe_mufu_accuracy(double* measured, double* model);
 /* New: when on != 0, the far-field entry points record CUDA events around
  * their main kernel (on the stream it is launched on). */
 int celeris_set_kernel_timing(int on);
@@ -118,6 +125,26 @@ int celeris_rs_field(int form, const double* px, const double* py,
                      double z, double k, int n, double half_window,
                      double* field_out, double* intensity_out, double* err_out);
 
+/* New: celeris_rs_field with the precision form's error stated two ways.
+ * err_out (may be NULL) receives the SAMPLED error: max |E_p - E64_p| over a
+ * pixel sample - 256 strided pixels, the centre pixel and the 11 x 11 pixels
+ * around the peak of |E| - recomputed in FP64 on the device, divided by
+ * max_p |E_p| over the whole grid. bound_out (may be NULL) receives an UPPER
+ * BOUND on max_p |E_p - E64_p| / max_p |E_p| over the whole grid from the error
+ * model of the precision-form arithmetic: the MUFU approximation errors
+ * (celeris_probe_mufu_accuracy) and the rounding of FP32 constants counted
+ * without cancellation, the FP32 rounding errors of the terms and of the tile
+ * sums counted as independent and mean zero with 8 standard deviations per
+ * pixel (probabilistic rounding-error analysis: exceeded with probability
+ * below 1e-13 per pixel under that model). Both are 0 for the plain form, and
+ * both cost one pass over the pillars (the bound) or ~380 FP64 pixel sums (the
+ * sample), run beside the field's download. */
+int celeris_rs_field_bounded(int form, const double* px, const double* py,
+                             const double* pt, int npil, double cx, double cy,
+                             double z, double k, int n, double half_window,
+                             double* field_out, double* intensity_out,
+                             double* err_out, double* bound_out);
+
 /* ---- far-field: device-buffer forms ---------------------------------------- */
 
 /* New: far-field with inputs resident on the device. d_field (2*n*n doubles)
@@ -133,20 +160,37 @@ int celeris_rs_field_dev(int form, const double* d_px, const double* d_py,
  * latency-critical loop in which the device-wide synchronisation of
  * cudaMalloc/cudaFree is not acceptable. It allocates nothing: its scratch (the
  * pillar records and the per-chunk partial sums) is a fixed 48 MiB array that
- * every GPU loading this library holds until the process exits. Inputs and
- * outputs are the caller's device buffers, as for celeris_rs_field_dev.
+ * every GPU holds from the moment the library's far-field module is loaded on
+ * it until the process exits. With CUDA's lazy module loading (the default)
+ * that happens at the first far-field call of any kind on the device, so the
+ * 48 MiB are taken then, from the device's free memory. Inputs and outputs are
+ * the caller's device buffers, as for celeris_rs_field_dev.
  * Limit: (16 B per pillar for CELERIS_FORM_F32C, 32 B for the plain form,
- * rounded up to 256 B) + 16 B per focal pixel must fit in 48 MiB (the
- * 785,456-pillar x 1024^2 metalens fits in both forms); larger requests return
- * CELERIS_ERR_TOO_LARGE. The first call on each device looks up the array's
- * device address (cudaGetSymbolAddress) and caches it; make that first call
- * before any stream capture begins. All calls share the one array: calls whose
- * kernels overlap on the GPU (different streams, or different host threads
- * without ordering) race on it and must be serialised by the caller. */
+ * rounded up to 256 B) + 16 B per focal pixel must fit in 48 MiB; the pillar
+ * axis is cut into fewer, longer chunks until every chunk's partial sums fit
+ * (the 785,456-pillar x 1024^2 metalens fits in both forms). Larger requests
+ * return CELERIS_ERR_TOO_LARGE. Set-up: the first call on each device (with
+ * that device current) loads the module and looks up the array's device
+ * address (cudaGetSymbolAddress), which is then cached. A call with n = 0 or
+ * npil = 0 does only that, so make one such call on each device before a
+ * memory pool takes the free memory and before any stream capture begins.
+ * All calls share the one array, which keeps the last call's contents: calls
+ * whose kernels overlap on the GPU (different streams, or different host
+ * threads without ordering) race on it and must be serialised by the caller. */
 int celeris_rs_field_noalloc(int form, const double* d_px, const double* d_py,
                              const double* d_pt, int npil, double cx, double cy,
                              double z, double k, int n, double half_window,
                              double* d_field, double* d_intensity, void* stream);
+
+/* New: rows [row0, row0 + nrows) of the n x n grid of celeris_rs_field_dev
+ * (the same pixel positions and arithmetic), for a focal grid split by rows
+ * over several devices: d_field holds nrows * n complex values (d_intensity
+ * nrows * n), row-major, row i = grid row row0 + i. */
+int celeris_rs_field_rows_dev(int form, const double* d_px, const double* d_py,
+                              const double* d_pt, int npil, double cx, double cy,
+                              double z, double k, int n, double half_window,
+                              int row0, int nrows, double* d_field,
+                              double* d_intensity, void* stream);
 
 /* New: adjoint (conjugate-transpose, pixel -> pillar) RS sum on the same grid:
  *   d_out[j] = sum_p conj(g_pj) * d_v[p],   g_pj = exp(i k R_pj) / R_pj.
@@ -162,18 +206,56 @@ int celeris_rs_adjoint_dev(int form, const double* d_px, const double* d_py,
                            int n, double half_window, const double* d_v,
                            double* d_out, void* stream);
 
+/* New: the adjoint over rows [row0, row0 + nrows) of the grid only: d_v holds
+ * nrows * n complex pixel values (row i = grid row row0 + i). The adjoint of a
+ * field split by rows is the sum of these partial adjoints (one all-reduce). */
+int celeris_rs_adjoint_rows_dev(int form, const double* d_px, const double* d_py,
+                                int npil, double cx, double cy, double z, double k,
+                                int n, double half_window, int row0, int nrows,
+                                const double* d_v, double* d_out, void* stream);
+
 /* New: sampled FP64 check of a computed field. For the pixel indices d_idx[0..ns)
- * recomputes E in the plain FP64 form and writes max|E - E64| over the sample
- * divided by max over all n*n pixels of |E| into *err_out (host). Synchronous. */
+ * and the 11 x 11 pixels around the peak of |E| recomputes E in the plain FP64
+ * form and writes max|E - E64| over the sample divided by max over all n*n
+ * pixels of |E| into *err_out (host). Synchronous. */
 int celeris_rs_check_dev(const double* d_px, const double* d_py,
                          const double* d_pt, int npil, double cx, double cy,
                          double z, double k, int n, double half_window,
                          const double* d_field, const int* d_idx, int ns,
                          double* err_out, void* stream);
 
-/* New: synchronize `stream` and report a device-side failure (a bounded wait
- * that ran out) recorded by an earlier asynchronous *_dev call. */
+/* New: the error bound of celeris_rs_field_bounded for a precision-form field
+ * d_field (n*n complex) computed on the device from these inputs: an upper
+ * bound on max_p |E_p - E64_p| / max_p |E_p|. Synchronous. */
+int celeris_rs_error_bound_dev(const double* d_px, const double* d_py,
+                               const double* d_pt, int npil, double cx, double cy,
+                               double z, double k, int n, double half_window,
+                               const double* d_field, double* bound_out,
+                               void* stream);
+
+/* New: synchronize `stream` and report a device-side failure recorded by an
+ * earlier asynchronous *_dev call on that stream: CELERIS_ERR_DEVICE_TIMEOUT (a
+ * bounded wait ran out) or CELERIS_ERR_INVALID_ARG (a pillar input or an
+ * adjoint pixel value was NaN or Inf; non-finite values propagate to the
+ * outputs). Host-buffer calls report these themselves. */
 int celeris_sync_status(void* stream);
+
+/* ---- failure-path diagnostics (tests of the error reporting) -------------- */
+
+/* New: run the bounded device wait of the far-field tile pipeline on a barrier
+ * that never completes, limited to `polls` polls: returns
+ * CELERIS_ERR_DEVICE_TIMEOUT with the device context intact (no trap). */
+int celeris_device_wait_selftest(unsigned polls);
+/* New: make the next `count` device allocations of this library fail as if
+ * cudaMalloc had (CELERIS_ERR_OOM, nothing allocated); 0 clears. The
+ * environment variable CELERIS_DEBUG_FAIL_ALLOC=<count> sets the same count
+ * when the library loads. */
+int celeris_debug_fail_alloc(int count);
+/* New: cap the QR iterations of the RCWA / eigensolver Schur stage at `cap`
+ * (0 restores the solver's own cap, 2n + 100), so a test can drive the
+ * non-convergence report (CELERIS_ERR_EIG_NOCONV, per-cell info > 0 like
+ * LAPACK's). Applies to the current device. */
+int celeris_debug_qr_iteration_cap(int cap);
 
 /* ---- RCWA ------------------------------------------------------------------ */
 
@@ -212,6 +294,9 @@ typedef struct celeris_rcwa_result {
  * with incident field (Ex0, Ey0). Synchronous, host buffers. */
 int celeris_solve_rcwa_2d(const celeris_rcwa_cell* cell, const double* Ex0,
                           const double* Ey0, celeris_rcwa_result* out);
+
+/* Every real field of a cell must be finite: a NaN or Inf returns
+ * CELERIS_ERR_INVALID_ARG (naming the cell in a batch) before any device work. */
 
 /* New: batched uneven cells. Each cell is solved once (one eigensolve, one
  * S-matrix) for BOTH the X (Ex0=1, Ey0=0) and Y (Ex0=0, Ey0=1) excitations;

@@ -271,3 +271,16 @@ def optimize_system(indices, f_um, d_um, wavelength, p_lo, p_hi, t_lo, t_hi, gri
     lib.ref_optimize_system(pm, f(f_um), f(d_um), f(wavelength), f(p_lo), f(p_hi), f(t_lo), f(t_hi), grid, M,
                             fill_samples, f(eff_weight), out.ctypes.data_as(_P))
     return out
+
+
+def optimize_pillar(indices, period, wavelength, target_phase, amplitude_weight, M, fill0, thickness0, max_iters):
+    """The reference's optimize_pillar (optimize.cpp:22-86) over the oracle's cell
+    solves. Returns dict(fill, thickness_um, phase, amplitude, loss, iterations)."""
+    lib = load()
+    mats, pm = _d(_mats(*indices))
+    out = np.zeros(6)
+    f = ctypes.c_double
+    lib.ref_optimize_pillar(pm, f(period), f(wavelength), f(target_phase), f(amplitude_weight), M, f(fill0),
+                            f(thickness0), max_iters, out.ctypes.data_as(_P))
+    return dict(fill=out[0], thickness_um=out[1], phase=out[2], amplitude=out[3], loss=out[4],
+                iterations=int(out[5]))

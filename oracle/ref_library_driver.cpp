@@ -17,6 +17,7 @@
 
 #include "celeris/design/achromatic.hpp"
 #include "celeris/design/metalens.hpp"
+#include "celeris/design/optimize.hpp"
 #include "celeris/design/pb_achromatic.hpp"
 #include "celeris/design/pb_metalens.hpp"
 #include "celeris/design/system_opt.hpp"
@@ -383,5 +384,24 @@ REF_API int ref_optimize_system(const double* mats, double f_um, double d_um, do
                                             nullptr);
     const double v[5] = {r.period_um, r.thickness_um, r.strehl, r.mean_amplitude, r.merit};
     for (int k = 0; k < 5; ++k) out[k] = v[k];
+    return 0;
+}
+
+// optimize_pillar (optimize.cpp:22-86): the reference's central differences and
+// Adam over (fill, thickness), every cell solve forwarded to the oracle.
+// mats = pillar, background, incident, substrate (re, im each).
+// out: fill, thickness_um, achieved_phase_rad, achieved_amplitude, loss, iterations.
+REF_API int ref_optimize_pillar(const double* mats, double period_um, double wavelength_um, double target_phase_rad,
+                                double amplitude_weight, int M, double fill0, double thickness0, int max_iters,
+                                double* out) {
+    const celeris::PillarTarget tgt{wavelength_um, target_phase_rad, amplitude_weight};
+    const auto r = celeris::optimize_pillar(mat(mats), mat(mats + 2), mat(mats + 4), mat(mats + 6), period_um, tgt, M,
+                                            fill0, thickness0, max_iters);
+    out[0] = r.fill;
+    out[1] = r.thickness_um;
+    out[2] = r.achieved_phase_rad;
+    out[3] = r.achieved_amplitude;
+    out[4] = r.loss;
+    out[5] = r.iterations;
     return 0;
 }

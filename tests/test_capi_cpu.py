@@ -101,3 +101,31 @@ def test_eig_arguments_are_rejected_before_device_work():
     assert lib.celeris_eig_general_batch(capi._dp(buf), 5000, 1, capi._dp(buf), capi._dp(buf), None) == \
         capi.ERR_TOO_LARGE
     assert lib.celeris_eig_general(None, 4, capi._dp(buf), capi._dp(buf)) == capi.ERR_INVALID_ARG
+
+
+def test_non_finite_rcwa_and_eig_inputs_are_rejected_before_device_work():
+    """A NaN or Inf in any real field of a cell, or in a matrix handed to the
+    eigensolver, is an argument error naming the cell / matrix, reported
+    without touching a device (the reference would carry it into Eigen and
+    return non-finite t, R, T)."""
+    import math
+
+    import numpy as np
+
+    base = dict(period_um=0.4, wavelength_um=0.633, n_inc=1.0, n_sub=1.46, eps_pillar=4.0, eps_bg=1.0,
+                fill_x=0.5, thickness_um=0.3, Mx=2)
+    for key, bad in (("fill_x", math.nan), ("thickness_um", math.inf), ("eps_pillar", complex(4.0, math.nan)),
+                     ("wavelength_um", math.inf), ("rotation_rad", -math.inf)):
+        cells = [capi.rcwa_cell(**base), capi.rcwa_cell(**{**base, key: bad})]
+        with pytest.raises(capi.CelerisError) as e:
+            capi.rcwa_batch(cells)
+        assert e.value.status == capi.ERR_INVALID_ARG, key
+        assert "cell 1" in str(e.value)
+    lib = capi.load()
+    A = np.eye(6, dtype=complex)
+    A2 = np.stack([A, A])
+    A2[1, 2, 3] = complex(0.0, math.nan)
+    out = np.zeros(2 * 2 * 36)
+    assert lib.celeris_eig_general_batch(capi._dp(A2.view(np.float64)), 6, 2, capi._dp(out), capi._dp(out), None) \
+        == capi.ERR_INVALID_ARG
+    assert b"matrix 1" in lib.celeris_last_error()

@@ -3,8 +3,9 @@
 Plain FP64 form: within 1e-10 of the oracle relative to the peak |E| on the
 complex field (and on |E|^2), on the reference's golden vectors and on the full
 70,688-pillar x 161^2 metalens. Precision (FP32-compensated) form: within 1e-5
-of the FP64 result relative to the peak |E|, and its stated error (sampled FP64
-re-evaluation) is an honest upper-bound-sized figure.
+of the FP64 result relative to the peak |E|; of its two stated errors the
+sampled FP64 re-evaluation never exceeds the true full-grid error and the model
+bound never falls below it.
 """
 import ctypes
 import os
@@ -13,7 +14,7 @@ import numpy as np
 import pytest
 
 from celeris_b200 import capi
-from celeris_b200.workloads import metalens_70k, metalens_785k, small_aperture
+from celeris_b200.workloads import FocalGrid, metalens_70k, metalens_785k, small_aperture
 from oracle import farfield as F
 
 pytestmark = pytest.mark.gpu
@@ -101,6 +102,79 @@ def test_metalens_785k_sampled_plain_and_full_f32c():
                                 form=capi.FORM_F32C, want_intensity=False, want_err=True)
     assert rel_err(E32, E) <= TOL_F32C
     assert err <= TOL_F32C
+
+
+STATED = {
+    "metalens_70k": lambda: metalens_70k(),
+    "metalens_785k": lambda: metalens_785k(),
+    # a focal distance FP32 cannot hold: the terms use z_f = (float)z
+    "metalens_70k_z100.3": lambda: (metalens_70k()[0], FocalGrid(161, 5.0, 100.3)),
+}
+
+
+@pytest.mark.parametrize("which", sorted(STATED))
+def test_stated_error_sampled_below_true_below_bound(which):
+    """The precision form's two stated errors on the full grid: the sampled FP64
+    re-evaluation never exceeds the true error against the FP64 form, and the
+    model bound never falls below it; the bound itself meets 1e-5."""
+    ap, g = STATED[which]()
+    args = (ap.px, ap.py, ap.t, 0.0, 0.0, g.z_um, ap.k, g.n, g.half_window_um)
+    E64, _, _ = capi.rs_field(*args, want_intensity=False)
+    E32, _, sampled, bound = capi.rs_field_bounded(*args)
+    true = np.max(np.abs(E32 - E64)) / np.max(np.abs(E32))
+    # the sample's FP64 sums differ from the FP64 form's only in summation order
+    assert sampled <= true + 1e-12, (sampled, true)
+    assert true <= bound, (true, bound)
+    assert bound <= TOL_F32C, bound
+    # the device-buffer form of the bound gives the same figure
+    import torch
+
+    dev = torch.device("cuda")
+    px, py, t = (torch.tensor(v, device=dev) for v in (ap.px, ap.py, ap.t))
+    Ed = torch.tensor(E32, device=dev)
+    b = np.zeros(1)
+    capi.check(capi.load().celeris_rs_error_bound_dev(
+        ctypes.c_void_p(px.data_ptr()), ctypes.c_void_p(py.data_ptr()), ctypes.c_void_p(t.data_ptr()), ap.npil,
+        0.0, 0.0, g.z_um, ap.k, g.n, g.half_window_um, ctypes.c_void_p(Ed.data_ptr()),
+        b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), None))
+    assert b[0] == pytest.approx(bound, rel=1e-9)
+
+
+def test_mufu_accuracy_within_the_bound_model():
+    """Every FP32 input of sin/cos.approx on [-pi_f, pi_f] and of rsqrt.approx on
+    [2^-10, 2^30), measured on this GPU against FP64: within the figures the
+    precision form's error bound assumes."""
+    r = capi.probe_mufu_accuracy()
+    for key in ("sin_abs", "cos_abs", "rsqrt_rel"):
+        assert 0.0 < r["measured"][key] <= r["model"][key], (key, r)
+
+
+def test_rows_split_matches_whole_grid():
+    """Row blocks of one grid (the multi-device split) put together give the
+    whole-grid field of both forms, to the FP64 rounding of the chunk sums."""
+    import torch
+
+    ap, g = metalens_70k()
+    dev = torch.device("cuda")
+    px, py, t = (torch.tensor(v, device=dev) for v in (ap.px, ap.py, ap.t))
+    lib = capi.load()
+    for form in (capi.FORM_PLAIN_F64, capi.FORM_F32C):
+        whole = torch.empty((g.n, g.n), dtype=torch.complex128, device=dev)
+        capi.check(lib.celeris_rs_field_dev(form, ctypes.c_void_p(px.data_ptr()), ctypes.c_void_p(py.data_ptr()),
+                                            ctypes.c_void_p(t.data_ptr()), ap.npil, 0.0, 0.0, g.z_um, ap.k, g.n,
+                                            g.half_window_um, ctypes.c_void_p(whole.data_ptr()), None, None))
+        parts = torch.empty_like(whole)
+        for r0, r1 in ((0, 37), (37, 100), (100, 161)):
+            blk = parts[r0:r1]
+            capi.check(lib.celeris_rs_field_rows_dev(
+                form, ctypes.c_void_p(px.data_ptr()), ctypes.c_void_p(py.data_ptr()), ctypes.c_void_p(t.data_ptr()),
+                ap.npil, 0.0, 0.0, g.z_um, ap.k, g.n, g.half_window_um, r0, r1 - r0,
+                ctypes.c_void_p(blk.data_ptr()), None, None))
+        torch.cuda.synchronize()
+        w, p = whole.cpu().numpy(), parts.cpu().numpy()
+        assert np.max(np.abs(w - p)) <= 1e-12 * np.max(np.abs(w)), form
+    assert lib.celeris_rs_field_rows_dev(0, None, None, None, 0, 0.0, 0.0, 1.0, 1.0, 8, 1.0, 5, 4, None, None,
+                                         None) == capi.ERR_INVALID_ARG
 
 
 def test_zx_caustic_matches_oracle():

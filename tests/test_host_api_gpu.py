@@ -131,3 +131,26 @@ def test_optimize_pillar_reduces_loss():
     r = cel.optimize_pillar(tio2, air, air, cel.materials.fused_silica(), 0.35, tgt, 3, 0.5, 0.6, 15)
     assert r.loss <= r0.loss
     assert 0.08 <= r.fill <= 0.92 and 0.2 <= r.thickness_um <= 1.0
+
+
+@pytest.mark.parametrize("iters", [0, 1, 15])
+def test_optimize_pillar_matches_reference_trajectory(iters):
+    """optimize_pillar against the reference's own optimize.cpp:22-86 (central
+    differences with h = 5e-3, Adam lr 0.04, box clamps), compiled into the
+    oracle build with every cell solve forwarded to the oracle's RCWA: the same
+    (fill, thickness, phase, |t|, loss) after 0, 1 and 15 steps."""
+    from oracle import library as OL
+
+    if not OL.available():
+        pytest.skip("oracle/_ref not built")
+    c = cel.Material.constant
+    mats = (c(2.4 + 0j, "pillar"), c(1.0 + 0j, "bg"), c(1.0 + 0j, "inc"), c(1.46 + 0j, "sub"))
+    tgt = cel.PillarTarget(0.532, 1.0, 0.25)
+    got = cel.optimize_pillar(*mats, 0.35, tgt, 3, 0.5, 0.6, iters)
+    want = OL.optimize_pillar((2.4, 1.0, 1.0, 1.46), 0.35, 0.532, 1.0, 0.25, 3, 0.5, 0.6, iters)
+    assert got.iterations == want["iterations"] == iters
+    assert abs(got.fill - want["fill"]) <= 1e-9
+    assert abs(got.thickness_um - want["thickness_um"]) <= 1e-9
+    assert abs(got.achieved_phase_rad - want["phase"]) <= 1e-9
+    assert abs(got.achieved_amplitude - want["amplitude"]) <= 1e-9
+    assert abs(got.loss - want["loss"]) <= 1e-9

@@ -126,6 +126,34 @@ def test_uneven_batch_matches_single_cell_solves():
         assert abs(one["tx0"] - res[2 * i]["tx0"]) <= 1e-12 * abs(one["tx0"])
 
 
+def test_uneven_4096_cells_against_oracle():
+    """Cells of the 4096-cell uneven workload (256^2 rasters, Laurent rule for
+    every shape, squares included: rcwa2d.cpp:335-340; eigensolve and branch:
+    rcwa2d.cpp:362-364) solved inside ONE uneven batch call of its first 384
+    cells, so bucketing by harmonic count and the wave split run as in the
+    measured batch. One cell of every (shape, M) pair, M = 3..7, plus a second
+    one for M in {3, 5, 7}, is compared with the oracle at 1e-10, with
+    R + T = 1 to 1e-10 (lossless, normal incidence)."""
+    from celeris_b200.workloads import rcwa_uneven_4096
+
+    cells = rcwa_uneven_4096()[:384]
+    res, info = capi.rcwa_batch([capi.rcwa_cell(**c) for c in cells])
+    assert np.all(info == 0)
+    picked = {}
+    for i, c in enumerate(cells):
+        key = (c["name"], c["Mx"])
+        want = 2 if c["Mx"] in (3, 5, 7) else 1
+        if len(picked.setdefault(key, [])) < want:
+            picked[key].append(i)
+    assert len(picked) == 15  # {square, circle, ring} x M = 3..7
+    for key, idx in sorted(picked.items()):
+        for i in idx:
+            c = cells[i]
+            assert c["grid"] == 256 and c["force_laurent"] == 1
+            check(res[2 * i], ref(c, 1.0, 0.0))
+            check(res[2 * i + 1], ref(c, 0.0, 1.0))
+
+
 def test_custom_excitation_single_cell():
     c = MIXED[1]
     Ex0, Ey0 = 0.6 + 0.2j, -0.3j

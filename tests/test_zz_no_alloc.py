@@ -36,7 +36,7 @@ def _run(fn, form, px, py, t, cx, cy, z, k, n, W):
 
 
 @pytest.mark.parametrize("form", [capi.FORM_PLAIN_F64, capi.FORM_F32C], ids=["plain_f64", "f32c"])
-@pytest.mark.parametrize("case", ["metalens_70k", "ragged_1025"])
+@pytest.mark.parametrize("case", ["metalens_70k", "ragged_1025", "merged_chunks_20011"])
 def test_noalloc_matches_allocating_entry_point_twice(form, case):
     import torch
 
@@ -44,9 +44,15 @@ def test_noalloc_matches_allocating_entry_point_twice(form, case):
     if case == "metalens_70k":
         ap, g = metalens_70k()
         args = (0.0, 0.0, g.z_um, ap.k, g.n, g.half_window_um)
-    else:
+    elif case == "ragged_1025":
         ap = small_aperture(1025, seed=7)
         args = (0.3, -0.2, ap.focal_um, ap.k, 37, 2.5)
+    else:
+        # 1024^2 pixels: one grid of partial sums is 16 MiB, so the precision
+        # form's usual pillar split (six or more chunks) does not fit in the
+        # 48 MiB scratch and the chunks are merged until it does
+        ap = small_aperture(20011, seed=5, spread_um=30.0, focal_um=200.0)
+        args = (0.0, 0.0, ap.focal_um, ap.k, 1024, 6.0)
     dev = torch.device("cuda")
     px, py, t = (torch.tensor(v, device=dev) for v in (ap.px, ap.py, ap.t))
     E_ref, I_ref = _run(lib.celeris_rs_field_dev, form, px, py, t, *args)
@@ -71,3 +77,13 @@ def test_noalloc_rejects_requests_beyond_its_scratch():
                                       ctypes.c_void_p(E.data_ptr()), None, None)
     assert st == capi.ERR_TOO_LARGE
     assert b"limit" in lib.celeris_last_error()
+
+
+def test_noalloc_set_up_call_with_nothing_to_compute():
+    """n = 0 (and no pillars) only sets up the scratch on the current device: the
+    call a caller makes before its memory pool takes the free memory."""
+    lib = capi.load()
+    assert lib.celeris_rs_field_noalloc(capi.FORM_F32C, None, None, None, 0, 0.0, 0.0, 30.0, 10.0, 0, 1.0,
+                                        None, None, None) == capi.OK
+    assert lib.celeris_rs_field_noalloc(capi.FORM_PLAIN_F64, None, None, None, 0, 0.0, 0.0, 30.0, 10.0, 0, 1.0,
+                                        None, None, None) == capi.OK

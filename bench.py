@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--case", default=None,
                     help="run one small named case and exit (ncu captures): ff785k_f32c_256, "
-                         "ff785k_f64_128, ff70k_f32c, ff70k_f64, ff70k_adj")
+                         "ff785k_f64_128, ff70k_f32c, ff70k_f64, ff70k_adj, rcwa_library, rcwa_M<m>_<ncell>")
     ap.add_argument("--reps", type=int, default=2)
     return ap.parse_args()
 
@@ -715,11 +715,15 @@ def run_case(name, reps):
 
     dev = torch.device("cuda")
     if name.startswith("rcwa"):
-        # rcwa_M<m>_<ncell>: uneven-batch cells of one harmonic count
-        from celeris_b200.workloads import rcwa_uneven_4096
+        # rcwa_library: the 64-cell library sweep; rcwa_M<m>_<ncell>: uneven-batch
+        # cells of one harmonic count
+        from celeris_b200.workloads import rcwa_library_64, rcwa_uneven_4096
 
-        _, m, nc = name.split("_")
-        cells = [c for c in rcwa_uneven_4096() if c["Mx"] == int(m[1:])][: int(nc)]
+        if name == "rcwa_library":
+            cells = rcwa_library_64()
+        else:
+            _, m, nc = name.split("_")
+            cells = [c for c in rcwa_uneven_4096() if c["Mx"] == int(m[1:])][: int(nc)]
         for _ in range(reps):
             capi.rcwa_batch([capi.rcwa_cell(**c) for c in cells])
         print(json.dumps({"case": name, "reps": reps, "cells": len(cells)}))

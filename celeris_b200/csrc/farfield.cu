@@ -330,13 +330,17 @@ __global__ void __launch_bounds__(kThreads, 3) rs_f32c_kernel(const float4* __re
     const int i0 = (strip - j * spr) * kPPT32;
     const int jj = min(j, g.ny - 1);
 
-    float fxr[kPPT32], fyr = 0.f, z = 0.f;
+    // pixel coordinates relative to the FP32 origin; the row's y as a float
+    // pair hi + lo (its lo part costs one scalar add per pillar record; x keeps
+    // its FP32 rounding, which the stated error bound counts)
+    float fxr[kPPT32], fyr = 0.f, fyl = 0.f, z = 0.f;
 #pragma unroll
     for (int q = 0; q < kPPT32; ++q) {
         double fx, fy, fz;
         pixel_pos(g, min(i0 + q, g.nx - 1), jj, fx, fy, fz);
         fxr[q] = (float)(fx - g.ox);
         fyr = (float)(fy - g.oy);
+        fyl = (float)((fy - g.oy) - (double)fyr);
         z = (float)fz;
     }
     const float z2 = z * z;
@@ -346,8 +350,8 @@ __global__ void __launch_bounds__(kThreads, 3) rs_f32c_kernel(const float4* __re
     f32x2 fx2[kPairs];
 #pragma unroll
     for (int h = 0; h < kPairs; ++h) fx2[h] = pk2(fxr[2 * h], fxr[2 * h + 1]);
-    const f32x2 NEG1 = dup2(-1.0f), NZ = dup2(-z), Z2X = dup2(2.0f * z), NHALF = dup2(-0.5f);
-    const f32x2 ILHI = dup2(il_hi), ILLO = dup2(il_lo), MAGIC = dup2(kMagic);
+    const f32x2 NEG1 = dup2(-1.0f), NEG2 = dup2(-2.0f), NZ = dup2(-z), Z2X = dup2(2.0f * z), NHALF = dup2(-0.5f);
+    const f32x2 ILHI = dup2(il_hi), NILHI = dup2(-il_hi), ILLO = dup2(il_lo), MAGIC = dup2(kMagic);
     const f32x2 TWOPI = dup2(6.28318530717958647692f);
 
     TilePipe<float4, kTile32> pipe;
@@ -369,16 +373,23 @@ __global__ void __launch_bounds__(kThreads, 3) rs_f32c_kernel(const float4* __re
 #pragma unroll 2
             for (int p = 0; p < cnt; ++p) {
                 const float4 r = tile[p];  // {x, y, |t|, arg t / 2pi}
-                const float dy = fyr - r.y;
+                // dy = sy + ey exactly (Fast2Sum): the rounding of fy - y would
+                // otherwise snap fy to the grid of y's exponent, the same shift
+                // for every pillar of that exponent - an error that adds up
+                // coherently near a focus
+                const float sy = fyr - r.y;
+                const float ey = (fyr - (sy + r.y)) + fyl;
                 const f32x2 RX = dup2(r.x), RW = dup2(r.w), RZ = dup2(r.z);
-                const f32x2 U0 = dup2(fmaf(dy, dy, z2));  // dy^2 + z^2 (seed only)
-                const f32x2 ND2 = dup2(-(dy * dy));        // -dy^2
+                const f32x2 U0 = dup2(fmaf(sy, sy, z2));                     // dy^2 + z^2 (seed only)
+                const f32x2 NDY2 = dup2(fmaf(sy, -sy, sy * (-2.0f * ey)));  // -(dy^2), to second order
 #pragma unroll
                 for (int h = 0; h < kPairs; ++h) {
-                    const f32x2 dx = fma2(RX, NEG1, fx2[h]);   // fx - x
-                    const f32x2 ndx = fma2(fx2[h], NEG1, RX);  // x - fx
-                    const f32x2 u = fma2(dx, dx, U0);          // R^2 (seed only)
-                    const f32x2 ns = fma2(dx, ndx, ND2);       // -rho^2, one rounding
+                    // dx = s + e exactly (Fast2Sum), -rho^2 = -(s^2 + 2 s e + dy^2)
+                    const f32x2 s = fma2(RX, NEG1, fx2[h]);               // fx - x, rounded
+                    const f32x2 e = fma2(add2(s, RX), NEG1, fx2[h]);      // its rounding error
+                    const f32x2 ndx = fma2(fx2[h], NEG1, RX);             // -s
+                    const f32x2 u = fma2(s, s, U0);                       // R^2 (seed only)
+                    const f32x2 ns = fma2(s, ndx, fma2(s, mul2(e, NEG2), NDY2));  // -rho^2
                     float ua, ub;
                     upk2(u, ua, ub);
                     const f32x2 ri = pk2(rsqrt_approx(ua), rsqrt_approx(ub));  // ~1/R
@@ -386,10 +397,17 @@ __global__ void __launch_bounds__(kThreads, 3) rs_f32c_kernel(const float4* __re
                     // Newton on f(d) = d^2 + 2 z d - rho^2 (exact root R - z)
                     const f32x2 gg = fma2(d0, d0, fma2(Z2X, d0, ns));
                     const f32x2 d = fma2(mul2(gg, ri), NHALF, d0);
-                    // phase in turns: (R - z)/lambda + arg(t)/2pi; k z is added in FP64
-                    const f32x2 th = fma2(d, ILHI, fma2(d, ILLO, RW));
-                    const f32x2 w = fma2(add2(th, MAGIC), NEG1, MAGIC);  // -(th rounded to an integer)
-                    const f32x2 ang = mul2(add2(th, w), TWOPI);          // in [-pi, pi]
+                    // phase in turns, (R - z)/lambda + arg(t)/2pi (k z is added in
+                    // FP64), reduced without rounding its integer part into the
+                    // fraction: p = d hi rounded (kept negated), r = d hi - p exactly
+                    // (fma), the integer nearest p removed exactly, then the small
+                    // parts r + d lo + psi added: the fraction carries ~u turns of
+                    // rounding instead of ~u |p|
+                    const f32x2 np = mul2(d, NILHI);                      // -p
+                    const f32x2 rp = fma2(d, ILHI, np);                   // d hi - p, exact
+                    const f32x2 t = add2(rp, fma2(d, ILLO, RW));          // rp + d lo + psi
+                    const f32x2 w = fma2(add2(np, MAGIC), NEG1, MAGIC);   // round(p)
+                    const f32x2 ang = mul2(fma2(add2(np, w), NEG1, t), TWOPI);  // 2 pi (p - round(p) + t), |.| <= 2 pi
                     const f32x2 a = mul2(RZ, ri);                         // |t| / R
                     float aa, ab;
                     upk2(ang, aa, ab);
@@ -440,7 +458,8 @@ __global__ void __launch_bounds__(kThreads, 3) rs_adj_f32c_kernel(const float4* 
         yj[h] = pk2((float)(py[a] - g.oy), (float)(py[b] - g.oy));
     }
     const f32x2 NEG1 = dup2(-1.0f), NZ = dup2(-z), Z2X = dup2(2.0f * z), NHALF = dup2(-0.5f);
-    const f32x2 Z2 = dup2(z * z), ILHI = dup2(il_hi), ILLO = dup2(il_lo), MAGIC = dup2(12582912.0f);
+    const f32x2 Z2 = dup2(z * z), ILHI = dup2(il_hi), NILHI = dup2(-il_hi), ILLO = dup2(il_lo);
+    const f32x2 MAGIC = dup2(12582912.0f);
     const f32x2 TWOPI = dup2(6.28318530717958647692f);
 
     TilePipe<float4, kTile32> pipe;
@@ -475,9 +494,12 @@ __global__ void __launch_bounds__(kThreads, 3) rs_adj_f32c_kernel(const float4* 
                     const f32x2 d0 = fma2(u, ri, NZ);
                     const f32x2 gg = fma2(d0, d0, fma2(Z2X, d0, ns));
                     const f32x2 d = fma2(mul2(gg, ri), NHALF, d0);           // R - z
-                    const f32x2 th = fma2(d, ILHI, mul2(d, ILLO));           // (R - z)/lambda, turns
-                    const f32x2 w = fma2(add2(th, MAGIC), NEG1, MAGIC);
-                    const f32x2 ang = mul2(add2(th, w), TWOPI);
+                    // (R - z)/lambda in turns, reduced exactly as in the forward kernel
+                    const f32x2 np = mul2(d, NILHI);
+                    const f32x2 rp = fma2(d, ILHI, np);
+                    const f32x2 t = fma2(d, ILLO, rp);
+                    const f32x2 w = fma2(add2(np, MAGIC), NEG1, MAGIC);
+                    const f32x2 ang = mul2(fma2(add2(np, w), NEG1, t), TWOPI);
                     float aa, ab;
                     upk2(ang, aa, ab);
                     const f32x2 pr = mul2(ri, pk2(cos_approx(aa), cos_approx(ab)));
@@ -624,12 +646,12 @@ __global__ void chunk_sum_kernel(const double2* __restrict__ partial, int nchunk
 
 // ---- stated error of the precision form ------------------------------------------
 // (1) Sampled: the field recomputed in FP64 at a set of pixels - a strided
-//     lattice, the centre pixel and the 11 x 11 pixels around the peak of |E|
+//     lattice, the centre pixel and the 21 x 21 pixels around the peak of |E|
 //     (where errors that add coherently are largest) - against the computed
 //     field there.
 // (2) Bound: an upper bound on max_p |E_p - E64_p| from the error model of the
 //     precision-form arithmetic (ff_bound_kernel).
-constexpr int kPeakHalf = 5;  // the peak neighbourhood is (2 kPeakHalf + 1)^2 pixels
+constexpr int kPeakHalf = 10;  // the peak neighbourhood is (2 kPeakHalf + 1)^2 pixels
 
 // acc[0]: bits of max_p |E_p| (FP64); acc[1]: (bits of (float)|E_p| << 32) | p,
 // so that atomicMax leaves the index of a peak pixel in the low word.
@@ -718,17 +740,25 @@ __global__ void rs_check_kernel(const double4* __restrict__ rec, int npil, Geom 
 // every pixel of the window. u = 2^-24 (FP32 round to nearest). With the
 // pillar's offset (xo, yo) from the FP32 origin and the window's half extents
 // (wx, wy), dxm = xo + wx and dym = yo + wy bound |dx|, |dy|, rho^2 <= dxm^2 +
-// dym^2 and delta = R - z <= dmax. Rounding of the FP32 coordinates, of dx,
-// dy and of rho^2 moves rho^2 by at most 6u (dxm^2 + dym^2), hence R - z by
-// that / (2|z|); the Newton step adds u dmax (1 + dmax / 2|z|) and the
-// quadratic remainder of its seed (from rsqrt.approx); the phase in turns
-// th = delta/lambda + psi rounds with u (dmax/lambda + 1/2) plus u for psi and
-// its sum, the reduced angle with u pi; the amplitude |t|/R with 6u.
-//   e_R(j)  = 2 pi (dDelta/lambda + u (dmax/lambda + 1/2) + u) + u pi + 6u
-// The MUFU approximations and the constants are systematic and are summed
-// without cancellation:
-//   e_D(j)  = kRsqrtRelErr + sqrt(2) kSinCosAbsErr + |2 pi_f - 2 pi| / 2
-//             + |z - z_f| / |z| + k |z - z_f| rho_max^2 / (2 z^2)
+// dym^2 and delta = R - z <= dmax.
+// Random part (rounding that depends on each pillar's own coordinates):
+// dx = s + e and dy = sy + ey are formed exactly (Fast2Sum), so rho^2 moves
+// only by the FP32 rounding of the pillar's coordinates (2u (dxm xo + dym
+// yo)), by a Fast2Sum residual that is not exact for pillars inside the window
+// (2u (dxm wx + dym wy)) and by its own three roundings (3u (dxm^2 + dym^2)):
+// at most 5u (dxm^2 + dym^2), counted 6u; R - z moves by that / (2|z|); the
+// Newton step adds u dmax (1 + dmax / 2|z|) and the quadratic remainder of its
+// seed (rsqrt.approx); the amplitude |t|/R rounds with 6u:
+//   e_R(j)  = 2 pi dDelta / lambda + 6u
+// Systematic part (the same for many pillars, so it can add up coherently near
+// a focus where the phases of all terms agree), summed without cancellation:
+// the phase reduction (psi rounded to FP32, d lo + psi, rp + that, the reduced
+// fraction of magnitude <= 1 turn: 3u turns; the product with 2 pi_f: u 2 pi
+// and |2 pi_f - 2 pi|), the MUFU approximations, the FP32 rounding of the
+// pixel's x coordinate (u wx, a shift of the pixel: k u wx dxm / |z|), and the
+// rounding of z:
+//   e_D(j)  = kRsqrtRelErr + sqrt(2) kSinCosAbsErr + 2 pi 4u + |2 pi_f - 2 pi|
+//             + k u wx dxm / |z| + |z - z_f| / |z| + k |z - z_f| rho_max^2 / (2 z^2)
 // with z_f = (float)z (the z the FP32 terms use; the global phase uses z).
 // Every term has magnitude a_j = |t_j| / R <= |t_j| / |z|. acc (doubles):
 // [0] sum_j a_j e_D(j), [1] sum_j (a_j e_R(j))^2, [2] bits of max_j a_j,
@@ -745,7 +775,7 @@ __global__ void ff_bound_kernel(const double* __restrict__ px, const double* __r
     const double wy = fmax(fabs(y_first - g.oy), fabs(y_last - g.oy));
     const double two_pi_f = (double)6.28318530717958647692f;
     const double eD0 = celeris_dev::kRsqrtRelErr + 1.4142135623730951 * celeris_dev::kSinCosAbsErr +
-                       0.5 * fabs(two_pi_f - 2.0 * pi) + dz / z;
+                       2.0 * pi * 4.0 * u + fabs(two_pi_f - 2.0 * pi) + dz / z;
     double sD = 0.0, sR = 0.0, sA = 0.0, amax = 0.0;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npil; j += gridDim.x * blockDim.x) {
         const double2 t = pt[j];
@@ -756,8 +786,8 @@ __global__ void ff_bound_kernel(const double* __restrict__ px, const double* __r
         const double dmax = rho2 / (R + z);
         const double seed = R * (celeris_dev::kRsqrtRelErr + 4.0 * u);
         const double dDelta = 6.0 * u * rho2 / (2.0 * z) + u * dmax * (1.0 + dmax / (2.0 * z)) + seed * seed / z;
-        const double eR = 2.0 * pi * (dDelta / lam + u * (dmax / lam + 0.5) + u) + u * pi + 6.0 * u;
-        const double eD = eD0 + k * dz * rho2 / (2.0 * z * z);
+        const double eR = 2.0 * pi * dDelta / lam + 6.0 * u;
+        const double eD = eD0 + k * u * wx * dxm / z + k * dz * rho2 / (2.0 * z * z);
         sD += a * eD;
         sR += (a * eR) * (a * eR);
         sA += a;
@@ -1227,17 +1257,22 @@ int download(void* dst, char* stage, const void* src, size_t bytes, cudaStream_t
     return CELERIS_OK;
 }
 
-// Sample of pixel indices for the stated error: a strided lattice plus the
-// centre pixel.
-std::vector<int> sample_pixels(int nx, int ny, int want) {
+// Sample of pixel indices for the stated error: a side x side lattice spread
+// over both axes of the grid, plus the centre pixel (the kernel adds the
+// neighbourhood of the peak).
+std::vector<int> sample_pixels(int nx, int ny, int side) {
     std::vector<int> idx;
     const long npix = (long)nx * ny;
-    if (npix <= want) {
+    if (npix <= (long)side * side) {
         for (int p = 0; p < npix; ++p) idx.push_back(p);
         return idx;
     }
-    const long stride = npix / want;
-    for (long p = stride / 2; p < npix && (int)idx.size() < want; p += stride) idx.push_back((int)p);
+    for (int a = 0; a < side; ++a)
+        for (int b = 0; b < side; ++b) {
+            const int j = (int)(((long)(2 * a + 1) * ny) / (2 * side));
+            const int i = (int)(((long)(2 * b + 1) * nx) / (2 * side));
+            idx.push_back(j * nx + i);
+        }
     idx.push_back((ny / 2) * nx + nx / 2);
     return idx;
 }
@@ -1258,7 +1293,7 @@ int ff_host(int form, const double* px, const double* py, const double* pt, int 
     const bool want_err = (form == CELERIS_FORM_F32C) && err_out && npil > 0;
     const bool want_bound = (form == CELERIS_FORM_F32C) && bound_out && npil > 0;
     std::vector<int> sidx;
-    if (want_err) sidx = sample_pixels(g.nx, g.ny, 256);
+    if (want_err) sidx = sample_pixels(g.nx, g.ny, 16);
 
     const size_t in_bytes = (size_t)npil * 4 * sizeof(double);
     const size_t fld_bytes = (size_t)npix * 2 * sizeof(double);

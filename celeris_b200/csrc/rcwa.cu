@@ -83,6 +83,14 @@ struct Bucket {
     const cplx* phy;  // [(4My+1) x ng]
     long long* dbg;   // optional per-cell counters, kDbgSlots each (CELERIS_RCWA_STAGE_CLOCKS=1), else NULL
     double* ord;      // optional per-order efficiencies: per cell and excitation [N][2] = (de_t, de_r), else NULL
+    // mirror-symmetric cells (sym != 0): the eigenproblem solved in its four
+    // parity classes; size class k (0: classes (+,+) and (-,-), 1: (+,-) and
+    // (-,+)) holds two m[k] x m[k] matrices per cell, matrix 2 cell + j
+    int sym;
+    double sym_tol;  // largest mirror asymmetry of M (relative to max |M|) the class split accepts
+    int m[2];
+    cplx *sH[2], *sZ[2], *sX[2], *sW[2], *sA[2], *sq[2];
+    int* sinfo[2];
 };
 
 __device__ __forceinline__ cplx* at(cplx* base, size_t stride, int c) { return base + stride * c; }
@@ -960,12 +968,205 @@ __global__ void __launch_bounds__(kRT) rcwa_epilogue(Bucket b) {
     }
 }
 
+// ---- mirror-symmetric cells: the eigenproblem in four parity classes -------------------------
+// A cell whose pattern is symmetric under x -> -x and under y -> -y (every
+// unrotated shape of rcwa2d.cpp:37-72) at normal incidence (kx0 = ky0 = 0) has
+// Kx odd and Ky even under the order map p -> -p (Px), and Einv, Exx, Eyy
+// invariant under it; so M = ep2 kp - kkT commutes with Sx = diag(Px, -Px)
+// (the two field blocks of rcwa2d.cpp:346-364) and likewise with Sy = diag(Py,
+// -Py). Their joint eigenspaces - parity classes (a, b), a, b = +-1 - split M
+// into four blocks of about n/4: the block-1 part of class (a, b) has parity
+// (a, b) under (Px, Py), the block-2 part parity (-a, -b). Each class has an
+// orthonormal basis of orbit vectors (the orders (+-p, +-q) of one orbit
+// combined with signs a, b and weight 1/sqrt(count)). With P_c that basis,
+//   M = sum_c P_c M_c P_c^T,  M_c = P_c^T M P_c,
+// so the eigenpairs of M are those of the M_c mapped by P_c: W = [P_c W_c]_c.
+// The eigen-stages then run on matrices of order ~n/4 (16x fewer QR
+// rotations per class, 64x fewer flops each); the S-matrix stages use the
+// full W unchanged, so t, R and T are those of the full eigensolve up to
+// rounding. A cell whose M is not mirror symmetric to rounding (a raster
+// sample falling exactly on a shape boundary one way and not the other) is
+// flagged kInfoAsym and solved again by the full eigensolve.
+constexpr int kInfoAsym = 1 << 29;
+
+// class c: 0 = (+,+), 1 = (-,-), 2 = (+,-), 3 = (-,+)
+__host__ __device__ __forceinline__ int sym_class_a(int c) { return (c == 0 || c == 2) ? 1 : -1; }
+__host__ __device__ __forceinline__ int sym_class_b(int c) { return (c == 0 || c == 3) ? 1 : -1; }
+__host__ __device__ __forceinline__ int sym_count(int M, int parity) { return parity > 0 ? M + 1 : M; }
+__host__ __device__ __forceinline__ int sym_class_size(int Mx, int My, int c) {
+    const int a = sym_class_a(c), b = sym_class_b(c);
+    return sym_count(Mx, a) * sym_count(My, b) + sym_count(Mx, -a) * sym_count(My, -b);
+}
+
+// Basis vector i of class c: its entries (2N-space indices and coefficients),
+// returns their count (1, 2 or 4).
+__device__ int sym_vector(int Mx, int My, int c, int i, int* idx, double* coef) {
+    const int N = (2 * Mx + 1) * (2 * My + 1);
+    const int a = sym_class_a(c), b = sym_class_b(c);
+    const int nu = sym_count(Mx, a) * sym_count(My, b);
+    int blk, pa, pb;  // field block, parities under Px, Py
+    if (i < nu) {
+        blk = 0, pa = a, pb = b;
+    } else {
+        i -= nu;
+        blk = 1, pa = -a, pb = -b;
+    }
+    const int nq = sym_count(My, pb);
+    const int p = i / nq + (pa > 0 ? 0 : 1), q = i % nq + (pb > 0 ? 0 : 1);
+    const int cnt = (p > 0 ? 2 : 1) * (q > 0 ? 2 : 1);
+    const double w = cnt == 4 ? 0.5 : (cnt == 2 ? 0.70710678118654752440 : 1.0);
+    int k = 0;
+    for (int sp = 0; sp < (p > 0 ? 2 : 1); ++sp)
+        for (int sq = 0; sq < (q > 0 ? 2 : 1); ++sq) {
+            const int pp = sp ? -p : p, qq = sq ? -q : q;
+            idx[k] = blk * N + (pp + Mx) * (2 * My + 1) + (qq + My);
+            coef[k] = w * (sp ? pa : 1) * (sq ? pb : 1);
+            ++k;
+        }
+    return k;
+}
+
+__device__ __forceinline__ cplx* sym_mat(const Bucket& b, cplx* const* base, int c, int cell) {
+    const int k = c >> 1, m = b.m[k];
+    return base[k] + (size_t)(2 * cell + (c & 1)) * m * m;
+}
+
+// M (in H) -> the four class matrices; flags a cell whose M is not mirror
+// symmetric to rounding.
+__global__ void __launch_bounds__(kRT) rcwa_sym_project(Bucket b) {
+    __shared__ double red[3][32];
+    const int cell = blockIdx.x;
+    const int N = b.N, n = b.n, Mx = b.Mx, My = b.My, ny = 2 * My + 1;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const cplx* H = at(b.H, b.s_nn, cell);
+    // symmetry check: M[k][l] = s(k) s(l) M[mirror k][mirror l] for both mirrors
+    double dx = 0.0, dy = 0.0, mx = 0.0;
+    for (int e = tid; e < n * n; e += nt) {
+        const int k = e / n, l = e % n;
+        const int bk = k / N, ok = k % N, bl = l / N, ol = l % N;
+        const int pk = ok / ny, qk = ok % ny, pl = ol / ny, ql = ol % ny;
+        const double sgn = (bk == bl) ? 1.0 : -1.0;
+        const cplx v = H[e];
+        const cplx vx = H[(size_t)(bk * N + (2 * Mx - pk) * ny + qk) * n + bl * N + (2 * Mx - pl) * ny + ql];
+        const cplx vy = H[(size_t)(bk * N + pk * ny + (2 * My - qk)) * n + bl * N + pl * ny + (2 * My - ql)];
+        dx = fmax(dx, cabs(csub(v, cscale(vx, sgn))));
+        dy = fmax(dy, cabs(csub(v, cscale(vy, sgn))));
+        mx = fmax(mx, cabs(v));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        dx = fmax(dx, __shfl_down_sync(0xffffffffu, dx, o));
+        dy = fmax(dy, __shfl_down_sync(0xffffffffu, dy, o));
+        mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    }
+    if ((tid & 31) == 0) {
+        red[0][tid >> 5] = dx;
+        red[1][tid >> 5] = dy;
+        red[2][tid >> 5] = mx;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double a = 0.0, c = 0.0, m = 0.0;
+        for (int w = 0; w < nt / 32; ++w) {
+            a = fmax(a, red[0][w]);
+            c = fmax(c, red[1][w]);
+            m = fmax(m, red[2][w]);
+        }
+        if (!(fmax(a, c) <= b.sym_tol * m) && b.info[cell] == 0) b.info[cell] = kInfoAsym;
+    }
+    // class matrices M_c = P_c^T M P_c
+    for (int c = 0; c < 4; ++c) {
+        const int m = b.m[c >> 1];
+        cplx* Mc = sym_mat(b, b.sH, c, cell);
+        for (int e = tid; e < m * m; e += nt) {
+            const int i = e / m, j = e % m;
+            int ii[4], jj[4];
+            double ci[4], cj[4];
+            const int ni = sym_vector(Mx, My, c, i, ii, ci), nj = sym_vector(Mx, My, c, j, jj, cj);
+            cplx acc = C(0.0, 0.0);
+            for (int u = 0; u < ni; ++u)
+                for (int v = 0; v < nj; ++v) acc = cadd(acc, cscale(H[(size_t)ii[u] * n + jj[v]], ci[u] * cj[v]));
+            Mc[e] = acc;
+        }
+    }
+}
+
+// W = [P_c W_c]_c and q = [q_c]_c (class order (+,+), (-,-), (+,-), (-,+)); a
+// class eigensolve failure becomes the cell's info.
+__global__ void __launch_bounds__(kRT) rcwa_sym_expand(Bucket b) {
+    const int cell = blockIdx.x;
+    const int n = b.n, Mx = b.Mx, My = b.My;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    cplx* W = at(b.W, b.s_nn, cell);
+    cplx* q1 = at(b.q1, b.s_n, cell);
+    for (int e = tid; e < n * n; e += nt) W[e] = C(0.0, 0.0);
+    __syncthreads();
+    int off = 0;
+    for (int c = 0; c < 4; ++c) {
+        const int k = c >> 1, m = b.m[k], mat = 2 * cell + (c & 1);
+        const cplx* Wc = b.sW[k] + (size_t)mat * m * m;
+        const cplx* qc = b.sq[k] + (size_t)mat * m;
+        for (int e = tid; e < m * m; e += nt) {
+            const int i = e / m, j = e % m;
+            int ii[4];
+            double ci[4];
+            const int ni = sym_vector(Mx, My, c, i, ii, ci);
+            const cplx w = Wc[e];
+            for (int u = 0; u < ni; ++u) W[(size_t)ii[u] * n + off + j] = cscale(w, ci[u]);
+        }
+        for (int j = tid; j < m; j += nt) q1[off + j] = qc[j];
+        if (tid == 0 && b.info[cell] == 0 && b.sinfo[k][mat] != 0) b.info[cell] = b.sinfo[k][mat];
+        off += m;
+    }
+}
+
+// The eigen-stage bucket of size class k of a mirror-symmetric bucket.
+Bucket sym_eig_bucket(const Bucket& b, int k) {
+    Bucket e;
+    std::memset(&e, 0, sizeof(e));
+    e.Mx = b.Mx;
+    e.My = b.My;
+    e.n = b.m[k];
+    e.N = e.n / 2;
+    e.ncell = 2 * b.ncell;
+    e.cells = b.cells;
+    e.H = b.sH[k];
+    e.Z = b.sZ[k];
+    e.X = b.sX[k];
+    e.W = b.sW[k];
+    e.A = b.sA[k];
+    e.q1 = b.sq[k];
+    e.info = b.sinfo[k];
+    e.s_nn = (size_t)e.n * e.n;
+    e.s_n = (size_t)e.n;
+    return e;
+}
+
 // ---- host side ------------------------------------------------------------------------------------
 struct HostCell {
     CellDev d;
     int Mx, My, ng;  // ng = 0: analytic rect path
     int index;       // position in the caller's array
+    int sym;         // 1: mirror-symmetric cell at normal incidence (eigenproblem in parity classes)
 };
+
+// The parity-class eigensolve applies to unrotated shapes (all mirror
+// symmetric, rcwa2d.cpp:37-72) at normal incidence with at least one order on
+// each side of 0 in x and y; CELERIS_RCWA_SYMMETRY=0 turns it off.
+bool symmetry_enabled() {
+    const char* e = std::getenv("CELERIS_RCWA_SYMMETRY");
+    return !(e && e[0] == '0');
+}
+// Mirror-asymmetry tolerance of the class split, relative to max |M|: rounding
+// leaves ~1e-15; one raster sample on the other side of a shape boundary
+// ~1e-6. CELERIS_RCWA_SYM_TOL overrides it (0 sends every cell to the full
+// eigensolve through the fallback, for tests of that path).
+double symmetry_tolerance() {
+    const char* e = std::getenv("CELERIS_RCWA_SYM_TOL");
+    return e ? std::atof(e) : 1e-9;
+}
+bool sym_eligible(const celeris_rcwa_cell& c) {
+    return c.theta_rad == 0.0 && c.rotation_rad == 0.0 && c.Mx >= 1 && c.My >= 1 && symmetry_enabled();
+}
 
 int validate(const celeris_rcwa_cell& c) {
     // every real input must be finite: a NaN or Inf would run through the
@@ -1021,6 +1222,7 @@ HostCell make_cell(const celeris_rcwa_cell& c, int index, double ex_re, double e
     // reference raster size max(128, 8(2 max(Mx, My) + 1)) (rcwa2d.cpp:337)
     h.ng = plain_rect ? 0 : (c.grid > 0 ? c.grid : std::max(128, 8 * (2 * std::max(c.Mx, c.My) + 1)));
     h.index = index;
+    h.sym = sym_eligible(c) ? 1 : 0;
     return h;
 }
 
@@ -1084,7 +1286,7 @@ bool tuning_enabled() {
 }
 
 struct BucketPlan {
-    int Mx, My, ng, N, n;
+    int Mx, My, ng, N, n, sym;
     std::vector<int> ids;  // indices into the cell list
     size_t per_cell = 0, bytes = 0;
     Bucket b;
@@ -1098,21 +1300,40 @@ size_t per_cell_bytes(int n, int nexc) {
            celeris_rt::align256(sizeof(CellDev)) + 14 * 256;
 }
 
+// the parity-class eigen-stage buffers of one mirror-symmetric cell: per size
+// class, two matrices with H, Z, X, W and the eigenvector scratch, q and info
+size_t sym_per_cell_bytes(int Mx, int My) {
+    size_t b = 0;
+    for (int k = 0; k < 2; ++k) {
+        const size_t m = (size_t)sym_class_size(Mx, My, 2 * k);
+        b += 2 * (5 * m * m + m) * sizeof(cplx) + 2 * sizeof(int);
+    }
+    return b + 14 * 256;
+}
+
 // The largest dynamic shared memory each stage kernel needs over a wave's
 // buckets; raised once per wave, outside any capture.
 struct SmemNeeds {
     size_t laurent = 0, rect = 0, hess_s = 0, hess_g = 0, smat = 0;
     bool aed = false;
-    void add(int Mx, int My, int ng, int n) {
+    void add_eig(int n) {
+        if (n <= kSmemEigMaxN) hess_s = std::max(hess_s, ((size_t)n * n + 2 * n) * sizeof(cplx));
+        else hess_g = std::max(hess_g, hess_stage_bytes(n));
+        aed = true;
+    }
+    void add(int Mx, int My, int ng, int n, int sym = 0) {
         if (ng > 0) {
             laurent = std::max(laurent, laurent_smem(Mx, My, ng));
         } else {
             const int nx = 2 * Mx + 1, ny = 2 * My + 1;
             rect = std::max(rect, ((size_t)2 * (nx * nx + ny * ny) + 2 * std::max(nx, ny)) * sizeof(cplx));
         }
-        if (n <= kSmemEigMaxN) hess_s = std::max(hess_s, ((size_t)n * n + 2 * n) * sizeof(cplx));
-        else hess_g = std::max(hess_g, hess_stage_bytes(n));
-        aed = true;
+        if (sym) {
+            add_eig(sym_class_size(Mx, My, 0));
+            add_eig(sym_class_size(Mx, My, 2));
+        } else {
+            add_eig(n);
+        }
         smat = std::max(smat, lu_stage_bytes(n));
     }
 };
@@ -1176,7 +1397,27 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
     if (ev) cudaEventRecord(ev[1], st);
     rcwa_build_M<<<nc, T[ST_BUILD], 0, st>>>(b, b.ng > 0 ? 1 : 0);
     if (ev) cudaEventRecord(ev[2], st);
-    if (n <= kSmemEigMaxN) {
+    if (b.sym) {
+        // the four parity classes: project, two eigen-stage buckets (sizes m[0],
+        // m[1], two matrices per cell each), expand into W and q
+        rcwa_sym_project<<<nc, T[ST_HESS], 0, st>>>(b);
+        Bucket e[2] = {sym_eig_bucket(b, 0), sym_eig_bucket(b, 1)};
+        for (int k = 0; k < 2; ++k) {
+            cudaMemsetAsync(e[k].info, 0, sizeof(int) * e[k].ncell, st);
+            const int m = e[k].n;
+            if (m <= kSmemEigMaxN)
+                rcwa_hess<true><<<e[k].ncell, T[ST_HESS], ((size_t)m * m + 2 * m) * sizeof(cplx), st>>>(e[k]);
+            else
+                rcwa_hess<false><<<e[k].ncell, T[ST_HESS], hess_stage_bytes(m), st>>>(e[k]);
+        }
+        if (ev) cudaEventRecord(ev[3], st);
+        for (int k = 0; k < 2; ++k)
+            rcwa_schur<<<e[k].ncell, kSchurThreads, schur_smem(e[k].ncell), st>>>(e[k]);
+        if (ev) cudaEventRecord(ev[4], st);
+        for (int k = 0; k < 2; ++k) rcwa_vec<<<e[k].ncell, T[ST_VEC], 0, st>>>(e[k]);
+        rcwa_sym_expand<<<nc, T[ST_VEC], 0, st>>>(b);
+        count_launch(8);
+    } else if (n <= kSmemEigMaxN) {
         const size_t sm = ((size_t)n * n + 2 * n) * sizeof(cplx);
         rcwa_hess<true><<<nc, T[ST_HESS], sm, st>>>(b);
         if (ev) cudaEventRecord(ev[3], st);
@@ -1186,11 +1427,13 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
         if (ev) cudaEventRecord(ev[3], st);
         rcwa_schur<<<nc, kSchurThreads, schur_smem(nc), st>>>(b);
     }
-    if (ev) cudaEventRecord(ev[4], st);
-    rcwa_vec<<<nc, T[ST_VEC], 0, st>>>(b);
+    if (!b.sym) {
+        if (ev) cudaEventRecord(ev[4], st);
+        rcwa_vec<<<nc, T[ST_VEC], 0, st>>>(b);
+    }
     if (ev) cudaEventRecord(ev[5], st);
     if (eig_only) {
-        count_launch(4);
+        count_launch(b.sym ? 1 : 4);
         return;
     }
     const size_t sm_stage = lu_stage_bytes(n);
@@ -1200,7 +1443,7 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
     if (ev) cudaEventRecord(ev[7], st);
     rcwa_epilogue<<<nc, T[ST_EPI], 0, st>>>(b);
     if (ev) cudaEventRecord(ev[8], st);
-    count_launch(7);
+    count_launch(b.sym ? 4 : 7);
 }
 
 // Time each stage at every candidate size on (up to) the first 2 x SMs cells
@@ -1307,8 +1550,9 @@ int ensure_streams(int nb) {
 int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_out, int nexc) {
     CEL_TRY(celeris_rt::require_device());
     // ---- plan: buckets by (Mx, My, raster), largest first so they start first
-    std::map<std::tuple<int, int, int>, std::vector<int>> by;
-    for (int i = 0; i < (int)cells.size(); ++i) by[std::make_tuple(cells[i].Mx, cells[i].My, cells[i].ng)].push_back(i);
+    std::map<std::tuple<int, int, int, int>, std::vector<int>> by;
+    for (int i = 0; i < (int)cells.size(); ++i)
+        by[std::make_tuple(cells[i].Mx, cells[i].My, cells[i].ng, cells[i].sym)].push_back(i);
     std::vector<BucketPlan> plans;
     CEL_TRY(ensure_streams(1));
     int dev = 0, smem_optin = 0;
@@ -1323,11 +1567,12 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
         p.Mx = std::get<0>(kv.first);
         p.My = std::get<1>(kv.first);
         p.ng = std::get<2>(kv.first);
+        p.sym = std::get<3>(kv.first);
         p.N = (2 * p.Mx + 1) * (2 * p.My + 1);
         p.n = 2 * p.N;
         if (p.ng > 0 && laurent_smem(p.Mx, p.My, p.ng) + 1024 > (size_t)smem_optin)
             return set_error(CELERIS_ERR_TOO_LARGE, "raster %d with M=(%d,%d) exceeds shared memory", p.ng, p.Mx, p.My);
-        p.per_cell = per_cell_bytes(p.n, nexc);
+        p.per_cell = per_cell_bytes(p.n, nexc) + (p.sym ? sym_per_cell_bytes(p.Mx, p.My) : 0);
         // split buckets that alone exceed the budget
         const size_t max_cells = std::max<size_t>(1, budget / std::max<size_t>(1, p.per_cell));
         for (size_t c0 = 0; c0 < kv.second.size(); c0 += max_cells) {
@@ -1425,6 +1670,18 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                 b.phx = static_cast<cplx*>(ws.take(sizeof(cplx) * (4 * p.Mx + 1) * p.ng));
                 b.phy = static_cast<cplx*>(ws.take(sizeof(cplx) * (4 * p.My + 1) * p.ng));
             }
+            b.sym = p.sym;
+            b.sym_tol = symmetry_tolerance();
+            if (p.sym) {
+                for (int k = 0; k < 2; ++k) {
+                    const size_t m = (size_t)sym_class_size(p.Mx, p.My, 2 * k);
+                    b.m[k] = (int)m;
+                    cplx** sm[] = {&b.sH[k], &b.sZ[k], &b.sX[k], &b.sW[k], &b.sA[k]};
+                    for (cplx** x : sm) *x = static_cast<cplx*>(ws.take(sizeof(cplx) * m * m * 2 * nc));
+                    b.sq[k] = static_cast<cplx*>(ws.take(sizeof(cplx) * m * 2 * nc));
+                    b.sinfo[k] = static_cast<int*>(ws.take(sizeof(int) * 2 * nc));
+                }
+            }
             hdesc[w] = reinterpret_cast<CellDev*>(pin);
             pin += celeris_rt::align256(sizeof(CellDev) * nc);
             hres_pin[w] = reinterpret_cast<celeris_rcwa_result*>(pin);
@@ -1432,9 +1689,9 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
             hinfo_pin[w] = reinterpret_cast<int*>(pin);
             pin += celeris_rt::align256(sizeof(int) * nc);
             for (int i = 0; i < nc; ++i) hdesc[w][i] = cells[p.ids[i]].d;
-            needs.add(p.Mx, p.My, p.ng, p.n);
+            needs.add(p.Mx, p.My, p.ng, p.n, p.sym);
             sig += "|" + std::to_string(p.Mx) + "," + std::to_string(p.My) + "," + std::to_string(p.ng) + "," +
-                   std::to_string(nc);
+                   std::to_string(p.sym) + "," + std::to_string(nc) + "," + std::to_string(b.sym_tol);
         }
         CEL_TRY(set_smem_limits(needs));
         // ---- tune unseen bucket shapes (descriptors must be on the device)
@@ -1444,7 +1701,7 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
             // key: shape and batch class (fewer than, or at least, one cell per SM)
             int sms = 148;
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            const auto key = std::make_tuple(p.Mx, p.My, 2 * p.ng + ((int)p.ids.size() >= sms ? 1 : 0));
+            const auto key = std::make_tuple(p.Mx, p.My, 4 * p.ng + 2 * p.sym + ((int)p.ids.size() >= sms ? 1 : 0));
             bool have = false;
             {
                 std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -1530,7 +1787,7 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                     cudaMemcpyAsync(const_cast<CellDev*>(p.b.cells), hdesc[w], sizeof(CellDev) * nc,
                                     cudaMemcpyHostToDevice, bs);
                     launch_bucket(p.b, cfgs[w], bs, nullptr);
-                    nk += (p.ng > 0 ? 3 : 1) + 7;
+                    nk += (p.ng > 0 ? 3 : 1) + (p.sym ? 12 : 7);
                     cudaMemcpyAsync(hres_pin[w], p.b.res, sizeof(celeris_rcwa_result) * nexc * nc,
                                     cudaMemcpyDeviceToHost, bs);
                     cudaMemcpyAsync(hinfo_pin[w], p.b.info, sizeof(int) * nc, cudaMemcpyDeviceToHost, bs);
@@ -1563,13 +1820,37 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
             }
         }
     }
+    // cells flagged as not mirror symmetric to rounding: solve again with the
+    // full eigensolve
+    std::vector<int> redo;
+    for (size_t i = 0; i < hinfo.size(); ++i)
+        if (hinfo[i] == kInfoAsym) redo.push_back((int)i);
+    if (!redo.empty()) {
+        std::vector<int> pos(cells.size(), -1);
+        for (int i = 0; i < (int)cells.size(); ++i) pos[cells[i].index] = i;
+        std::vector<HostCell> sub;
+        for (size_t j = 0; j < redo.size(); ++j) {
+            HostCell h = cells[pos[redo[j]]];
+            h.sym = 0;
+            h.index = (int)j;
+            sub.push_back(h);
+        }
+        std::vector<celeris_rcwa_result> sub_out(sub.size() * nexc);
+        std::vector<int> sub_info(sub.size(), 0);
+        CEL_TRY(run_cells(sub, sub_out.data(), sub_info.data(), nexc));
+        for (size_t j = 0; j < redo.size(); ++j) {
+            for (int e = 0; e < nexc; ++e) hres[(size_t)redo[j] * nexc + e] = sub_out[j * nexc + e];
+            hinfo[redo[j]] = sub_info[j];
+        }
+    }
     std::memcpy(out, hres.data(), sizeof(celeris_rcwa_result) * hres.size());
     int first_bad = -1;
     for (size_t i = 0; i < hinfo.size(); ++i) {
         if (info_out) info_out[i] = hinfo[i];
         if (hinfo[i] != 0 && first_bad < 0) first_bad = (int)i;
     }
-    if (first_bad >= 0) {
+    // with an info array the per-cell codes are the report (LAPACK style)
+    if (first_bad >= 0 && !info_out) {
         const int v = hinfo[first_bad];
         return set_error(v > 0 ? CELERIS_ERR_EIG_NOCONV : CELERIS_ERR_SINGULAR,
                          "cell %d: %s (info %d)", first_bad,
@@ -1932,7 +2213,8 @@ int celeris_rcwa_tuning_report(char* buf, int len) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     for (const auto& kv : tune_table()) {
         s += "Mx=" + std::to_string(std::get<0>(kv.first)) + " My=" + std::to_string(std::get<1>(kv.first)) +
-             " grid=" + std::to_string(std::get<2>(kv.first) / 2) +
+             " grid=" + std::to_string(std::get<2>(kv.first) / 4) +
+             ((std::get<2>(kv.first) & 2) ? " parity-classes" : "") +
              ((std::get<2>(kv.first) & 1) ? " batch>=SMs:" : " batch<SMs:");
         for (int st = 0; st < ST_COUNT; ++st)
             s += std::string(" ") + kStageNames[st] + "=" + std::to_string(kv.second.threads[st]);

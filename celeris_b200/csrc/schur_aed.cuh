@@ -94,11 +94,11 @@ __device__ __forceinline__ void grot_cols(cplx* B, int ld, int k, double c, cplx
 // triangular form, U <- U Q (rows [0, mu)). One warp. Returns 0, or the
 // (1-based) row where the iteration cap ran out.
 __device__ int warp_schur_small(int m, cplx* B, int ld, cplx* U, int ldu, int mu, int lane,
-                                 long long* nrot = nullptr) {
+                                 long long* nrot = nullptr, int iter_cap = 0) {
     const double eps = 2.220446049250313e-16;
     const double smallnum = 2.2250738585072014e-308 * (m / eps);
     int hi = m - 1, it = 0, total = 0;
-    const int max_total = 30 * m;
+    const int max_total = iter_cap > 0 ? min(iter_cap, 30 * m) : 30 * m;
     while (hi > 0) {
         // l = largest index in [1, hi] with a negligible subdiagonal (0 if none)
         int l = 0;
@@ -682,7 +682,8 @@ __device__ int blk_schur_aed(int n, cplx* H, int ldh, cplx* Z, int ldz, AedShare
             const long long t0 = clock64();
             load_window(H, ldh, lo, L, sh);
             if (warp == 0) {
-                const int info = warp_schur_small(L, &sh->B[0][0], WMAX + 1, &sh->U[0][0], WMAX + 1, L, lane);
+                const int info = warp_schur_small(L, &sh->B[0][0], WMAX + 1, &sh->U[0][0], WMAX + 1, L, lane,
+                                                  nullptr, iter_cap);
                 if (lane == 0 && info) sh->info = lo + info;
             }
             __syncthreads();

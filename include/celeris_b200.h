@@ -81,7 +81,7 @@ int celeris_probe_dmma(double* fma_per_s);
 /* New: measured accuracy of the MUFU approximations the precision-form
  * far-field uses, over EVERY FP32 input of their ranges on the current device:
  * measured[0] = max |sin.approx(x) - sin(x)| and measured[1] the same for cos,
- * over all x in [-pi_f, pi_f]; measured[2] = max |rsqrt.approx(x) sqrt(x) - 1|
+ * over all x in [-6.284, 6.284]; measured[2] = max |rsqrt.approx(x) sqrt(x) - 1|
  * over all x in [2^-10, 2^30) (references in FP64). model[0..2] receive the
  * figures the stated error bound of the precision form assumes for the same
  * three quantities; the bound is valid on a device where measured <= model. */
@@ -127,8 +127,8 @@ int celeris_rs_field(int form, const double* px, const double* py,
 
 /* New: celeris_rs_field with the precision form's error stated two ways.
  * err_out (may be NULL) receives the SAMPLED error: max |E_p - E64_p| over a
- * pixel sample - 256 strided pixels, the centre pixel and the 11 x 11 pixels
- * around the peak of |E| - recomputed in FP64 on the device, divided by
+ * pixel sample - a 16 x 16 lattice over the grid, the centre pixel and the
+ * 21 x 21 pixels around the peak of |E| - recomputed in FP64 on the device, divided by
  * max_p |E_p| over the whole grid. bound_out (may be NULL) receives an UPPER
  * BOUND on max_p |E_p - E64_p| / max_p |E_p| over the whole grid from the error
  * model of the precision-form arithmetic: the MUFU approximation errors
@@ -137,7 +137,7 @@ int celeris_rs_field(int form, const double* px, const double* py,
  * sums counted as independent and mean zero with 8 standard deviations per
  * pixel (probabilistic rounding-error analysis: exceeded with probability
  * below 1e-13 per pixel under that model). Both are 0 for the plain form, and
- * both cost one pass over the pillars (the bound) or ~380 FP64 pixel sums (the
+ * both cost one pass over the pillars (the bound) or ~700 FP64 pixel sums (the
  * sample), run beside the field's download. */
 int celeris_rs_field_bounded(int form, const double* px, const double* py,
                              const double* pt, int npil, double cx, double cy,
@@ -215,7 +215,7 @@ int celeris_rs_adjoint_rows_dev(int form, const double* d_px, const double* d_py
                                 const double* d_v, double* d_out, void* stream);
 
 /* New: sampled FP64 check of a computed field. For the pixel indices d_idx[0..ns)
- * and the 11 x 11 pixels around the peak of |E| recomputes E in the plain FP64
+ * and the 21 x 21 pixels around the peak of |E| recomputes E in the plain FP64
  * form and writes max|E - E64| over the sample divided by max over all n*n
  * pixels of |E| into *err_out (host). Synchronous. */
 int celeris_rs_check_dev(const double* d_px, const double* d_py,
@@ -302,7 +302,14 @@ int celeris_solve_rcwa_2d(const celeris_rcwa_cell* cell, const double* Ex0,
  * S-matrix) for BOTH the X (Ex0=1, Ey0=0) and Y (Ex0=0, Ey0=1) excitations;
  * out receives 2*ncell results: out[2c] = X, out[2c+1] = Y. Cells are bucketed
  * by harmonic count internally. info (ncell ints, may be NULL) receives 0 or the
- * eigensolve failure code per cell. Synchronous, host buffers. */
+ * failure code per cell: > 0 the QR eigensolve did not converge (LAPACK-style
+ * index), < 0 an exactly singular pivot; with info the call returns CELERIS_OK
+ * and reports failures there only, without info a failure returns
+ * CELERIS_ERR_EIG_NOCONV / CELERIS_ERR_SINGULAR naming the first failing cell.
+ * Cells symmetric under both mirrors at normal incidence (every unrotated
+ * shape, theta = 0) solve the eigenproblem in its four parity classes (the same
+ * eigenpairs at a quarter of the order; CELERIS_RCWA_SYMMETRY=0 turns it off).
+ * Synchronous, host buffers. */
 int celeris_rcwa_batch(const celeris_rcwa_cell* cells, int ncell,
                        celeris_rcwa_result* out, int* info);
 

@@ -56,14 +56,20 @@ def test_injected_allocation_failure_is_oom_without_leak():
 
     lib = capi.load()
     a = small_aperture(513, seed=4)
+
+    def failing_host_call():
+        # host-buffer call on a new thread: its device I/O buffer is the first allocation
+        assert lib.celeris_debug_fail_alloc(1) == capi.OK
+        return _in_fresh_thread(lambda: lib.celeris_propagate_psf(
+            capi._dp(a.px), capi._dp(a.py), capi._dp(a.t.view(np.float64)), a.npil, 0.0, 0.0, a.focal_um, a.k, 9,
+            1.0, capi._dp(np.zeros(81))))
+
+    # the first thread of this kind also sets up the CUDA runtime's own per-thread
+    # state; the second failing call must leave device memory exactly as it found it
+    assert failing_host_call() == capi.ERR_OOM
     torch.cuda.synchronize()
     free0 = torch.cuda.mem_get_info()[0]
-    # host-buffer call on a new thread: its device I/O buffer is the first allocation
-    assert lib.celeris_debug_fail_alloc(1) == capi.OK
-    st = _in_fresh_thread(lambda: lib.celeris_propagate_psf(
-        capi._dp(a.px), capi._dp(a.py), capi._dp(a.t.view(np.float64)), a.npil, 0.0, 0.0, a.focal_um, a.k, 9, 1.0,
-        capi._dp(np.zeros(81))))
-    assert st == capi.ERR_OOM
+    assert failing_host_call() == capi.ERR_OOM
     torch.cuda.synchronize()
     assert torch.cuda.mem_get_info()[0] == free0
     # device-buffer call on a stream this library has not seen: its workspace arena

@@ -38,7 +38,14 @@ def test_field_and_adjoint_split_over_devices(form):
     v = torch.conj(whole) / whole.abs().max()
     adj = T.rs_adjoint_dev(px, py, v, grid, form).cpu().numpy()
     adj_split = MG.rs_adjoint_multi(ap.px, ap.py, v, grid, form, devices=_devices()).cpu().numpy()
-    assert np.max(np.abs(adj_split - adj)) <= 1e-12 * np.max(np.abs(adj))
+    # the adjoint tiles the pixels, so a row split regroups its FP32 tile sums in
+    # the precision form: there the split agrees to that form's accuracy
+    # against the FP64 adjoint (1e-5 of the largest output), in FP64 to rounding
+    if form == capi.FORM_F32C:
+        adj64 = T.rs_adjoint_dev(px, py, v, grid, capi.FORM_PLAIN_F64).cpu().numpy()
+        assert np.max(np.abs(adj_split - adj64)) <= 1e-5 * np.max(np.abs(adj64))
+    else:
+        assert np.max(np.abs(adj_split - adj)) <= 1e-12 * np.max(np.abs(adj))
 
 
 def test_rcwa_batch_split_over_devices():

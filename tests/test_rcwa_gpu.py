@@ -231,3 +231,49 @@ def test_selftest8_known_answers_and_high_orders():
     res, info = capi.rcwa_batch([capi.rcwa_cell(**c) for c in shapes])
     assert np.all(info == 0)
     assert max(abs(res[2 * k]["sum_de"] - 1.0) for k in range(3)) < 2e-3
+
+
+def _batch_with_env(cells, **env):
+    import os
+
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        return capi.rcwa_batch([capi.rcwa_cell(**c) for c in cells])
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
+SYM_CELLS = [c for c in MIXED if c.get("theta_rad", 0.0) == 0.0 and c.get("rotation_rad", 0.0) == 0.0
+             and c["Mx"] >= 1 and c.get("My", c["Mx"]) >= 1] + [LOSSY, LARGE[0], LARGE[1]]
+
+
+def test_parity_class_eigensolve_matches_full_eigensolve():
+    """Mirror-symmetric cells at normal incidence solve the eigenproblem in its
+    four parity classes (orders of ~n/4); the results equal those of the full
+    eigensolve (CELERIS_RCWA_SYMMETRY=0) to rounding."""
+    full, info_f = _batch_with_env(SYM_CELLS, CELERIS_RCWA_SYMMETRY="0")
+    cls, info_c = _batch_with_env(SYM_CELLS)
+    assert np.all(info_f == 0) and np.all(info_c == 0)
+    for a, b in zip(cls, full):
+        scale = max(abs(b["tx0"]), abs(b["ty0"]))
+        for key in ("tx0", "ty0"):
+            assert abs(a[key] - b[key]) <= 1e-11 * scale, (key, a[key], b[key])
+        for key in ("R", "T", "de_t0", "de_r0"):
+            assert abs(a[key] - b[key]) <= 1e-11
+
+
+def test_asymmetric_cells_fall_back_to_the_full_eigensolve():
+    """A cell whose M is not mirror symmetric to the tolerance is flagged and
+    solved again by the full eigensolve: with the tolerance 0 every cell takes
+    that path, and the results are the full eigensolve's."""
+    full, _ = _batch_with_env(SYM_CELLS, CELERIS_RCWA_SYMMETRY="0")
+    redo, info = _batch_with_env(SYM_CELLS, CELERIS_RCWA_SYM_TOL="0")
+    assert np.all(info == 0)
+    for a, b in zip(redo, full):
+        assert abs(a["tx0"] - b["tx0"]) <= 1e-13 * abs(b["tx0"])
+        assert abs(a["R"] - b["R"]) <= 1e-13

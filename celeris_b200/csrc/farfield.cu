@@ -114,6 +114,36 @@ __global__ void ff_pack_f64(const double* __restrict__ px, const double* __restr
     rec[j] = make_double4(px[j], py[j], t.x, t.y);
 }
 
+// ---- pixel grid of the precision form ----------------------------------------------
+// Pillar coordinates are rounded to FP32 relative to the FP32 origin (ulp <=
+// G below). A pixel is split into a base on the grid of step G = 2^(ilogb(L) -
+// 23), the ulp of L = the largest |x - ox|, |y - oy| of a pillar plus the
+// largest pixel offset, and a small offset c from it: base - x then rounds (if
+// at all) only bits of x, never bits of the pixel, and the offset enters rho^2
+// through c (2 (base - x) + c), a product with the pillar. Rounding fx - x
+// directly would snap fx to the grid of x's exponent - the same shift for
+// every pillar of that exponent - and adding a pixel-only value to an FP32
+// number likewise rounds it the same way for every pillar of one exponent:
+// errors that add up coherently near a focus.
+__host__ __device__ __forceinline__ double grid_step(double L) {
+    L = fmax(L, 1e-30);
+    return ldexp(1.0, ilogb(L) - 23);
+}
+
+// ext[0] = bits of max_j max(|x_j - ox|, |y_j - oy|)
+__global__ void ff_extent_kernel(const double* __restrict__ px, const double* __restrict__ py, int npil, double ox,
+                                 double oy, unsigned long long* __restrict__ ext) {
+    double m = 0.0;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npil; j += gridDim.x * blockDim.x)
+        m = fmax(m, fmax(fabs(px[j] - ox), fabs(py[j] - oy)));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(ext, (unsigned long long)__double_as_longlong(m));
+}
+
+__device__ __forceinline__ double ext_grid(const unsigned long long* ext, double wmax) {
+    return grid_step(__longlong_as_double((long long)*ext) + wmax);
+}
+
 __global__ void ff_pack_f32(const double* __restrict__ px, const double* __restrict__ py,
                             const double2* __restrict__ pt, int npil, double ox, double oy, int slot,
                             float4* __restrict__ rec) {
@@ -296,6 +326,11 @@ __device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
     asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
     return d;
 }
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
 __device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
     f32x2 d;
     asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
@@ -316,10 +351,12 @@ __device__ __forceinline__ void two_sum_acc(float& s, float& c, float x) {
     s = t;
 }
 
+template <bool ZLO>
 __global__ void __launch_bounds__(kThreads, 3) rs_f32c_kernel(const float4* __restrict__ rec,
                                                            int npil, int chunk_len, Geom g,
                                                            float il_hi, float il_lo,
-                                                           double2* __restrict__ partial) {
+                                                           const unsigned long long* __restrict__ ext,
+                                                           double wmax, double2* __restrict__ partial) {
     __shared__ __align__(128) float4 buf[kStages][kTile32];
     __shared__ __align__(8) uint64_t full[kStages];
 
@@ -330,27 +367,38 @@ __global__ void __launch_bounds__(kThreads, 3) rs_f32c_kernel(const float4* __re
     const int i0 = (strip - j * spr) * kPPT32;
     const int jj = min(j, g.ny - 1);
 
-    // pixel coordinates relative to the FP32 origin; the row's y as a float
-    // pair hi + lo (its lo part costs one scalar add per pillar record; x keeps
-    // its FP32 rounding, which the stated error bound counts)
-    float fxr[kPPT32], fyr = 0.f, fyl = 0.f, z = 0.f;
-#pragma unroll
-    for (int q = 0; q < kPPT32; ++q) {
+    // pixel coordinates relative to the FP32 origin (see grid_step): the row's
+    // y as a grid value and its offset fr_y (|fr_y| <= G/2); the thread's x as
+    // a base on the grid plus per-pixel offsets c_q (|c_q| <= G/2 + 5 steps):
+    // dx_q = s0 + c_q with s0 = base - x
+    const double G = ext_grid(ext, wmax);
+    float bx = 0.f, cq[kPPT32], fyq = 0.f, fyo = 0.f, nfr2 = 0.f, z = 0.f, zl = 0.f;
+    {
         double fx, fy, fz;
-        pixel_pos(g, min(i0 + q, g.nx - 1), jj, fx, fy, fz);
-        fxr[q] = (float)(fx - g.ox);
-        fyr = (float)(fy - g.oy);
-        fyl = (float)((fy - g.oy) - (double)fyr);
+        pixel_pos(g, min(i0, g.nx - 1), jj, fx, fy, fz);
+        const double xb = rint((fx - g.ox) / G) * G, yq = rint((fy - g.oy) / G) * G, fr = (fy - g.oy) - yq;
+        bx = (float)xb;
+        fyq = (float)yq;
+        fyo = (float)(-2.0 * fr);
+        nfr2 = (float)(-fr * fr);
         z = (float)fz;
+        zl = (float)(fz - (double)z);  // z = z + zl to ~u^2 |z|
+#pragma unroll
+        for (int q = 0; q < kPPT32; ++q) {
+            pixel_pos(g, min(i0 + q, g.nx - 1), jj, fx, fy, fz);
+            cq[q] = (float)((fx - g.ox) - xb);
+        }
     }
     const float z2 = z * z;
     const float kMagic = 12582912.0f;  // 1.5 * 2^23: x + M - M rounds x to an integer
     // pixel pairs and the constants of the packed term arithmetic
     constexpr int kPairs = kPPT32 / 2;
-    f32x2 fx2[kPairs];
+    f32x2 c2[kPairs];
 #pragma unroll
-    for (int h = 0; h < kPairs; ++h) fx2[h] = pk2(fxr[2 * h], fxr[2 * h + 1]);
-    const f32x2 NEG1 = dup2(-1.0f), NEG2 = dup2(-2.0f), NZ = dup2(-z), Z2X = dup2(2.0f * z), NHALF = dup2(-0.5f);
+    for (int h = 0; h < kPairs; ++h) c2[h] = pk2(cq[2 * h], cq[2 * h + 1]);
+    const f32x2 Z2P = dup2(z2);
+    const f32x2 NZ = dup2(-z), Z2X = dup2(2.0f * z), NHALF = dup2(-0.5f);
+    const f32x2 Z2L = dup2(2.0f * zl);
     const f32x2 ILHI = dup2(il_hi), NILHI = dup2(-il_hi), ILLO = dup2(il_lo), MAGIC = dup2(kMagic);
     const f32x2 TWOPI = dup2(6.28318530717958647692f);
 
@@ -373,29 +421,24 @@ __global__ void __launch_bounds__(kThreads, 3) rs_f32c_kernel(const float4* __re
 #pragma unroll 2
             for (int p = 0; p < cnt; ++p) {
                 const float4 r = tile[p];  // {x, y, |t|, arg t / 2pi}
-                // dy = sy + ey exactly (Fast2Sum): the rounding of fy - y would
-                // otherwise snap fy to the grid of y's exponent, the same shift
-                // for every pillar of that exponent - an error that adds up
-                // coherently near a focus
-                const float sy = fyr - r.y;
-                const float ey = (fyr - (sy + r.y)) + fyl;
-                const f32x2 RX = dup2(r.x), RW = dup2(r.w), RZ = dup2(r.z);
-                const f32x2 U0 = dup2(fmaf(sy, sy, z2));                     // dy^2 + z^2 (seed only)
-                const f32x2 NDY2 = dup2(fmaf(sy, -sy, sy * (-2.0f * ey)));  // -(dy^2), to second order
+                // s0 = base - x, sy = fy - y (grid values: only bits of x, y
+                // can round off); -(s0^2 + dy^2), dy = sy + fr_y
+                const float s0 = bx - r.x, sy = fyq - r.y;
+                const f32x2 RW = dup2(r.w), RZ = dup2(r.z), NS02 = dup2(-2.0f * s0);
+                const f32x2 NB = dup2(fmaf(s0, -s0, fmaf(sy, -sy, fmaf(sy, fyo, nfr2))));
 #pragma unroll
                 for (int h = 0; h < kPairs; ++h) {
-                    // dx = s + e exactly (Fast2Sum), -rho^2 = -(s^2 + 2 s e + dy^2)
-                    const f32x2 s = fma2(RX, NEG1, fx2[h]);               // fx - x, rounded
-                    const f32x2 e = fma2(add2(s, RX), NEG1, fx2[h]);      // its rounding error
-                    const f32x2 ndx = fma2(fx2[h], NEG1, RX);             // -s
-                    const f32x2 u = fma2(s, s, U0);                       // R^2 (seed only)
-                    const f32x2 ns = fma2(s, ndx, fma2(s, mul2(e, NEG2), NDY2));  // -rho^2
+                    // -rho^2 = -(s0^2 + dy^2) - c (2 s0 + c)
+                    const f32x2 ns = fma2(sub2(NS02, c2[h]), c2[h], NB);
+                    const f32x2 u = sub2(Z2P, ns);                        // R^2 (seed, amplitude)
                     float ua, ub;
                     upk2(u, ua, ub);
                     const f32x2 ri = pk2(rsqrt_approx(ua), rsqrt_approx(ub));  // ~1/R
                     const f32x2 d0 = fma2(u, ri, NZ);          // ~R - z
-                    // Newton on f(d) = d^2 + 2 z d - rho^2 (exact root R - z)
-                    const f32x2 gg = fma2(d0, d0, fma2(Z2X, d0, ns));
+                    // Newton on f(d) = d^2 + 2 (z + zl) d - rho^2 (root R - z for
+                    // the FP64 z, so the FP64 phase k z applied later matches)
+                    const f32x2 gg = ZLO ? fma2(d0, d0, fma2(Z2X, d0, fma2(Z2L, d0, ns)))
+                                         : fma2(d0, d0, fma2(Z2X, d0, ns));
                     const f32x2 d = fma2(mul2(gg, ri), NHALF, d0);
                     // phase in turns, (R - z)/lambda + arg(t)/2pi (k z is added in
                     // FP64), reduced without rounding its integer part into the
@@ -406,8 +449,8 @@ __global__ void __launch_bounds__(kThreads, 3) rs_f32c_kernel(const float4* __re
                     const f32x2 np = mul2(d, NILHI);                      // -p
                     const f32x2 rp = fma2(d, ILHI, np);                   // d hi - p, exact
                     const f32x2 t = add2(rp, fma2(d, ILLO, RW));          // rp + d lo + psi
-                    const f32x2 w = fma2(add2(np, MAGIC), NEG1, MAGIC);   // round(p)
-                    const f32x2 ang = mul2(fma2(add2(np, w), NEG1, t), TWOPI);  // 2 pi (p - round(p) + t), |.| <= 2 pi
+                    const f32x2 w = sub2(MAGIC, add2(np, MAGIC));         // round(p)
+                    const f32x2 ang = mul2(sub2(t, add2(np, w)), TWOPI);  // 2 pi (p - round(p) + t), |.| <= 2 pi
                     const f32x2 a = mul2(RZ, ri);                         // |t| / R
                     float aa, ab;
                     upk2(ang, aa, ab);
@@ -561,9 +604,9 @@ __global__ void rs_reduce_kernel(const double2* __restrict__ partial, int nchunk
         const int j = p / g.nx;
         double fx, fy, fz;
         pixel_pos(g, 0, j, fx, fy, fz);
-        // the FP32 terms hold the phase of R - z_f, z_f = (float)z; with the
-        // global phase k z (not k z_f) the field's phase error from rounding z
-        // is k |z - z_f| (1 - z/R), not k |z - z_f|
+        // the FP32 terms hold the phase of R - z for z carried as a float pair
+        // (the precision forward) or R - z_f, z_f = (float)z (the adjoint); the
+        // global phase k z uses the FP64 z
         double s, c;
         sincos(k * fz, &s, &c);
         const double r = er * c - ei * s;
@@ -737,42 +780,44 @@ __global__ void rs_check_kernel(const double4* __restrict__ rec, int npil, Geom 
 }
 
 // Error model of one precision-form term (rs_f32c_kernel), per pillar j, for
-// every pixel of the window. u = 2^-24 (FP32 round to nearest). With the
-// pillar's offset (xo, yo) from the FP32 origin and the window's half extents
-// (wx, wy), dxm = xo + wx and dym = yo + wy bound |dx|, |dy|, rho^2 <= dxm^2 +
-// dym^2 and delta = R - z <= dmax.
-// Random part (rounding that depends on each pillar's own coordinates):
-// dx = s + e and dy = sy + ey are formed exactly (Fast2Sum), so rho^2 moves
-// only by the FP32 rounding of the pillar's coordinates (2u (dxm xo + dym
-// yo)), by a Fast2Sum residual that is not exact for pillars inside the window
-// (2u (dxm wx + dym wy)) and by its own three roundings (3u (dxm^2 + dym^2)):
-// at most 5u (dxm^2 + dym^2), counted 6u; R - z moves by that / (2|z|); the
-// Newton step adds u dmax (1 + dmax / 2|z|) and the quadratic remainder of its
-// seed (rsqrt.approx); the amplitude |t|/R rounds with 6u:
+// every pixel of the window. u = 2^-24 (FP32 round to nearest), G the pixel
+// grid step (grid_step), cmax = G/2 + 5 pixel steps the largest offset of a
+// pixel from its thread's base. With the pillar's offset (xo, yo) from the
+// FP32 origin and the window's largest pixel offset w, dxm = xo + w and dym =
+// yo + w bound |dx|, |dy|, rho^2 <= dxm^2 + dym^2 and delta = R - z <= dmax.
+// Random part (depends on each pillar's own coordinates): the FP32 rounding of
+// the pillar's x, y (u xo, u yo) and of base - x, fy - y (which can only drop
+// bits of x, y: u dxm, u dym) moves rho^2 by at most 4u (dxm^2 + dym^2), its
+// assembly rounds by at most 4u (dxm^2 + dym^2) more; R - z moves by that /
+// (2|z|); the Newton step adds u dmax (1 + dmax / 2|z|) and the quadratic
+// remainder of its seed (rsqrt.approx); the amplitude |t|/R rounds with 6u:
 //   e_R(j)  = 2 pi dDelta / lambda + 6u
 // Systematic part (the same for many pillars, so it can add up coherently near
 // a focus where the phases of all terms agree), summed without cancellation:
 // the phase reduction (psi rounded to FP32, d lo + psi, rp + that, the reduced
 // fraction of magnitude <= 1 turn: 3u turns; the product with 2 pi_f: u 2 pi
 // and |2 pi_f - 2 pi|), the MUFU approximations, the FP32 rounding of the
-// pixel's x coordinate (u wx, a shift of the pixel: k u wx dxm / |z|), and the
-// rounding of z:
+// pixel's offsets (u cmax in x, u G in y: a shift of the pixel), and what is
+// left of the rounding of z once it is carried as a float pair z_f + z_l
+// (dz = |z - z_f - z_l|, ~u^2 |z|):
 //   e_D(j)  = kRsqrtRelErr + sqrt(2) kSinCosAbsErr + 2 pi 4u + |2 pi_f - 2 pi|
-//             + k u wx dxm / |z| + |z - z_f| / |z| + k |z - z_f| rho_max^2 / (2 z^2)
-// with z_f = (float)z (the z the FP32 terms use; the global phase uses z).
+//             + k u (cmax dxm + G dym) / |z| + dz / |z| + k dz rho_max^2 / (2 z^2)
 // Every term has magnitude a_j = |t_j| / R <= |t_j| / |z|. acc (doubles):
 // [0] sum_j a_j e_D(j), [1] sum_j (a_j e_R(j))^2, [2] bits of max_j a_j,
-// [3] sum_j a_j.
+// [3] sum_j a_j; ext: the coordinate extent word of ff_extent_kernel.
 __global__ void ff_bound_kernel(const double* __restrict__ px, const double* __restrict__ py,
                                 const double2* __restrict__ pt, int npil, Geom g, double k,
+                                const unsigned long long* __restrict__ ext, double wmax,
                                 double* __restrict__ acc) {
     const double u = 5.9604644775390625e-08;  // 2^-24
     const double pi = 3.14159265358979323846;
-    const double z = fabs(g.z), zf = fabs((double)(float)g.z), dz = fabs(z - zf);
+    // the terms use z as the float pair z_f + z_l; what remains of its rounding
+    const double zf = (double)(float)g.z, zl = (double)(float)(g.z - zf);
+    const double z = fabs(g.z), dz = fabs(g.z - zf - zl);
     const double lam = 2.0 * pi / k;
-    const double wx = fmax(fabs(g.a0 - g.ox), fabs(g.a0 + (g.nx - 1) * g.a1 - g.ox));
-    const double y_first = g.b0 + g.row0 * g.b1, y_last = g.b0 + (g.row0 + g.ny - 1) * g.b1;
-    const double wy = fmax(fabs(y_first - g.oy), fabs(y_last - g.oy));
+    const double G = ext_grid(ext, wmax);
+    const double pstep = g.mode == GEOM_PSF ? fabs(g.a1) : fabs(g.a1 - g.a0) / fmax(1.0, (double)(g.nx - 1));
+    const double cmax = 0.5 * G + (kPPT32 - 1) * pstep;
     const double two_pi_f = (double)6.28318530717958647692f;
     const double eD0 = celeris_dev::kRsqrtRelErr + 1.4142135623730951 * celeris_dev::kSinCosAbsErr +
                        2.0 * pi * 4.0 * u + fabs(two_pi_f - 2.0 * pi) + dz / z;
@@ -780,14 +825,14 @@ __global__ void ff_bound_kernel(const double* __restrict__ px, const double* __r
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npil; j += gridDim.x * blockDim.x) {
         const double2 t = pt[j];
         const double a = hypot(t.x, t.y) / z;
-        const double dxm = fabs(px[j] - g.ox) + wx, dym = fabs(py[j] - g.oy) + wy;
+        const double dxm = fabs(px[j] - g.ox) + wmax, dym = fabs(py[j] - g.oy) + wmax;
         const double rho2 = dxm * dxm + dym * dym;
         const double R = sqrt(rho2 + z * z);
         const double dmax = rho2 / (R + z);
         const double seed = R * (celeris_dev::kRsqrtRelErr + 4.0 * u);
-        const double dDelta = 6.0 * u * rho2 / (2.0 * z) + u * dmax * (1.0 + dmax / (2.0 * z)) + seed * seed / z;
+        const double dDelta = 8.0 * u * rho2 / (2.0 * z) + u * dmax * (1.0 + dmax / (2.0 * z)) + seed * seed / z;
         const double eR = 2.0 * pi * dDelta / lam + 6.0 * u;
-        const double eD = eD0 + k * u * wx * dxm / z + k * dz * rho2 / (2.0 * z * z);
+        const double eD = eD0 + k * u * (cmax * dxm + G * dym) / z + k * dz * rho2 / (2.0 * z * z);
         sD += a * eD;
         sR += (a * eR) * (a * eR);
         sA += a;
@@ -936,6 +981,27 @@ Geom zx_geom(double xmin, double xmax, int nx, double zmin, double zmax, int nz)
     return g;
 }
 
+// Largest pixel offset from the FP32 origin over the grid (either axis).
+double window_extent(const Geom& g) {
+    if (g.mode == GEOM_ZX) return std::max(std::fabs(g.a0), std::fabs(g.a1));  // x only; y = 0
+    const double x0 = g.a0 - g.ox, x1 = g.a0 + (g.nx - 1) * g.a1 - g.ox;
+    const double y0 = g.b0 + g.row0 * g.b1 - g.oy, y1 = g.b0 + (g.row0 + g.ny - 1) * g.b1 - g.oy;
+    return std::max(std::max(std::fabs(x0), std::fabs(x1)), std::max(std::fabs(y0), std::fabs(y1)));
+}
+
+// Whether z needs its FP32 lo part (z not exactly a float): every row of a
+// PSF grid shares z; a ZX grid's rows differ and always carry it.
+bool needs_zlo(const Geom& g) { return g.mode == GEOM_ZX || (double)(float)g.z != g.z; }
+
+// The precision-form kernel launch (the two z variants).
+void launch_f32c(dim3 grid, cudaStream_t st, const float4* rec, int npil, int chunk_len, const Geom& g, float hi,
+                 float lo, const unsigned long long* ext, double wmax, double2* partial) {
+    if (needs_zlo(g))
+        rs_f32c_kernel<true><<<grid, kThreads, 0, st>>>(rec, npil, chunk_len, g, hi, lo, ext, wmax, partial);
+    else
+        rs_f32c_kernel<false><<<grid, kThreads, 0, st>>>(rec, npil, chunk_len, g, hi, lo, ext, wmax, partial);
+}
+
 // Optional CUDA-event timing of the main kernel (bench instrumentation).
 std::atomic<int> g_time_kernels{0};
 struct KernelTimer {
@@ -988,14 +1054,19 @@ int ff_run(int form, const double* d_px, const double* d_py, const double* d_pt,
     Workspace& ws = Workspace::for_stream(st);
     const size_t rec_bytes = (size_t)npil * (f32 ? sizeof(float4) : sizeof(double4));
     const size_t part_bytes = (size_t)nchunk * npix * sizeof(double2);
-    CEL_TRY(ws.reserve(st, celeris_rt::align256(rec_bytes) + celeris_rt::align256(part_bytes)));
+    CEL_TRY(ws.reserve(st, celeris_rt::align256(rec_bytes) + celeris_rt::align256(part_bytes) + 256));
     void* rec = ws.take(rec_bytes);
     double2* partial = static_cast<double2*>(ws.take(part_bytes));
+    unsigned long long* ext = static_cast<unsigned long long*>(ws.take(sizeof(unsigned long long)));
+    const double wmax = window_extent(g);
 
     const int pb = (npil + 255) / 256;
     if (f32) {
+        CEL_CUDA(cudaMemsetAsync(ext, 0, sizeof(unsigned long long), st));
+        ff_extent_kernel<<<std::min(pb, 4 * sm_count()), 256, 0, st>>>(d_px, d_py, npil, g.ox, g.oy, ext);
         ff_pack_f32<<<pb, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil,
                                         g.ox, g.oy, g.slot, static_cast<float4*>(rec));
+        count_launch(1);
     } else {
         ff_pack_f64<<<pb, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil,
                                         g.slot, static_cast<double4*>(rec));
@@ -1006,8 +1077,7 @@ int ff_run(int form, const double* d_px, const double* d_py, const double* d_pt,
         const double il = k / (2.0 * 3.14159265358979323846);  // 1/lambda in turns per micron
         const float hi = (float)il;
         const float lo = (float)(il - (double)hi);
-        rs_f32c_kernel<<<grid, kThreads, 0, st>>>(static_cast<const float4*>(rec), npil, chunk_len, g, hi, lo,
-                                                  partial);
+        launch_f32c(grid, st, static_cast<const float4*>(rec), npil, chunk_len, g, hi, lo, ext, wmax, partial);
     } else {
         rs_f64_kernel<<<grid, kThreads, 0, st>>>(static_cast<const double4*>(rec), npil,
                                                  chunk_len, g, k, partial);
@@ -1079,7 +1149,7 @@ int ff_adjoint(const double* d_px, const double* d_py, int npil, const Geom& g0,
 
 // Accumulator words of the stated-error evaluation (device and host copies):
 // [0] bits of max |E|, [1] peak key, [2] bits of max sampled |E - E64|,
-// [3..6] the sums of ff_bound_kernel.
+// [3..6] the sums of ff_bound_kernel, [7] the coordinate extent.
 constexpr int kAccWords = 8;
 
 // Enqueue the stated-error evaluation of the field d_field on st: the sampled
@@ -1110,9 +1180,11 @@ int ff_check_enqueue(const double* d_px, const double* d_py, const double* d_pt,
         launches += 2;
     }
     if (want_bound) {
+        const double wmax = window_extent(g);
+        ff_extent_kernel<<<2 * sm_count(), 256, 0, st>>>(d_px, d_py, npil, g.ox, g.oy, acc + 7);
         ff_bound_kernel<<<2 * sm_count(), 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil, g,
-                                                        k, reinterpret_cast<double*>(acc + 3));
-        launches += 1;
+                                                        k, acc + 7, wmax, reinterpret_cast<double*>(acc + 3));
+        launches += 2;
     }
     count_launch(launches);
     CEL_CUDA(cudaGetLastError());
@@ -1434,7 +1506,9 @@ int ff_run_noalloc(int form, const double* d_px, const double* d_py, const doubl
     const int tile = f32 ? kTile32 : kTile64;
     const long spr = (g.nx + ppt - 1) / ppt;
     const int ctas_pix = (int)((spr * g.ny + kThreads - 1) / kThreads);
-    const size_t rec_bytes = celeris_rt::align256((size_t)npil * (f32 ? sizeof(float4) : sizeof(double4)));
+    // scratch: pillar records | the coordinate extent word (256 B) | partial sums
+    const size_t rec_bytes =
+        celeris_rt::align256((size_t)npil * (f32 ? sizeof(float4) : sizeof(double4))) + 256;
     const size_t part_one = (size_t)npix * sizeof(double2);
     if (rec_bytes + part_one > kNoAllocScratchBytes)
         return set_error(CELERIS_ERR_TOO_LARGE,
@@ -1450,12 +1524,17 @@ int ff_run_noalloc(int form, const double* d_px, const double* d_py, const doubl
         nchunk = (ntiles + tiles_per - 1) / tiles_per;
     }
     void* rec = base;
+    unsigned long long* ext = reinterpret_cast<unsigned long long*>(static_cast<char*>(base) + rec_bytes - 256);
     double2* partial = reinterpret_cast<double2*>(static_cast<char*>(base) + rec_bytes);
+    const double wmax = window_extent(g);
     const int pb = (npil + 255) / 256;
-    if (f32)
+    if (f32) {
+        CEL_CUDA(cudaMemsetAsync(ext, 0, sizeof(unsigned long long), st));
+        ff_extent_kernel<<<std::min(pb, 4 * sm_count()), 256, 0, st>>>(d_px, d_py, npil, g.ox, g.oy, ext);
         ff_pack_f32<<<pb, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil, g.ox, g.oy,
                                         g.slot, static_cast<float4*>(rec));
-    else
+        count_launch(1);
+    } else
         ff_pack_f64<<<pb, 256, 0, st>>>(d_px, d_py, reinterpret_cast<const double2*>(d_pt), npil, g.slot,
                                         static_cast<double4*>(rec));
     dim3 grid(ctas_pix, nchunk);
@@ -1463,8 +1542,7 @@ int ff_run_noalloc(int form, const double* d_px, const double* d_py, const doubl
         const double il = k / (2.0 * 3.14159265358979323846);
         const float hi = (float)il;
         const float lo = (float)(il - (double)hi);
-        rs_f32c_kernel<<<grid, kThreads, 0, st>>>(static_cast<const float4*>(rec), npil, chunk_len, g, hi, lo,
-                                                  partial);
+        launch_f32c(grid, st, static_cast<const float4*>(rec), npil, chunk_len, g, hi, lo, ext, wmax, partial);
     } else {
         rs_f64_kernel<<<grid, kThreads, 0, st>>>(static_cast<const double4*>(rec), npil, chunk_len, g, k, partial);
     }

@@ -54,7 +54,7 @@ using celeris_rt::Workspace;
 constexpr double PI = 3.14159265358979323846;
 constexpr int kRT = 256;            // threads per CTA
 constexpr int kDbgSlots = 16;       // diagnostic counters per cell
-constexpr int kSmemEigMaxN = 112;   // eigensolve in shared memory up to this n
+constexpr int kSmemEigMaxN = 116;   // Hessenberg reduction in shared memory up to this n ((n^2 + 2n) 16 B <= 227 KB)
 
 struct CellDev {
     double omega;  // k0 = 2 pi / lambda (c = 1 units, omega = k0)
@@ -91,6 +91,11 @@ struct Bucket {
     int m[2];
     cplx *sH[2], *sZ[2], *sX[2], *sW[2], *sA[2], *sq[2];
     int* sinfo[2];
+    // S-matrix in the two excited classes, matrix 2 cell + c (c = 0: (+,+), the
+    // Y excitation; c = 1: (-,-), the X excitation), order m[0]: layer kp,
+    // incident diag(kz) kp^-1, substrate kp diag(1/kz), and the work matrices
+    cplx *cKp, *cC0, *cKs, *cA, *cT11, *cT11lu, *cT12, *cS12, *cQ, *cSQ, *cCm, *cvec;
+    int* cpiv;
 };
 
 __device__ __forceinline__ cplx* at(cplx* base, size_t stride, int c) { return base + stride * c; }
@@ -1031,14 +1036,42 @@ __device__ __forceinline__ cplx* sym_mat(const Bucket& b, cplx* const* base, int
     return base[k] + (size_t)(2 * cell + (c & 1)) * m * m;
 }
 
-// M (in H) -> the four class matrices; flags a cell whose M is not mirror
-// symmetric to rounding.
+// Entry (k, l) of a per-order block operator of a homogeneous half-space
+// (non-zero only within one order: the 2 x 2 block of indices i, N + i).
+// which = 0: incident diag(kz) kp^-1 (rcwa2d.cpp:376-388, P1 of the first
+// interface); which = 1: substrate kp diag(1/kz) (K of the last interface).
+__device__ cplx halfspace_entry(const Bucket& b, const CellDev& c, int which, int k, int l) {
+    const int N = b.N;
+    const int ok = k % N, ol = l % N;
+    if (ok != ol) return C(0.0, 0.0);
+    const cplx nr = which == 0 ? c.n_inc : c.n_sub;
+    const cplx er = cmul(nr, nr), ier = cinv(er);
+    const cplx kx = kx_of(b, c, ok), ky = ky_of(b, c, ok);
+    cplx ka, kb, kc, kd;
+    kp_uniform(ier, c.omega, kx, ky, ka, kb, kc, kd);
+    const cplx kz = kz_uniform(er, c.omega, kx, ky);
+    const int r = k / N, s = l / N;
+    if (which == 0) {  // kz [[kd, -kb], [-kc, ka]] / det
+        const cplx idet = cmul(kz, cinv(csub(cmul(ka, kd), cmul(kb, kc))));
+        const cplx v = r == 0 ? (s == 0 ? kd : cneg(kb)) : (s == 0 ? cneg(kc) : ka);
+        return cmul(v, idet);
+    }
+    const cplx v = r == 0 ? (s == 0 ? ka : kb) : (s == 0 ? kc : kd);
+    return cmul(v, cinv(kz));
+}
+
+// M (in H) -> the class matrices of the two excited classes (c = 0, 1) for the
+// eigen-stages, and their layer kp (kp = w^2 - J Einv J^T, J = [-Ky; Kx],
+// rcwa2d.cpp:346-352) and half-space operators for the class S-matrix;
+// flags a cell whose M is not mirror symmetric to the tolerance.
 __global__ void __launch_bounds__(kRT) rcwa_sym_project(Bucket b) {
     __shared__ double red[3][32];
     const int cell = blockIdx.x;
+    const CellDev cd = b.cells[cell];
     const int N = b.N, n = b.n, Mx = b.Mx, My = b.My, ny = 2 * My + 1;
     const int tid = threadIdx.x, nt = blockDim.x;
     const cplx* H = at(b.H, b.s_nn, cell);
+    const cplx* Einv = at(b.Einv, b.s_NN, cell);
     // symmetry check: M[k][l] = s(k) s(l) M[mirror k][mirror l] for both mirrors
     double dx = 0.0, dy = 0.0, mx = 0.0;
     for (int e = tid; e < n * n; e += nt) {
@@ -1073,49 +1106,178 @@ __global__ void __launch_bounds__(kRT) rcwa_sym_project(Bucket b) {
         }
         if (!(fmax(a, c) <= b.sym_tol * m) && b.info[cell] == 0) b.info[cell] = kInfoAsym;
     }
-    // class matrices M_c = P_c^T M P_c
-    for (int c = 0; c < 4; ++c) {
-        const int m = b.m[c >> 1];
-        cplx* Mc = sym_mat(b, b.sH, c, cell);
+    // P_c^T X P_c for X = M, the layer kp and the two half-space operators
+    const double w2 = cd.omega * cd.omega;
+    const int m = b.m[0];
+    for (int c = 0; c < 2; ++c) {
+        const size_t mi = (size_t)(2 * cell + c) * m * m;
+        cplx* Mc = b.sH[0] + mi;
+        cplx* Kp = b.cKp + mi;
+        cplx* C0 = b.cC0 + mi;
+        cplx* Ks = b.cKs + mi;
         for (int e = tid; e < m * m; e += nt) {
             const int i = e / m, j = e % m;
             int ii[4], jj[4];
             double ci[4], cj[4];
             const int ni = sym_vector(Mx, My, c, i, ii, ci), nj = sym_vector(Mx, My, c, j, jj, cj);
-            cplx acc = C(0.0, 0.0);
+            cplx am = C(0.0, 0.0), ak = C(0.0, 0.0), a0 = C(0.0, 0.0), as = C(0.0, 0.0);
             for (int u = 0; u < ni; ++u)
-                for (int v = 0; v < nj; ++v) acc = cadd(acc, cscale(H[(size_t)ii[u] * n + jj[v]], ci[u] * cj[v]));
-            Mc[e] = acc;
+                for (int v = 0; v < nj; ++v) {
+                    const int k = ii[u], l = jj[v];
+                    const double w = ci[u] * cj[v];
+                    am = cadd(am, cscale(H[(size_t)k * n + l], w));
+                    // kp[k][l] = w^2 [k == l] - J(k) Einv[ord k][ord l] J(l)
+                    const cplx Jk = k < N ? cneg(ky_of(b, cd, k)) : kx_of(b, cd, k - N);
+                    const cplx Jl = l < N ? cneg(ky_of(b, cd, l)) : kx_of(b, cd, l - N);
+                    cplx kp = cneg(cmul(Jk, cmul(Einv[(size_t)(k % N) * N + (l % N)], Jl)));
+                    if (k == l) kp.x += w2;
+                    ak = cadd(ak, cscale(kp, w));
+                    a0 = cadd(a0, cscale(halfspace_entry(b, cd, 0, k, l), w));
+                    as = cadd(as, cscale(halfspace_entry(b, cd, 1, k, l), w));
+                }
+            Mc[e] = am;
+            Kp[e] = ak;
+            C0[e] = a0;
+            Ks[e] = as;
         }
     }
 }
 
-// W = [P_c W_c]_c and q = [q_c]_c (class order (+,+), (-,-), (+,-), (-,+)); a
-// class eigensolve failure becomes the cell's info.
-__global__ void __launch_bounds__(kRT) rcwa_sym_expand(Bucket b) {
-    const int cell = blockIdx.x;
-    const int n = b.n, Mx = b.Mx, My = b.My;
+// The S-matrix of one excited class: rcwa_smat1 and rcwa_smat2 restricted to
+// the class, with the class's one excitation (class 0: Y, a0 = -e_i0; class 1:
+// X, a0 = e_{N+i0}, rcwa2d.cpp:403-411). In the class basis the half-spaces'
+// phi stays I and their kz stays diagonal (kz is even in p and q), so the
+// reference's recursion carries over with every matrix of order m:
+//   A = kp W,  P = C0 A diag(1/q),  T11 = (W + P)/2,  T12 = (W - P)/2,
+//   [S12 | u] = T11^-1 [-T12 D | a0],
+//   Q = diag(q) A^-1 Ks W,  (I + Q - D S12 + D S12 Q) y = 2 D u,
+//   aN = W y,  y2 = (y - Q y)/2,  b0 = T12 (u + S12 y2) + T11 D y2.
+// Writes aN and b0 (class basis) to the class vector area.
+// dynamic smem: LU staging (2m + LNB^2 complex)
+__global__ void __launch_bounds__(kRT) rcwa_sym_smat(Bucket b) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    cplx* stg = reinterpret_cast<cplx*>(smem);
+    __shared__ GemmSmem gs;
+    __shared__ RedScratch rs;
+    const int mi = blockIdx.x, cell = mi >> 1, c = mi & 1;
+    const CellDev cd = b.cells[cell];
+    const int m = b.m[0], N = b.N, Mx = b.Mx, My = b.My;
     const int tid = threadIdx.x, nt = blockDim.x;
-    cplx* W = at(b.W, b.s_nn, cell);
-    cplx* q1 = at(b.q1, b.s_n, cell);
-    for (int e = tid; e < n * n; e += nt) W[e] = C(0.0, 0.0);
+    const size_t o2 = (size_t)mi * m * m;
+    const cplx* W = b.sW[0] + o2;
+    const cplx* q = b.sq[0] + (size_t)mi * m;
+    const cplx *Kp = b.cKp + o2, *C0 = b.cC0 + o2, *Ks = b.cKs + o2;
+    cplx *A = b.cA + o2, *T11 = b.cT11 + o2, *T11lu = b.cT11lu + o2, *T12 = b.cT12 + o2;
+    cplx *Q = b.cQ + o2, *SQ = b.cSQ + o2, *Cm = b.cCm + o2;
+    cplx* S = b.cS12 + (size_t)mi * m * (m + 1);
+    cplx* vec = b.cvec + (size_t)mi * 8 * m;  // aN | b0 | y | Q y | y2 | u + S12 y2 | D y2
+    int* piv = b.cpiv + (size_t)mi * m;
+    const int ld = m + 1;
+    const cplx one = C(1.0, 0.0), zero = C(0.0, 0.0);
+    // A = kp W, then P = C0 A (into T12), T11 = (W + P diag(1/q))/2, T12 = (W - P diag(1/q))/2
+    blk_gemm(m, m, m, one, Kp, m, W, m, zero, A, m, &gs);
+    blk_gemm(m, m, m, one, C0, m, A, m, zero, T12, m, &gs);
+    for (int e = tid; e < m * m; e += nt) {
+        const cplx p = cmul(T12[e], cinv(q[e % m]));
+        const cplx w = W[e];
+        const cplx t = cscale(cadd(w, p), 0.5);
+        T11[e] = t;
+        T11lu[e] = t;
+        T12[e] = cscale(csub(w, p), 0.5);
+    }
     __syncthreads();
-    int off = 0;
-    for (int c = 0; c < 4; ++c) {
-        const int k = c >> 1, m = b.m[k], mat = 2 * cell + (c & 1);
-        const cplx* Wc = b.sW[k] + (size_t)mat * m * m;
-        const cplx* qc = b.sq[k] + (size_t)mat * m;
-        for (int e = tid; e < m * m; e += nt) {
-            const int i = e / m, j = e % m;
+    // [-T12 D | a0]: a0 of the class's excitation in the class basis
+    const int i0 = Mx * (2 * My + 1) + My;
+    const int k0 = c == 1 ? N + i0 : i0;
+    const double s0 = c == 1 ? 1.0 : -1.0;
+    for (int e = tid; e < m * ld; e += nt) {
+        const int i = e / ld, j = e % ld;
+        cplx v;
+        if (j < m) {
+            v = cneg(cmul(T12[(size_t)i * m + j], cexpi(cscale(q[j], cd.h))));
+        } else {
             int ii[4];
             double ci[4];
             const int ni = sym_vector(Mx, My, c, i, ii, ci);
-            const cplx w = Wc[e];
-            for (int u = 0; u < ni; ++u) W[(size_t)ii[u] * n + off + j] = cscale(w, ci[u]);
+            double a = 0.0;
+            for (int u = 0; u < ni; ++u)
+                if (ii[u] == k0) a += s0 * ci[u];
+            v = C(a, 0.0);
         }
-        for (int j = tid; j < m; j += nt) q1[off + j] = qc[j];
-        if (tid == 0 && b.info[cell] == 0 && b.sinfo[k][mat] != 0) b.info[cell] = b.sinfo[k][mat];
-        off += m;
+        S[e] = v;
+    }
+    __syncthreads();
+    int info = blk_lu_blocked(m, T11lu, m, piv, &rs, stg, &gs);
+    if (tid == 0 && info) atomicCAS(&b.info[cell], 0, -info);
+    blk_lu_solve_blocked(m, T11lu, m, piv, ld, S, ld, stg, &gs);  // [S12 | u]
+    // interface to the substrate: Q = diag(q) A^-1 Ks W
+    blk_gemm(m, m, m, one, Ks, m, W, m, zero, Q, m, &gs);
+    info = blk_lu_blocked(m, A, m, piv, &rs, stg, &gs);
+    if (tid == 0 && info) atomicCAS(&b.info[cell], 0, -info);
+    blk_lu_solve_blocked(m, A, m, piv, m, Q, m, stg, &gs);
+    for (int e = tid; e < m * m; e += nt) Q[e] = cmul(q[e / m], Q[e]);
+    blk_gemm(m, m, m, one, S, ld, Q, m, zero, SQ, m, &gs);  // S12 Q
+    cplx *aN = vec, *b0 = vec + m, *y = vec + 2 * m, *Qy = vec + 3 * m, *y2 = vec + 4 * m, *zz = vec + 5 * m,
+         *dy2 = vec + 6 * m;
+    for (int e = tid; e < m * m; e += nt) {
+        const int i = e / m, j = e % m;
+        const cplx d = cexpi(cscale(q[i], cd.h));
+        cplx v = cadd(Q[e], cmul(d, csub(SQ[e], S[(size_t)i * ld + j])));
+        if (i == j) v.x += 1.0;
+        Cm[e] = v;
+    }
+    for (int i = tid; i < m; i += nt) y[i] = cscale(cmul(cexpi(cscale(q[i], cd.h)), S[(size_t)i * ld + m]), 2.0);
+    __syncthreads();
+    info = blk_lu_blocked(m, Cm, m, piv, &rs, stg, &gs);
+    if (tid == 0 && info) atomicCAS(&b.info[cell], 0, -info);
+    blk_lu_solve_blocked(m, Cm, m, piv, 1, y, 1, stg, &gs);  // y
+    blk_gemm(m, 1, m, one, W, m, y, 1, zero, aN, 1, &gs);    // aN = W y
+    blk_gemm(m, 1, m, one, Q, m, y, 1, zero, Qy, 1, &gs);    // Q y
+    for (int i = tid; i < m; i += nt) {
+        const cplx v = cscale(csub(y[i], Qy[i]), 0.5);
+        y2[i] = v;
+        zz[i] = S[(size_t)i * ld + m];                              // u
+        dy2[i] = cmul(cexpi(cscale(q[i], cd.h)), v);                // D y2
+    }
+    blk_gemm(m, 1, m, one, S, ld, y2, 1, one, zz, 1, &gs);    // u + S12 y2
+    blk_gemm(m, 1, m, one, T12, m, zz, 1, zero, b0, 1, &gs);  // T12 (u + S12 y2)
+    blk_gemm(m, 1, m, one, T11, m, dy2, 1, one, b0, 1, &gs);  // + T11 D y2
+}
+
+// aN and b0 of both excitations into the full basis (the vector area the
+// epilogue reads: aN_X, aN_Y, b0_X, b0_Y); a class eigensolve failure becomes
+// the cell's info (it is the cause of any later singular pivot).
+__global__ void __launch_bounds__(kRT) rcwa_sym_expand(Bucket b) {
+    const int cell = blockIdx.x;
+    const int n = b.n, Mx = b.Mx, My = b.My, m = b.m[0];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    cplx* vec = at(b.vec, 10 * b.s_n, cell);
+    for (int e = tid; e < 4 * (int)b.s_n; e += nt) vec[e] = C(0.0, 0.0);
+    __syncthreads();
+    for (int c = 0; c < 2; ++c) {
+        const int mi = 2 * cell + c;
+        const cplx* cv = b.cvec + (size_t)mi * 8 * m;
+        cplx* dst_a = vec + (c == 1 ? 0 : b.s_n);       // aN_X : aN_Y
+        cplx* dst_b = vec + (c == 1 ? 2 : 3) * b.s_n;   // b0_X : b0_Y
+        for (int i = tid; i < m; i += nt) {
+            int ii[4];
+            double ci[4];
+            const int ni = sym_vector(Mx, My, c, i, ii, ci);
+            for (int u = 0; u < ni; ++u) {
+                dst_a[ii[u]] = cscale(cv[i], ci[u]);
+                dst_b[ii[u]] = cscale(cv[m + i], ci[u]);
+            }
+        }
+    }
+    (void)n;
+    if (tid == 0 && b.info[cell] != kInfoAsym) {
+        for (int c = 0; c < 2; ++c) {
+            const int e = b.sinfo[0][2 * cell + c];
+            if (e != 0) {
+                b.info[cell] = e;
+                break;
+            }
+        }
     }
 }
 
@@ -1300,21 +1462,25 @@ size_t per_cell_bytes(int n, int nexc) {
            celeris_rt::align256(sizeof(CellDev)) + 14 * 256;
 }
 
-// the parity-class eigen-stage buffers of one mirror-symmetric cell: per size
-// class, two matrices with H, Z, X, W and the eigenvector scratch, q and info
-size_t sym_per_cell_bytes(int Mx, int My) {
-    size_t b = 0;
-    for (int k = 0; k < 2; ++k) {
-        const size_t m = (size_t)sym_class_size(Mx, My, 2 * k);
-        b += 2 * (5 * m * m + m) * sizeof(cplx) + 2 * sizeof(int);
-    }
-    return b + 14 * 256;
+// Device memory of one mirror-symmetric cell: of the full-order buffers only
+// H (M, and the Laurent LU scratch), Z, X (build_M's products), the Fourier
+// operators, the vector area and pivots; per excited class (two per cell) the
+// eigen-stage matrices H, Z, X, W, scratch, q and info, and the class S-matrix's
+// ten m x m matrices, S12 (m x (m + 1)), 8 m vector entries and m pivots.
+size_t sym_per_cell_bytes(int Mx, int My, int nexc) {
+    const int N = (2 * Mx + 1) * (2 * My + 1), n = 2 * N;
+    const size_t m = (size_t)sym_class_size(Mx, My, 0);
+    const size_t full = (3 * (size_t)n * n + 3 * (size_t)N * N + 10 * (size_t)n) * sizeof(cplx) +
+                        (size_t)n * sizeof(int) + sizeof(int) + sizeof(celeris_rcwa_result) * nexc + sizeof(CellDev);
+    const size_t cls = 2 * ((5 * m * m + m) * sizeof(cplx) + sizeof(int)) +
+                       2 * ((10 * m * m + m * (m + 1) + 8 * m) * sizeof(cplx) + m * sizeof(int));
+    return full + cls + 32 * 256;
 }
 
 // The largest dynamic shared memory each stage kernel needs over a wave's
 // buckets; raised once per wave, outside any capture.
 struct SmemNeeds {
-    size_t laurent = 0, rect = 0, hess_s = 0, hess_g = 0, smat = 0;
+    size_t laurent = 0, rect = 0, hess_s = 0, hess_g = 0, smat = 0, smat_sym = 0;
     bool aed = false;
     void add_eig(int n) {
         if (n <= kSmemEigMaxN) hess_s = std::max(hess_s, ((size_t)n * n + 2 * n) * sizeof(cplx));
@@ -1330,11 +1496,11 @@ struct SmemNeeds {
         }
         if (sym) {
             add_eig(sym_class_size(Mx, My, 0));
-            add_eig(sym_class_size(Mx, My, 2));
+            smat_sym = std::max(smat_sym, lu_stage_bytes(sym_class_size(Mx, My, 0)));
         } else {
             add_eig(n);
+            smat = std::max(smat, lu_stage_bytes(n));
         }
-        smat = std::max(smat, lu_stage_bytes(n));
     }
 };
 
@@ -1371,6 +1537,7 @@ int set_smem_limits(const SmemNeeds& s) {
         CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_smat1), s.smat));
         CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_smat2), s.smat));
     }
+    if (s.smat_sym) CEL_TRY(raise_dyn_smem(reinterpret_cast<const void*>(rcwa_sym_smat), s.smat_sym));
     return CELERIS_OK;
 }
 
@@ -1398,25 +1565,30 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
     rcwa_build_M<<<nc, T[ST_BUILD], 0, st>>>(b, b.ng > 0 ? 1 : 0);
     if (ev) cudaEventRecord(ev[2], st);
     if (b.sym) {
-        // the four parity classes: project, two eigen-stage buckets (sizes m[0],
-        // m[1], two matrices per cell each), expand into W and q
+        // the two excited parity classes: project, eigen-stages (two matrices
+        // of order m[0] per cell), the class S-matrix, expand into the
+        // epilogue's vectors
         rcwa_sym_project<<<nc, T[ST_HESS], 0, st>>>(b);
-        Bucket e[2] = {sym_eig_bucket(b, 0), sym_eig_bucket(b, 1)};
-        for (int k = 0; k < 2; ++k) {
-            cudaMemsetAsync(e[k].info, 0, sizeof(int) * e[k].ncell, st);
-            const int m = e[k].n;
-            if (m <= kSmemEigMaxN)
-                rcwa_hess<true><<<e[k].ncell, T[ST_HESS], ((size_t)m * m + 2 * m) * sizeof(cplx), st>>>(e[k]);
-            else
-                rcwa_hess<false><<<e[k].ncell, T[ST_HESS], hess_stage_bytes(m), st>>>(e[k]);
-        }
+        const Bucket e = sym_eig_bucket(b, 0);
+        cudaMemsetAsync(e.info, 0, sizeof(int) * e.ncell, st);
+        const int m = e.n;
+        if (m <= kSmemEigMaxN)
+            rcwa_hess<true><<<e.ncell, T[ST_HESS], ((size_t)m * m + 2 * m) * sizeof(cplx), st>>>(e);
+        else
+            rcwa_hess<false><<<e.ncell, T[ST_HESS], hess_stage_bytes(m), st>>>(e);
         if (ev) cudaEventRecord(ev[3], st);
-        for (int k = 0; k < 2; ++k)
-            rcwa_schur<<<e[k].ncell, kSchurThreads, schur_smem(e[k].ncell), st>>>(e[k]);
+        rcwa_schur<<<e.ncell, kSchurThreads, schur_smem(e.ncell), st>>>(e);
         if (ev) cudaEventRecord(ev[4], st);
-        for (int k = 0; k < 2; ++k) rcwa_vec<<<e[k].ncell, T[ST_VEC], 0, st>>>(e[k]);
-        rcwa_sym_expand<<<nc, T[ST_VEC], 0, st>>>(b);
+        rcwa_vec<<<e.ncell, T[ST_VEC], 0, st>>>(e);
+        if (ev) cudaEventRecord(ev[5], st);
+        rcwa_sym_smat<<<e.ncell, T[ST_SMAT1], lu_stage_bytes(m), st>>>(b);
+        if (ev) cudaEventRecord(ev[6], st);
+        rcwa_sym_expand<<<nc, T[ST_SMAT2], 0, st>>>(b);
+        if (ev) cudaEventRecord(ev[7], st);
+        rcwa_epilogue<<<nc, T[ST_EPI], 0, st>>>(b);
+        if (ev) cudaEventRecord(ev[8], st);
         count_launch(8);
+        return;
     } else if (n <= kSmemEigMaxN) {
         const size_t sm = ((size_t)n * n + 2 * n) * sizeof(cplx);
         rcwa_hess<true><<<nc, T[ST_HESS], sm, st>>>(b);
@@ -1427,13 +1599,11 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
         if (ev) cudaEventRecord(ev[3], st);
         rcwa_schur<<<nc, kSchurThreads, schur_smem(nc), st>>>(b);
     }
-    if (!b.sym) {
-        if (ev) cudaEventRecord(ev[4], st);
-        rcwa_vec<<<nc, T[ST_VEC], 0, st>>>(b);
-    }
+    if (ev) cudaEventRecord(ev[4], st);
+    rcwa_vec<<<nc, T[ST_VEC], 0, st>>>(b);
     if (ev) cudaEventRecord(ev[5], st);
     if (eig_only) {
-        count_launch(b.sym ? 1 : 4);
+        count_launch(4);
         return;
     }
     const size_t sm_stage = lu_stage_bytes(n);
@@ -1443,7 +1613,7 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
     if (ev) cudaEventRecord(ev[7], st);
     rcwa_epilogue<<<nc, T[ST_EPI], 0, st>>>(b);
     if (ev) cudaEventRecord(ev[8], st);
-    count_launch(b.sym ? 4 : 7);
+    count_launch(7);
 }
 
 // Time each stage at every candidate size on (up to) the first 2 x SMs cells
@@ -1572,7 +1742,7 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
         p.n = 2 * p.N;
         if (p.ng > 0 && laurent_smem(p.Mx, p.My, p.ng) + 1024 > (size_t)smem_optin)
             return set_error(CELERIS_ERR_TOO_LARGE, "raster %d with M=(%d,%d) exceeds shared memory", p.ng, p.Mx, p.My);
-        p.per_cell = per_cell_bytes(p.n, nexc) + (p.sym ? sym_per_cell_bytes(p.Mx, p.My) : 0);
+        p.per_cell = p.sym ? sym_per_cell_bytes(p.Mx, p.My, nexc) : per_cell_bytes(p.n, nexc);
         // split buckets that alone exceed the budget
         const size_t max_cells = std::max<size_t>(1, budget / std::max<size_t>(1, p.per_cell));
         for (size_t c0 = 0; c0 < kv.second.size(); c0 += max_cells) {
@@ -1655,13 +1825,15 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
             b.s_n = (size_t)p.n;
             CellDev* dcells = static_cast<CellDev*>(ws.take(sizeof(CellDev) * nc));
             b.cells = dcells;
+            // full-order buffers: the class path needs only H, Z, X (M and
+            // build_M's products) besides the Fourier operators and vectors
             cplx** mats[] = {&b.H, &b.Z, &b.X, &b.W, &b.A, &b.T11, &b.T11lu, &b.T12};
-            for (cplx** m : mats) *m = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_nn * nc));
-            b.S12 = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_ns * nc));
+            for (int k = 0; k < (p.sym ? 3 : 8); ++k) *mats[k] = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_nn * nc));
+            if (!p.sym) b.S12 = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_ns * nc));
             b.Einv = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_NN * nc));
             b.Exx = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_NN * nc));
             b.Eyy = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_NN * nc));
-            b.q1 = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_n * nc));
+            if (!p.sym) b.q1 = static_cast<cplx*>(ws.take(sizeof(cplx) * b.s_n * nc));
             b.vec = static_cast<cplx*>(ws.take(sizeof(cplx) * 10 * b.s_n * nc));
             b.piv = static_cast<int*>(ws.take(sizeof(int) * b.s_n * nc));
             b.info = static_cast<int*>(ws.take(sizeof(int) * nc));
@@ -1673,14 +1845,19 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
             b.sym = p.sym;
             b.sym_tol = symmetry_tolerance();
             if (p.sym) {
-                for (int k = 0; k < 2; ++k) {
-                    const size_t m = (size_t)sym_class_size(p.Mx, p.My, 2 * k);
-                    b.m[k] = (int)m;
-                    cplx** sm[] = {&b.sH[k], &b.sZ[k], &b.sX[k], &b.sW[k], &b.sA[k]};
-                    for (cplx** x : sm) *x = static_cast<cplx*>(ws.take(sizeof(cplx) * m * m * 2 * nc));
-                    b.sq[k] = static_cast<cplx*>(ws.take(sizeof(cplx) * m * 2 * nc));
-                    b.sinfo[k] = static_cast<int*>(ws.take(sizeof(int) * 2 * nc));
-                }
+                // the two excited classes (order m[0]), two matrices per cell
+                const size_t m = (size_t)sym_class_size(p.Mx, p.My, 0), mm = m * m * 2 * nc;
+                b.m[0] = (int)m;
+                b.m[1] = sym_class_size(p.Mx, p.My, 2);
+                cplx** sm[] = {&b.sH[0], &b.sZ[0], &b.sX[0], &b.sW[0], &b.sA[0]};
+                for (cplx** x : sm) *x = static_cast<cplx*>(ws.take(sizeof(cplx) * mm));
+                b.sq[0] = static_cast<cplx*>(ws.take(sizeof(cplx) * m * 2 * nc));
+                b.sinfo[0] = static_cast<int*>(ws.take(sizeof(int) * 2 * nc));
+                cplx** cm[] = {&b.cKp, &b.cC0, &b.cKs, &b.cA, &b.cT11, &b.cT11lu, &b.cT12, &b.cQ, &b.cSQ, &b.cCm};
+                for (cplx** x : cm) *x = static_cast<cplx*>(ws.take(sizeof(cplx) * mm));
+                b.cS12 = static_cast<cplx*>(ws.take(sizeof(cplx) * m * (m + 1) * 2 * nc));
+                b.cvec = static_cast<cplx*>(ws.take(sizeof(cplx) * 8 * m * 2 * nc));
+                b.cpiv = static_cast<int*>(ws.take(sizeof(int) * m * 2 * nc));
             }
             hdesc[w] = reinterpret_cast<CellDev*>(pin);
             pin += celeris_rt::align256(sizeof(CellDev) * nc);
@@ -1787,7 +1964,7 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                     cudaMemcpyAsync(const_cast<CellDev*>(p.b.cells), hdesc[w], sizeof(CellDev) * nc,
                                     cudaMemcpyHostToDevice, bs);
                     launch_bucket(p.b, cfgs[w], bs, nullptr);
-                    nk += (p.ng > 0 ? 3 : 1) + (p.sym ? 12 : 7);
+                    nk += (p.ng > 0 ? 3 : 1) + (p.sym ? 8 : 7);
                     cudaMemcpyAsync(hres_pin[w], p.b.res, sizeof(celeris_rcwa_result) * nexc * nc,
                                     cudaMemcpyDeviceToHost, bs);
                     cudaMemcpyAsync(hinfo_pin[w], p.b.info, sizeof(int) * nc, cudaMemcpyDeviceToHost, bs);

@@ -399,7 +399,7 @@ __global__ void __launch_bounds__(kThreads, 3) rs_f32c_kernel(const float4* __re
     const f32x2 Z2P = dup2(z2);
     const f32x2 NZ = dup2(-z), Z2X = dup2(2.0f * z), NHALF = dup2(-0.5f);
     const f32x2 Z2L = dup2(2.0f * zl);
-    const f32x2 ILHI = dup2(il_hi), NILHI = dup2(-il_hi), ILLO = dup2(il_lo), MAGIC = dup2(kMagic);
+    const f32x2 ILHI = dup2(il_hi), ILLO = dup2(il_lo), MAGIC = dup2(kMagic);
     const f32x2 TWOPI = dup2(6.28318530717958647692f);
 
     TilePipe<float4, kTile32> pipe;
@@ -440,17 +440,10 @@ __global__ void __launch_bounds__(kThreads, 3) rs_f32c_kernel(const float4* __re
                     const f32x2 gg = ZLO ? fma2(d0, d0, fma2(Z2X, d0, fma2(Z2L, d0, ns)))
                                          : fma2(d0, d0, fma2(Z2X, d0, ns));
                     const f32x2 d = fma2(mul2(gg, ri), NHALF, d0);
-                    // phase in turns, (R - z)/lambda + arg(t)/2pi (k z is added in
-                    // FP64), reduced without rounding its integer part into the
-                    // fraction: p = d hi rounded (kept negated), r = d hi - p exactly
-                    // (fma), the integer nearest p removed exactly, then the small
-                    // parts r + d lo + psi added: the fraction carries ~u turns of
-                    // rounding instead of ~u |p|
-                    const f32x2 np = mul2(d, NILHI);                      // -p
-                    const f32x2 rp = fma2(d, ILHI, np);                   // d hi - p, exact
-                    const f32x2 t = add2(rp, fma2(d, ILLO, RW));          // rp + d lo + psi
-                    const f32x2 w = sub2(MAGIC, add2(np, MAGIC));         // round(p)
-                    const f32x2 ang = mul2(sub2(t, add2(np, w)), TWOPI);  // 2 pi (p - round(p) + t), |.| <= 2 pi
+                    // phase in turns: (R - z)/lambda + arg(t)/2pi; k z is added in FP64
+                    const f32x2 th = fma2(d, ILHI, fma2(d, ILLO, RW));
+                    const f32x2 w = sub2(MAGIC, add2(th, MAGIC));         // -(th rounded to an integer)
+                    const f32x2 ang = mul2(add2(th, w), TWOPI);           // in [-pi, pi]
                     const f32x2 a = mul2(RZ, ri);                         // |t| / R
                     float aa, ab;
                     upk2(ang, aa, ab);
@@ -785,22 +778,23 @@ __global__ void rs_check_kernel(const double4* __restrict__ rec, int npil, Geom 
 // pixel from its thread's base. With the pillar's offset (xo, yo) from the
 // FP32 origin and the window's largest pixel offset w, dxm = xo + w and dym =
 // yo + w bound |dx|, |dy|, rho^2 <= dxm^2 + dym^2 and delta = R - z <= dmax.
-// Random part (depends on each pillar's own coordinates): the FP32 rounding of
-// the pillar's x, y (u xo, u yo) and of base - x, fy - y (which can only drop
-// bits of x, y: u dxm, u dym) moves rho^2 by at most 4u (dxm^2 + dym^2), its
-// assembly rounds by at most 4u (dxm^2 + dym^2) more; R - z moves by that /
-// (2|z|); the Newton step adds u dmax (1 + dmax / 2|z|) and the quadratic
-// remainder of its seed (rsqrt.approx); the amplitude |t|/R rounds with 6u:
-//   e_R(j)  = 2 pi dDelta / lambda + 6u
+// Random part (roundings whose error depends on each pillar's own data): the
+// FP32 rounding of the pillar's x, y (u xo, u yo) and of base - x, fy - y
+// (which can only drop bits of x, y: u dxm, u dym) moves rho^2 by at most
+// 4u (dxm^2 + dym^2), its assembly rounds by at most 4u (dxm^2 + dym^2) more;
+// R - z moves by that / (2|z|); the Newton step adds u dmax (1 + dmax / 2|z|)
+// and the quadratic remainder of its seed (rsqrt.approx); the phase in turns
+// th = d hi + (d lo + psi) rounds with u (dmax/lambda + 1/2) plus u for psi and
+// the inner sum (its low bits come from d, i.e. from the pillar's own R - z),
+// the reduced angle with u pi; the amplitude |t|/R rounds with 6u:
+//   e_R(j)  = 2 pi (dDelta/lambda + u (dmax/lambda + 1/2) + u) + u pi + 6u
 // Systematic part (the same for many pillars, so it can add up coherently near
 // a focus where the phases of all terms agree), summed without cancellation:
-// the phase reduction (psi rounded to FP32, d lo + psi, rp + that, the reduced
-// fraction of magnitude <= 1 turn: 3u turns; the product with 2 pi_f: u 2 pi
-// and |2 pi_f - 2 pi|), the MUFU approximations, the FP32 rounding of the
-// pixel's offsets (u cmax in x, u G in y: a shift of the pixel), and what is
-// left of the rounding of z once it is carried as a float pair z_f + z_l
-// (dz = |z - z_f - z_l|, ~u^2 |z|):
-//   e_D(j)  = kRsqrtRelErr + sqrt(2) kSinCosAbsErr + 2 pi 4u + |2 pi_f - 2 pi|
+// the MUFU approximations, the 2 pi_f constant (|2 pi_f - 2 pi| / 2 on a
+// fraction <= 1/2), the FP32 rounding of the pixel's offsets (u cmax in x, u G
+// in y: a shift of the pixel), and what is left of the rounding of z once it is
+// carried as a float pair z_f + z_l (dz = |z - z_f - z_l|, ~u^2 |z|):
+//   e_D(j)  = kRsqrtRelErr + sqrt(2) kSinCosAbsErr + |2 pi_f - 2 pi| / 2
 //             + k u (cmax dxm + G dym) / |z| + dz / |z| + k dz rho_max^2 / (2 z^2)
 // Every term has magnitude a_j = |t_j| / R <= |t_j| / |z|. acc (doubles):
 // [0] sum_j a_j e_D(j), [1] sum_j (a_j e_R(j))^2, [2] bits of max_j a_j,
@@ -820,7 +814,7 @@ __global__ void ff_bound_kernel(const double* __restrict__ px, const double* __r
     const double cmax = 0.5 * G + (kPPT32 - 1) * pstep;
     const double two_pi_f = (double)6.28318530717958647692f;
     const double eD0 = celeris_dev::kRsqrtRelErr + 1.4142135623730951 * celeris_dev::kSinCosAbsErr +
-                       2.0 * pi * 4.0 * u + fabs(two_pi_f - 2.0 * pi) + dz / z;
+                       0.5 * fabs(two_pi_f - 2.0 * pi) + dz / z;
     double sD = 0.0, sR = 0.0, sA = 0.0, amax = 0.0;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < npil; j += gridDim.x * blockDim.x) {
         const double2 t = pt[j];
@@ -831,7 +825,7 @@ __global__ void ff_bound_kernel(const double* __restrict__ px, const double* __r
         const double dmax = rho2 / (R + z);
         const double seed = R * (celeris_dev::kRsqrtRelErr + 4.0 * u);
         const double dDelta = 8.0 * u * rho2 / (2.0 * z) + u * dmax * (1.0 + dmax / (2.0 * z)) + seed * seed / z;
-        const double eR = 2.0 * pi * dDelta / lam + 6.0 * u;
+        const double eR = 2.0 * pi * (dDelta / lam + u * (dmax / lam + 0.5) + u) + u * pi + 6.0 * u;
         const double eD = eD0 + k * u * (cmax * dxm + G * dym) / z + k * dz * rho2 / (2.0 * z * z);
         sD += a * eD;
         sR += (a * eR) * (a * eR);

@@ -156,10 +156,10 @@ extern "C" int celeris_probe_mufu_accuracy(double* measured, double* model) {
     unsigned long long* d = nullptr;
     CEL_CUDA(cudaMalloc(&d, 4 * sizeof(unsigned long long)));
     CEL_CUDA(cudaMemset(d, 0, 4 * sizeof(unsigned long long)));
-    const float range_f = 6.2840f;  // the precision form's reduced angles: |ang| <= 2 pi (1 + 2e-6)
-    uint32_t range_bits;
-    memcpy(&range_bits, &range_f, sizeof(range_bits));
-    probe_sincos_exhaustive<<<sms * 16, 256>>>(range_bits, d);
+    const float pi_f = 3.14159265358979323846f;  // the precision form's reduced angles: |ang| <= pi_f
+    uint32_t pi_bits;
+    memcpy(&pi_bits, &pi_f, sizeof(pi_bits));
+    probe_sincos_exhaustive<<<sms * 16, 256>>>(pi_bits, d);
     const float lo_f = 0x1p-10f, hi_f = 0x1p30f;
     uint32_t lo_bits, hi_bits;
     memcpy(&lo_bits, &lo_f, sizeof(lo_bits));

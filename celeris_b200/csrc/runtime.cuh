@@ -106,8 +106,8 @@ constexpr uint32_t kSpinLimit = 1u << 26;
 // Accuracy model of the MUFU approximations in the precision-form far-field
 // terms; the error bound that form states rests on these two figures:
 //   kSinCosAbsErr  max |sin.approx.ftz.f32(x) - sin(x)| (and the same for cos)
-//                  over every FP32 x in [-6.284, 6.284] (the kernel's reduced
-//                  phase range, |x| <= 2 pi (1 + 2e-6))
+//                  over every FP32 x in [-pi_f, pi_f], pi_f = 3.14159274f (the
+//                  kernel's reduced phase range)
 //   kRsqrtRelErr   max |rsqrt.approx.ftz.f32(x) sqrt(x) - 1| over every normal
 //                  FP32 x in [2^-10, 2^30)
 // celeris_probe_mufu_accuracy measures both exhaustively on the current device

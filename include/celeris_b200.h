@@ -81,7 +81,7 @@ int celeris_probe_dmma(double* fma_per_s);
 /* New: measured accuracy of the MUFU approximations the precision-form
  * far-field uses, over EVERY FP32 input of their ranges on the current device:
  * measured[0] = max |sin.approx(x) - sin(x)| and measured[1] the same for cos,
- * over all x in [-6.284, 6.284]; measured[2] = max |rsqrt.approx(x) sqrt(x) - 1|
+ * over all x in [-pi_f, pi_f]; measured[2] = max |rsqrt.approx(x) sqrt(x) - 1|
  * over all x in [2^-10, 2^30) (references in FP64). model[0..2] receive the
  * figures the stated error bound of the precision form assumes for the same
  * three quantities; the bound is valid on a device where measured <= model. */

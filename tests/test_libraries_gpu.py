@@ -209,10 +209,17 @@ def test_jones_hwp_atom_and_rotated_pb_check():
     assert np.max(np.abs(got - Jw)) <= 1e-10 * np.max(np.abs(Jw))
     a = cel.find_hwp_atom(pil, bg, inc, sub, 0.4, 0.633, 0.6, 0.2, 0.8, 4, 3)
     aw = OL.find_hwp_atom((N_PIL, N_BG, N_INC, N_SUB), 0.4, 0.633, 0.6, 0.2, 0.8, 4, 3)
-    assert (a.fill_x, a.fill_y) == (aw["fill_x"], aw["fill_y"])
-    assert abs(a.t_x - aw["t_x"]) <= 1e-9 and abs(a.t_y - aw["t_y"]) <= 1e-9
     assert a.conversion_efficiency == pytest.approx(aw["efficiency"], abs=1e-9)
-    assert a.retardance_deg == pytest.approx(aw["retardance"], abs=1e-7)
+    if (a.fill_x, a.fill_y) == (aw["fill_x"], aw["fill_y"]):
+        assert abs(a.t_x - aw["t_x"]) <= 1e-9 and abs(a.t_y - aw["t_y"]) <= 1e-9
+        assert a.retardance_deg == pytest.approx(aw["retardance"], abs=1e-7)
+    else:
+        # on a square period the atom and its x <-> y mirror image convert exactly
+        # equally (|t_x - t_y| is symmetric), so the reference's first-maximum
+        # rule (pb_metalens.cpp:57-72) meets an exact tie that rounding breaks
+        assert (a.fill_x, a.fill_y) == (aw["fill_y"], aw["fill_x"])
+        assert abs(a.t_x - aw["t_y"]) <= 1e-9 and abs(a.t_y - aw["t_x"]) <= 1e-9
+        assert a.retardance_deg == pytest.approx(-aw["retardance"], abs=1e-7)
     rots = [0.0, 0.3, 0.7, 1.2]
     v = cel.verify_pb_phase(pil, bg, inc, sub, 0.4, 0.633, a, rots, 2)
     vw = OL.verify_pb_phase((N_PIL, N_BG, N_INC, N_SUB), 0.4, 0.633, a.fill_x, a.fill_y, 0.6, rots, 2)

@@ -384,30 +384,41 @@ __device__ void blk_gemm(int m, int n, int k, cplx alpha, const cplx* A, int lda
 }
 
 // ---- rank-1 update ----------------------------------------------------------------------
-// A[i][j] -= x[i] * y[j] (or * conj(y[j])) for i < rows, j < cols. Each thread
-// first loads kU elements of A, then updates and stores them, so kU loads per
-// thread are in flight at once (a load-use-store loop would wait on every load,
-// the compiler being unable to move loads past stores to the same array).
-// x and y are shared-memory vectors.
-constexpr int kU = 8;
+// A[i][j] -= x[i] * y[j] (or * conj(y[j])) for i < rows, j < cols. Warps take
+// rows, lanes take columns (32 apart, up to 128 columns per pass, y held in
+// registers for the pass); each warp loads two rows' elements before it stores
+// any (a load-use-store loop would wait on every load, the compiler being
+// unable to move loads past stores to the same array), so up to 8 loads per
+// thread are in flight, and no index is divided.
+// x and y are shared-memory vectors that do not overlap A.
 template <bool CONJ_Y>
 __device__ __forceinline__ void blk_rank1(int rows, int cols, cplx* A, int lda, const cplx* x, const cplx* y) {
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int total = rows * cols;
-    for (int e0 = tid; e0 < total; e0 += kU * nt) {
-        cplx v[kU];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int j0 = 0; j0 < cols; j0 += 128) {
+        cplx yy[4];
+        bool ok[4];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            const int e = e0 + u * nt;
-            if (e < total) v[u] = A[(size_t)(e / cols) * lda + (e % cols)];
+        for (int u = 0; u < 4; ++u) {
+            const int j = j0 + 32 * u + lane;
+            ok[u] = j < cols;
+            yy[u] = ok[u] ? (CONJ_Y ? cconj(y[j]) : y[j]) : C(0.0, 0.0);
         }
+        for (int i = warp; i < rows; i += 2 * nwarp) {
+            const int i2 = i + nwarp;
+            const bool two = i2 < rows;
+            cplx* r1 = A + (size_t)i * lda + j0 + lane;
+            cplx* r2 = A + (size_t)(two ? i2 : i) * lda + j0 + lane;
+            cplx a[4], c[4];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            const int e = e0 + u * nt;
-            if (e < total) {
-                const int i = e / cols, j = e % cols;
-                const cplx yy = CONJ_Y ? cconj(y[j]) : y[j];
-                A[(size_t)i * lda + j] = cfms(x[i], yy, v[u]);
+            for (int u = 0; u < 4; ++u) {
+                if (ok[u]) a[u] = r1[32 * u];
+                if (ok[u] && two) c[u] = r2[32 * u];
+            }
+            const cplx x1 = x[i], x2 = two ? x[i2] : C(0.0, 0.0);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (ok[u]) r1[32 * u] = cfms(x1, yy[u], a[u]);
+                if (ok[u] && two) r2[32 * u] = cfms(x2, yy[u], c[u]);
             }
         }
     }

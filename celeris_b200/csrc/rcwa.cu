@@ -86,8 +86,9 @@ struct Bucket {
     // mirror-symmetric cells (sym != 0): the eigenproblem solved in its four
     // parity classes; size class k (0: classes (+,+) and (-,-), 1: (+,-) and
     // (-,+)) holds two m[k] x m[k] matrices per cell, matrix 2 cell + j
-    int sym;
-    double sym_tol;  // largest mirror asymmetry of M (relative to max |M|) the class split accepts
+    int sym;         // 0: full path; 1: both excited classes; 2: also C4-symmetric (one class)
+    int ncls, cls0;  // excited classes solved per cell (2, or 1 = class 1 only) and the first one
+    double sym_tol;  // largest asymmetry of M (relative to max |M|) the class split accepts
     int m[2];
     cplx *sH[2], *sZ[2], *sX[2], *sW[2], *sA[2], *sq[2];
     int* sinfo[2];
@@ -991,7 +992,11 @@ __global__ void __launch_bounds__(kRT) rcwa_epilogue(Bucket b) {
 // full W unchanged, so t, R and T are those of the full eigensolve up to
 // rounding. A cell whose M is not mirror symmetric to rounding (a raster
 // sample falling exactly on a shape boundary one way and not the other) is
-// flagged kInfoAsym and solved again by the full eigensolve.
+// flagged kInfoAsym and solved again by the full eigensolve. When the cell is
+// also symmetric under the 90 degree rotation R (square period, Mx = My,
+// fill_x = fill_y), R commutes with every operator and maps the X excitation
+// onto the Y excitation, so only the X class is solved and the Y solution is R
+// applied to the X one (a cell that fails that check to rounding is flagged too).
 constexpr int kInfoAsym = 1 << 29;
 
 // class c: 0 = (+,+), 1 = (-,-), 2 = (+,-), 3 = (-,+)
@@ -1029,11 +1034,6 @@ __device__ int sym_vector(int Mx, int My, int c, int i, int* idx, double* coef) 
             ++k;
         }
     return k;
-}
-
-__device__ __forceinline__ cplx* sym_mat(const Bucket& b, cplx* const* base, int c, int cell) {
-    const int k = c >> 1, m = b.m[k];
-    return base[k] + (size_t)(2 * cell + (c & 1)) * m * m;
 }
 
 // Entry (k, l) of a per-order block operator of a homogeneous half-space
@@ -1106,11 +1106,46 @@ __global__ void __launch_bounds__(kRT) rcwa_sym_project(Bucket b) {
         }
         if (!(fmax(a, c) <= b.sym_tol * m) && b.info[cell] == 0) b.info[cell] = kInfoAsym;
     }
+    if (b.ncls == 1) {
+        // C4 (90 degree rotation R: order (p, q) -> (-q, p), u' = -v, v' = u)
+        // must commute with M too: M[rho k][rho l] = sigma(k) sigma(l) M[k][l]
+        double dr = 0.0, mr = 0.0;
+        for (int e = tid; e < n * n; e += nt) {
+            const int k = e / n, l = e % n;
+            const int bk = k / N, ok = k % N, bl = l / N, ol = l % N;
+            const int pk = ok / ny - Mx, qk = ok % ny - My, pl = ol / ny - Mx, ql = ol % ny - My;
+            const int rk = (1 - bk) * N + (-qk + Mx) * ny + (pk + My);
+            const int rl = (1 - bl) * N + (-ql + Mx) * ny + (pl + My);
+            const double sgn = ((bk == 1) != (bl == 1)) ? -1.0 : 1.0;
+            const cplx v = H[e];
+            dr = fmax(dr, cabs(csub(H[(size_t)rk * n + rl], cscale(v, sgn))));
+            mr = fmax(mr, cabs(v));
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            dr = fmax(dr, __shfl_down_sync(0xffffffffu, dr, o));
+            mr = fmax(mr, __shfl_down_sync(0xffffffffu, mr, o));
+        }
+        __syncthreads();
+        if ((tid & 31) == 0) {
+            red[0][tid >> 5] = dr;
+            red[2][tid >> 5] = mr;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double a = 0.0, m = 0.0;
+            for (int w = 0; w < nt / 32; ++w) {
+                a = fmax(a, red[0][w]);
+                m = fmax(m, red[2][w]);
+            }
+            if (!(a <= b.sym_tol * m) && b.info[cell] == 0) b.info[cell] = kInfoAsym;
+        }
+    }
     // P_c^T X P_c for X = M, the layer kp and the two half-space operators
     const double w2 = cd.omega * cd.omega;
     const int m = b.m[0];
-    for (int c = 0; c < 2; ++c) {
-        const size_t mi = (size_t)(2 * cell + c) * m * m;
+    for (int cc = 0; cc < b.ncls; ++cc) {
+        const int c = b.cls0 + cc;
+        const size_t mi = (size_t)(b.ncls * cell + cc) * m * m;
         cplx* Mc = b.sH[0] + mi;
         cplx* Kp = b.cKp + mi;
         cplx* C0 = b.cC0 + mi;
@@ -1159,7 +1194,7 @@ __global__ void __launch_bounds__(kRT) rcwa_sym_smat(Bucket b) {
     cplx* stg = reinterpret_cast<cplx*>(smem);
     __shared__ GemmSmem gs;
     __shared__ RedScratch rs;
-    const int mi = blockIdx.x, cell = mi >> 1, c = mi & 1;
+    const int mi = blockIdx.x, cell = mi / b.ncls, c = b.cls0 + mi % b.ncls;
     const CellDev cd = b.cells[cell];
     const int m = b.m[0], N = b.N, Mx = b.Mx, My = b.My;
     const int tid = threadIdx.x, nt = blockDim.x;
@@ -1249,13 +1284,13 @@ __global__ void __launch_bounds__(kRT) rcwa_sym_smat(Bucket b) {
 // the cell's info (it is the cause of any later singular pivot).
 __global__ void __launch_bounds__(kRT) rcwa_sym_expand(Bucket b) {
     const int cell = blockIdx.x;
-    const int n = b.n, Mx = b.Mx, My = b.My, m = b.m[0];
+    const int N = b.N, n = b.n, Mx = b.Mx, My = b.My, m = b.m[0], ny = 2 * My + 1;
     const int tid = threadIdx.x, nt = blockDim.x;
     cplx* vec = at(b.vec, 10 * b.s_n, cell);
     for (int e = tid; e < 4 * (int)b.s_n; e += nt) vec[e] = C(0.0, 0.0);
     __syncthreads();
-    for (int c = 0; c < 2; ++c) {
-        const int mi = 2 * cell + c;
+    for (int cc = 0; cc < b.ncls; ++cc) {
+        const int c = b.cls0 + cc, mi = b.ncls * cell + cc;
         const cplx* cv = b.cvec + (size_t)mi * 8 * m;
         cplx* dst_a = vec + (c == 1 ? 0 : b.s_n);       // aN_X : aN_Y
         cplx* dst_b = vec + (c == 1 ? 2 : 3) * b.s_n;   // b0_X : b0_Y
@@ -1269,10 +1304,23 @@ __global__ void __launch_bounds__(kRT) rcwa_sym_expand(Bucket b) {
             }
         }
     }
-    (void)n;
+    if (b.ncls == 1) {
+        // C4-symmetric cell: the Y solution is the X solution rotated by 90
+        // degrees, R e_k = sigma(k) e_{rho k}: rho(u at (p, q)) = v at (-q, p)
+        // with sigma = +1, rho(v at (p, q)) = u at (-q, p) with sigma = -1
+        __syncthreads();
+        for (int k = tid; k < n; k += nt) {
+            const int bk = k / N, ok = k % N;
+            const int pk = ok / ny - Mx, qk = ok % ny - My;
+            const int rk = (1 - bk) * N + (-qk + Mx) * ny + (pk + My);
+            const double sg = bk == 1 ? -1.0 : 1.0;
+            vec[b.s_n + rk] = cscale(vec[k], sg);
+            vec[3 * b.s_n + rk] = cscale(vec[2 * b.s_n + k], sg);
+        }
+    }
     if (tid == 0 && b.info[cell] != kInfoAsym) {
-        for (int c = 0; c < 2; ++c) {
-            const int e = b.sinfo[0][2 * cell + c];
+        for (int cc = 0; cc < b.ncls; ++cc) {
+            const int e = b.sinfo[0][b.ncls * cell + cc];
             if (e != 0) {
                 b.info[cell] = e;
                 break;
@@ -1289,7 +1337,7 @@ Bucket sym_eig_bucket(const Bucket& b, int k) {
     e.My = b.My;
     e.n = b.m[k];
     e.N = e.n / 2;
-    e.ncell = 2 * b.ncell;
+    e.ncell = b.ncls * b.ncell;
     e.cells = b.cells;
     e.H = b.sH[k];
     e.Z = b.sZ[k];
@@ -1384,7 +1432,11 @@ HostCell make_cell(const celeris_rcwa_cell& c, int index, double ex_re, double e
     // reference raster size max(128, 8(2 max(Mx, My) + 1)) (rcwa2d.cpp:337)
     h.ng = plain_rect ? 0 : (c.grid > 0 ? c.grid : std::max(128, 8 * (2 * std::max(c.Mx, c.My) + 1)));
     h.index = index;
-    h.sym = sym_eligible(c) ? 1 : 0;
+    // 2: also symmetric under the 90 degree rotation (square period, Mx = My,
+    // fill_x = fill_y; every shape of rcwa2d.cpp:37-72 is then C4 symmetric):
+    // the Y solution is the rotated X solution and one class is solved
+    h.sym = !sym_eligible(c) ? 0
+            : (c.period_x_um == c.period_y_um && c.Mx == c.My && c.fill_x == c.fill_y) ? 2 : 1;
     return h;
 }
 
@@ -1467,13 +1519,13 @@ size_t per_cell_bytes(int n, int nexc) {
 // operators, the vector area and pivots; per excited class (two per cell) the
 // eigen-stage matrices H, Z, X, W, scratch, q and info, and the class S-matrix's
 // ten m x m matrices, S12 (m x (m + 1)), 8 m vector entries and m pivots.
-size_t sym_per_cell_bytes(int Mx, int My, int nexc) {
+size_t sym_per_cell_bytes(int Mx, int My, int nexc, int ncls) {
     const int N = (2 * Mx + 1) * (2 * My + 1), n = 2 * N;
     const size_t m = (size_t)sym_class_size(Mx, My, 0);
     const size_t full = (3 * (size_t)n * n + 3 * (size_t)N * N + 10 * (size_t)n) * sizeof(cplx) +
                         (size_t)n * sizeof(int) + sizeof(int) + sizeof(celeris_rcwa_result) * nexc + sizeof(CellDev);
-    const size_t cls = 2 * ((5 * m * m + m) * sizeof(cplx) + sizeof(int)) +
-                       2 * ((10 * m * m + m * (m + 1) + 8 * m) * sizeof(cplx) + m * sizeof(int));
+    const size_t cls = ncls * (((5 * m * m + m) * sizeof(cplx) + sizeof(int)) +
+                               ((10 * m * m + m * (m + 1) + 8 * m) * sizeof(cplx) + m * sizeof(int)));
     return full + cls + 32 * 256;
 }
 
@@ -1742,7 +1794,7 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
         p.n = 2 * p.N;
         if (p.ng > 0 && laurent_smem(p.Mx, p.My, p.ng) + 1024 > (size_t)smem_optin)
             return set_error(CELERIS_ERR_TOO_LARGE, "raster %d with M=(%d,%d) exceeds shared memory", p.ng, p.Mx, p.My);
-        p.per_cell = p.sym ? sym_per_cell_bytes(p.Mx, p.My, nexc) : per_cell_bytes(p.n, nexc);
+        p.per_cell = p.sym ? sym_per_cell_bytes(p.Mx, p.My, nexc, p.sym == 2 ? 1 : 2) : per_cell_bytes(p.n, nexc);
         // split buckets that alone exceed the budget
         const size_t max_cells = std::max<size_t>(1, budget / std::max<size_t>(1, p.per_cell));
         for (size_t c0 = 0; c0 < kv.second.size(); c0 += max_cells) {
@@ -1846,18 +1898,21 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
             b.sym_tol = symmetry_tolerance();
             if (p.sym) {
                 // the two excited classes (order m[0]), two matrices per cell
-                const size_t m = (size_t)sym_class_size(p.Mx, p.My, 0), mm = m * m * 2 * nc;
+                b.ncls = p.sym == 2 ? 1 : 2;
+                b.cls0 = p.sym == 2 ? 1 : 0;
+                const size_t nm = (size_t)b.ncls * nc;  // class matrices in the bucket
+                const size_t m = (size_t)sym_class_size(p.Mx, p.My, 0), mm = m * m * nm;
                 b.m[0] = (int)m;
                 b.m[1] = sym_class_size(p.Mx, p.My, 2);
                 cplx** sm[] = {&b.sH[0], &b.sZ[0], &b.sX[0], &b.sW[0], &b.sA[0]};
                 for (cplx** x : sm) *x = static_cast<cplx*>(ws.take(sizeof(cplx) * mm));
-                b.sq[0] = static_cast<cplx*>(ws.take(sizeof(cplx) * m * 2 * nc));
-                b.sinfo[0] = static_cast<int*>(ws.take(sizeof(int) * 2 * nc));
+                b.sq[0] = static_cast<cplx*>(ws.take(sizeof(cplx) * m * nm));
+                b.sinfo[0] = static_cast<int*>(ws.take(sizeof(int) * nm));
                 cplx** cm[] = {&b.cKp, &b.cC0, &b.cKs, &b.cA, &b.cT11, &b.cT11lu, &b.cT12, &b.cQ, &b.cSQ, &b.cCm};
                 for (cplx** x : cm) *x = static_cast<cplx*>(ws.take(sizeof(cplx) * mm));
-                b.cS12 = static_cast<cplx*>(ws.take(sizeof(cplx) * m * (m + 1) * 2 * nc));
-                b.cvec = static_cast<cplx*>(ws.take(sizeof(cplx) * 8 * m * 2 * nc));
-                b.cpiv = static_cast<int*>(ws.take(sizeof(int) * m * 2 * nc));
+                b.cS12 = static_cast<cplx*>(ws.take(sizeof(cplx) * m * (m + 1) * nm));
+                b.cvec = static_cast<cplx*>(ws.take(sizeof(cplx) * 8 * m * nm));
+                b.cpiv = static_cast<int*>(ws.take(sizeof(int) * m * nm));
             }
             hdesc[w] = reinterpret_cast<CellDev*>(pin);
             pin += celeris_rt::align256(sizeof(CellDev) * nc);

@@ -101,6 +101,16 @@ struct Bucket {
 
 __device__ __forceinline__ cplx* at(cplx* base, size_t stride, int c) { return base + stride * c; }
 
+// Mirror-symmetric cells (Bucket::sym != 0): per-cell info code of a cell found
+// not symmetric to the tolerance, which is solved again by the full path.
+constexpr int kInfoAsym = 1 << 29;
+
+// Parity classes under the two mirrors p -> -p, q -> -q.
+// class c: 0 = (+,+), 1 = (-,-), 2 = (+,-), 3 = (-,+)
+__host__ __device__ __forceinline__ int sym_class_a(int c) { return (c == 0 || c == 2) ? 1 : -1; }
+__host__ __device__ __forceinline__ int sym_class_b(int c) { return (c == 0 || c == 3) ? 1 : -1; }
+__host__ __device__ __forceinline__ int sym_count(int M, int parity) { return parity > 0 ? M + 1 : M; }
+
 __device__ __forceinline__ void order_pq(const Bucket& b, int i, int& p, int& q) {
     const int ny = 2 * b.My + 1;
     p = i / ny - b.Mx;
@@ -245,7 +255,140 @@ __global__ void rcwa_phase_table(int ng, int mmax, cplx* ph) {
     ph[e] = C(co / ng, s / ng);
 }
 
-// dynamic smem: counts [ng*ng] u8 | G1 [(4Mx+1) * ng] | Ge [(4Mx+1)(4My+1)]
+// 1 / sqrt(cnt) for cnt = 2^e, e in 0..4: the product of two orbit-vector
+// weights (1, 1/sqrt2 or 1/2 each) with no rounding beyond the one constant.
+__device__ __forceinline__ double orbit_weight(int e) {
+    return (e & 1) ? ldexp(0.70710678118654752440, -(e >> 1)) : ldexp(1.0, -(e >> 1));
+}
+
+// Position of order (p, q) in scalar parity class c: its index in the class
+// basis (orbit vectors of (|p|, |q|)) and the sign of its entry there, or
+// -1 when the orbit has no vector in that class (p = 0 in an odd-x class, or
+// q = 0 in an odd-y class). *e gains log2 of the orbit size.
+__device__ __forceinline__ int scalar_class_index(int My, int c, int p, int q, double* sgn, int* e) {
+    const int a = sym_class_a(c), bb = sym_class_b(c);
+    if ((p == 0 && a < 0) || (q == 0 && bb < 0)) return -1;
+    const int ap = abs(p), aq = abs(q);
+    *sgn = (p < 0 && a < 0 ? -1.0 : 1.0) * (q < 0 && bb < 0 ? -1.0 : 1.0);
+    *e += (ap > 0) + (aq > 0);
+    return (ap - (a > 0 ? 0 : 1)) * sym_count(My, bb) + (aq - (bb > 0 ? 0 : 1));
+}
+
+// Einv = epsT^-1 of a mirror-symmetric cell (Bucket::sym != 0). The Laurent
+// matrix epsT[(p,q)][(p',q')] = Ge[p-p'][q-q'] commutes with both mirrors when
+// Ge is even in dp and in dq, so in the scalar parity basis (unit orbit vectors
+// of (|p|, |q|) with signs a^[p<0] b^[q<0]) it is block diagonal with four blocks
+// of orders (Mx + [a>0]) (My + [b>0]). Each block is factored and inverted on
+// its own (about N^3/16 of the work of the full inverse) and Einv assembled:
+//   Einv[k][l] = sum_c s_c(k) s_c(l) B_c^-1[i_c(k)][i_c(l)].
+// A Ge that is not even to the symmetry tolerance flags the cell kInfoAsym (it
+// is solved again by the full path). work: 2 N^2 complex (blocks, then their
+// inverses); smem: the kernel's dynamic shared memory, Ge's region included.
+__device__ void laurent_inverse_by_class(const Bucket& b, int cell, const cplx* Ge, cplx* work, cplx* Einv,
+                                         unsigned char* smem, RedScratch* rs) {
+    const int Mx = b.Mx, My = b.My, N = b.N, my4 = 4 * My + 1, mx4 = 4 * Mx + 1;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    double dev = 0.0, mag = 0.0;
+    for (int e = tid; e < mx4 * my4; e += nt) {
+        const int pi = e / my4, qi = e % my4;
+        const cplx v = Ge[e];
+        dev = fmax(dev, fmax(cabs(csub(v, Ge[(mx4 - 1 - pi) * my4 + qi])), cabs(csub(v, Ge[pi * my4 + (my4 - 1 - qi)]))));
+        mag = fmax(mag, cabs(v));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        dev = fmax(dev, __shfl_down_sync(0xffffffffu, dev, o));
+        mag = fmax(mag, __shfl_down_sync(0xffffffffu, mag, o));
+    }
+    if ((tid & 31) == 0) {
+        rs->d[tid >> 5] = dev;
+        rs->d[32 + (tid >> 5)] = mag;
+    }
+    // assemble the four blocks B_c = S_c^T epsT S_c and identity right-hand sides
+    size_t off = 0;
+    for (int c = 0; c < 4; ++c) {
+        const int a = sym_class_a(c), bb = sym_class_b(c);
+        const int nb = sym_count(My, bb), s = sym_count(Mx, a) * nb;
+        cplx* B = work + off;
+        cplx* R = work + (size_t)N * N + off;
+        for (int e = tid; e < s * s; e += nt) {
+            const int i = e / s, j = e % s;
+            const int pi = i / nb + (a > 0 ? 0 : 1), qi = i % nb + (bb > 0 ? 0 : 1);
+            const int pj = j / nb + (a > 0 ? 0 : 1), qj = j % nb + (bb > 0 ? 0 : 1);
+            const double w = orbit_weight((pi > 0) + (qi > 0) + (pj > 0) + (qj > 0));
+            cplx v = C(0.0, 0.0);
+            for (int sp = 1; sp >= (pi > 0 ? -1 : 1); sp -= 2)
+                for (int sq = 1; sq >= (qi > 0 ? -1 : 1); sq -= 2)
+                    for (int tp = 1; tp >= (pj > 0 ? -1 : 1); tp -= 2)
+                        for (int tq = 1; tq >= (qj > 0 ? -1 : 1); tq -= 2) {
+                            const double sg = (sp < 0 ? a : 1) * (sq < 0 ? bb : 1) * (tp < 0 ? a : 1) * (tq < 0 ? bb : 1);
+                            const cplx g = Ge[(sp * pi - tp * pj + 2 * Mx) * my4 + (sq * qi - tq * qj + 2 * My)];
+                            v = cadd(v, cscale(g, sg));
+                        }
+            B[e] = cscale(v, w);
+            R[e] = C(i == j ? 1.0 : 0.0, 0.0);
+        }
+        off += (size_t)s * s;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double d = 0.0, m = 0.0;
+        for (int w = 0; w < nt / 32; ++w) {
+            d = fmax(d, rs->d[w]);
+            m = fmax(m, rs->d[32 + w]);
+        }
+        if (!(d < b.sym_tol * m) && b.info[cell] == 0) b.info[cell] = kInfoAsym;  // strict: tolerance 0 flags all
+    }
+    // Ge is dead: the LU staging and GEMM tiles overlay the raster region
+    cplx* stg = reinterpret_cast<cplx*>(smem);
+    GemmSmem* gs = reinterpret_cast<GemmSmem*>(stg + 2 * N + LNB * LNB);
+    int* piv = b.piv + b.s_n * cell;
+    off = 0;
+    for (int c = 0; c < 4; ++c) {
+        const int s = sym_count(Mx, sym_class_a(c)) * sym_count(My, sym_class_b(c));
+        if (s == 0) continue;
+        cplx* B = work + off;
+        const int info = blk_lu_blocked(s, B, s, piv, rs, stg, gs);
+        if (info != 0 && tid == 0 && b.info[cell] == 0) b.info[cell] = -info;
+        blk_lu_solve_blocked(s, B, s, piv, s, work + (size_t)N * N + off, s, stg, gs);
+        off += (size_t)s * s;
+    }
+    __syncthreads();
+    size_t offs[4];
+    off = 0;
+    for (int c = 0; c < 4; ++c) {
+        offs[c] = off;
+        const int s = sym_count(Mx, sym_class_a(c)) * sym_count(My, sym_class_b(c));
+        off += (size_t)s * s;
+    }
+    for (int e = tid; e < N * N; e += nt) {
+        int p, q, pp, qq;
+        order_pq(b, e / N, p, q);
+        order_pq(b, e % N, pp, qq);
+        cplx v = C(0.0, 0.0);
+        for (int c = 0; c < 4; ++c) {
+            double si, sj;
+            int ex = 0;
+            const int i = scalar_class_index(My, c, p, q, &si, &ex);
+            const int j = scalar_class_index(My, c, pp, qq, &sj, &ex);
+            if (i < 0 || j < 0) continue;
+            const int s = sym_count(Mx, sym_class_a(c)) * sym_count(My, sym_class_b(c));
+            const cplx r = work[(size_t)N * N + offs[c] + (size_t)i * s + j];
+            v = cadd(v, cscale(r, si * sj * orbit_weight(ex)));
+        }
+        Einv[e] = v;
+    }
+}
+
+// Rows of G1 in shared memory: at least 4, so that the per-axis sample tables
+// of the raster (2 x 4 ng doubles) fit in the same region.
+__host__ __device__ __forceinline__ int laurent_g1_rows(int Mx) { return 4 * Mx + 1 > 4 ? 4 * Mx + 1 : 4; }
+
+// The sample coordinate (rcwa2d.cpp:88-89) of subsample s of pixel i.
+__device__ __forceinline__ double raster_coord(int i, int s, int ng) { return (i + (s + 0.5) / 4) / ng - 0.5; }
+
+// dynamic smem: G1 [laurent_g1_rows(Mx) * ng] | Ge [(4Mx+1)(4My+1)] | counts [ng*ng] u8,
+// counts stored column-major (cnt[ix * ng + iy]) so that the row sums of G1 read
+// consecutive bytes across a warp.
 __global__ void __launch_bounds__(kRT) rcwa_fourier_laurent(Bucket b) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ RedScratch rs;
@@ -255,32 +398,84 @@ __global__ void __launch_bounds__(kRT) rcwa_fourier_laurent(Bucket b) {
     const int mx4 = 4 * b.Mx + 1, my4 = 4 * b.My + 1;
     const int tid = threadIdx.x, nt = blockDim.x;
     cplx* G1 = reinterpret_cast<cplx*>(smem);
-    cplx* Ge = G1 + (size_t)mx4 * ng;
+    cplx* Ge = G1 + (size_t)laurent_g1_rows(b.Mx) * ng;
     unsigned char* cnt = reinterpret_cast<unsigned char*>(Ge + (size_t)mx4 * my4);
-    // 4x4 supersampled inside counts (rcwa2d.cpp:82-94)
-    for (int e = tid; e < ng * ng; e += nt) {
-        const int iy = e / ng, ix = e % ng;
-        int hit = 0;
-        for (int sy = 0; sy < 4; ++sy)
-            for (int sx = 0; sx < 4; ++sx) {
-                const double xf = (ix + (sx + 0.5) / 4) / ng - 0.5;
-                const double yf = (iy + (sy + 0.5) / 4) / ng - 0.5;
-                if (inside_shape(c, xf, yf)) ++hit;
+    // 4x4 supersampled inside counts (rcwa2d.cpp:74-95). Unrotated, every shape
+    // test factors into per-axis terms: the sample coordinates (or their scaled
+    // squares) are tabulated once per axis in the G1 region, and each of a
+    // pixel's 16 samples combines one entry of each table with the reference's
+    // own roundings (u*u and v*v rounded separately, then added).
+    const double ax = c.fill_x * 0.5, ay = c.fill_y * 0.5;
+    const bool round_shape = c.shape == CELERIS_SHAPE_ELLIPSE || c.shape == CELERIS_SHAPE_RING;
+    if (c.rot != 0.0 || (round_shape && (ax <= 0.0 || ay <= 0.0))) {
+        for (int e = tid; e < ng * ng; e += nt) {
+            const int ix = e / ng, iy = e % ng;
+            int hit = 0;
+            for (int sy = 0; sy < 4; ++sy)
+                for (int sx = 0; sx < 4; ++sx)
+                    if (inside_shape(c, raster_coord(ix, sx, ng), raster_coord(iy, sy, ng))) ++hit;
+            cnt[e] = (unsigned char)hit;
+        }
+    } else {
+        double* tx = reinterpret_cast<double*>(G1);
+        double* ty = tx + 4 * ng;
+        const double hx = ax * c.shape_param, hy = ay * c.shape_param;
+        for (int t = tid; t < 4 * ng; t += nt) {
+            const double xf = raster_coord(t >> 2, t & 3, ng), yf = xf;  // square raster: one coordinate set
+            if (round_shape) {
+                const double u = xf / ax, v = yf / ay;
+                tx[t] = __dmul_rn(u, u);
+                ty[t] = __dmul_rn(v, v);
+            } else {  // bit 0: within the main half-width, bit 1: within the cross arm's
+                tx[t] = (fabs(xf) <= ax ? 1.0 : 0.0) + (fabs(xf) <= hx ? 2.0 : 0.0);
+                ty[t] = (fabs(yf) <= ay ? 1.0 : 0.0) + (fabs(yf) <= hy ? 2.0 : 0.0);
             }
-        cnt[e] = (unsigned char)hit;
+        }
+        __syncthreads();
+        const double ri2 = __dmul_rn(c.shape_param, c.shape_param);
+        for (int e = tid; e < ng * ng; e += nt) {
+            const int ix = e / ng, iy = e % ng;
+            double X[4], Y[4];
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                X[s] = tx[4 * ix + s];
+                Y[s] = ty[4 * iy + s];
+            }
+            int hit = 0;
+#pragma unroll
+            for (int sy = 0; sy < 4; ++sy)
+#pragma unroll
+                for (int sx = 0; sx < 4; ++sx) {
+                    bool in;
+                    if (round_shape) {
+                        const double r2 = __dadd_rn(X[sx], Y[sy]);
+                        in = r2 <= 1.0 && (c.shape == CELERIS_SHAPE_ELLIPSE || r2 >= ri2);
+                    } else {
+                        const int bx = (int)X[sx], by = (int)Y[sy];
+                        in = c.shape == CELERIS_SHAPE_RECT ? ((bx & by & 1) != 0)
+                                                           : (((bx >> 1) & by & 1) != 0 || ((by >> 1) & bx & 1) != 0);
+                    }
+                    hit += in ? 1 : 0;
+                }
+            cnt[e] = (unsigned char)hit;
+        }
+        __syncthreads();  // the tables are dead: G1 overwrites them
     }
     __syncthreads();
     const cplx dE = csub(c.eps_p, c.eps_b);
-    // G1[dp][iy] = sum_ix eps[iy][ix] PX[dp][ix]   (rcwa2d.cpp:170-177)
-    for (int e = tid; e < mx4 * ng; e += nt) {
-        const int dpi = e / ng, iy = e % ng;
-        const cplx* ph = b.phx + (size_t)dpi * ng;
-        cplx s = C(0.0, 0.0);
+    // G1[dp][iy] = sum_ix eps[iy][ix] PX[dp][ix]   (rcwa2d.cpp:170-177); four
+    // rows dp per thread share the raster reads and give four independent chains
+    for (int e = tid; e < ((mx4 + 3) >> 2) * ng; e += nt) {
+        const int dp0 = 4 * (e / ng), iy = e % ng;
+        const int nd = min(4, mx4 - dp0);
+        cplx s[4] = {C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0)};
         for (int ix = 0; ix < ng; ++ix) {
-            const cplx eps = cadd(c.eps_b, cscale(dE, cnt[iy * ng + ix] / 16.0));
-            s = cfma(eps, ph[ix], s);
+            const cplx eps = cadd(c.eps_b, cscale(dE, cnt[ix * ng + iy] / 16.0));
+#pragma unroll
+            for (int d = 0; d < 4; ++d)
+                if (d < nd) s[d] = cfma(eps, b.phx[(size_t)(dp0 + d) * ng + ix], s[d]);
         }
-        G1[e] = s;
+        for (int d = 0; d < nd; ++d) G1[(size_t)(dp0 + d) * ng + iy] = s[d];
     }
     __syncthreads();
     // Ge[dp][dq] = sum_iy G1[dp][iy] PY[dq][iy]   (rcwa2d.cpp:179-185)
@@ -303,8 +498,14 @@ __global__ void __launch_bounds__(kRT) rcwa_fourier_laurent(Bucket b) {
         order_pq(b, col, pp, qq);
         const cplx v = Ge[(p - pp + 2 * b.Mx) * my4 + (q - qq + 2 * b.My)];
         Exx[e] = v;
-        lu[e] = v;
-        Einv[e] = C(r == col ? 1.0 : 0.0, 0.0);
+        if (!b.sym) {
+            lu[e] = v;
+            Einv[e] = C(r == col ? 1.0 : 0.0, 0.0);
+        }
+    }
+    if (b.sym) {
+        laurent_inverse_by_class(b, cell, Ge, lu, Einv, smem, &rs);
+        return;
     }
     __syncthreads();
     // the raster, G1 and Ge are dead: the LU staging and GEMM tiles overlay them
@@ -990,19 +1191,16 @@ __global__ void __launch_bounds__(kRT) rcwa_epilogue(Bucket b) {
 // The eigen-stages then run on matrices of order ~n/4 (16x fewer QR
 // rotations per class, 64x fewer flops each); the S-matrix stages use the
 // full W unchanged, so t, R and T are those of the full eigensolve up to
-// rounding. A cell whose M is not mirror symmetric to rounding (a raster
-// sample falling exactly on a shape boundary one way and not the other) is
-// flagged kInfoAsym and solved again by the full eigensolve. When the cell is
+// rounding. M_c is built straight from the scalar parity blocks of Exx, Eyy
+// and Einv (rcwa_sym_build; the Laurent Einv itself comes from four block
+// inverses), never forming M. A cell whose eps operators are not mirror
+// symmetric to rounding (a raster sample falling exactly on a shape boundary
+// one way and not the other) is flagged kInfoAsym and solved again by the full
+// eigensolve. When the cell is
 // also symmetric under the 90 degree rotation R (square period, Mx = My,
 // fill_x = fill_y), R commutes with every operator and maps the X excitation
 // onto the Y excitation, so only the X class is solved and the Y solution is R
 // applied to the X one (a cell that fails that check to rounding is flagged too).
-constexpr int kInfoAsym = 1 << 29;
-
-// class c: 0 = (+,+), 1 = (-,-), 2 = (+,-), 3 = (-,+)
-__host__ __device__ __forceinline__ int sym_class_a(int c) { return (c == 0 || c == 2) ? 1 : -1; }
-__host__ __device__ __forceinline__ int sym_class_b(int c) { return (c == 0 || c == 3) ? 1 : -1; }
-__host__ __device__ __forceinline__ int sym_count(int M, int parity) { return parity > 0 ? M + 1 : M; }
 __host__ __device__ __forceinline__ int sym_class_size(int Mx, int My, int c) {
     const int a = sym_class_a(c), b = sym_class_b(c);
     return sym_count(Mx, a) * sym_count(My, b) + sym_count(Mx, -a) * sym_count(My, -b);
@@ -1060,91 +1258,158 @@ __device__ cplx halfspace_entry(const Bucket& b, const CellDev& c, int which, in
     return cmul(v, cinv(kz));
 }
 
-// M (in H) -> the class matrices of the two excited classes (c = 0, 1) for the
-// eigen-stages, and their layer kp (kp = w^2 - J Einv J^T, J = [-Ky; Kx],
-// rcwa2d.cpp:346-352) and half-space operators for the class S-matrix;
-// flags a cell whose M is not mirror symmetric to the tolerance.
-__global__ void __launch_bounds__(kRT) rcwa_sym_project(Bucket b) {
-    __shared__ double red[3][32];
+// Orbit (p, q) >= 0 of index i in scalar parity class (a, bb).
+__device__ __forceinline__ void scalar_orbit(int My, int a, int bb, int i, int& p, int& q) {
+    const int nb = sym_count(My, bb);
+    p = i / nb + (a > 0 ? 0 : 1);
+    q = i % nb + (bb > 0 ? 0 : 1);
+}
+// Index of orbit (p, q) >= 0 in scalar parity class (a, bb), -1 if it has none there.
+__device__ __forceinline__ int scalar_orbit_index(int My, int a, int bb, int p, int q) {
+    if ((p == 0 && a < 0) || (q == 0 && bb < 0)) return -1;
+    return (p - (a > 0 ? 0 : 1)) * sym_count(My, bb) + (q - (bb > 0 ? 0 : 1));
+}
+// Entry (i, j) of S^T E S for the unit orbit vectors S of scalar class (a, bb)
+// and an N x N order-space operator E that commutes with both mirrors.
+__device__ cplx scalar_block_entry(const cplx* E, int N, int Mx, int My, int a, int bb, int i, int j) {
+    const int ny = 2 * My + 1;
+    int pi, qi, pj, qj;
+    scalar_orbit(My, a, bb, i, pi, qi);
+    scalar_orbit(My, a, bb, j, pj, qj);
+    cplx v = C(0.0, 0.0);
+    for (int sp = 1; sp >= (pi > 0 ? -1 : 1); sp -= 2)
+        for (int sq = 1; sq >= (qi > 0 ? -1 : 1); sq -= 2) {
+            const cplx* row = E + (size_t)((sp * pi + Mx) * ny + (sq * qi + My)) * N;
+            const int si = (sp < 0 ? a : 1) * (sq < 0 ? bb : 1);
+            for (int tp = 1; tp >= (pj > 0 ? -1 : 1); tp -= 2)
+                for (int tq = 1; tq >= (qj > 0 ? -1 : 1); tq -= 2) {
+                    const int sg = si * (tp < 0 ? a : 1) * (tq < 0 ? bb : 1);
+                    v = cadd(v, cscale(row[(tp * pj + Mx) * ny + (tq * qj + My)], (double)sg));
+                }
+        }
+    return cscale(v, orbit_weight((pi > 0) + (qi > 0) + (pj > 0) + (qj > 0)));
+}
+
+// The class operators of a mirror-symmetric cell, built from the scalar parity
+// blocks of its eps operators (on the class path this replaces the full
+// M = [Eyy; Exx] J Einv J' + ... of rcwa_build_M and its projection).
+// Vector class c = (a, b) has its u field block in scalar class (a, b) and its
+// v block in (-a, -b). Every operator of M maps parity classes onto parity
+// classes: with kx0 = ky0 = 0, Kx takes the unit orbit vector of (|p|, |q|) in
+// class (a, b) to kx = -2 pi |p| / px times the orbit vector of the same orbit
+// in (-a, b), and Ky likewise in q. So with Eu = Eyy^(a,b), Ev = Exx^(-a,-b)
+// and G = Einv^(a,-b), the one block of Einv that the class meets, and s(j) the
+// index in (a, -b) of the orbit of j (its k is 0 where it has none):
+//   Yt = Lt G, Lt[i][t] = Eu[i][t] (-ky(t));   Yb = Lb G, Lb[l][t] = Ev[l][t] kx(t)
+//   M(u,u) = Yt[i][s(j)] ky(j) + w^2 Eu[i][j] - [i = j] kx^2
+//   M(u,v) = -Yt[i][s(j)] kx(j) - [same orbit] kx ky
+//   M(v,u) = Yb[l][s(j)] ky(j) - [same orbit] ky kx
+//   M(v,v) = w^2 Ev[l][m] - Yb[l][s(m)] kx(m) - [l = m] ky^2
+// (the order-space M of rcwa_build_M), the layer kp = w^2 - J Einv J^T
+// (rcwa2d.cpp:346-352) as kp(u,u) = w^2 [i = j] - ky G ky, kp(u,v) = ky G kx,
+// kp(v,u) = kx G ky, kp(v,v) = w^2 [i = j] - kx G kx, and each half-space
+// operator as the 2 x 2 block of an orbit's representative order (|p|, |q|) (its
+// u-v entries are odd in p and in q, the u-u and v-v entries even).
+// Flags kInfoAsym when Exx, Eyy or Einv is not mirror symmetric to the
+// tolerance, or, for a C4 bucket (ncls = 1), when Eyy[k][l] != Exx[rho k][rho l]
+// or Einv[rho k][rho l] != Einv[k][l] (rho: order (p, q) -> (-q, p)); these
+// make M commute with the mirrors (and with R).
+// Scratch: the cell's full-order Z and X (free on the class path).
+__global__ void __launch_bounds__(kRT) rcwa_sym_build(Bucket b) {
+    __shared__ GemmSmem gs;
+    __shared__ double red[6][32];
     const int cell = blockIdx.x;
     const CellDev cd = b.cells[cell];
-    const int N = b.N, n = b.n, Mx = b.Mx, My = b.My, ny = 2 * My + 1;
+    const int N = b.N, Mx = b.Mx, My = b.My, ny = 2 * My + 1;
     const int tid = threadIdx.x, nt = blockDim.x;
-    const cplx* H = at(b.H, b.s_nn, cell);
+    const cplx* Exx = at(b.Exx, b.s_NN, cell);
+    const cplx* Eyy = b.ng > 0 ? Exx : at(b.Eyy, b.s_NN, cell);
     const cplx* Einv = at(b.Einv, b.s_NN, cell);
-    // symmetry check: M[k][l] = s(k) s(l) M[mirror k][mirror l] for both mirrors
-    double dx = 0.0, dy = 0.0, mx = 0.0;
-    for (int e = tid; e < n * n; e += nt) {
-        const int k = e / n, l = e % n;
-        const int bk = k / N, ok = k % N, bl = l / N, ol = l % N;
-        const int pk = ok / ny, qk = ok % ny, pl = ol / ny, ql = ol % ny;
-        const double sgn = (bk == bl) ? 1.0 : -1.0;
-        const cplx v = H[e];
-        const cplx vx = H[(size_t)(bk * N + (2 * Mx - pk) * ny + qk) * n + bl * N + (2 * Mx - pl) * ny + ql];
-        const cplx vy = H[(size_t)(bk * N + pk * ny + (2 * My - qk)) * n + bl * N + pl * ny + (2 * My - ql)];
-        dx = fmax(dx, cabs(csub(v, cscale(vx, sgn))));
-        dy = fmax(dy, cabs(csub(v, cscale(vy, sgn))));
-        mx = fmax(mx, cabs(v));
+    // symmetry of the ingredients: deviation and magnitude of Exx, Eyy, Einv
+    double dv[3] = {0.0, 0.0, 0.0}, mg[3] = {0.0, 0.0, 0.0};
+    for (int e = tid; e < N * N; e += nt) {
+        const int k = e / N, l = e % N;
+        const int pk = k / ny - Mx, qk = k % ny - My, pl = l / ny - Mx, ql = l % ny - My;
+        const size_t ex = (size_t)((-pk + Mx) * ny + qk + My) * N + (-pl + Mx) * ny + ql + My;
+        const size_t ey = (size_t)((pk + Mx) * ny - qk + My) * N + (pl + Mx) * ny - ql + My;
+        const cplx* X[3] = {Exx, Eyy, Einv};
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            const cplx v = X[t][e];
+            dv[t] = fmax(dv[t], fmax(cabs(csub(v, X[t][ex])), cabs(csub(v, X[t][ey]))));
+            mg[t] = fmax(mg[t], cabs(v));
+        }
+        if (b.ncls == 1) {  // rho k = (-qk, pk): Mx = My, so ny indexes both axes
+            const size_t er = (size_t)((-qk + Mx) * ny + pk + My) * N + (-ql + Mx) * ny + pl + My;
+            dv[1] = fmax(dv[1], cabs(csub(Eyy[e], Exx[er])));
+            dv[2] = fmax(dv[2], cabs(csub(Einv[e], Einv[er])));
+        }
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        dx = fmax(dx, __shfl_down_sync(0xffffffffu, dx, o));
-        dy = fmax(dy, __shfl_down_sync(0xffffffffu, dy, o));
-        mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
-    }
-    if ((tid & 31) == 0) {
-        red[0][tid >> 5] = dx;
-        red[1][tid >> 5] = dy;
-        red[2][tid >> 5] = mx;
-    }
+#pragma unroll
+    for (int t = 0; t < 3; ++t)
+        for (int o = 16; o > 0; o >>= 1) {
+            dv[t] = fmax(dv[t], __shfl_down_sync(0xffffffffu, dv[t], o));
+            mg[t] = fmax(mg[t], __shfl_down_sync(0xffffffffu, mg[t], o));
+        }
+    if ((tid & 31) == 0)
+        for (int t = 0; t < 3; ++t) {
+            red[t][tid >> 5] = dv[t];
+            red[3 + t][tid >> 5] = mg[t];
+        }
     __syncthreads();
     if (tid == 0) {
-        double a = 0.0, c = 0.0, m = 0.0;
-        for (int w = 0; w < nt / 32; ++w) {
-            a = fmax(a, red[0][w]);
-            c = fmax(c, red[1][w]);
-            m = fmax(m, red[2][w]);
-        }
-        if (!(fmax(a, c) <= b.sym_tol * m) && b.info[cell] == 0) b.info[cell] = kInfoAsym;
-    }
-    if (b.ncls == 1) {
-        // C4 (90 degree rotation R: order (p, q) -> (-q, p), u' = -v, v' = u)
-        // must commute with M too: M[rho k][rho l] = sigma(k) sigma(l) M[k][l]
-        double dr = 0.0, mr = 0.0;
-        for (int e = tid; e < n * n; e += nt) {
-            const int k = e / n, l = e % n;
-            const int bk = k / N, ok = k % N, bl = l / N, ol = l % N;
-            const int pk = ok / ny - Mx, qk = ok % ny - My, pl = ol / ny - Mx, ql = ol % ny - My;
-            const int rk = (1 - bk) * N + (-qk + Mx) * ny + (pk + My);
-            const int rl = (1 - bl) * N + (-ql + Mx) * ny + (pl + My);
-            const double sgn = ((bk == 1) != (bl == 1)) ? -1.0 : 1.0;
-            const cplx v = H[e];
-            dr = fmax(dr, cabs(csub(H[(size_t)rk * n + rl], cscale(v, sgn))));
-            mr = fmax(mr, cabs(v));
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            dr = fmax(dr, __shfl_down_sync(0xffffffffu, dr, o));
-            mr = fmax(mr, __shfl_down_sync(0xffffffffu, mr, o));
-        }
-        __syncthreads();
-        if ((tid & 31) == 0) {
-            red[0][tid >> 5] = dr;
-            red[2][tid >> 5] = mr;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            double a = 0.0, m = 0.0;
+        bool asym = false;
+        for (int t = 0; t < 3; ++t) {
+            double d = 0.0, m = 0.0;
             for (int w = 0; w < nt / 32; ++w) {
-                a = fmax(a, red[0][w]);
-                m = fmax(m, red[2][w]);
+                d = fmax(d, red[t][w]);
+                m = fmax(m, red[3 + t][w]);
             }
-            if (!(a <= b.sym_tol * m) && b.info[cell] == 0) b.info[cell] = kInfoAsym;
+            asym = asym || !(d < b.sym_tol * m);  // strict: tolerance 0 flags every cell
         }
+        if (asym && b.info[cell] == 0) b.info[cell] = kInfoAsym;
     }
-    // P_c^T X P_c for X = M, the layer kp and the two half-space operators
     const double w2 = cd.omega * cd.omega;
     const int m = b.m[0];
+    cplx* Zs = at(b.Z, b.s_nn, cell);
+    cplx* Xs = at(b.X, b.s_nn, cell);
     for (int cc = 0; cc < b.ncls; ++cc) {
         const int c = b.cls0 + cc;
+        const int a = sym_class_a(c), bb = sym_class_b(c);
+        const int su = sym_count(Mx, a) * sym_count(My, bb);    // u block: (a, b)
+        const int sv = sym_count(Mx, -a) * sym_count(My, -bb);  // v block: (-a, -b)
+        const int st = sym_count(Mx, a) * sym_count(My, -bb);   // Einv block: (a, -b)
+        cplx* Eu = Zs;
+        cplx* Ev = Eu + (size_t)su * su;
+        cplx* G = Ev + (size_t)sv * sv;
+        cplx* Lt = G + (size_t)st * st;
+        cplx* Lb = Xs;
+        cplx* Yt = Lb + (size_t)sv * st;
+        cplx* Yb = Yt + (size_t)su * st;
+        __syncthreads();  // the previous class's readers of the scratch are done
+        for (int e = tid; e < su * su; e += nt) Eu[e] = scalar_block_entry(Eyy, N, Mx, My, a, bb, e / su, e % su);
+        for (int e = tid; e < sv * sv; e += nt) Ev[e] = scalar_block_entry(Exx, N, Mx, My, -a, -bb, e / sv, e % sv);
+        for (int e = tid; e < st * st; e += nt) G[e] = scalar_block_entry(Einv, N, Mx, My, a, -bb, e / st, e % st);
+        __syncthreads();
+        // Lt[i][t] = Eu[i][orbit t in (a, b)] (-ky(t)), Lb[l][t] = Ev[l][orbit t in (-a, -b)] kx(t)
+        for (int e = tid; e < (su + sv) * st; e += nt) {
+            const int r = e / st, t = e % st;
+            int pt, qt;
+            scalar_orbit(My, a, -bb, t, pt, qt);
+            if (r < su) {
+                const int j = scalar_orbit_index(My, a, bb, pt, qt);
+                const double ky = -(2.0 * PI * (double)qt / cd.py);
+                Lt[(size_t)r * st + t] = j < 0 ? C(0.0, 0.0) : cscale(Eu[(size_t)r * su + j], -ky);
+            } else {
+                const int l = r - su;
+                const int j = scalar_orbit_index(My, -a, -bb, pt, qt);
+                const double kx = -(2.0 * PI * (double)pt / cd.px);
+                Lb[(size_t)l * st + t] = j < 0 ? C(0.0, 0.0) : cscale(Ev[(size_t)l * sv + j], kx);
+            }
+        }
+        blk_gemm(su, st, st, C(1.0, 0.0), Lt, st, G, st, C(0.0, 0.0), Yt, st, &gs);
+        blk_gemm(sv, st, st, C(1.0, 0.0), Lb, st, G, st, C(0.0, 0.0), Yb, st, &gs);
+        __syncthreads();
         const size_t mi = (size_t)(b.ncls * cell + cc) * m * m;
         cplx* Mc = b.sH[0] + mi;
         cplx* Kp = b.cKp + mi;
@@ -1152,28 +1417,49 @@ __global__ void __launch_bounds__(kRT) rcwa_sym_project(Bucket b) {
         cplx* Ks = b.cKs + mi;
         for (int e = tid; e < m * m; e += nt) {
             const int i = e / m, j = e % m;
-            int ii[4], jj[4];
-            double ci[4], cj[4];
-            const int ni = sym_vector(Mx, My, c, i, ii, ci), nj = sym_vector(Mx, My, c, j, jj, cj);
-            cplx am = C(0.0, 0.0), ak = C(0.0, 0.0), a0 = C(0.0, 0.0), as = C(0.0, 0.0);
-            for (int u = 0; u < ni; ++u)
-                for (int v = 0; v < nj; ++v) {
-                    const int k = ii[u], l = jj[v];
-                    const double w = ci[u] * cj[v];
-                    am = cadd(am, cscale(H[(size_t)k * n + l], w));
-                    // kp[k][l] = w^2 [k == l] - J(k) Einv[ord k][ord l] J(l)
-                    const cplx Jk = k < N ? cneg(ky_of(b, cd, k)) : kx_of(b, cd, k - N);
-                    const cplx Jl = l < N ? cneg(ky_of(b, cd, l)) : kx_of(b, cd, l - N);
-                    cplx kp = cneg(cmul(Jk, cmul(Einv[(size_t)(k % N) * N + (l % N)], Jl)));
-                    if (k == l) kp.x += w2;
-                    ak = cadd(ak, cscale(kp, w));
-                    a0 = cadd(a0, cscale(halfspace_entry(b, cd, 0, k, l), w));
-                    as = cadd(as, cscale(halfspace_entry(b, cd, 1, k, l), w));
-                }
-            Mc[e] = am;
-            Kp[e] = ak;
-            C0[e] = a0;
-            Ks[e] = as;
+            const bool ui = i < su, uj = j < su;
+            const int li = ui ? i : i - su, lj = uj ? j : j - su;
+            int pi, qi, pj, qj;
+            scalar_orbit(My, ui ? a : -a, ui ? bb : -bb, li, pi, qi);
+            scalar_orbit(My, uj ? a : -a, uj ? bb : -bb, lj, pj, qj);
+            const int si = scalar_orbit_index(My, a, -bb, pi, qi), sj = scalar_orbit_index(My, a, -bb, pj, qj);
+            const double kxi = -(2.0 * PI * (double)pi / cd.px), kyi = -(2.0 * PI * (double)qi / cd.py);
+            const double kxj = -(2.0 * PI * (double)pj / cd.px), kyj = -(2.0 * PI * (double)qj / cd.py);
+            const bool same = pi == pj && qi == qj;
+            const cplx g = (si >= 0 && sj >= 0) ? G[(size_t)si * st + sj] : C(0.0, 0.0);
+            cplx mv, kv;
+            if (ui && uj) {
+                mv = cscale(Eu[(size_t)li * su + lj], w2);
+                if (sj >= 0) mv = cadd(mv, cscale(Yt[(size_t)li * st + sj], kyj));
+                if (i == j) mv.x -= kxi * kxi;
+                kv = cscale(g, -kyi * kyj);
+                if (i == j) kv.x += w2;
+            } else if (ui) {
+                mv = sj >= 0 ? cscale(Yt[(size_t)li * st + sj], -kxj) : C(0.0, 0.0);
+                if (same) mv.x -= kxi * kyi;
+                kv = cscale(g, kyi * kxj);
+            } else if (uj) {
+                mv = sj >= 0 ? cscale(Yb[(size_t)li * st + sj], kyj) : C(0.0, 0.0);
+                if (same) mv.x -= kyi * kxi;
+                kv = cscale(g, kxi * kyj);
+            } else {
+                mv = cscale(Ev[(size_t)li * sv + lj], w2);
+                if (sj >= 0) mv = csub(mv, cscale(Yb[(size_t)li * st + sj], kxj));
+                if (i == j) mv.x -= kyi * kyi;
+                kv = cscale(g, -kxi * kxj);
+                if (i == j) kv.x += w2;
+            }
+            Mc[e] = mv;
+            Kp[e] = kv;
+            cplx h0 = C(0.0, 0.0), hs = C(0.0, 0.0);
+            if (same) {  // the representative order (|p|, |q|) of the orbit, in each field block
+                const int o = (pi + Mx) * ny + (qi + My);
+                const int k = (ui ? 0 : N) + o, l = (uj ? 0 : N) + o;
+                h0 = halfspace_entry(b, cd, 0, k, l);
+                hs = halfspace_entry(b, cd, 1, k, l);
+            }
+            C0[e] = h0;
+            Ks[e] = hs;
         }
     }
 }
@@ -1366,10 +1652,11 @@ bool symmetry_enabled() {
     const char* e = std::getenv("CELERIS_RCWA_SYMMETRY");
     return !(e && e[0] == '0');
 }
-// Mirror-asymmetry tolerance of the class split, relative to max |M|: rounding
+// Mirror-asymmetry tolerance of the class split, relative to the largest entry
+// of each eps operator (Exx, Eyy, Einv and the Laurent coefficients): rounding
 // leaves ~1e-15; one raster sample on the other side of a shape boundary
-// ~1e-6. CELERIS_RCWA_SYM_TOL overrides it (0 sends every cell to the full
-// eigensolve through the fallback, for tests of that path).
+// ~1e-6. CELERIS_RCWA_SYM_TOL overrides it (the test is strict, so 0 sends
+// every cell to the full eigensolve through the fallback, for tests of that path).
 double symmetry_tolerance() {
     const char* e = std::getenv("CELERIS_RCWA_SYM_TOL");
     return e ? std::atof(e) : 1e-9;
@@ -1465,7 +1752,7 @@ size_t lu_stage_bytes(int n) { return (size_t)(2 * n + LNB * LNB) * sizeof(cplx)
 size_t laurent_smem(int Mx, int My, int ng) {
     const size_t mx4 = 4 * Mx + 1, my4 = 4 * My + 1;
     const int N = (2 * Mx + 1) * (2 * My + 1);
-    const size_t raster = (mx4 * ng + mx4 * my4) * sizeof(cplx) + (size_t)ng * ng;
+    const size_t raster = ((size_t)laurent_g1_rows(Mx) * ng + mx4 * my4) * sizeof(cplx) + (size_t)ng * ng;
     return std::max(raster, lu_stage_bytes(N) + sizeof(GemmSmem));
 }
 
@@ -1614,13 +1901,12 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
         count_launch(1);
     }
     if (ev) cudaEventRecord(ev[1], st);
-    rcwa_build_M<<<nc, T[ST_BUILD], 0, st>>>(b, b.ng > 0 ? 1 : 0);
-    if (ev) cudaEventRecord(ev[2], st);
     if (b.sym) {
-        // the two excited parity classes: project, eigen-stages (two matrices
-        // of order m[0] per cell), the class S-matrix, expand into the
-        // epilogue's vectors
-        rcwa_sym_project<<<nc, T[ST_HESS], 0, st>>>(b);
+        // the excited parity classes: their operators (in place of build_M),
+        // eigen-stages (ncls matrices of order m[0] per cell), the class
+        // S-matrix, expand into the epilogue's vectors
+        rcwa_sym_build<<<nc, T[ST_BUILD], 0, st>>>(b);
+        if (ev) cudaEventRecord(ev[2], st);
         const Bucket e = sym_eig_bucket(b, 0);
         cudaMemsetAsync(e.info, 0, sizeof(int) * e.ncell, st);
         const int m = e.n;
@@ -1639,9 +1925,12 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
         if (ev) cudaEventRecord(ev[7], st);
         rcwa_epilogue<<<nc, T[ST_EPI], 0, st>>>(b);
         if (ev) cudaEventRecord(ev[8], st);
-        count_launch(8);
+        count_launch(7);
         return;
-    } else if (n <= kSmemEigMaxN) {
+    }
+    rcwa_build_M<<<nc, T[ST_BUILD], 0, st>>>(b, b.ng > 0 ? 1 : 0);
+    if (ev) cudaEventRecord(ev[2], st);
+    if (n <= kSmemEigMaxN) {
         const size_t sm = ((size_t)n * n + 2 * n) * sizeof(cplx);
         rcwa_hess<true><<<nc, T[ST_HESS], sm, st>>>(b);
         if (ev) cudaEventRecord(ev[3], st);
@@ -2019,7 +2308,7 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                     cudaMemcpyAsync(const_cast<CellDev*>(p.b.cells), hdesc[w], sizeof(CellDev) * nc,
                                     cudaMemcpyHostToDevice, bs);
                     launch_bucket(p.b, cfgs[w], bs, nullptr);
-                    nk += (p.ng > 0 ? 3 : 1) + (p.sym ? 8 : 7);
+                    nk += (p.ng > 0 ? 3 : 1) + 7;
                     cudaMemcpyAsync(hres_pin[w], p.b.res, sizeof(celeris_rcwa_result) * nexc * nc,
                                     cudaMemcpyDeviceToHost, bs);
                     cudaMemcpyAsync(hinfo_pin[w], p.b.info, sizeof(int) * nc, cudaMemcpyDeviceToHost, bs);

@@ -1632,6 +1632,7 @@ Bucket sym_eig_bucket(const Bucket& b, int k) {
     e.A = b.sA[k];
     e.q1 = b.sq[k];
     e.info = b.sinfo[k];
+    e.dbg = b.dbg;  // the stage-clock counters hold 2 slots per cell
     e.s_nn = (size_t)e.n * e.n;
     e.s_n = (size_t)e.n;
     return e;
@@ -2248,9 +2249,9 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                 const int nc = (int)p.ids.size();
                 CEL_CUDA(cudaMemcpyAsync(const_cast<CellDev*>(p.b.cells), hdesc[w], sizeof(CellDev) * nc,
                                          cudaMemcpyHostToDevice, st));
-                long long* dbg = nullptr;
-                CEL_CUDA(cudaMalloc(&dbg, sizeof(long long) * kDbgSlots * nc));
-                CEL_CUDA(cudaMemsetAsync(dbg, 0, sizeof(long long) * kDbgSlots * nc, st));
+                long long* dbg = nullptr;  // 2 nc slots: a class bucket has up to two matrices per cell
+                CEL_CUDA(cudaMalloc(&dbg, sizeof(long long) * kDbgSlots * 2 * nc));
+                CEL_CUDA(cudaMemsetAsync(dbg, 0, sizeof(long long) * kDbgSlots * 2 * nc, st));
                 p.b.dbg = dbg;
                 cudaEvent_t ev[ST_COUNT + 1];
                 for (auto& e : ev) cudaEventCreate(&e);
@@ -2259,10 +2260,10 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                                          cudaMemcpyDeviceToHost, st));
                 CEL_CUDA(cudaMemcpyAsync(hinfo_pin[w], p.b.info, sizeof(int) * nc, cudaMemcpyDeviceToHost, st));
                 CEL_CUDA(cudaStreamSynchronize(st));
-                std::vector<long long> h(kDbgSlots * nc);
-                cudaMemcpy(h.data(), dbg, sizeof(long long) * kDbgSlots * nc, cudaMemcpyDeviceToHost);
+                std::vector<long long> h(kDbgSlots * 2 * nc);
+                cudaMemcpy(h.data(), dbg, sizeof(long long) * kDbgSlots * 2 * nc, cudaMemcpyDeviceToHost);
                 double sw = 0, ph[kDbgSlots] = {};
-                for (int i = 0; i < nc; ++i) {
+                for (int i = 0; i < 2 * nc; ++i) {
                     sw += (double)h[kDbgSlots * i + 6];
                     for (int q = 0; q < kDbgSlots; ++q) ph[q] += (double)h[kDbgSlots * i + q];
                 }
@@ -2276,12 +2277,14 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                 }
                 char buf[64];
                 std::snprintf(buf, sizeof(buf), " | sweeps/cell %.1f", sw / nc);
-                char buf2[320];
+                char buf2[480];
                 std::snprintf(buf2, sizeof(buf2), " | schur Mcycles/cell: aed %.2f (qr %.2f, %.0f rot) aed_far %.2f sweep %.2f (%.0f steps) sweep_far %.2f small %.2f"
-                              " | hess Mcycles/cell: columns %.2f (matvec %.2f) updates %.2f\n",
+                              " | hess Mcycles/cell: columns %.2f (matvec %.2f) updates %.2f"
+                              " | small QR Mcycles/cell: aed chase %.2f deferred %.2f, block chase %.2f deferred %.2f\n",
                               ph[0] / nc * 1e-6, ph[5] / nc * 1e-6, ph[8] / nc, ph[1] / nc * 1e-6, ph[2] / nc * 1e-6,
                               ph[7] / nc, ph[3] / nc * 1e-6, ph[4] / nc * 1e-6, ph[9] / nc * 1e-6, ph[10] / nc * 1e-6,
-                              ph[11] / nc * 1e-6);
+                              ph[11] / nc * 1e-6, ph[12] / nc * 1e-6, ph[13] / nc * 1e-6, ph[14] / nc * 1e-6,
+                              ph[15] / nc * 1e-6);
                 std::fprintf(stderr, "%s%s%s", line.c_str(), buf, buf2);
                 for (auto& e : ev) cudaEventDestroy(e);
                 cudaFree(dbg);

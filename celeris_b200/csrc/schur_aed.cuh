@@ -50,6 +50,8 @@ struct AedShared {
     int lo, hi, done, info, nsweep, nsu, nd, nshift, nxt, win_end, ws, we, it;
     cplx shift[NSH];
     unsigned umask[WMAX / 8];  // bit q of umask[c]: block U[4q..4q+3][8c..8c+7] has a non-zero
+    double qc[WMAX];           // rotations of one small-QR sweep (deferred column rotations)
+    cplx qs[WMAX];
 };
 
 // ---- warp-level helpers on shared matrices ------------------------------------------------
@@ -90,17 +92,139 @@ __device__ __forceinline__ void grot_cols(cplx* B, int ld, int k, double c, cplx
     }
 }
 
+// Single-shift QR of a Hessenberg block B (m x m, m <= 64, shared) with the
+// rotations accumulated into U (mu x m, mu <= 64). The bulge chase of a sweep
+// (rotations k = l .. hi-1) needs only the band around the diagonal: rotation
+// k + 1 is a function of the 2 x 2 block at k, the subdiagonal below it and
+// the bulge, so warp 0 keeps that band in registers (the same values in every
+// lane) and derives each rotation without a shared-memory round trip. Its
+// lanes also carry the columns right of the band (lane j % 32): row rotation
+// k mixes the running B[k][j] (a register) with the untouched B[k+1][j],
+// stores the final B[k][j], and column k + 2 enters the band by a shuffle of
+// its running value. Nothing in the chase reads the rows above the band or
+// U, so their column rotations are deferred: warp 0 records the sweep's
+// rotations, and then every thread carries one row of B (from the rotation
+// after it left the band) or of U through all of them. Each element sees the
+// same rotations, in the same order and with the same arithmetic, as the plain
+// sweep (rows k, k+1 over columns >= k-1, then columns k, k+1 over rows <= k+2).
+__device__ __forceinline__ void rot_rows2(cplx x, cplx y, double c, cplx s, cplx ms, cplx& xo, cplx& yo) {
+    xo = cfma(s, y, cscale(x, c));
+    yo = cfma(ms, x, cscale(y, c));
+}
+__device__ __forceinline__ void rot_cols2(cplx x, cplx y, double c, cplx cs, cplx ns, cplx& xo, cplx& yo) {
+    xo = cfma(cs, y, cscale(x, c));
+    yo = cfma(ns, x, cscale(y, c));
+}
+// givens() without branches (the same c, s in every case), so that the chase
+// step below stays one block the compiler can schedule as a whole.
+__device__ __forceinline__ void givens_sel(cplx a, cplx b, double& c, cplx& s) {
+    const double na = cnorm2(a), nb = cnorm2(b);
+    const double ia = rsqrt(na), ir = rsqrt(na + nb);
+    const cplx sg = cscale(cmul(a, cconj(b)), ia * ir), s0 = cscale(cconj(b), ir);
+    c = nb == 0.0 ? 1.0 : (na == 0.0 ? 0.0 : na * ia * ir);
+    s = nb == 0.0 ? C(0.0, 0.0) : (na == 0.0 ? s0 : sg);
+}
+// The chase of one sweep by warp 0 (NS: column slots per lane, m <= 32 NS).
+// Records rotation k in qc/qs[k - l]; leaves B[k][k+1] holding row k's value
+// after column rotation k (the start of its deferred chain).
+template <int NS>
+__device__ void qr_chase(int m, cplx* B, int ld, int l, int hi, cplx shift, double* qc, cplx* qs, int lane) {
+    const cplx Z0 = C(0.0, 0.0);
+    cplx P = B[l * ld + l], Q = B[l * ld + l + 1], R = B[(l + 1) * ld + l], S = B[(l + 1) * ld + l + 1];
+    cplx T = (l + 2 <= hi) ? B[(l + 2) * ld + l + 1] : Z0;
+    cplx a = csub(P, shift), bb = R;
+    cplx cc[NS];  // running values of columns lane + 32 t right of the band
+    int ci[NS];   // those columns, clamped into the matrix for the loads
+#pragma unroll
+    for (int t = 0; t < NS; ++t) {
+        const int i = lane + 32 * t;
+        ci[t] = min(i, m - 1);
+        cc[t] = (i >= l + 2 && i < m) ? B[l * ld + i] : Z0;
+    }
+    for (int k = l; k < hi; ++k) {
+        // loads first: row k+1 right of the band and the next band entries
+        // are untouched by this sweep so far
+        cplx yr[NS];
+#pragma unroll
+        for (int t = 0; t < NS; ++t) yr[t] = B[(k + 1) * ld + ci[t]];
+        const int j2 = min(k + 2, m - 1), j3 = min(k + 3, m - 1);
+        const cplx Sn = B[j2 * ld + j2], Tn = B[j3 * ld + j2];
+        double c;
+        cplx s;
+        givens_sel(a, bb, c, s);
+        const cplx ms = cneg(cconj(s)), cs = cconj(s), ns = cneg(s);
+        const cplx rn = cfma(s, bb, cscale(a, c));  // B[k][k-1] after the row rotation (k > l)
+        cplx xr[NS];
+#pragma unroll
+        for (int t = 0; t < NS; ++t) {
+            cplx yo;
+            rot_rows2(cc[t], yr[t], c, s, ms, xr[t], yo);
+            if (lane + 32 * t >= k + 2) cc[t] = yo;
+        }
+        // the band: rows k, k+1 then columns k, k+1 (row k+2 gains the bulge)
+        cplx P1, Q1, R1, S1, P2, Q2, R2, S2, bul, Rn;
+        rot_rows2(P, R, c, s, ms, P1, R1);
+        rot_rows2(Q, S, c, s, ms, Q1, S1);
+        rot_cols2(P1, Q1, c, cs, ns, P2, Q2);
+        rot_cols2(R1, S1, c, cs, ns, R2, S2);
+        rot_cols2(Z0, T, c, cs, ns, bul, Rn);  // T = 0 past the active block
+        // column k+2 enters the band (its running value after row rotation k)
+        const int j = k + 2;
+        const cplx v = (NS == 1 || j < 32) ? cc[0] : cc[NS - 1];
+        const cplx Qn = C(__shfl_sync(0xffffffffu, v.x, j & 31), __shfl_sync(0xffffffffu, v.y, j & 31));
+#pragma unroll
+        for (int t = 0; t < NS; ++t) {
+            const int i = lane + 32 * t;
+            if (i >= k + 2 && i < m) B[k * ld + i] = xr[t];
+        }
+        if (lane == 0) {
+            qc[k - l] = c;
+            qs[k - l] = s;
+            if (k > l) {
+                B[k * ld + k - 1] = rn;
+                B[(k + 1) * ld + k - 1] = Z0;
+            }
+            B[k * ld + k] = P2;
+            B[k * ld + k + 1] = Q2;
+            if (k + 1 == hi) {
+                B[(k + 1) * ld + k] = R2;
+                B[(k + 1) * ld + k + 1] = S2;
+            }
+        }
+        a = R2;
+        bb = bul;
+        P = S2;
+        Q = Qn;
+        R = Rn;
+        S = Sn;
+        T = (k + 3 <= hi) ? Tn : Z0;
+        __syncwarp();
+    }
+#pragma unroll
+    for (int t = 0; t < NS; ++t) {
+        const int i = lane + 32 * t;
+        if (i >= hi + 1 && i < m) B[hi * ld + i] = cc[t];
+    }
+}
+
 // Single-shift QR of the m x m upper Hessenberg matrix B (shared, ld) to upper
-// triangular form, U <- U Q (rows [0, mu)). One warp. Returns 0, or the
-// (1-based) row where the iteration cap ran out.
-__device__ int warp_schur_small(int m, cplx* B, int ld, cplx* U, int ldu, int mu, int lane,
-                                 long long* nrot = nullptr, int iter_cap = 0) {
+// triangular form, U <- U Q (rows [0, mu)). Called by every thread of the
+// block; warp 0 chases, all threads apply the deferred column rotations.
+// Returns 0, or the (1-based) row where the iteration cap ran out (the same
+// value in every thread).
+// tprof (optional): clock64 sums of [0] the chases (warp 0) and [1] the
+// deferred rotations (thread 0).
+__device__ __noinline__ int blk_schur_small(int m, cplx* B, int ld, cplx* U, int ldu, int mu, AedShared* sh,
+                               long long* nrot = nullptr, int iter_cap = 0, long long* tprof = nullptr) {
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     const double eps = 2.220446049250313e-16;
     const double smallnum = 2.2250738585072014e-308 * (m / eps);
     int hi = m - 1, it = 0, total = 0;
+    long long rot_count = 0;  // written to *nrot once: a global update per sweep stalls the chase
     const int max_total = iter_cap > 0 ? min(iter_cap, 30 * m) : 30 * m;
     while (hi > 0) {
-        // l = largest index in [1, hi] with a negligible subdiagonal (0 if none)
+        // l = largest index in [1, hi] with a negligible subdiagonal (0 if
+        // none); every warp reads the same B and finds the same l
         int l = 0;
         for (int base = hi; base >= 1 && l == 0; base -= 32) {
             const int i = base - lane;
@@ -112,44 +236,63 @@ __device__ int warp_schur_small(int m, cplx* B, int ld, cplx* U, int ldu, int mu
             const unsigned msk = __ballot_sync(0xffffffffu, f);
             if (msk) l = base - (__ffs(msk) - 1);
         }
-        __syncwarp();
-        if (l > 0 && lane == 0) B[l * ld + l - 1] = C(0.0, 0.0);
-        __syncwarp();
-        if (l == hi) {
+        cplx shift = C(0.0, 0.0);
+        const bool deflated = l == hi;
+        if (!deflated) {
+            if (it + 1 == 10 || it + 1 == 20) {
+                shift = cadd(B[hi * ld + hi],
+                             C(0.75 * fabs(B[hi * ld + hi - 1].x) + fabs(B[hi * ld + hi - 1].y), 0.0));
+            } else {
+                shift = wilkinson(B[(hi - 1) * ld + hi - 1], B[(hi - 1) * ld + hi], B[hi * ld + hi - 1],
+                                  B[hi * ld + hi]);
+            }
+        }
+        __syncthreads();  // every read of this step's deflation test and shift is done
+        if (l > 0 && tid == 0) B[l * ld + l - 1] = C(0.0, 0.0);
+        if (deflated) {
             --hi;
             it = 0;
+            __syncthreads();
             continue;
         }
-        if (++total > max_total) return hi + 1;
+        if (++total > max_total) {
+            if (nrot && tid == 0) *nrot += rot_count;
+            return hi + 1;
+        }
         ++it;
-        cplx shift;
-        if (it == 10 || it == 20) {
-            shift = cadd(B[hi * ld + hi], C(0.75 * fabs(B[hi * ld + hi - 1].x) + fabs(B[hi * ld + hi - 1].y), 0.0));
-        } else {
-            shift = wilkinson(B[(hi - 1) * ld + hi - 1], B[(hi - 1) * ld + hi], B[hi * ld + hi - 1], B[hi * ld + hi]);
+        rot_count += hi - l;
+        if (warp == 0) {
+            const long long tc0 = clock64();
+            if (m <= 32)
+                qr_chase<1>(m, B, ld, l, hi, shift, sh->qc, sh->qs, lane);
+            else
+                qr_chase<2>(m, B, ld, l, hi, shift, sh->qc, sh->qs, lane);
+            if (tprof && lane == 0) tprof[0] += clock64() - tc0;
         }
-        if (nrot && lane == 0) *nrot += hi - l;
-        for (int k = l; k < hi; ++k) {
-            cplx a, b;
-            if (k == l) {
-                a = csub(B[l * ld + l], shift);
-                b = B[(l + 1) * ld + l];
-            } else {
-                a = B[k * ld + k - 1];
-                b = B[(k + 1) * ld + k - 1];
+        __syncthreads();
+        const long long td0 = clock64();
+        // deferred column rotations: row r of B from the rotation after it
+        // left the band (rows above the block from l), every row of U from l
+        for (int q = tid; q < hi + mu; q += nt) {
+            const bool isu = q >= hi;
+            const int r = isu ? q - hi : q;
+            cplx* row = isu ? U + r * ldu : B + r * ld;
+            const int k0 = isu ? l : max(l, r + 1);
+            cplx carry = row[k0];
+            for (int k = k0; k < hi; ++k) {
+                const double c = sh->qc[k - l];
+                const cplx s = sh->qs[k - l];
+                cplx xo, yo;
+                rot_cols2(carry, row[k + 1], c, cconj(s), cneg(s), xo, yo);
+                row[k] = xo;
+                carry = yo;
             }
-            double c;
-            cplx s;
-            givens(a, b, c, s);
-            __syncwarp();
-            wrot_rows(B, ld, k, c, s, k == l ? l : k - 1, m, lane);
-            __syncwarp();
-            if (k > l && lane == 0) B[(k + 1) * ld + k - 1] = C(0.0, 0.0);
-            wrot_cols(B, ld, k, c, s, 0, min(k + 2, hi) + 1, lane);
-            wrot_cols(U, ldu, k, c, s, 0, mu, lane);
-            __syncwarp();
+            row[hi] = carry;
         }
+        __syncthreads();
+        if (tprof && tid == 0) tprof[1] += clock64() - td0;
     }
+    if (nrot && tid == 0) *nrot += rot_count;
     return 0;
 }
 
@@ -399,9 +542,10 @@ __device__ void aed(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, int hi, A
     cplx* B = &sh->B[0][0];
     cplx* U = &sh->U[0][0];
     constexpr int ldb = WMAX + 1, ldu = WMAX + 1;
+    const long long ts0 = clock64();
+    const int info = blk_schur_small(jw, B, ldb, U, ldu, jw, sh, prof ? prof + 8 : nullptr, 0,
+                                     prof ? prof + 12 : nullptr);
     if (warp == 0) {
-        const long long ts0 = clock64();
-        const int info = warp_schur_small(jw, B, ldb, U, ldu, jw, lane, prof ? prof + 8 : nullptr);
         if (prof && lane == 0) prof[5] += clock64() - ts0;
         int nsu = jw, ilst = 0;
         if (info == 0) {
@@ -681,11 +825,9 @@ __device__ int blk_schur_aed(int n, cplx* H, int ldh, cplx* Z, int ldz, AedShare
             // the whole block in shared memory
             const long long t0 = clock64();
             load_window(H, ldh, lo, L, sh);
-            if (warp == 0) {
-                const int info = warp_schur_small(L, &sh->B[0][0], WMAX + 1, &sh->U[0][0], WMAX + 1, L, lane,
-                                                  nullptr, iter_cap);
-                if (lane == 0 && info) sh->info = lo + info;
-            }
+            const int info = blk_schur_small(L, &sh->B[0][0], WMAX + 1, &sh->U[0][0], WMAX + 1, L, sh, nullptr,
+                                             iter_cap, prof ? prof + 14 : nullptr);
+            if (tid == 0 && info) sh->info = lo + info;
             __syncthreads();
             store_window(H, ldh, lo, L, sh, true);
             far_all(n, H, ldh, Z, ldz, lo, hi + 1, sh);

@@ -680,6 +680,115 @@ __device__ int blk_lu_blocked(int n, cplx* A, int lda, int* piv, RedScratch* rs,
     return info;
 }
 
+// ---- Gauss-Jordan in shared memory ----------------------------------------------------
+// For matrices small enough to sit in shared memory whole. Each column step
+// takes three barriers: warp 0 finds the pivot (first max |re|+|im|, as
+// blk_lu) with shuffles; every thread then swaps rows k and p and stages the
+// pivot row (scaled by 1/a_kk) and the pivot column; every thread then
+// applies the rank-1 elimination to its entries. No triangular solve follows,
+// so there are no serial chains besides the pivot search.
+// Step k of either routine; ncol columns of M (ld) take part, column k itself
+// is handled by the caller's rule (solve: it becomes e_k; inverse: it turns
+// into the k-th column of the inverse, Gauss-Jordan in place).
+template <bool INVERSE>
+__device__ __forceinline__ bool gj_step(int n, int ncol, cplx* M, int ld, int k, cplx* rowv, cplx* colv,
+                                        int* sp, cplx* sd) {
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
+    if (tid < 32) {  // warp 0: the pivot
+        double best = -1.0;
+        int bi = k;
+        for (int i = k + lane; i < n; i += 32) {
+            const double v = cabs1(M[i * ld + k]);
+            if (v > best) {
+                best = v;
+                bi = i;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_down_sync(0xffffffffu, best, o);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) {
+                best = ov;
+                bi = oi;
+            }
+        }
+        if (lane == 0) {
+            *sp = bi;
+            const cplx akk = M[bi * ld + k];
+            *sd = (akk.x == 0.0 && akk.y == 0.0) ? C(0.0, 0.0) : cinv(akk);
+        }
+    }
+    __syncthreads();
+    const int p = *sp;
+    const cplx d = *sd;
+    if (d.x == 0.0 && d.y == 0.0) return false;  // singular: the same decision in every thread
+    // swap rows k and p; stage the scaled pivot row and the pivot column
+    for (int j = tid; j < ncol; j += nt) {
+        const cplx vk = M[k * ld + j], vp = M[p * ld + j];
+        if (p != k) M[p * ld + j] = vk;
+        rowv[j] = cmul(vp, d);
+    }
+    for (int i = tid; i < n; i += nt) colv[i] = i == p ? M[k * ld + k] : (i == k ? C(0.0, 0.0) : M[i * ld + k]);
+    __syncthreads();
+    // eliminate: M[i][j] -= colv[i] rowv[j] (i != k); row k <- rowv. A warp
+    // per row, lanes over its columns (no index division)
+    const int j0 = INVERSE ? 0 : k + 1;  // solve: the columns left of k (and k) are done
+    const int warp = tid >> 5, nwarp = nt >> 5;
+    for (int i = warp; i < n; i += nwarp) {
+        cplx* row = M + i * ld;
+        if (i == k) {
+            for (int j = j0 + lane; j < ncol; j += 32) row[j] = (INVERSE && j == k) ? d : rowv[j];
+        } else {
+            const cplx ci = colv[i];
+            for (int j = j0 + lane; j < ncol; j += 32)
+                row[j] = (INVERSE && j == k) ? cneg(cmul(ci, d)) : cfms(ci, rowv[j], row[j]);
+        }
+    }
+    __syncthreads();
+    return true;
+}
+
+// [A | B] (n x (n + nrhs), shared; an odd ld keeps column walks free of bank
+// conflicts) -> B <- A^-1 B by Gauss-Jordan with partial pivoting (A is
+// destroyed). scratch: 2 (n + nrhs) + 1 complex and one int of shared memory.
+// Returns 0 or the 1-based column of a zero pivot.
+__device__ int blk_gj_solve_smem(int n, int nrhs, cplx* M, int ld, cplx* scratch, int* sp) {
+    cplx* rowv = scratch;
+    cplx* colv = scratch + n + nrhs;
+    cplx* sd = colv + n + nrhs;
+    __syncthreads();
+    for (int k = 0; k < n; ++k)
+        if (!gj_step<false>(n, n + nrhs, M, ld, k, rowv, colv, sp, sd)) return k + 1;
+    return 0;
+}
+
+// A (n x n, shared, ld) <- A^-1 in place by Gauss-Jordan with partial pivoting
+// (rows swapped during the sweep, the inverse's columns swapped back after it).
+// scratch: 2 n + 1 complex; piv: n ints of shared memory.
+__device__ int blk_gj_inverse_smem(int n, cplx* A, int ld, cplx* scratch, int* piv, int* sp) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    cplx* rowv = scratch;
+    cplx* colv = scratch + n;
+    cplx* sd = colv + n;
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        if (!gj_step<true>(n, n, A, ld, k, rowv, colv, sp, sd)) return k + 1;
+        if (tid == 0) piv[k] = *sp;
+    }
+    __syncthreads();
+    for (int k = n - 1; k >= 0; --k) {
+        const int p = piv[k];
+        if (p != k)
+            for (int i = tid; i < n; i += nt) {
+                const cplx t = A[i * ld + k];
+                A[i * ld + k] = A[i * ld + p];
+                A[i * ld + p] = t;
+            }
+        __syncthreads();
+    }
+    return 0;
+}
+
 // B (n x nrhs) <- A^{-1} B from the factors of blk_lu / blk_lu_blocked, by
 // block rows: a small triangular solve per block (one thread per RHS column)
 // and a blk_gemm update of the remaining rows. stage: >= LNB*LNB complex.

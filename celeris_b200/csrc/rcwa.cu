@@ -53,7 +53,7 @@ using celeris_rt::Workspace;
 
 constexpr double PI = 3.14159265358979323846;
 constexpr int kRT = 256;            // threads per CTA
-constexpr int kDbgSlots = 16;       // diagnostic counters per cell
+constexpr int kDbgSlots = 24;       // diagnostic counters per cell
 constexpr int kSmemEigMaxN = 116;   // Hessenberg reduction in shared memory up to this n ((n^2 + 2n) 16 B <= 227 KB)
 
 struct CellDev {
@@ -278,8 +278,9 @@ __device__ __forceinline__ int scalar_class_index(int My, int c, int p, int q, d
 // matrix epsT[(p,q)][(p',q')] = Ge[p-p'][q-q'] commutes with both mirrors when
 // Ge is even in dp and in dq, so in the scalar parity basis (unit orbit vectors
 // of (|p|, |q|) with signs a^[p<0] b^[q<0]) it is block diagonal with four blocks
-// of orders (Mx + [a>0]) (My + [b>0]). Each block is factored and inverted on
-// its own (about N^3/16 of the work of the full inverse) and Einv assembled:
+// of orders (Mx + [a>0]) (My + [b>0]). Each block is inverted on its own, in
+// place in shared memory by Gauss-Jordan with partial pivoting (about N^3/16 of
+// the work of the full inverse, and no triangular solves), and Einv assembled:
 //   Einv[k][l] = sum_c s_c(k) s_c(l) B_c^-1[i_c(k)][i_c(l)].
 // A Ge that is not even to the symmetry tolerance flags the cell kInfoAsym (it
 // is solved again by the full path). work: 2 N^2 complex (blocks, then their
@@ -309,7 +310,6 @@ __device__ void laurent_inverse_by_class(const Bucket& b, int cell, const cplx* 
         const int a = sym_class_a(c), bb = sym_class_b(c);
         const int nb = sym_count(My, bb), s = sym_count(Mx, a) * nb;
         cplx* B = work + off;
-        cplx* R = work + (size_t)N * N + off;
         for (int e = tid; e < s * s; e += nt) {
             const int i = e / s, j = e % s;
             const int pi = i / nb + (a > 0 ? 0 : 1), qi = i % nb + (bb > 0 ? 0 : 1);
@@ -325,7 +325,6 @@ __device__ void laurent_inverse_by_class(const Bucket& b, int cell, const cplx* 
                             v = cadd(v, cscale(g, sg));
                         }
             B[e] = cscale(v, w);
-            R[e] = C(i == j ? 1.0 : 0.0, 0.0);
         }
         off += (size_t)s * s;
     }
@@ -338,21 +337,26 @@ __device__ void laurent_inverse_by_class(const Bucket& b, int cell, const cplx* 
         }
         if (!(d < b.sym_tol * m) && b.info[cell] == 0) b.info[cell] = kInfoAsym;  // strict: tolerance 0 flags all
     }
-    // Ge is dead: the LU staging and GEMM tiles overlay the raster region
-    cplx* stg = reinterpret_cast<cplx*>(smem);
-    GemmSmem* gs = reinterpret_cast<GemmSmem*>(stg + 2 * N + LNB * LNB);
-    int* piv = b.piv + b.s_n * cell;
+    // Ge is dead: each block is inverted in place in shared memory over the
+    // raster region (Gauss-Jordan, laurent_smem() reserves the largest block)
     off = 0;
     for (int c = 0; c < 4; ++c) {
         const int s = sym_count(Mx, sym_class_a(c)) * sym_count(My, sym_class_b(c));
         if (s == 0) continue;
-        cplx* B = work + off;
-        const int info = blk_lu_blocked(s, B, s, piv, rs, stg, gs);
+        const int ld = s | 1;  // odd: the pivot search's column walk spreads over the banks
+        cplx* Ms = reinterpret_cast<cplx*>(smem);
+        cplx* scr = Ms + (size_t)s * ld;
+        int* gpiv = reinterpret_cast<int*>(scr + 2 * s + 1);
+        int* sp = gpiv + s;
+        const cplx* B = work + off;
+        for (int e = tid; e < s * s; e += nt) Ms[(e / s) * ld + e % s] = B[e];
+        const int info = blk_gj_inverse_smem(s, Ms, ld, scr, gpiv, sp);
         if (info != 0 && tid == 0 && b.info[cell] == 0) b.info[cell] = -info;
-        blk_lu_solve_blocked(s, B, s, piv, s, work + (size_t)N * N + off, s, stg, gs);
+        cplx* R = work + (size_t)N * N + off;
+        for (int e = tid; e < s * s; e += nt) R[e] = Ms[(e / s) * ld + e % s];
+        __syncthreads();
         off += (size_t)s * s;
     }
-    __syncthreads();
     size_t offs[4];
     off = 0;
     for (int c = 0; c < 4; ++c) {
@@ -1464,6 +1468,14 @@ __global__ void __launch_bounds__(kRT) rcwa_sym_build(Bucket b) {
     }
 }
 
+// Class S-matrix solves by Gauss-Jordan in shared memory when the widest
+// augmented system [T11 | -T12 D | a0] (m x (2m + 1)) fits in 128 KB (classes
+// up to m = 61, M <= 5 on square cells); larger classes use the blocked LU.
+__host__ __device__ constexpr size_t sym_gj_bytes(int m) {
+    return ((size_t)m * (2 * m + 2) + 2 * (2 * m + 1) + 1) * 16 + 16;
+}
+__host__ __device__ constexpr bool sym_gj_fits(int m) { return sym_gj_bytes(m) <= 128 * 1024; }
+
 // The S-matrix of one excited class: rcwa_smat1 and rcwa_smat2 restricted to
 // the class, with the class's one excitation (class 0: Y, a0 = -e_i0; class 1:
 // X, a0 = e_{N+i0}, rcwa2d.cpp:403-411). In the class basis the half-spaces'
@@ -1474,7 +1486,7 @@ __global__ void __launch_bounds__(kRT) rcwa_sym_build(Bucket b) {
 //   Q = diag(q) A^-1 Ks W,  (I + Q - D S12 + D S12 Q) y = 2 D u,
 //   aN = W y,  y2 = (y - Q y)/2,  b0 = T12 (u + S12 y2) + T11 D y2.
 // Writes aN and b0 (class basis) to the class vector area.
-// dynamic smem: LU staging (2m + LNB^2 complex)
+// dynamic smem: sym_smat_smem(m) (LU staging, or the Gauss-Jordan systems)
 __global__ void __launch_bounds__(kRT) rcwa_sym_smat(Bucket b) {
     extern __shared__ __align__(16) unsigned char smem[];
     cplx* stg = reinterpret_cast<cplx*>(smem);
@@ -1495,6 +1507,16 @@ __global__ void __launch_bounds__(kRT) rcwa_sym_smat(Bucket b) {
     int* piv = b.cpiv + (size_t)mi * m;
     const int ld = m + 1;
     const cplx one = C(1.0, 0.0), zero = C(0.0, 0.0);
+    // stage clocks: per-phase clock64 sums in slots 16.. of the cell's counters
+    long long* pf = (b.dbg && tid == 0) ? b.dbg + kDbgSlots * (size_t)mi + 16 : nullptr;
+    long long tp = clock64();
+    auto phase = [&](int k) {
+        if (pf) {
+            const long long t = clock64();
+            pf[k] += t - tp;
+            tp = t;
+        }
+    };
     // A = kp W, then P = C0 A (into T12), T11 = (W + P diag(1/q))/2, T12 = (W - P diag(1/q))/2
     blk_gemm(m, m, m, one, Kp, m, W, m, zero, A, m, &gs);
     blk_gemm(m, m, m, one, C0, m, A, m, zero, T12, m, &gs);
@@ -1528,16 +1550,56 @@ __global__ void __launch_bounds__(kRT) rcwa_sym_smat(Bucket b) {
         S[e] = v;
     }
     __syncthreads();
-    int info = blk_lu_blocked(m, T11lu, m, piv, &rs, stg, &gs);
-    if (tid == 0 && info) atomicCAS(&b.info[cell], 0, -info);
-    blk_lu_solve_blocked(m, T11lu, m, piv, ld, S, ld, stg, &gs);  // [S12 | u]
+    phase(0);
+    const bool gj = sym_gj_fits(m);
+    const int lg = 2 * m + 1;  // the augmented systems' row stride in shared memory (odd)
+    cplx* gscr = stg + (size_t)m * lg;
+    int* gsp = reinterpret_cast<int*>(gscr + 2 * (2 * m + 1) + 1);
+    // [A | X] (X: nx columns of a global row-major array, ldx) -> X <- A^-1 X in shared memory
+    auto gj_solve = [&](const cplx* Am, int lda, cplx* X, int ldx, int nx) {
+        const int w = m + nx;
+        for (int e = tid; e < m * w; e += nt) {
+            const int i = e / w, j = e % w;
+            stg[i * lg + j] = j < m ? Am[(size_t)i * lda + j] : X[(size_t)i * ldx + j - m];
+        }
+        const int inf = blk_gj_solve_smem(m, nx, stg, lg, gscr, gsp);
+        if (tid == 0 && inf) atomicCAS(&b.info[cell], 0, -inf);
+        for (int e = tid; e < m * nx; e += nt) X[(size_t)(e / nx) * ldx + e % nx] = stg[(e / nx) * lg + m + e % nx];
+        __syncthreads();
+    };
+    int info = 0;
+    if (gj) {
+        gj_solve(T11, m, S, ld, m + 1);  // [S12 | u]
+        phase(1);
+    } else {
+        info = blk_lu_blocked(m, T11lu, m, piv, &rs, stg, &gs);
+        if (tid == 0 && info) atomicCAS(&b.info[cell], 0, -info);
+        __syncthreads();
+        phase(1);
+        blk_lu_solve_blocked(m, T11lu, m, piv, ld, S, ld, stg, &gs);  // [S12 | u]
+    }
+    __syncthreads();
+    phase(2);
     // interface to the substrate: Q = diag(q) A^-1 Ks W
     blk_gemm(m, m, m, one, Ks, m, W, m, zero, Q, m, &gs);
-    info = blk_lu_blocked(m, A, m, piv, &rs, stg, &gs);
-    if (tid == 0 && info) atomicCAS(&b.info[cell], 0, -info);
-    blk_lu_solve_blocked(m, A, m, piv, m, Q, m, stg, &gs);
+    __syncthreads();
+    phase(3);
+    if (gj) {
+        gj_solve(A, m, Q, m, m);
+        phase(4);
+    } else {
+        info = blk_lu_blocked(m, A, m, piv, &rs, stg, &gs);
+        if (tid == 0 && info) atomicCAS(&b.info[cell], 0, -info);
+        __syncthreads();
+        phase(4);
+        blk_lu_solve_blocked(m, A, m, piv, m, Q, m, stg, &gs);
+    }
+    __syncthreads();
+    phase(5);
     for (int e = tid; e < m * m; e += nt) Q[e] = cmul(q[e / m], Q[e]);
     blk_gemm(m, m, m, one, S, ld, Q, m, zero, SQ, m, &gs);  // S12 Q
+    __syncthreads();
+    phase(6);
     cplx *aN = vec, *b0 = vec + m, *y = vec + 2 * m, *Qy = vec + 3 * m, *y2 = vec + 4 * m, *zz = vec + 5 * m,
          *dy2 = vec + 6 * m;
     for (int e = tid; e < m * m; e += nt) {
@@ -1549,9 +1611,13 @@ __global__ void __launch_bounds__(kRT) rcwa_sym_smat(Bucket b) {
     }
     for (int i = tid; i < m; i += nt) y[i] = cscale(cmul(cexpi(cscale(q[i], cd.h)), S[(size_t)i * ld + m]), 2.0);
     __syncthreads();
-    info = blk_lu_blocked(m, Cm, m, piv, &rs, stg, &gs);
-    if (tid == 0 && info) atomicCAS(&b.info[cell], 0, -info);
-    blk_lu_solve_blocked(m, Cm, m, piv, 1, y, 1, stg, &gs);  // y
+    if (gj) {
+        gj_solve(Cm, m, y, 1, 1);  // y
+    } else {
+        info = blk_lu_blocked(m, Cm, m, piv, &rs, stg, &gs);
+        if (tid == 0 && info) atomicCAS(&b.info[cell], 0, -info);
+        blk_lu_solve_blocked(m, Cm, m, piv, 1, y, 1, stg, &gs);  // y
+    }
     blk_gemm(m, 1, m, one, W, m, y, 1, zero, aN, 1, &gs);    // aN = W y
     blk_gemm(m, 1, m, one, Q, m, y, 1, zero, Qy, 1, &gs);    // Q y
     for (int i = tid; i < m; i += nt) {
@@ -1563,6 +1629,8 @@ __global__ void __launch_bounds__(kRT) rcwa_sym_smat(Bucket b) {
     blk_gemm(m, 1, m, one, S, ld, y2, 1, one, zz, 1, &gs);    // u + S12 y2
     blk_gemm(m, 1, m, one, T12, m, zz, 1, zero, b0, 1, &gs);  // T12 (u + S12 y2)
     blk_gemm(m, 1, m, one, T11, m, dy2, 1, one, b0, 1, &gs);  // + T11 D y2
+    __syncthreads();
+    phase(7);
 }
 
 // aN and b0 of both excitations into the full basis (the vector area the
@@ -1750,11 +1818,20 @@ size_t hess_stage_bytes(int n) { return (size_t)(n + LNB * LNB + 2 * LNB) * size
 // staging of blk_lu_blocked and the matvecs of the S-matrix kernels
 size_t lu_stage_bytes(int n) { return (size_t)(2 * n + LNB * LNB) * sizeof(cplx); }
 
+// dynamic shared memory of rcwa_sym_smat for class order m
+size_t sym_smat_smem(int m) {
+    return std::max(lu_stage_bytes(m), sym_gj_fits(m) ? sym_gj_bytes(m) : (size_t)0);
+}
+
 size_t laurent_smem(int Mx, int My, int ng) {
     const size_t mx4 = 4 * Mx + 1, my4 = 4 * My + 1;
     const int N = (2 * Mx + 1) * (2 * My + 1);
     const size_t raster = ((size_t)laurent_g1_rows(Mx) * ng + mx4 * my4) * sizeof(cplx) + (size_t)ng * ng;
-    return std::max(raster, lu_stage_bytes(N) + sizeof(GemmSmem));
+    // the class path inverts its largest scalar parity block in place: s x (s + 1)
+    // + 2 s + 1 complex, s + 1 ints
+    const size_t sb = (size_t)(Mx + 1) * (My + 1);
+    const size_t gj = (sb * (sb + 1) + 2 * sb + 1) * sizeof(cplx) + (sb + 1) * sizeof(int);
+    return std::max(std::max(raster, gj), lu_stage_bytes(N) + sizeof(GemmSmem));
 }
 
 // ---- stage configuration and autotuning -------------------------------------------------
@@ -1836,7 +1913,7 @@ struct SmemNeeds {
         }
         if (sym) {
             add_eig(sym_class_size(Mx, My, 0));
-            smat_sym = std::max(smat_sym, lu_stage_bytes(sym_class_size(Mx, My, 0)));
+            smat_sym = std::max(smat_sym, sym_smat_smem(sym_class_size(Mx, My, 0)));
         } else {
             add_eig(n);
             smat = std::max(smat, lu_stage_bytes(n));
@@ -1920,7 +1997,7 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
         if (ev) cudaEventRecord(ev[4], st);
         rcwa_vec<<<e.ncell, T[ST_VEC], 0, st>>>(e);
         if (ev) cudaEventRecord(ev[5], st);
-        rcwa_sym_smat<<<e.ncell, T[ST_SMAT1], lu_stage_bytes(m), st>>>(b);
+        rcwa_sym_smat<<<e.ncell, T[ST_SMAT1], sym_smat_smem(m), st>>>(b);
         if (ev) cudaEventRecord(ev[6], st);
         rcwa_sym_expand<<<nc, T[ST_SMAT2], 0, st>>>(b);
         if (ev) cudaEventRecord(ev[7], st);
@@ -2277,14 +2354,17 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
                 }
                 char buf[64];
                 std::snprintf(buf, sizeof(buf), " | sweeps/cell %.1f", sw / nc);
-                char buf2[480];
+                char buf2[640];
                 std::snprintf(buf2, sizeof(buf2), " | schur Mcycles/cell: aed %.2f (qr %.2f, %.0f rot) aed_far %.2f sweep %.2f (%.0f steps) sweep_far %.2f small %.2f"
                               " | hess Mcycles/cell: columns %.2f (matvec %.2f) updates %.2f"
-                              " | small QR Mcycles/cell: aed chase %.2f deferred %.2f, block chase %.2f deferred %.2f\n",
+                              " | small QR Mcycles/cell: aed chase %.2f deferred %.2f, block chase %.2f deferred %.2f"
+                              " | class smat Mcycles/cell: kpW+C0A %.2f LU(T11) %.2f solve %.2f KsW %.2f LU(A) %.2f solve %.2f S12Q %.2f rest %.2f\n",
                               ph[0] / nc * 1e-6, ph[5] / nc * 1e-6, ph[8] / nc, ph[1] / nc * 1e-6, ph[2] / nc * 1e-6,
                               ph[7] / nc, ph[3] / nc * 1e-6, ph[4] / nc * 1e-6, ph[9] / nc * 1e-6, ph[10] / nc * 1e-6,
                               ph[11] / nc * 1e-6, ph[12] / nc * 1e-6, ph[13] / nc * 1e-6, ph[14] / nc * 1e-6,
-                              ph[15] / nc * 1e-6);
+                              ph[15] / nc * 1e-6, ph[16] / nc * 1e-6, ph[17] / nc * 1e-6, ph[18] / nc * 1e-6,
+                              ph[19] / nc * 1e-6, ph[20] / nc * 1e-6, ph[21] / nc * 1e-6, ph[22] / nc * 1e-6,
+                              ph[23] / nc * 1e-6);
                 std::fprintf(stderr, "%s%s%s", line.c_str(), buf, buf2);
                 for (auto& e : ev) cudaEventDestroy(e);
                 cudaFree(dbg);

@@ -409,11 +409,12 @@ def measure_rcwa(peaks, quick=False, with_cpu=True, sampler=None):
     lib = rcwa_library_64()
     lc = [capi.rcwa_cell(**c) for c in lib]
     capi.rcwa_batch(lc)
-    t = []
-    for _ in range(11):  # ~12 ms host-synchronous calls: the median of 11 rides out host-side jitter
-        t0 = time.perf_counter()
+    t, tcpu = [], []
+    for _ in range(11):  # host-synchronous calls: the median of 11 rides out host-side jitter
+        t0, c0 = time.perf_counter(), time.process_time()
         capi.rcwa_batch(lc)
         t.append(time.perf_counter() - t0)
+        tcpu.append(time.process_time() - c0)
     dt = float(np.median(t))
     t0 = time.perf_counter()
     for c in lc[:8]:
@@ -426,7 +427,11 @@ def measure_rcwa(peaks, quick=False, with_cpu=True, sampler=None):
                             "roofline": {"bound": "fp64", "achieved": fl / dt, "peak": p_fp64, "unit": "FLOP/s",
                                          "frac": fl / dt / p_fp64,
                                          "flops": "of the method run (parity-class solve of mirror-symmetric cells)"},
-                            "reference_method_flops_per_s": fl_ref / dt}
+                            "reference_method_flops_per_s": fl_ref / dt,
+                            # per-call spread and host CPU time (process, all threads): a wall time far
+                            # above the CPU time is time the calling thread spent waiting, not working
+                            "calls_ms": {"min": 1e3 * min(t), "median": 1e3 * dt, "max": 1e3 * max(t),
+                                         "cpu_median": 1e3 * float(np.median(tcpu))}}
     if with_cpu:
         try:
             out["library_64_M3"]["cpu_baseline"] = rcwa_library_cpu_baseline(lib)

@@ -30,6 +30,7 @@
 #include <cmath>
 
 #include <algorithm>
+#include <chrono>
 #include <complex>
 #include <cstdio>
 #include <cstdlib>
@@ -2136,6 +2137,33 @@ int ensure_streams(int nb) {
     return CELERIS_OK;
 }
 
+// Free device memory, cached per device for the batch planner.
+struct FreeMemCache {
+    std::mutex mu;
+    std::map<int, std::pair<size_t, std::chrono::steady_clock::time_point>> by_dev;
+};
+FreeMemCache& free_mem_cache() {
+    static FreeMemCache c;
+    return c;
+}
+int query_free_memory(int dev, size_t* free_b) {
+    size_t total_b = 0;
+    CEL_CUDA(cudaMemGetInfo(free_b, &total_b));
+    FreeMemCache& c = free_mem_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    c.by_dev[dev] = {*free_b, std::chrono::steady_clock::now()};
+    return CELERIS_OK;
+}
+// The cached figure if it is under 2 s old, else 0.
+size_t cached_free_memory(int dev) {
+    FreeMemCache& c = free_mem_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    const auto it = c.by_dev.find(dev);
+    if (it == c.by_dev.end()) return 0;
+    const double age = std::chrono::duration<double>(std::chrono::steady_clock::now() - it->second.second).count();
+    return age < 2.0 ? it->second.first : 0;
+}
+
 int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_out, int nexc) {
     CEL_TRY(celeris_rt::require_device());
     // ---- plan: buckets by (Mx, My, raster), largest first so they start first
@@ -2143,48 +2171,75 @@ int run_cells(std::vector<HostCell>& cells, celeris_rcwa_result* out, int* info_
     for (int i = 0; i < (int)cells.size(); ++i)
         by[std::make_tuple(cells[i].Mx, cells[i].My, cells[i].ng, cells[i].sym)].push_back(i);
     std::vector<BucketPlan> plans;
+    std::vector<std::vector<int>> waves;
     CEL_TRY(ensure_streams(1));
     int dev = 0, smem_optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    size_t free_b = 0, total_b = 0;
-    CEL_CUDA(cudaMemGetInfo(&free_b, &total_b));
     Workspace& ws0 = Workspace::for_stream(t_ctx.main);
-    const size_t budget = (size_t)(0.6 * (double)(free_b + ws0.capacity()));
-    for (auto& kv : by) {
-        BucketPlan p;
-        p.Mx = std::get<0>(kv.first);
-        p.My = std::get<1>(kv.first);
-        p.ng = std::get<2>(kv.first);
-        p.sym = std::get<3>(kv.first);
-        p.N = (2 * p.Mx + 1) * (2 * p.My + 1);
-        p.n = 2 * p.N;
-        if (p.ng > 0 && laurent_smem(p.Mx, p.My, p.ng) + 1024 > (size_t)smem_optin)
-            return set_error(CELERIS_ERR_TOO_LARGE, "raster %d with M=(%d,%d) exceeds shared memory", p.ng, p.Mx, p.My);
-        p.per_cell = p.sym ? sym_per_cell_bytes(p.Mx, p.My, nexc, p.sym == 2 ? 1 : 2) : per_cell_bytes(p.n, nexc);
-        // split buckets that alone exceed the budget
-        const size_t max_cells = std::max<size_t>(1, budget / std::max<size_t>(1, p.per_cell));
-        for (size_t c0 = 0; c0 < kv.second.size(); c0 += max_cells) {
-            BucketPlan q = p;
-            const size_t c1 = std::min(kv.second.size(), c0 + max_cells);
-            q.ids.assign(kv.second.begin() + c0, kv.second.begin() + c1);
-            q.bytes = q.per_cell * q.ids.size() +
-                      (q.ng > 0 ? celeris_rt::align256(((size_t)(4 * q.Mx + 1) + (4 * q.My + 1)) * q.ng * sizeof(cplx)) + 512
-                                : 0);
-            plans.push_back(q);
-        }
+    // the memory budget: a free-memory figure up to 2 s old is used only when
+    // the resulting plan needs no larger arena (no allocation can then fail);
+    // the query itself is a driver call that costs ~0.1-1 ms, a sizeable part
+    // of a small batch
+    bool fresh = false;
+    size_t free_b = cached_free_memory(dev);
+    if (free_b == 0) {
+        CEL_TRY(query_free_memory(dev, &free_b));
+        fresh = true;
     }
-    std::sort(plans.begin(), plans.end(), [](const BucketPlan& a, const BucketPlan& b) { return a.n > b.n; });
-    // ---- waves of buckets that fit the memory budget together
-    std::vector<std::vector<int>> waves;
-    size_t acc = 0;
-    for (int i = 0; i < (int)plans.size(); ++i) {
-        if (waves.empty() || acc + plans[i].bytes > budget) {
-            waves.emplace_back();
-            acc = 0;
+    auto make_plan = [&](size_t free_now) -> int {
+        plans.clear();
+        waves.clear();
+        const size_t budget = (size_t)(0.6 * (double)(free_now + ws0.capacity()));
+        for (auto& kv : by) {
+            BucketPlan p;
+            p.Mx = std::get<0>(kv.first);
+            p.My = std::get<1>(kv.first);
+            p.ng = std::get<2>(kv.first);
+            p.sym = std::get<3>(kv.first);
+            p.N = (2 * p.Mx + 1) * (2 * p.My + 1);
+            p.n = 2 * p.N;
+            if (p.ng > 0 && laurent_smem(p.Mx, p.My, p.ng) + 1024 > (size_t)smem_optin)
+                return set_error(CELERIS_ERR_TOO_LARGE, "raster %d with M=(%d,%d) exceeds shared memory", p.ng, p.Mx, p.My);
+            p.per_cell = p.sym ? sym_per_cell_bytes(p.Mx, p.My, nexc, p.sym == 2 ? 1 : 2) : per_cell_bytes(p.n, nexc);
+            // split buckets that alone exceed the budget
+            const size_t max_cells = std::max<size_t>(1, budget / std::max<size_t>(1, p.per_cell));
+            for (size_t c0 = 0; c0 < kv.second.size(); c0 += max_cells) {
+                BucketPlan q = p;
+                const size_t c1 = std::min(kv.second.size(), c0 + max_cells);
+                q.ids.assign(kv.second.begin() + c0, kv.second.begin() + c1);
+                q.bytes = q.per_cell * q.ids.size() +
+                          (q.ng > 0 ? celeris_rt::align256(((size_t)(4 * q.Mx + 1) + (4 * q.My + 1)) * q.ng *
+                                                           sizeof(cplx)) + 512
+                                    : 0);
+                plans.push_back(q);
+            }
         }
-        waves.back().push_back(i);
-        acc += plans[i].bytes;
+        std::sort(plans.begin(), plans.end(), [](const BucketPlan& a, const BucketPlan& b) { return a.n > b.n; });
+        // ---- waves of buckets that fit the memory budget together
+        size_t acc = 0;
+        for (int i = 0; i < (int)plans.size(); ++i) {
+            if (waves.empty() || acc + plans[i].bytes > budget) {
+                waves.emplace_back();
+                acc = 0;
+            }
+            waves.back().push_back(i);
+            acc += plans[i].bytes;
+        }
+        return CELERIS_OK;
+    };
+    CEL_TRY(make_plan(free_b));
+    if (!fresh) {
+        size_t max_need = 0;
+        for (const auto& wave : waves) {
+            size_t need = 0;
+            for (int i : wave) need += plans[i].bytes + 4096;
+            max_need = std::max(max_need, need);
+        }
+        if (max_need > ws0.capacity()) {  // the arena must grow: plan on a fresh figure
+            CEL_TRY(query_free_memory(dev, &free_b));
+            CEL_TRY(make_plan(free_b));
+        }
     }
     std::vector<celeris_rcwa_result> hres(cells.size() * nexc);
     std::vector<int> hinfo(cells.size(), 0);

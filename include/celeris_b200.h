@@ -308,8 +308,12 @@ int celeris_solve_rcwa_2d(const celeris_rcwa_cell* cell, const double* Ex0,
  * CELERIS_ERR_EIG_NOCONV / CELERIS_ERR_SINGULAR naming the first failing cell.
  * Cells symmetric under both mirrors at normal incidence (every unrotated
  * shape, theta = 0) solve the eigenproblem in its four parity classes (the same
- * eigenpairs at a quarter of the order; CELERIS_RCWA_SYMMETRY=0 turns it off).
- * Synchronous, host buffers. */
+ * eigenpairs at a quarter of the order; CELERIS_RCWA_SYMMETRY=0 turns it off),
+ * only the two excited classes, and only one of them when the cell is also
+ * symmetric under a 90-degree rotation (square period, Mx = My, fill_x =
+ * fill_y). A cell whose Fourier operators are not symmetric to within
+ * CELERIS_RCWA_SYM_TOL (default 1e-9) of their largest entry is solved again at
+ * full order (0 forces that for every cell). Synchronous, host buffers. */
 int celeris_rcwa_batch(const celeris_rcwa_cell* cells, int ncell,
                        celeris_rcwa_result* out, int* info);
 

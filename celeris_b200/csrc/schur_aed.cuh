@@ -779,10 +779,12 @@ __device__ void chain_sweep(int n, cplx* H, int ldh, cplx* Z, int ldz, int lo, i
 }
 
 // prof (optional, per cell): clock64 sums of [AED local, AED far, sweep local,
-// sweep far, small blocks, AED QR], [7] chain steps, [8] AED QR rotations.
+// sweep far, small blocks, AED QR], [7] chain steps, [8] AED QR rotations,
+// [12, 13] the AED window QR's chases and deferred rotations, [14, 15] those of
+// the final blocks.
 __device__ int blk_schur_aed(int n, cplx* H, int ldh, cplx* Z, int ldz, AedShared* sh, long long* prof,
                              int iter_cap = 0) {
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, nt = blockDim.x;
     const double eps = 2.220446049250313e-16;
     const double smallnum = 2.2250738585072014e-308 * (n / eps);
     if (tid == 0) {

@@ -572,8 +572,11 @@ __global__ void __launch_bounds__(kRT) rcwa_build_M(Bucket b, int laurent) {
 // dynamic smem: SMEM: H [n*n] | v [n] | w [n] (rank-1 updates on the shared
 // copy); otherwise the staging of blk_hessenberg_blocked (scratch in X, which
 // is free until the eigenvectors).
+// The shared-memory variant may run 512 threads: for the larger orders its
+// shared block leaves one CTA per SM, and the column steps are latency-bound.
+constexpr int kHessBigThreads = 512;
 template <bool SMEM>
-__global__ void __launch_bounds__(kRT) rcwa_hess(Bucket b) {
+__global__ void __launch_bounds__(SMEM ? kHessBigThreads : kRT) rcwa_hess(Bucket b) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ RedScratch rs;
     const int cell = blockIdx.x;
@@ -1814,6 +1817,11 @@ size_t schur_smem(int ncell) {
 }
 
 // staging of blk_hessenberg_blocked
+// Threads of the shared-memory Hessenberg kernel: 512 once H no longer lets
+// two CTAs share an SM (order > 80), else the tuned size.
+int hess_smem_threads(int n, int tuned) {
+    return (size_t)n * n * sizeof(cplx) > 100 * 1024 ? kHessBigThreads : tuned;
+}
 size_t hess_stage_bytes(int n) { return (size_t)(n + LNB * LNB + 2 * LNB) * sizeof(cplx); }
 
 // staging of blk_lu_blocked and the matvecs of the S-matrix kernels
@@ -1990,7 +1998,8 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
         cudaMemsetAsync(e.info, 0, sizeof(int) * e.ncell, st);
         const int m = e.n;
         if (m <= kSmemEigMaxN)
-            rcwa_hess<true><<<e.ncell, T[ST_HESS], ((size_t)m * m + 2 * m) * sizeof(cplx), st>>>(e);
+            rcwa_hess<true><<<e.ncell, hess_smem_threads(m, T[ST_HESS]), ((size_t)m * m + 2 * m) * sizeof(cplx),
+                              st>>>(e);
         else
             rcwa_hess<false><<<e.ncell, T[ST_HESS], hess_stage_bytes(m), st>>>(e);
         if (ev) cudaEventRecord(ev[3], st);
@@ -2011,7 +2020,7 @@ void launch_bucket(const Bucket& b, const StageCfg& cfg, cudaStream_t st, cudaEv
     if (ev) cudaEventRecord(ev[2], st);
     if (n <= kSmemEigMaxN) {
         const size_t sm = ((size_t)n * n + 2 * n) * sizeof(cplx);
-        rcwa_hess<true><<<nc, T[ST_HESS], sm, st>>>(b);
+        rcwa_hess<true><<<nc, hess_smem_threads(n, T[ST_HESS]), sm, st>>>(b);
         if (ev) cudaEventRecord(ev[3], st);
         rcwa_schur<<<nc, kSchurThreads, schur_smem(nc), st>>>(b);
     } else {

@@ -890,7 +890,22 @@ __device__ void blk_hessenberg_refl(int n, cplx* H, int ldh, cplx* refl, cplx* v
         blk_rank1<false>(m, n - k - 1, H + (size_t)(k + 1) * ldh + k + 1, ldh, v, w + k + 1);
         for (int i = tid; i < m; i += nt) H[(size_t)(k + 1 + i) * ldh + k] = (i == 0) ? alpha : C(0.0, 0.0);
         __syncthreads();
-        blk_matvec_rows(n, m, H + k + 1, ldh, v, w, beta, warp, lane, nwarp);
+        if (m <= 48) {
+            // short rows: one thread per row, no shuffle reduction on the chain
+            for (int i = tid; i < n; i += nt) {
+                const cplx* row = H + (size_t)i * ldh + k + 1;
+                cplx acc[4] = {C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0), C(0.0, 0.0)};
+                int j = 0;
+                for (; j + 4 <= m; j += 4) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) acc[u] = cfma(row[j + u], v[j + u], acc[u]);
+                }
+                for (; j < m; ++j) acc[0] = cfma(row[j], v[j], acc[0]);
+                w[i] = cscale(cadd(cadd(acc[0], acc[1]), cadd(acc[2], acc[3])), beta);
+            }
+        } else {
+            blk_matvec_rows(n, m, H + k + 1, ldh, v, w, beta, warp, lane, nwarp);
+        }
         __syncthreads();
         blk_rank1<true>(n, m, H + k + 1, ldh, w, v);
         __syncthreads();
